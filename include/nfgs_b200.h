@@ -1,0 +1,230 @@
+/*
+ * nfgs_b200.h - C ABI of the B200-native NFGS (Gaussian-separated NFPT)
+ * reconstruction library (libnfgs_b200.so).
+ *
+ * The reference exposes this path as the Python class NFGSSolverGPU
+ * (nfgs_solver.py:3905 in spaceprod/NFGS).  Each entry point below replaces
+ * one method of that class; the citation beside it names the reference
+ * method.  Plain C types only: host pointers for host data, no torch types,
+ * no C++ exceptions across the boundary.  Every call returns an NFGS_*
+ * status; nfgs_last_error() gives a message for the calling thread.
+ *
+ * Threading: a handle is used by one host thread at a time.  Each handle
+ * owns a CUDA stream on the device that was current at nfgs_create().
+ */
+#ifndef NFGS_B200_H
+#define NFGS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define NFGS_OK 0
+#define NFGS_EINVAL 1         /* invalid argument (ValueError in the reference) */
+#define NFGS_ECUDA 2          /* CUDA runtime error */
+#define NFGS_ENOMEM 3         /* device allocation failed */
+#define NFGS_ESTATE 4         /* wrong call order (RuntimeError in the reference) */
+#define NFGS_EPOLICY 5        /* zero-mode / harmonic policy violation (ValueError) */
+#define NFGS_ETIMEDOUT 6      /* a bounded device wait ran out */
+#define NFGS_EUNSUPPORTED 7   /* option outside the production NFGS branch */
+
+/* storage types */
+#define NFGS_F32 0
+#define NFGS_F64 1
+
+/* enumerations of reference string options */
+#define NFGS_HZM_OMIT 0                    /* horizontal_zero_mode_policy="omit" */
+#define NFGS_HZM_FROZEN_LINEAR_HARMONIC 1  /* "frozen_linear_harmonic" (default) */
+#define NFGS_MEANBZ_UNIFORM_OPEN 0
+#define NFGS_MEANBZ_REQUIRE_BALANCED 1
+#define NFGS_MEANBZ_USER_SUPPLIED 2
+#define NFGS_POLICY_ERROR 0                /* zero-mode policies */
+#define NFGS_POLICY_WARN_PROJECT 1
+#define NFGS_POLICY_PROJECT 2
+#define NFGS_HARM_DIAGNOSE 0               /* harmonic_residual_policy */
+#define NFGS_HARM_WARN 1
+#define NFGS_HARM_ERROR 2
+#define NFGS_POLARITY_BOTH 0
+#define NFGS_POLARITY_POSITIVE 1
+#define NFGS_POLARITY_NEGATIVE 2
+#define NFGS_JZ_DERIVE_LEGACY_HELPER 0     /* bottom_current_grid_mode="legacy_helper" */
+#define NFGS_JZ_DERIVE_CALC_GRID 1         /* "calculation_grid" */
+#define NFGS_JZ_PROVIDED 2                 /* "provided" */
+
+/* stop reasons (history["stop_reason"]) */
+#define NFGS_STOP_RUNNING 0
+#define NFGS_STOP_MAX_ITER 1
+#define NFGS_STOP_TOL 2
+#define NFGS_STOP_SIGMA_IMPROVEMENT 3
+#define NFGS_STOP_SIGMA_STALL 4
+#define NFGS_STOP_MAX_ROLLBACKS 5
+#define NFGS_STOP_POLICY_ERROR 6
+
+/* Calculation grid and observed field of view (host-computed sizing,
+ * nfgs_solver.py:771-819). */
+typedef struct NfgsGeom {
+    int32_t nx, ny, nz;          /* calculation grid */
+    double dx, dy, dz;
+    int32_t input_nx, input_ny, input_nz; /* constructor grid */
+    int32_t pad_x, pad_y;        /* calculation_pad_xy */
+    int32_t dtype;               /* NFGS_F32 or NFGS_F64 */
+} NfgsGeom;
+
+/* NFGS policy (constructor keywords, nfgs_solver.py:3925-4349). */
+typedef struct NfgsParams {
+    double robin_weight;           /* bottom_divergence_robin_weight (rho) */
+    double projection_weight;      /* bottom_divergence_projection_weight */
+    double alpha_max;              /* alpha clip bound 1/h * factor; <= 0 disables */
+    double weak_field_floor_b2;
+    double mean_mode_tolerance;
+    double source_zero_mode_tolerance;
+    double user_open_bz;           /* user_supplied_open_bz (MEANBZ_USER_SUPPLIED) */
+    int32_t horizontal_zero_mode;  /* NFGS_HZM_* */
+    int32_t mean_bz_policy;        /* NFGS_MEANBZ_* */
+    int32_t d0_policy;             /* NFGS_POLICY_* */
+    int32_t source_policy;         /* NFGS_POLICY_* */
+    int32_t harmonic_policy;       /* NFGS_HARM_* */
+    int32_t gaussian_spectral;     /* 1: "spectral", 0: "fd" */
+    int32_t face_parallel_exact_jz;/* bottom_parallel_current_mode */
+    int32_t buffer_thickness;      /* 0: no window */
+    int32_t buffer_xy_only;
+} NfgsParams;
+
+/* set_bottom_vector_boundary keywords (nfgs_solver.py:4661, 2000-2113). */
+typedef struct NfgsBoundaryOpts {
+    int32_t ny_obs, nx_obs;   /* shape of the supplied maps */
+    int32_t zero_net_current;
+    int32_t smooth_passes;
+    int32_t ijzbcor;
+    int32_t jz_mode;          /* NFGS_JZ_* */
+    int32_t nzo;              /* observed height (fields crop and sigma box) */
+    int32_t fov_y0, fov_x0;   /* placement of the observed maps in the calc grid */
+    int32_t src_y0, src_x0;   /* first copied row/column of the maps (crop) */
+    int32_t copy_ny, copy_nx; /* copied extent */
+} NfgsBoundaryOpts;
+
+/* Number of doubles nfgs_set_boundary() writes to diag_out. */
+#define NFGS_NDIAG 40
+
+/* iterate() stop rule (nfgs_solver.py:3522-3562). */
+typedef struct NfgsStop {
+    int32_t max_iter;
+    int32_t patience;
+    double tol;
+    double mu;
+    double sigma_improvement_tol;  /* <= 0 disables */
+    int32_t polarity_mask;         /* NFGS_POLARITY_* */
+    int32_t adaptive_mu;
+    double mu_min, mu_max, mu_backoff, mu_growth;
+    int32_t growth_streak;
+    int32_t max_rollbacks;
+    double divergence_factor;
+    int32_t check_every;           /* iterations per host status poll (>= 1) */
+    int32_t use_graph;             /* capture the per-iteration launches in a CUDA graph */
+} NfgsStop;
+
+/* Number of doubles per history row written by nfgs_iterate_end(). */
+#define NFGS_HIST_COLS 8
+/* columns: sigma, divB, energy, mu, rollback, sigma_rel_change,
+ *          energy_rel_change, source_zero_mode_ratio */
+
+typedef struct NfgsIterResult {
+    int32_t n_hist;          /* rows written to hist */
+    int32_t best_iter;
+    int32_t final_iter;
+    int32_t stop_reason;     /* NFGS_STOP_* */
+    int32_t rollbacks;
+    int32_t kernel_launches; /* kernels this library launched in the call */
+    double best_sigma;
+    double final_sigma;
+    double final_vs_best_B_relative;
+    double sigma0, divB0, energy0;
+    double last_sigma_improvement; /* NaN when no step was accepted */
+    double init_source_zero_mode_ratio;
+    double device_ms;        /* CUDA-event time of the whole iterate call */
+} NfgsIterResult;
+
+/* NFGSSolverGPU.__init__ (nfgs_solver.py:3925-4349 -> 736-937):
+ * validates the geometry, allocates every device buffer for the grid. */
+int nfgs_create(const NfgsGeom* geom, const NfgsParams* params, void** handle_out);
+
+/* NFGSSolverGPU.set_bottom_vector_boundary / set_bottom_boundary
+ * (nfgs_solver.py:4661, 4548-4596): host maps (row-major ny_obs x nx_obs,
+ * FP64) are copied to the device, embedded, bottom Jz is derived (or jz is
+ * used when jz_mode == NFGS_JZ_PROVIDED), the toroidal boundary and the
+ * Gaussian separation (nfgs_solver.py:4671-4919) are built on the device.
+ * diag_out (NFGS_NDIAG doubles, may be NULL) receives the separation
+ * diagnostics in the order documented in nfgs_b200/solver.py. */
+int nfgs_set_boundary(void* handle, const double* bx, const double* by, const double* bz,
+                      const double* jz, const NfgsBoundaryOpts* opts, double* diag_out);
+
+/* NFGSSolverGPU.iterate, split so that a per-step host callback can run
+ * between steps (nfgs_solver.py:6937 -> 3522-3850):
+ *   begin   - gs_cfcf initial state (nfgs_solver.py:6613-6645) and its sigma;
+ *   advance - up to max_steps NFPT iterations on the device (no host sync
+ *             inside), returns the stop reason (NFGS_STOP_RUNNING if none);
+ *   end     - selects the best-sigma state, fills the result and history. */
+int nfgs_iterate_begin(void* handle, const NfgsStop* stop);
+/* sigma, divB, energy of the initial state after nfgs_iterate_begin()
+ * (the "Initial" line of verbose iterate, nfgs_solver.py:3612-3622). */
+int nfgs_iterate_initial(void* handle, double* scalars3);
+int nfgs_iterate_advance(void* handle, int32_t max_steps, int32_t* stop_reason, int32_t* n_done);
+int nfgs_iterate_end(void* handle, NfgsIterResult* result, double* hist, int32_t hist_rows);
+
+/* History rows [first, first + n) written so far by the running iterate
+ * (for verbose printing and per-step callbacks); returns the row count
+ * in *n_total. */
+int nfgs_get_history(void* handle, int32_t first, int32_t n, double* out, int32_t* n_total);
+
+/* Convenience: begin + advance until stopped + end. */
+int nfgs_iterate(void* handle, const NfgsStop* stop, NfgsIterResult* result, double* hist,
+                 int32_t hist_rows);
+
+/* NFGSSolverGPU.fields_to_numpy (nfgs_solver.py:2881-2903).
+ * which: 0 = stored solution (best state after iterate), 1 = current state.
+ * out: 6 consecutive (nz_out, ny_out, nx_out) FP64 blocks Bx,By,Bz,Jx,Jy,Jz;
+ * crop != 0 crops to the observed field of view. dims_out (3 ints) gets
+ * the output shape. */
+int nfgs_fields(void* handle, int32_t which, int32_t crop, double* out, int32_t* dims_out);
+
+/* Single-step access used by parity tests and by per_step_callback:
+ * reconstructs the state of `which` and returns phi_c, A_z (FP64, full
+ * calc grid), and its sigma/divB/energy. */
+int nfgs_get_scalars_state(void* handle, int32_t which, double* phi, double* az, double* scalars3);
+
+/* One NFPT step from the current state with relaxation mu (no stop logic),
+ * nfgs_solver.py:6647-6935.  The new state becomes current. */
+int nfgs_step(void* handle, double mu, int32_t polarity_mask);
+
+/* NFGSSolverGPU.gaussian_above_bottom_field (nfgs_solver.py:4921-4946):
+ * out is (3, ny, nx) FP64. */
+int nfgs_gaussian_above(void* handle, double* out);
+
+/* Fixed 2-D products of the boundary set-up (FP64, calc grid, (ny, nx)):
+ * which = 0 Bz_obs, 1 Bx_obs, 2 By_obs, 3 Jz_obs, 4 Az_bottom, 5 Jz_T,
+ * 6 Phi_above_bottom, 7 Bz_above, 8 D0, 9 bottom_dphi_c_target. */
+int nfgs_get_plane(void* handle, int32_t which, double* out);
+
+/* B_background volume (3, nz, ny, nx), FP64. */
+int nfgs_get_background(void* handle, double* out);
+
+/* Post-solve source diagnostics (nfgs_solver.py:7014-7196), scalar keys in
+ * the order documented in nfgs_b200/solver.py (NFGS_NSRCDIAG doubles). */
+#define NFGS_NSRCDIAG 12
+int nfgs_source_diagnostics(void* handle, double* out);
+
+int nfgs_destroy(void* handle);
+
+/* Message for the last failing call on this thread ("" if none). */
+const char* nfgs_last_error(void);
+
+/* Library build identification (sm arch, version). */
+const char* nfgs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NFGS_B200_H */

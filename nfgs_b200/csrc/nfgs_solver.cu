@@ -1,0 +1,1871 @@
+// NFGS B200 solver: handle, boundary set-up, iteration driver, C ABI.
+//
+// Reference: nfgs_solver.py (spaceprod/NFGS), class NFGSSolverGPU
+// (nfgs_solver.py:3905-7196) and its bases.  Each exported entry point
+// names the reference method it replaces in include/nfgs_b200.h.
+#include "../../include/nfgs_b200.h"
+#include "nfgs_common.cuh"
+#include "nfgs_gemm.cuh"
+#include "nfgs_iter.cuh"
+#include "nfgs_setup.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(NFGS_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+#define TRY(call)                     \
+    do {                              \
+        int r_ = (call);              \
+        if (r_ != NFGS_OK) return r_; \
+    } while (0)
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Device buffer helper
+// ---------------------------------------------------------------------------
+struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct Handle {
+    NfgsGeom geom{};
+    NfgsParams prm{};
+    Geo g{};
+    int f32 = 1;
+    size_t esz = 4;
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<Buf> owned;
+    int launches = 0;
+
+    long long PI = 0;  // interior modes (nx-2)(ny-2)
+
+    // transform matrices, row-major [out][in]
+    double *dctx = nullptr, *idctx = nullptr, *dcty = nullptr, *idcty = nullptr;
+    double *dstx = nullptr, *idstx = nullptr, *dsty = nullptr, *idsty = nullptr;
+    void *dctx_t = nullptr, *idctx_t = nullptr, *dcty_t = nullptr, *idcty_t = nullptr;
+    void *dstx_t = nullptr, *idstx_t = nullptr, *dsty_t = nullptr, *idsty_t = nullptr;
+
+    // spectral tables
+    double *lamN = nullptr, *kN = nullptr, *lamNs = nullptr, *lamD = nullptr, *alx = nullptr, *aly = nullptr;
+    // z factor tables
+    double *zr_c = nullptr, *zr_i = nullptr, *zr_il = nullptr, *zr_ci = nullptr, *zr_ii = nullptr;
+    int* zr_rc = nullptr;
+    double *zd_c = nullptr, *zd_i = nullptr, *zd_il = nullptr, *zd_ci = nullptr, *zd_ii = nullptr;
+    int* zd_rc = nullptr;
+
+    // boundary products (FP64 planes)
+    double *bz_obs = nullptr, *bx_obs = nullptr, *by_obs = nullptr, *jz_obs = nullptr, *az_bot = nullptr,
+           *jz_t = nullptr, *phi_above = nullptr, *bz_above = nullptr, *d0 = nullptr, *dphi_tgt = nullptr;
+    double *phi_above_hat = nullptr, *phi_below_hat = nullptr;  // modal (P)
+    double *phi_bot_hat = nullptr, *der_hat = nullptr, *az_bot_hat = nullptr;
+    double *bbg_d = nullptr;  // 3V FP64 background (kept for diagnostics)
+    // storage-type constants
+    void *bbg = nullptr, *bzobs_t = nullptr, *jzt_t = nullptr, *phiab_t = nullptr, *dphi_t = nullptr;
+    void *wx = nullptr, *wy = nullptr, *wz = nullptr;
+    double hx = 0.0, hy = 0.0;
+    int use_h = 0;
+    double open_bz = 0.0;
+    int boundary_set = 0;
+    int fov_y0 = 0, fov_x0 = 0, nyo = 0, nxo = 0, nzo = 0;
+    Box box{};
+
+    // state and work (storage type)
+    StateTab st{};
+    StateTab* st_dev = nullptr;
+    void *B = nullptr, *jz = nullptr, *jpf = nullptr, *jb = nullptr, *sb = nullptr, *sj = nullptr,
+         *tmpA = nullptr, *tmpB = nullptr;
+    double *pface = nullptr, *psrc = nullptr, *s00 = nullptr, *scal = nullptr;
+    int nb_face = 0, nb_src = 0;
+    dim3 sgrid, sblock;
+
+    // iteration control
+    DevCtl* ctl = nullptr;
+    DevCtl* ctl_h = nullptr;  // pinned mirror
+    int* consts = nullptr;    // device ints: [0]=0 [1]=1 [2]=2
+    double* hist = nullptr;
+    int hist_rows = 0;
+    int iter_active = 0;
+    int solution = -1;  // state index holding the stored solution
+    NfgsStop stop{};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    double init_zr = 0.0;
+    float total_ms = 0.0f;
+    int graph_kernels = 0;
+    int cur_host = 0;       // current state index outside iterate
+    void* bscratch = nullptr;  // 3V storage-type scratch (final-vs-best)
+    double* dscratch = nullptr; // V FP64 scratch for host transfers
+    int nzo_crop = 0;
+    std::vector<void*> setup_scratch;  // freed at the end of a boundary set-up
+};
+
+template <typename T>
+static int alloc(Handle* h, T** p, size_t bytes) {
+    void* q = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return fail(NFGS_ENOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    h->owned.push_back({q, bytes});
+    *p = (T*)q;
+    return NFGS_OK;
+}
+
+static void free_all(Handle* h) {
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    for (auto& b : h->owned) cudaFree(b.p);
+    h->owned.clear();
+    if (h->ctl_h) cudaFreeHost(h->ctl_h);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->s) cudaStreamDestroy(h->s);
+}
+
+// ---------------------------------------------------------------------------
+// Transform helpers.  Matrices are row-major [out][in].
+//   apply_x: out(r, c) = sum_m M[c][m] in(r, m)      (rows contiguous)
+//   apply_y: out(b, r, c) = sum_m M[r][m] in(b, m, c) (per plane)
+// ---------------------------------------------------------------------------
+template <typename T>
+static int apply_x(Handle* h, const void* M, const void* in, long long in_rs, long long in_bs, void* out,
+                   long long out_rs, long long out_bs, int rows, int K, int N, int batch, void* const* ctab = nullptr,
+                   const int* csel = nullptr, const DevCtl* ctl = nullptr) {
+    GemmArgs a{};
+    a.A = in; a.a_rs = in_rs; a.a_cs = 1; a.a_bs = in_bs;
+    a.B = M; a.b_rs = 1; a.b_cs = K; a.b_bs = 0;
+    a.C = out; a.c_rs = out_rs; a.c_cs = 1; a.c_bs = out_bs;
+    a.M = rows; a.N = N; a.K = K; a.batch = batch;
+    a.c_table = ctab; a.c_sel = csel; a.ctl = ctl;
+    h->launches++;
+    CK(launch_gemm<T>(a, h->s));
+    return NFGS_OK;
+}
+
+template <typename T>
+static int apply_y(Handle* h, const void* M, const void* in, long long in_rs, long long in_bs, void* out,
+                   long long out_rs, long long out_bs, int K, int N, int cols, int batch,
+                   const DevCtl* ctl = nullptr) {
+    GemmArgs a{};
+    a.A = M; a.a_rs = K; a.a_cs = 1; a.a_bs = 0;
+    a.B = in; a.b_rs = in_rs; a.b_cs = 1; a.b_bs = in_bs;
+    a.C = out; a.c_rs = out_rs; a.c_cs = 1; a.c_bs = out_bs;
+    a.M = N; a.N = cols; a.K = K; a.batch = batch;
+    a.ctl = ctl;
+    h->launches++;
+    CK(launch_gemm<T>(a, h->s));
+    return NFGS_OK;
+}
+
+// 2-D FP64 transforms of one (ny, nx) map (batch planes of pitch P).
+static int dct2_d(Handle* h, const double* in, double* out, double* tmp, int batch = 1) {
+    const int nx = h->g.nx, ny = h->g.ny;
+    const long long P = h->g.P;
+    TRY(apply_x<double>(h, h->dctx, in, nx, P, tmp, nx, P, ny, nx, nx, batch));
+    TRY(apply_y<double>(h, h->dcty, tmp, nx, P, out, nx, P, ny, ny, nx, batch));
+    return NFGS_OK;
+}
+
+static int idct2_d(Handle* h, const double* in, double* out, double* tmp, int batch = 1) {
+    const int nx = h->g.nx, ny = h->g.ny;
+    const long long P = h->g.P;
+    TRY(apply_x<double>(h, h->idctx, in, nx, P, tmp, nx, P, ny, nx, nx, batch));
+    TRY(apply_y<double>(h, h->idcty, tmp, nx, P, out, nx, P, ny, ny, nx, batch));
+    return NFGS_OK;
+}
+
+static std::vector<double> d2h(Handle* h, const double* p, size_t n) {
+    std::vector<double> v(n);
+    cudaMemcpyAsync(v.data(), p, n * sizeof(double), cudaMemcpyDeviceToHost, h->s);
+    cudaStreamSynchronize(h->s);
+    return v;
+}
+
+// reductions of n FP64 values: sum, sum of squares, sum |x|, max |x|
+static int reduce4(Handle* h, const double* a, long long n, double out[4]) {
+    k_reduce4<<<1, 1024, 0, h->s>>>(a, n, h->scal);
+    h->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, h->scal, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    return NFGS_OK;
+}
+
+static double rms_of(Handle* h, const double* a, long long n, int* rc) {
+    double r[4];
+    *rc = reduce4(h, a, n, r);
+    return std::sqrt(r[1] / (double)n);
+}
+
+// Copy FP64 -> storage type
+static int to_storage(Handle* h, const double* src, void* dst, long long n) {
+    if (h->f32) {
+        float* d = (float*)dst;
+        CK(launch_map(n, h->s, [=] __device__(long long i) { d[i] = (float)src[i]; }));
+    } else {
+        CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, h->s));
+    }
+    h->launches++;
+    return NFGS_OK;
+}
+
+static int from_storage(Handle* h, const void* src, double* dst, long long n) {
+    if (h->f32) {
+        const float* s = (const float*)src;
+        CK(launch_map(n, h->s, [=] __device__(long long i) { dst[i] = (double)s[i]; }));
+    } else {
+        CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice, h->s));
+    }
+    h->launches++;
+    return NFGS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Host-built tables
+// ---------------------------------------------------------------------------
+static std::vector<double> dct_matrix(int n, bool inverse) {
+    std::vector<double> m((size_t)n * n);
+    const double s = inverse ? 1.0 / (2.0 * (n - 1)) : 1.0;
+    for (int k = 0; k < n; ++k)
+        for (int q = 0; q < n; ++q) {
+            double w = (q == 0 || q == n - 1) ? 1.0 : 2.0;
+            // exact reduction of k*q modulo 2(n-1) keeps the argument small
+            long long a = ((long long)k * q) % (2LL * (n - 1));
+            m[(size_t)k * n + q] = s * w * std::cos(M_PI * (double)a / (double)(n - 1));
+        }
+    return m;
+}
+
+static std::vector<double> dst_matrix(int n, bool inverse) {
+    std::vector<double> m((size_t)n * n);
+    const double s = inverse ? 1.0 / (2.0 * (n + 1)) : 1.0;
+    for (int k = 0; k < n; ++k)
+        for (int q = 0; q < n; ++q) {
+            long long a = ((long long)(k + 1) * (q + 1)) % (2LL * (n + 1));
+            m[(size_t)k * n + q] = s * 2.0 * std::sin(M_PI * (double)a / (double)(n + 1));
+        }
+    return m;
+}
+
+static int upload(Handle* h, double** dp, const std::vector<double>& v) {
+    TRY(alloc(h, dp, v.size() * sizeof(double)));
+    CK(cudaMemcpy(*dp, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return NFGS_OK;
+}
+
+static int upload_t(Handle* h, void** dp, const std::vector<double>& v) {
+    TRY(alloc(h, dp, v.size() * h->esz));
+    if (h->f32) {
+        std::vector<float> f(v.begin(), v.end());
+        CK(cudaMemcpy(*dp, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+    } else {
+        CK(cudaMemcpy(*dp, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+    }
+    return NFGS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Stencil pass launchers
+// ---------------------------------------------------------------------------
+template <typename T>
+static int run_stencil(Handle* h, const int* sel, const int* skip, int with_src, int polarity, int raw_j = 0) {
+    const Geo& g = h->g;
+    k_recon<T><<<h->sgrid, h->sblock, 0, h->s>>>(g, h->st, sel, skip, (const T*)h->bbg, (const T*)h->bzobs_t,
+                                                 (const T*)h->jzt_t, (T)h->hx, (T)h->hy, h->use_h, (T*)h->B,
+                                                 (T*)h->jz);
+    CK(cudaGetLastError());
+    double am = h->prm.alpha_max;
+    k_face<T><<<h->sgrid, h->sblock, 0, h->s>>>(g, skip, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz, h->box,
+                                                (T)(am > 0 && std::isfinite(am) ? am : -1.0),
+                                                (T)h->prm.weak_field_floor_b2, (T*)h->jpf, (T*)h->jb, h->pface,
+                                                raw_j);
+    CK(cudaGetLastError());
+    h->launches += 2;
+    if (with_src) {
+        SrcOpts o{polarity, h->prm.face_parallel_exact_jz, h->wx != nullptr};
+        k_src<T><<<h->sgrid, h->sblock, 0, h->s>>>(g, skip, (const T*)h->jpf, (const T*)h->jb, (const T*)h->jzt_t,
+                                                   (const T*)h->bzobs_t, o, (const T*)h->wx, (const T*)h->wy,
+                                                   (const T*)h->wz, (T*)h->sb, (T*)h->sj, h->psrc);
+        CK(cudaGetLastError());
+        h->launches++;
+    }
+    return NFGS_OK;
+}
+
+// Forward transforms of S_B (all planes, DCT-I) and S_J (planes 1..nz-2,
+// interior DST-I), z-solves, inverse transforms into the candidate state.
+template <typename T>
+static int run_solve(Handle* h, const DevCtl* ctl, const int* cand_sel, int zero_sources) {
+    const Geo& g = h->g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const long long P = g.P, PI = h->PI;
+    const int nxi = nx - 2, nyi = ny - 2;
+    const int* skip = ctl ? &ctl->stopped : nullptr;
+    if (!zero_sources) {
+        {
+            TRY(apply_x<T>(h, h->dctx_t, h->sb, nx, P, h->tmpA, nx, P, ny * nz, nx, nx, 1, nullptr, nullptr, ctl));
+            TRY(apply_y<T>(h, h->dcty_t, h->tmpA, nx, P, h->sb, nx, P, ny, ny, nx, nz, ctl));
+            if (nz > 2) {
+                const char* sjp = (const char*)h->sj + (size_t)PI * h->esz;
+                char* tbp = (char*)h->tmpB + (size_t)PI * h->esz;
+                TRY(apply_x<T>(h, h->dstx_t, sjp, nxi, PI, tbp, nxi, PI, nyi * (nz - 2), nxi, nxi, 1, nullptr, nullptr,
+                               ctl));
+                TRY(apply_y<T>(h, h->dsty_t, tbp, nxi, PI, (void*)sjp, nxi, PI, nyi, nyi, nxi, nz - 2, ctl));
+            }
+        }
+    } else {
+        CK(cudaMemsetAsync(h->sb, 0, g.V * h->esz, h->s));
+        CK(cudaMemsetAsync(h->sj, 0, (size_t)nz * PI * h->esz, h->s));
+    }
+    ZTab tr{h->zr_c, h->zr_i, h->zr_il, h->zr_ci, h->zr_ii, h->zr_rc};
+    ZTab td{h->zd_c, h->zd_i, h->zd_il, h->zd_ci, h->zd_ii, h->zd_rc};
+    int nbr = (int)((P + 255) / 256);
+    int nbd = nz > 2 ? (int)((PI + 255) / 256) : 0;
+    k_zsolve<T><<<nbr + nbd, 256, 0, h->s>>>(g, skip, (T*)h->sb, tr, h->lamNs, h->phi_bot_hat, h->der_hat,
+                                             h->prm.robin_weight, h->s00, nz > 2 ? (T*)h->sj : nullptr, td, h->lamD,
+                                             h->az_bot_hat, nbr);
+    CK(cudaGetLastError());
+    h->launches++;
+    if (ctl != nullptr) {
+        k_zero_mode<<<1, 32, 0, h->s>>>(g, (DevCtl*)ctl, h->s00);
+        CK(cudaGetLastError());
+        h->launches++;
+    }
+    // inverse: planes 1..nz-1 of the Robin chain into phi[cand]
+    {
+        const char* shp = (const char*)h->sb + (size_t)P * h->esz;
+        char* tap = (char*)h->tmpA + (size_t)P * h->esz;
+        void* const* ptab = (void* const*)h->st_dev->phi;
+        {
+            TRY(apply_y<T>(h, h->idcty_t, shp, nx, P, tap, nx, P, ny, ny, nx, nz - 1, ctl));
+            TRY(apply_x<T>(h, h->idctx_t, tap, nx, P, (void*)(intptr_t)(P * h->esz), nx, P, ny * (nz - 1), nx, nx, 1,
+                           ptab, cand_sel, ctl));
+        }
+    }
+    if (nz > 2) {
+        const char* sjp = (const char*)h->sj + (size_t)PI * h->esz;
+        char* tbp = (char*)h->tmpB + (size_t)PI * h->esz;
+        void* const* atab = (void* const*)h->st_dev->az;
+        {
+            TRY(apply_y<T>(h, h->idsty_t, sjp, nxi, PI, tbp, nxi, PI, nyi, nyi, nxi, nz - 2, ctl));
+            // output: interior rows/cols of planes 1..nz-2 (offset P + nx + 1)
+            TRY(apply_x<T>(h, h->idstx_t, tbp, nxi, PI, (void*)(intptr_t)((P + nx + 1) * h->esz), nx, P, nyi, nxi, nxi,
+                           nz - 2, atab, cand_sel, ctl));
+        }
+    }
+    return NFGS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Control kernels
+// ---------------------------------------------------------------------------
+// Deterministic column sums of block partials by one warp per column.
+__global__ void k_sum_partials(const double* pf, int nbf, const double* ps, int nbs, double* out6) {
+    const int col = blockIdx.x;  // 0..4 face columns, 5 source column
+    const double* base = col < 5 ? pf : ps;
+    const int stride = col < 5 ? 5 : 1;
+    const int off = col < 5 ? col : 0;
+    const int nb = col < 5 ? nbf : nbs;
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += base[(long long)b * stride + off];
+    __shared__ double sh[32];
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) out6[col] = t;
+    }
+}
+
+__device__ __forceinline__ void scal_from_sums(Geo g, const double* s, double& sigma, double& divb, double& energy) {
+    sigma = s[0] / fmax(s[1], 1e-30);
+    double delta = fmin(g.dx, fmin(g.dy, g.dz));
+    divb = (s[2] / (double)g.V) / (6.0 * (s[3] / (double)g.V) / delta + 1e-12);
+    energy = s[4] * g.dx * g.dy * g.dz / 2.0;
+}
+
+__device__ __forceinline__ void pick_cand(DevCtl* c) {
+    for (int q = 0; q < 3; ++q)
+        if (q != c->cur && q != c->best) { c->cand = q; return; }
+}
+
+// Initial state statistics (nfgs_solver.py:3612-3614).
+__global__ void k_ctl_init(Geo g, DevCtl* c, const double* sums, double* hist) {
+    double sigma, divb, energy;
+    scal_from_sums(g, sums, sigma, divb, energy);
+    c->sigma0 = sigma; c->divb0 = divb; c->e0 = energy;
+    c->best_sigma = sigma; c->prev_sigma = sigma; c->prev_energy = energy; c->cur_sigma = sigma;
+    c->sumsb2 = sums[5];
+    c->n = 0; c->cur = 0; c->best = 0;
+    pick_cand(c);
+    if (c->max_iter <= 0) { c->stopped = 1; c->stop_reason = 1; }
+    (void)hist;
+}
+
+// One step of the stop rule (nfgs_solver.py:3658-3814).
+__global__ void k_ctl_step(Geo g, DevCtl* c, const double* sums, double* hist) {
+    if (c->stopped) { c->not_rollback = 1; return; }
+    double sigma, divb, energy;
+    scal_from_sums(g, sums, sigma, divb, energy);
+    const int n = c->n + 1;
+    double* row = hist + (long long)c->n_hist * NFGS_HCOLS;
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    bool diverged = !isfinite(sigma) || sigma > c->div_factor * fmax(c->best_sigma, 1e-30);
+    c->rollback_now = 0;
+    if (c->adaptive && diverged) {
+        c->rollbacks += 1;
+        c->mu_cur = fmax(c->mu_cur * c->mu_backoff, c->mu_min);
+        c->cur = c->best;
+        c->cur_sigma = c->best_sigma;
+        c->streak = 0;
+        row[0] = sigma; row[1] = nan; row[2] = nan; row[3] = c->mu_cur; row[4] = 1.0;
+        row[5] = nan; row[6] = nan; row[7] = c->zero_ratio_last;
+        c->n_hist += 1;
+        c->prev_energy = nan;
+        c->rollback_now = 1;
+        c->n = n;
+        if (c->rollbacks >= c->max_rollbacks) { c->stopped = 1; c->stop_reason = 5; }
+    } else {
+        c->cur = c->cand;
+        double src = fabs(sigma - c->prev_sigma) / fmax(fabs(c->prev_sigma), 1e-30);
+        double pe = c->prev_energy;
+        double erc = fabs(energy - pe) / fmax(fabs(pe), 1e-30);
+        row[0] = sigma; row[1] = divb; row[2] = energy; row[3] = c->mu_cur; row[4] = 0.0;
+        row[5] = src; row[6] = erc; row[7] = c->zero_ratio_last;
+        c->n_hist += 1;
+        c->prev_energy = energy;
+        c->final_iter = n;
+        c->cur_sigma = sigma;
+        double imp = c->prev_sigma - sigma;
+        c->last_imp = imp; c->have_last_imp = 1;
+        c->prev_sigma = sigma;
+        c->flat = (imp < c->eps) ? c->flat + 1 : 0;
+        if (sigma < c->best_sigma) {
+            c->best_sigma = sigma; c->best_iter = n; c->best = c->cur; c->stall = 0; c->streak += 1;
+            if (c->adaptive && c->streak >= c->growth_streak) {
+                c->mu_cur = fmin(c->mu_cur * c->mu_growth, c->mu_max);
+                c->streak = 0;
+            }
+        } else {
+            c->stall += 1;
+            c->streak = 0;
+        }
+        c->n = n;
+        c->sumsb2 = sums[5];
+        if (sigma < c->tol) { c->stopped = 1; c->stop_reason = 2; }
+        else if (c->use_imp && c->flat >= c->flat_required) { c->stopped = 1; c->stop_reason = 3; }
+        else if (c->patience > 0 && c->stall >= c->patience) { c->stopped = 1; c->stop_reason = 4; }
+    }
+    if (!c->stopped && n >= c->max_iter) { c->stopped = 1; c->stop_reason = 1; }
+    pick_cand(c);
+    c->not_rollback = (c->rollback_now && !c->stopped) ? 0 : 1;
+}
+
+// After a rollback the restored state's sources were recomputed.
+__global__ void k_ctl_rollback_sources(DevCtl* c, const double* sums) {
+    if (c->not_rollback) return;
+    c->sumsb2 = sums[5];
+}
+
+// ---------------------------------------------------------------------------
+// Boundary set-up
+// ---------------------------------------------------------------------------
+struct Fortran {
+    int nx, ny, nz, bfx, bfy;
+};
+
+static int mudpack_axis(int n) {
+    if (n < 2) return n < 1 ? 1 : n;
+    double r = (double)n;
+    int e2 = (int)std::ceil(std::log((r - 1.0) / 2.0) / std::log(2.0)) + 1;
+    int e3 = (int)std::ceil(std::log((r - 1.0) / 3.0) / std::log(2.0)) + 1;
+    int n2 = 2 * (1 << (e2 - 1)) + 1;
+    int n3 = 3 * (1 << (e3 - 1)) + 1;
+    return n2 < n3 ? n2 : n3;
+}
+
+template <typename T>
+static int build_constants(Handle* h);
+
+static int setup_boundary(Handle* h, const double* bx_h, const double* by_h, const double* bz_h, const double* jz_h,
+                          const NfgsBoundaryOpts* o, double* diag) {
+    const Geo& g = h->g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const long long P = g.P, PI = h->PI;
+    cudaStream_t s = h->s;
+    double dg[NFGS_NDIAG];
+    for (int q = 0; q < NFGS_NDIAG; ++q) dg[q] = 0.0;
+    const size_t nobs = (size_t)o->ny_obs * o->nx_obs;
+    double *up = nullptr;
+    TRY(alloc(h, &up, 4 * nobs * sizeof(double)));
+    CK(cudaMemcpyAsync(up, bx_h, nobs * 8, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(up + nobs, by_h, nobs * 8, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(up + 2 * nobs, bz_h, nobs * 8, cudaMemcpyHostToDevice, s));
+    if (o->jz_mode == NFGS_JZ_PROVIDED) CK(cudaMemcpyAsync(up + 3 * nobs, jz_h, nobs * 8, cudaMemcpyHostToDevice, s));
+    double *w;  // scratch planes
+    TRY(alloc(h, &w, 16 * (size_t)P * sizeof(double)));
+    CK(cudaMemsetAsync(w, 0, 16 * (size_t)P * sizeof(double), s));
+    double *bxo = h->bx_obs, *byo = h->by_obs, *bzo = h->bz_obs, *jzo = h->jz_obs;
+    CK(cudaMemsetAsync(bxo, 0, P * 8, s));
+    CK(cudaMemsetAsync(byo, 0, P * 8, s));
+    CK(cudaMemsetAsync(bzo, 0, P * 8, s));
+    CK(cudaMemsetAsync(jzo, 0, P * 8, s));
+    {
+        dim3 gr((o->copy_nx + 127) / 128, o->copy_ny);
+        int rf = h->f32;
+        k_embed<<<gr, 128, 0, s>>>(up, o->nx_obs, bxo, nx, o->fov_y0, o->fov_x0, o->src_y0, o->src_x0, o->copy_ny,
+                                   o->copy_nx, rf);
+        k_embed<<<gr, 128, 0, s>>>(up + nobs, o->nx_obs, byo, nx, o->fov_y0, o->fov_x0, o->src_y0, o->src_x0,
+                                   o->copy_ny, o->copy_nx, rf);
+        k_embed<<<gr, 128, 0, s>>>(up + 2 * nobs, o->nx_obs, bzo, nx, o->fov_y0, o->fov_x0, o->src_y0, o->src_x0,
+                                   o->copy_ny, o->copy_nx, rf);
+        if (o->jz_mode == NFGS_JZ_PROVIDED)
+            k_embed<<<gr, 128, 0, s>>>(up + 3 * nobs, o->nx_obs, jzo, nx, o->fov_y0, o->fov_x0, o->src_y0, o->src_x0,
+                                       o->copy_ny, o->copy_nx, rf);
+        CK(cudaGetLastError());
+        h->launches += 4;
+    }
+    // --- bottom Jz (nfgs_solver.py:1498-1567, 4489-4546)
+    if (o->jz_mode != NFGS_JZ_PROVIDED) {
+        int legacy = o->jz_mode == NFGS_JZ_DERIVE_LEGACY_HELPER;
+        int hnx = nx, hny = ny, bx0 = 0, by0 = 0;
+        if (legacy) {
+            hnx = mudpack_axis(nx);
+            hny = mudpack_axis(ny);
+            bx0 = (hnx - nx) / 2;
+            by0 = (hny - ny) / 2;
+        }
+        double* jzh = nullptr;
+        TRY(alloc(h, &jzh, (size_t)hnx * hny * 8));
+        h->setup_scratch.push_back(jzh);
+        dim3 gr((hnx + 127) / 128, hny);
+        k_jz_raw<<<gr, 128, 0, s>>>(bxo, byo, nx, ny, hnx, hny, bx0, by0, g.dx, g.dy, jzh);
+        CK(cudaGetLastError());
+        double fp = 1.0, fn = 1.0;
+        int mode = o->ijzbcor;
+        if (mode >= 2 && hnx >= 3 && hny >= 3) {
+            k_cell_sums<<<1, 1024, 0, s>>>(jzh, hnx, hny, h->scal);
+            CK(cudaGetLastError());
+            double cs[3];
+            CK(cudaMemcpyAsync(cs, h->scal, 24, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            double tot = cs[0], pos = cs[1], neg = cs[2];
+            double tgt = 0.0;
+            bool have = true;
+            if (mode == 2) tgt = pos - 0.5 * tot;
+            else if (mode == 3) tgt = std::max(pos, std::fabs(neg));
+            else if (mode == 4) tgt = std::min(pos, std::fabs(neg));
+            else have = false;
+            if (have) {
+                if (std::fabs(pos) > 0.0) fp = tgt / pos;
+                if (std::fabs(neg) > 0.0) fn = tgt / std::fabs(neg);
+            }
+        }
+        dim3 gc((nx + 127) / 128, ny);
+        k_jz_finish<<<gc, 128, 0, s>>>(jzh, hnx, hny, bx0, by0, fp, fn, legacy, jzo, nx, ny);
+        CK(cudaGetLastError());
+        h->launches += 3;
+    }
+    // --- smoothing (nfgs_solver.py:2085-2090)
+    if (o->smooth_passes > 0) {
+        double* arr[4] = {bzo, jzo, bxo, byo};
+        for (int a = 0; a < 4; ++a)
+            for (int pass = 0; pass < o->smooth_passes; ++pass) {
+                dim3 gc((nx + 127) / 128, ny);
+                k_smooth<<<gc, 128, 0, s>>>(arr[a], w, nx, ny);
+                CK(cudaMemcpyAsync(arr[a], w, P * 8, cudaMemcpyDeviceToDevice, s));
+                h->launches++;
+            }
+        CK(cudaGetLastError());
+    }
+    int rc = 0;
+    if (o->zero_net_current) {
+        double r[4];
+        TRY(reduce4(h, jzo, P, r));
+        double mean = r[0] / (double)P;
+        CK(launch_map(P, s, [=] __device__(long long i) { jzo[i] -= mean; }));
+    }
+    // --- Az_bottom: endpoint-Dirichlet 2-D Poisson of -Jz (nfgs_solver.py:1132-1144)
+    const int nxi = nx - 2, nyi = ny - 2;
+    double *t1 = w + P, *t2 = w + 2 * P, *t3 = w + 3 * P, *t4 = w + 4 * P, *t5 = w + 5 * P, *t6 = w + 6 * P,
+           *t7 = w + 7 * P, *t8 = w + 8 * P;
+    {
+        double* lamD = h->lamD;
+        CK(launch_map(PI, s, [=] __device__(long long q) {
+            long long j = q / nxi, i = q % nxi;
+            t1[q] = -jzo[(j + 1) * nx + (i + 1)];
+        }));
+        TRY(apply_x<double>(h, h->dstx, t1, nxi, PI, t2, nxi, PI, nyi, nxi, nxi, 1));
+        TRY(apply_y<double>(h, h->dsty, t2, nxi, PI, t3, nxi, PI, nyi, nyi, nxi, 1));
+        CK(launch_map(PI, s, [=] __device__(long long q) { t3[q] /= lamD[q]; }));
+        TRY(apply_y<double>(h, h->idsty, t3, nxi, PI, t2, nxi, PI, nyi, nyi, nxi, 1));
+        TRY(apply_x<double>(h, h->idstx, t2, nxi, PI, t1, nxi, PI, nyi, nxi, nxi, 1));
+        double* azb = h->az_bot;
+        CK(launch_map(P, s, [=] __device__(long long q) {
+            long long j = q / nx, i = q % nx;
+            azb[q] = (j >= 1 && j <= ny - 2 && i >= 1 && i <= nx - 2) ? t1[(j - 1) * nxi + (i - 1)] : 0.0;
+        }));
+        if (h->f32) CK(launch_map(P, s, [=] __device__(long long q) { azb[q] = (double)(float)azb[q]; }));
+        // Jz_T = -lap_xy Az_bottom, edges zeroed (nfgs_solver.py:3039-3046)
+        double* jzt = h->jz_t;
+        double dx = g.dx, dy = g.dy;
+        CK(launch_map(P, s, [=] __device__(long long q) {
+            int j = (int)(q / nx), i = (int)(q % nx);
+            double v = -lap2d(azb, nx, ny, j, i, dx, dy);
+            if (i == 0 || i == nx - 1 || j == 0 || j == ny - 1) v = 0.0;
+            jzt[q] = v;
+        }));
+        dg[21] = rms_of(h, jzo, P, &rc); TRY(rc);
+        dg[22] = rms_of(h, jzt, P, &rc); TRY(rc);
+        CK(launch_map(P, s, [=] __device__(long long q) { t2[q] = jzo[q] - jzt[q]; }));
+        dg[23] = rms_of(h, t2, P, &rc); TRY(rc);
+    }
+    // --- Gaussian separation (nfgs_solver.py:4671-4919)
+    const double norm = 4.0 * (double)std::max(nx - 1, 1) * (double)std::max(ny - 1, 1);
+    double *bxh = t4, *byh = t5, *bzh = t6;
+    TRY(dct2_d(h, bxo, bxh, t1));
+    TRY(dct2_d(h, byo, byh, t1));
+    TRY(dct2_d(h, bzo, bzh, t1));
+    {
+        double m0[1], m1[1], m2[1];
+        CK(cudaMemcpyAsync(m0, bxh, 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(m1, byh, 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(m2, bzh, 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        dg[0] = m0[0] / norm; dg[1] = m1[0] / norm; dg[2] = m2[0] / norm;
+        double r[4];
+        TRY(reduce4(h, bxo, P, r)); dg[3] = r[0] / P;
+        TRY(reduce4(h, byo, P, r)); dg[4] = r[0] / P;
+        TRY(reduce4(h, bzo, P, r)); dg[5] = r[0] / P;
+        double flux = std::fabs(r[0]) / std::max(r[2], 1e-30);
+        dg[7] = flux;
+        double res_mean = dg[2];
+        double res_scale = std::max(std::sqrt(r[1] / P), 1e-30);
+        if (h->prm.mean_bz_policy == NFGS_MEANBZ_UNIFORM_OPEN || h->prm.mean_bz_policy == NFGS_MEANBZ_REQUIRE_BALANCED) {
+            if (h->prm.mean_bz_policy == NFGS_MEANBZ_REQUIRE_BALANCED && flux > h->prm.mean_mode_tolerance) {
+                char b[256];
+                snprintf(b, sizeof b, "The residual bottom Bz is not flux balanced: fraction=%.6e, tolerance=%.6e.", flux,
+                         h->prm.mean_mode_tolerance);
+                return fail(NFGS_EPOLICY, b);
+            }
+            h->open_bz = res_mean;
+        } else {
+            h->open_bz = h->prm.user_open_bz;
+            double ratio = std::fabs(res_mean - h->open_bz) / res_scale;
+            if (ratio > h->prm.mean_mode_tolerance) {
+                char b[256];
+                snprintf(b, sizeof b,
+                         "user_supplied_open_bz does not match the residual Bz zero mode: ratio=%.6e, tolerance=%.6e.",
+                         ratio, h->prm.mean_mode_tolerance);
+                return fail(NFGS_EPOLICY, b);
+            }
+        }
+        dg[6] = h->open_bz;
+    }
+    // divergence modes d_hat (spectral) or FD divergence
+    double* dh = t7;
+    double *alx = h->alx, *aly = h->aly;
+    double dx = g.dx, dy = g.dy, dz = g.dz;
+    auto spectral_div_hat = [&](const double* ax, const double* ay, double* out) -> int {
+        // dstx_dcty_hat(ax): DCT along y, then DST along x of columns 1..nx-2
+        TRY(apply_y<double>(h, h->dcty, ax, nx, P, t1, nx, P, ny, ny, nx, 1));
+        CK(cudaMemsetAsync(t2, 0, P * 8, s));
+        TRY(apply_x<double>(h, h->dstx, t1 + 1, nx, P, t2 + 1, nx, P, ny, nxi, nxi, 1));
+        // dctx_dsty_hat(ay): DCT along x, then DST along y of rows 1..ny-2
+        TRY(apply_x<double>(h, h->dctx, ay, nx, P, t1, nx, P, ny, nx, nx, 1));
+        CK(cudaMemsetAsync(t3, 0, P * 8, s));
+        TRY(apply_y<double>(h, h->dsty, t1 + nx, nx, P, t3 + nx, nx, P, nyi, nyi, nx, 1));
+        CK(launch_map(P, s, [=] __device__(long long q) {
+            long long j = q / nx, i = q % nx;
+            out[q] = alx[i] * t2[q] + aly[j] * t3[q];
+        }));
+        return NFGS_OK;
+    };
+    double* D0 = h->d0;
+    if (h->prm.gaussian_spectral) {
+        TRY(spectral_div_hat(bxo, byo, dh));
+        TRY(idct2_d(h, dh, D0, t1));
+    } else {
+        CK(launch_map(P, s, [=] __device__(long long q) {
+            int j = (int)(q / nx), i = (int)(q % nx);
+            D0[q] = d2d(bxo, nx, ny, j, i, 0, dx) + d2d(byo, nx, ny, j, i, 1, dy);
+        }));
+        TRY(dct2_d(h, D0, dh, t1));
+    }
+    {
+        double m[1];
+        CK(cudaMemcpyAsync(m, dh, 8, cudaMemcpyDeviceToHost, s));
+        double r[4];
+        TRY(reduce4(h, D0, P, r));
+        double d0m = m[0] / norm;
+        double ratio = std::fabs(d0m) / std::max(std::sqrt(r[1] / P), 1e-30);
+        dg[8] = d0m;
+        dg[9] = ratio;
+        if (ratio > h->prm.mean_mode_tolerance) {
+            if (h->prm.d0_policy == NFGS_POLICY_ERROR) {
+                char b[256];
+                snprintf(b, sizeof b,
+                         "The bottom vector field is incompatible with the zero-mean endpoint-Neumann GS model "
+                         "ratio=%.6e exceeds tolerance=%.6e.",
+                         ratio, h->prm.mean_mode_tolerance);
+                return fail(NFGS_EPOLICY, b);
+            }
+            if (h->prm.d0_policy == NFGS_POLICY_WARN_PROJECT) dg[30] = 1.0;
+        }
+    }
+    // modal split (nfgs_solver.py:4798-4856)
+    double *bzbh = t8, *pbh = h->phi_below_hat, *pah = h->phi_above_hat, *dpth = t1;
+    double *lamN = h->lamN, *kN = h->kN;
+    double* bzah = t2;
+    CK(launch_map(P, s, [=] __device__(long long q) {
+        double dq = q == 0 ? 0.0 : dh[q];
+        double bzn = q == 0 ? 0.0 : bzh[q];
+        double ks = q == 0 ? 1.0 : kN[q];
+        double ls = q == 0 ? 1.0 : lamN[q];
+        double below = q == 0 ? 0.0 : 0.5 * (bzn + dq / ks);
+        double above = q == 0 ? 0.0 : 0.5 * (bzn - dq / ks);
+        bzbh[q] = below;
+        bzah[q] = above;
+        pbh[q] = q == 0 ? 0.0 : below / ls;
+        pah[q] = q == 0 ? 0.0 : above / ls;
+        dpth[q] = q == 0 ? 0.0 : -dq / ls;
+    }));
+    // 2-D products
+    double* t9 = w + 9 * P;
+    double* t10 = w + 10 * P;
+    TRY(idct2_d(h, bzah, h->bz_above, t9));
+    TRY(idct2_d(h, pah, h->phi_above, t9));
+    TRY(idct2_d(h, dpth, t10, t9));  // idct2(dphi_total_hat)
+    // 3-D background, batches of planes through FP64 transforms
+    const long long V = g.V;
+    double* bbg = h->bbg_d;
+    double* zmod;
+    double* zout;
+    const int chunk = 16;
+    TRY(alloc(h, &zmod, (size_t)chunk * P * 8));
+    TRY(alloc(h, &zout, (size_t)chunk * P * 8));
+    double* ztmp;
+    TRY(alloc(h, &ztmp, (size_t)chunk * P * 8));
+    double open = h->open_bz;
+    const int spectral = h->prm.gaussian_spectral;
+    double* phib3 = nullptr;  // phi_below planes (needed for FD horizontals and diagnostics)
+    TRY(alloc(h, &phib3, (size_t)V * 8));
+    for (int z0 = 0; z0 < nz; z0 += chunk) {
+        const int nb = std::min(chunk, nz - z0);
+        // phi_below(z) = idct2(exp(-k z) phi_below_hat)
+        CK(launch_map((long long)nb * P, s, [=] __device__(long long q) {
+            long long p = q / P, m = q % P;
+            double z = (double)(z0 + p) * dz;
+            zmod[q] = exp(-z * kN[m]) * pbh[m];
+        }));
+        TRY(idct2_d(h, zmod, phib3 + (size_t)z0 * P, ztmp, nb));
+        // bz_below(z)
+        CK(launch_map((long long)nb * P, s, [=] __device__(long long q) {
+            long long p = q / P, m = q % P;
+            double z = (double)(z0 + p) * dz;
+            zmod[q] = exp(-z * kN[m]) * bzbh[m];
+        }));
+        TRY(idct2_d(h, zmod, zout, ztmp, nb));
+        CK(launch_map((long long)nb * P, s, [=] __device__(long long q) {
+            bbg[2 * V + (long long)z0 * P + q] = zout[q] + open;
+        }));
+        if (spectral) {
+            // bx_below = -gx, gx = IDST_x(IDCT_y(-alpha_x * dphi_dz_hat)),
+            // dphi_dz_hat = -k exp(-kz) phi_below_hat (nfgs_solver.py:4847-4852)
+            CK(launch_map((long long)nb * P, s, [=] __device__(long long q) {
+                long long p = q / P, m = q % P;
+                double z = (double)(z0 + p) * dz;
+                double dpz = -kN[m] * exp(-z * kN[m]) * pbh[m];
+                zmod[q] = -alx[m % nx] * dpz;
+            }));
+            TRY(apply_y<double>(h, h->idcty, zmod, nx, P, ztmp, nx, P, ny, ny, nx, nb));
+            CK(cudaMemsetAsync(zout, 0, (size_t)nb * P * 8, s));
+            TRY(apply_x<double>(h, h->idstx, ztmp + 1, nx, P, zout + 1, nx, P, ny, nxi, nxi, nb));
+            CK(launch_map((long long)nb * P, s, [=] __device__(long long q) {
+                bbg[(long long)z0 * P + q] = -zout[q];
+            }));
+            CK(launch_map((long long)nb * P, s, [=] __device__(long long q) {
+                long long p = q / P, m = q % P;
+                double z = (double)(z0 + p) * dz;
+                double dpz = -kN[m] * exp(-z * kN[m]) * pbh[m];
+                zmod[q] = -aly[m / nx] * dpz;
+            }));
+            TRY(apply_x<double>(h, h->idctx, zmod, nx, P, ztmp, nx, P, ny * nb, nx, nx, 1));
+            CK(cudaMemsetAsync(zout, 0, (size_t)nb * P * 8, s));
+            TRY(apply_y<double>(h, h->idsty, ztmp + nx, nx, P, zout + nx, nx, P, nyi, nyi, nx, nb));
+            CK(launch_map((long long)nb * P, s, [=] __device__(long long q) {
+                bbg[V + (long long)z0 * P + q] = -zout[q];
+            }));
+        }
+    }
+    if (!spectral) {
+        // bx_below = -Dx(Dz phi_below), by_below = -Dy(Dz phi_below)
+        CK(launch_map(V, s, [=] __device__(long long q) {
+            int k = (int)(q / P);
+            long long r = q % P;
+            int j = (int)(r / nx), i = (int)(r % nx);
+            auto dzp = [&](int jj, int ii) {
+                auto f = [&](int kk) { return phib3[(long long)kk * P + (long long)jj * nx + ii]; };
+                if (k == 0) return (-3.0 * f(0) + 4.0 * f(1) - f(2)) / (2.0 * dz);
+                if (k == nz - 1) return (3.0 * f(nz - 1) - 4.0 * f(nz - 2) + f(nz - 3)) / (2.0 * dz);
+                return (f(k + 1) - f(k - 1)) / (2.0 * dz);
+            };
+            auto dxf = [&](int ii) { return dzp(j, ii); };
+            auto dyf = [&](int jj) { return dzp(jj, i); };
+            double gx, gy;
+            if (i == 0) gx = (-3.0 * dxf(0) + 4.0 * dxf(1) - dxf(2)) / (2.0 * dx);
+            else if (i == nx - 1) gx = (3.0 * dxf(nx - 1) - 4.0 * dxf(nx - 2) + dxf(nx - 3)) / (2.0 * dx);
+            else gx = (dxf(i + 1) - dxf(i - 1)) / (2.0 * dx);
+            if (j == 0) gy = (-3.0 * dyf(0) + 4.0 * dyf(1) - dyf(2)) / (2.0 * dy);
+            else if (j == ny - 1) gy = (3.0 * dyf(ny - 1) - 4.0 * dyf(ny - 2) + dyf(ny - 3)) / (2.0 * dy);
+            else gy = (dyf(j + 1) - dyf(j - 1)) / (2.0 * dy);
+            bbg[q] = -gx;
+            bbg[V + q] = -gy;
+        }));
+    }
+    // bottom_dphi_c_target = idct2(dphi_total_hat) - Dz(phi_below)(0)
+    {
+        double* tg = h->dphi_tgt;
+        CK(launch_map(P, s, [=] __device__(long long q) {
+            double dzp0 = (-3.0 * phib3[q] + 4.0 * phib3[P + q] - phib3[2 * P + q]) / (2.0 * dz);
+            tg[q] = t10[q] - dzp0;
+        }));
+    }
+    // diagnostics: bottom reconstruction and the scalar-background invariant
+    {
+        double* bza = h->bz_above;
+        CK(launch_map(P, s, [=] __device__(long long q) { t9[q] = bbg[2 * V + q] + bza[q] - bzo[q]; }));
+        double r[4];
+        TRY(reduce4(h, t9, P, r));
+        dg[10] = std::sqrt(r[1] / P);
+        dg[11] = r[3];
+        double* inv;
+        TRY(alloc(h, &inv, (size_t)V * 8));
+        h->setup_scratch.push_back(inv);
+        CK(launch_map(V, s, [=] __device__(long long q) {
+            int k = (int)(q / P);
+            long long rr = q % P;
+            int j = (int)(rr / nx), i = (int)(rr % nx);
+            double lz = lap2d(phib3 + (long long)k * P, nx, ny, j, i, dx, dy);
+            inv[q] = (lz + open) - bbg[2 * V + q];
+        }));
+        TRY(reduce4(h, inv, V, r));
+        dg[12] = std::sqrt(r[1] / (3.0 * V));
+    }
+    // harmonic residual (nfgs_solver.py:4962-5029)
+    {
+        double *rx = w + 11 * P, *ry = w + 12 * P;  // residual maps
+        double* azb = h->az_bot;
+        // dphi_hat = k (phi_above_hat - phi_below_hat)
+        double* dph = t10;
+        CK(launch_map(P, s, [=] __device__(long long q) { dph[q] = kN[q] * (pah[q] - pbh[q]); }));
+        double* gxm = t7;
+        double* gym = t8;
+        if (spectral) {
+            // gx = IDST_x(IDCT_y(-alpha_x dphi_hat)) on interior columns
+            CK(launch_map(P, s, [=] __device__(long long q) { t1[q] = -alx[q % nx] * dph[q]; }));
+            TRY(apply_y<double>(h, h->idcty, t1, nx, P, t2, nx, P, ny, ny, nx, 1));
+            CK(cudaMemsetAsync(gxm, 0, P * 8, s));
+            TRY(apply_x<double>(h, h->idstx, t2 + 1, nx, P, gxm + 1, nx, P, ny, nxi, nxi, 1));
+            CK(launch_map(P, s, [=] __device__(long long q) { t1[q] = -aly[q / nx] * dph[q]; }));
+            TRY(apply_x<double>(h, h->idctx, t1, nx, P, t2, nx, P, ny, nx, nx, 1));
+            CK(cudaMemsetAsync(gym, 0, P * 8, s));
+            TRY(apply_y<double>(h, h->idsty, t2 + nx, nx, P, gym + nx, nx, P, nyi, nyi, nx, 1));
+        } else {
+            double* dphi = t1;
+            TRY(idct2_d(h, dph, dphi, t2));
+            CK(launch_map(P, s, [=] __device__(long long q) {
+                int j = (int)(q / nx), i = (int)(q % nx);
+                gxm[q] = d2d(dphi, nx, ny, j, i, 0, dx);
+                gym[q] = d2d(dphi, nx, ny, j, i, 1, dy);
+            }));
+        }
+        CK(launch_map(P, s, [=] __device__(long long q) {
+            int j = (int)(q / nx), i = (int)(q % nx);
+            double btx = d2d(azb, nx, ny, j, i, 1, dy);
+            double bty = -d2d(azb, nx, ny, j, i, 0, dx);
+            rx[q] = bxo[q] - (-gxm[q] + btx);
+            ry[q] = byo[q] - (-gym[q] + bty);
+        }));
+        // constant modes via the DCT-I (0,0) weights
+        double* cs = t5;
+        TRY(dct2_d(h, rx, cs, t1));
+        double cx[1], cy[1];
+        CK(cudaMemcpyAsync(cx, cs, 8, cudaMemcpyDeviceToHost, s));
+        TRY(dct2_d(h, ry, cs, t1));
+        CK(cudaMemcpyAsync(cy, cs, 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        double hxc = cx[0] / norm, hyc = cy[0] / norm;
+        dg[15] = hxc; dg[16] = hyc;
+        dg[17] = std::sqrt(0.5 * (hxc * hxc + hyc * hyc));
+        double r[4], r2[4];
+        TRY(reduce4(h, rx, P, r));
+        TRY(reduce4(h, ry, P, r2));
+        double res_rms = std::sqrt((r[1] + r2[1]) / (2.0 * P));
+        // nonconstant rms: sum (x - c)^2 = sum x^2 - 2 c sum x + n c^2
+        double ncs = (r[1] - 2 * hxc * r[0] + P * hxc * hxc) + (r2[1] - 2 * hyc * r2[0] + P * hyc * hyc);
+        dg[18] = std::sqrt(std::max(ncs, 0.0) / (2.0 * P));
+        double ro1[4], ro2[4];
+        TRY(reduce4(h, bxo, P, ro1));
+        TRY(reduce4(h, byo, P, ro2));
+        double obs_rms = std::sqrt((ro1[1] + ro2[1]) / (2.0 * P));
+        double ratio = res_rms / std::max(obs_rms, 1e-30);
+        dg[13] = res_rms;
+        dg[14] = ratio;
+        // divergence and curl of the residual
+        double* dv = t6;
+        if (spectral) {
+            TRY(spectral_div_hat(rx, ry, t4));
+            TRY(idct2_d(h, t4, dv, t1));
+        } else {
+            CK(launch_map(P, s, [=] __device__(long long q) {
+                int j = (int)(q / nx), i = (int)(q % nx);
+                dv[q] = d2d(rx, nx, ny, j, i, 0, dx) + d2d(ry, nx, ny, j, i, 1, dy);
+            }));
+        }
+        dg[19] = rms_of(h, dv, P, &rc); TRY(rc);
+        CK(launch_map(P, s, [=] __device__(long long q) {
+            int j = (int)(q / nx), i = (int)(q % nx);
+            t4[q] = d2d(ry, nx, ny, j, i, 0, dx) - d2d(rx, nx, ny, j, i, 1, dy);
+        }));
+        dg[20] = rms_of(h, t4, P, &rc); TRY(rc);
+        if (ratio > h->prm.mean_mode_tolerance) {
+            if (h->prm.harmonic_policy == NFGS_HARM_ERROR) {
+                char b[256];
+                snprintf(b, sizeof b,
+                         "Bottom horizontal reconstruction leaves a finite-domain harmonic residual ratio=%.6e, "
+                         "tolerance=%.6e.",
+                         ratio, h->prm.mean_mode_tolerance);
+                return fail(NFGS_EPOLICY, b);
+            }
+            if (h->prm.harmonic_policy == NFGS_HARM_WARN) dg[31] = 1.0;
+        }
+        if (h->prm.horizontal_zero_mode == NFGS_HZM_FROZEN_LINEAR_HARMONIC) {
+            h->hx = hxc; h->hy = hyc; h->use_h = 1;
+        } else {
+            h->hx = h->hy = 0.0; h->use_h = 0;
+        }
+    }
+    dg[24] = (double)o->jz_mode;
+    CK(cudaStreamSynchronize(s));
+    // release the set-up scratch (kept allocations are the handle's)
+    {
+        std::vector<void*> drop = {up, w, zmod, zout, ztmp, phib3};
+        for (void* p : h->setup_scratch) drop.push_back(p);
+        h->setup_scratch.clear();
+        for (auto it = h->owned.begin(); it != h->owned.end();) {
+            bool d = false;
+            for (void* p : drop) d = d || (it->p == p);
+            if (d) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+        }
+    }
+    if (diag) std::memcpy(diag, dg, sizeof dg);
+    if (h->f32) TRY(build_constants<float>(h));
+    else TRY(build_constants<double>(h));
+    h->boundary_set = 1;
+    h->solution = -1;
+    h->iter_active = 0;
+    return NFGS_OK;
+}
+
+// Storage-type constants, modal boundary data, factor tables and state
+// buffer boundary planes.
+template <typename T>
+static int build_constants(Handle* h) {
+    const Geo& g = h->g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const long long P = g.P, V = g.V, PI = h->PI;
+    cudaStream_t s = h->s;
+    TRY(to_storage(h, h->bbg_d, h->bbg, 3 * V));
+    TRY(to_storage(h, h->bz_obs, h->bzobs_t, P));
+    TRY(to_storage(h, h->jz_t, h->jzt_t, P));
+    TRY(to_storage(h, h->phi_above, h->phiab_t, P));
+    TRY(to_storage(h, h->dphi_tgt, h->dphi_t, P));
+    // modal boundary data from the storage-rounded planes
+    double *tmp, *tmp2;
+    TRY(alloc(h, &tmp, (size_t)P * 8));
+    TRY(alloc(h, &tmp2, (size_t)P * 8));
+    TRY(from_storage(h, h->phiab_t, tmp2, P));
+    TRY(dct2_d(h, tmp2, h->phi_bot_hat, tmp));
+    TRY(from_storage(h, h->dphi_t, tmp2, P));
+    TRY(dct2_d(h, tmp2, h->der_hat, tmp));
+    {
+        double *a = h->phi_bot_hat, *b = h->der_hat;
+        CK(launch_map(1, s, [=] __device__(long long) { a[0] = 0.0; b[0] = 0.0; }));
+    }
+    const int nxi = nx - 2, nyi = ny - 2;
+    {
+        // DST-I of the (storage-rounded) Az_bottom interior
+        double* azb = h->az_bot;
+        int f32 = h->f32;
+        CK(launch_map(PI, s, [=] __device__(long long q) {
+            long long j = q / nxi, i = q % nxi;
+            double v = azb[(j + 1) * nx + (i + 1)];
+            tmp2[q] = f32 ? (double)(float)v : v;
+        }));
+        TRY(apply_x<double>(h, h->dstx, tmp2, nxi, PI, tmp, nxi, PI, nyi, nxi, nxi, 1));
+        TRY(apply_y<double>(h, h->dsty, tmp, nxi, PI, h->az_bot_hat, nxi, PI, nyi, nyi, nxi, 1));
+    }
+    // factor tables
+    k_ztables<<<(unsigned)((P + 255) / 256), 256, 0, s>>>(g, 0, h->prm.robin_weight, h->lamN, h->kN, h->zr_c, h->zr_i,
+                                                          h->zr_il, h->zr_ci, h->zr_ii, h->zr_rc);
+    CK(cudaGetLastError());
+    if (nz > 2) {
+        k_ztables<<<(unsigned)((PI + 255) / 256), 256, 0, s>>>(g, 1, 0.0, h->lamD, nullptr, h->zd_c, h->zd_i, h->zd_il,
+                                                               h->zd_ci, h->zd_ii, h->zd_rc);
+        CK(cudaGetLastError());
+    }
+    // state buffers: zero, then the fixed bottom planes
+    void* azb_t = nullptr;
+    TRY(alloc(h, &azb_t, P * h->esz));
+    TRY(to_storage(h, h->az_bot, azb_t, P));
+    for (int b = 0; b < 3; ++b) {
+        CK(cudaMemsetAsync(h->st.phi[b], 0, V * h->esz, s));
+        CK(cudaMemsetAsync(h->st.az[b], 0, V * h->esz, s));
+        CK(cudaMemcpyAsync(h->st.phi[b], h->phiab_t, P * h->esz, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(h->st.az[b], azb_t, P * h->esz, cudaMemcpyDeviceToDevice, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    for (auto it = h->owned.begin(); it != h->owned.end();) {
+        if (it->p == tmp || it->p == tmp2 || it->p == azb_t) { cudaFree(it->p); it = h->owned.erase(it); }
+        else ++it;
+    }
+    return NFGS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Iteration driver
+// ---------------------------------------------------------------------------
+template <typename T>
+static int enqueue_iteration(Handle* h) {
+    DevCtl* c = h->ctl;
+    // solve from the sources of the current state into the candidate buffer
+    TRY(run_solve<T>(h, c, &c->cand, 0));
+    {
+        const long long P = h->g.P;
+        k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(
+            h->g, h->st, c, 1, 1.0, &c->cand, &c->cur, (const T*)h->phiab_t, (const T*)h->dphi_t,
+            h->prm.projection_weight, 1);
+        CK(cudaGetLastError());
+        h->launches++;
+    }
+    TRY(run_stencil<T>(h, &c->cand, &c->stopped, 1, h->stop.polarity_mask));
+    k_sum_partials<<<6, 256, 0, h->s>>>(h->pface, h->nb_face, h->psrc, h->nb_src, h->scal);
+    CK(cudaGetLastError());
+    k_ctl_step<<<1, 1, 0, h->s>>>(h->g, c, h->scal, h->hist);
+    CK(cudaGetLastError());
+    h->launches += 2;
+    if (h->stop.adaptive_mu) {
+        TRY(run_stencil<T>(h, &c->cur, &c->not_rollback, 1, h->stop.polarity_mask));
+        k_sum_partials<<<6, 256, 0, h->s>>>(h->pface, h->nb_face, h->psrc, h->nb_src, h->scal);
+        k_ctl_rollback_sources<<<1, 1, 0, h->s>>>(c, h->scal);
+        CK(cudaGetLastError());
+        h->launches += 2;
+    }
+    return NFGS_OK;
+}
+
+template <typename T>
+static int iterate_begin_t(Handle* h, const NfgsStop* stop) {
+    if (!h->boundary_set)
+        return fail(NFGS_ESTATE, "NFGS boundary is not set. Call set_bottom_vector_boundary() first.");
+    h->stop = *stop;
+    if (h->stop.check_every < 1) h->stop.check_every = 1;
+    int rows = std::max(stop->max_iter, 0) + 2;
+    if (rows > h->hist_rows) {
+        if (h->hist) {
+            for (auto it = h->owned.begin(); it != h->owned.end();) {
+                if (it->p == h->hist) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+            }
+        }
+        TRY(alloc(h, &h->hist, (size_t)rows * NFGS_HCOLS * 8));
+        h->hist_rows = rows;
+    }
+    if (h->gexec) { cudaGraphExecDestroy(h->gexec); h->gexec = nullptr; }
+    if (h->graph) { cudaGraphDestroy(h->graph); h->graph = nullptr; }
+    DevCtl c{};
+    c.cur = 0; c.best = 0; c.cand = 1;
+    c.max_iter = stop->max_iter;
+    c.patience = stop->patience;
+    c.flat_required = std::max(stop->patience, 1);
+    c.use_imp = stop->sigma_improvement_tol > 0.0;
+    c.eps = c.use_imp ? stop->sigma_improvement_tol : 0.0;
+    c.adaptive = stop->adaptive_mu;
+    c.growth_streak = stop->growth_streak;
+    c.max_rollbacks = stop->max_rollbacks;
+    c.source_policy = h->prm.source_policy;
+    c.tol = stop->tol;
+    c.mu_min = stop->mu_min; c.mu_max = stop->mu_max; c.mu_backoff = stop->mu_backoff; c.mu_growth = stop->mu_growth;
+    c.div_factor = stop->divergence_factor;
+    c.src_tol = h->prm.source_zero_mode_tolerance;
+    c.mu_cur = stop->mu;
+    c.not_rollback = 1;
+    CK(cudaMemcpyAsync(h->ctl, &c, sizeof c, cudaMemcpyHostToDevice, h->s));
+    h->launches = 0;
+    CK(cudaEventRecord(h->ev0, h->s));
+    // gs_cfcf: zero-source modal solves into state 0 (nfgs_solver.py:6630-6645)
+    TRY(run_solve<T>(h, nullptr, &h->consts[0], 1));
+    {
+        const long long P = h->g.P;
+        k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(
+            h->g, h->st, nullptr, 0, 1.0, &h->consts[0], &h->consts[0], (const T*)h->phiab_t, (const T*)h->dphi_t,
+            h->prm.projection_weight, 0);
+        CK(cudaGetLastError());
+        h->launches++;
+    }
+    TRY(run_stencil<T>(h, &h->consts[0], nullptr, 1, stop->polarity_mask));
+    k_sum_partials<<<6, 256, 0, h->s>>>(h->pface, h->nb_face, h->psrc, h->nb_src, h->scal);
+    k_ctl_init<<<1, 1, 0, h->s>>>(h->g, h->ctl, h->scal, h->hist);
+    CK(cudaGetLastError());
+    h->launches += 2;
+    h->init_zr = 0.0;
+    h->iter_active = 1;
+    h->solution = -1;
+    h->total_ms = 0.0f;
+    return NFGS_OK;
+}
+
+template <typename T>
+static int iterate_advance_t(Handle* h, int max_steps, int32_t* stop_reason, int32_t* n_done) {
+    if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
+    CK(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    int done = 0;
+    while (!h->ctl_h->stopped && done < max_steps) {
+        int k = std::min(h->stop.check_every, max_steps - done);
+        if (h->stop.use_graph) {
+            if (!h->gexec) {
+                CK(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+                int before = h->launches;
+                int r = enqueue_iteration<T>(h);
+                cudaGraph_t gr = nullptr;
+                cudaError_t e = cudaStreamEndCapture(h->s, &gr);
+                if (r != NFGS_OK) { if (gr) cudaGraphDestroy(gr); return r; }
+                CK(e);
+                h->graph = gr;
+                CK(cudaGraphInstantiate(&h->gexec, h->graph, 0));
+                h->launches = before;  // counted per graph launch below
+                size_t nn = 0;
+                CK(cudaGraphGetNodes(h->graph, nullptr, &nn));
+                std::vector<cudaGraphNode_t> nodes(nn);
+                CK(cudaGraphGetNodes(h->graph, nodes.data(), &nn));
+                int kn = 0;
+                for (auto nd : nodes) {
+                    cudaGraphNodeType t;
+                    CK(cudaGraphNodeGetType(nd, &t));
+                    kn += (t == cudaGraphNodeTypeKernel);
+                }
+                h->graph_kernels = kn;
+            }
+            for (int q = 0; q < k; ++q) CK(cudaGraphLaunch(h->gexec, h->s));
+            h->launches += k * h->graph_kernels;
+        } else {
+            for (int q = 0; q < k; ++q) TRY(enqueue_iteration<T>(h));
+        }
+        done += k;
+        CK(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->s));
+        CK(cudaStreamSynchronize(h->s));
+    }
+    if (stop_reason) *stop_reason = h->ctl_h->stopped ? h->ctl_h->stop_reason : NFGS_STOP_RUNNING;
+    if (n_done) *n_done = h->ctl_h->n;
+    return NFGS_OK;
+}
+
+}  // namespace
+
+namespace {
+
+// Fields of a state (nfgs_solver.py:2881-2903): B from k_recon, J_z state,
+// J_x,y = vertical faces mapped to centres with zero walls and top
+// (nfgs_solver.py:5780-5794, 5935-5941).
+template <typename T>
+__global__ void k_gather_fields(Geo g, const T* __restrict__ B, const T* __restrict__ jz, const T* __restrict__ jf,
+                                int nzc, int y0, int ny_c, int x0, int nx_c, double* __restrict__ out) {
+    long long n = (long long)nzc * ny_c * nx_c;
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    int k = (int)(q / ((long long)ny_c * nx_c));
+    long long r = q % ((long long)ny_c * nx_c);
+    int j = (int)(r / nx_c) + y0, i = (int)(r % nx_c) + x0;
+    const long long P = g.P, V = g.V, FV = (long long)(g.nz - 1) * P;
+    const long long c = (long long)k * P + (long long)j * g.nx + i;
+    const long long pq = (long long)j * g.nx + i;
+    out[q] = (double)B[c];
+    out[n + q] = (double)B[V + c];
+    out[2 * n + q] = (double)B[2 * V + c];
+    bool wall = (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1 || k == g.nz - 1);
+    double jx = 0.0, jy = 0.0;
+    if (!wall) {
+        if (k == 0) {
+            jx = (double)jf[pq];
+            jy = (double)jf[FV + pq];
+        } else {
+            jx = 0.5 * ((double)jf[(long long)(k - 1) * P + pq] + (double)jf[(long long)k * P + pq]);
+            jy = 0.5 * ((double)jf[FV + (long long)(k - 1) * P + pq] + (double)jf[FV + (long long)k * P + pq]);
+            // match the storage-type average of the reference (0.5 * (a + b) in T)
+            jx = (double)(T(0.5) * (jf[(long long)(k - 1) * P + pq] + jf[(long long)k * P + pq]));
+            jy = (double)(T(0.5) * (jf[FV + (long long)(k - 1) * P + pq] + jf[FV + (long long)k * P + pq]));
+        }
+    }
+    out[3 * n + q] = jx;
+    out[4 * n + q] = jy;
+    out[5 * n + q] = (double)jz[c];
+}
+
+template <typename T>
+__global__ void k_diff_sums(const T* __restrict__ a, const T* __restrict__ b, long long n, double* out) {
+    __shared__ double sh[2 * 32];
+    double v[2] = {0, 0};
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        double x = (double)a[q], y = (double)b[q];
+        v[0] += (x - y) * (x - y);
+        v[1] += y * y;
+    }
+    block_reduce<2>(v, sh);
+    if (threadIdx.x == 0) { out[2 * blockIdx.x] = v[0]; out[2 * blockIdx.x + 1] = v[1]; }
+}
+
+static int resolve_state(Handle* h, int which, int* idx) {
+    if (which == 0) {
+        if (h->solution < 0) return fail(NFGS_ESTATE, "No solution stored; call iterate() first.");
+        *idx = h->solution;
+    } else {
+        *idx = h->cur_host;
+    }
+    return NFGS_OK;
+}
+
+static void host_scalars(const Geo& g, const double* s, double out[3]) {
+    out[0] = s[0] / std::max(s[1], 1e-30);
+    double delta = std::min(g.dx, std::min(g.dy, g.dz));
+    out[1] = (s[2] / (double)g.V) / (6.0 * (s[3] / (double)g.V) / delta + 1e-12);
+    out[2] = s[4] * g.dx * g.dy * g.dz / 2.0;
+}
+
+template <typename T>
+static int state_scalars(Handle* h, int idx, double out[3]) {
+    TRY(run_stencil<T>(h, &h->consts[idx], nullptr, 0, 0));
+    k_sum_partials<<<6, 256, 0, h->s>>>(h->pface, h->nb_face, h->psrc, h->nb_src, h->scal);
+    CK(cudaGetLastError());
+    double sums[6];
+    CK(cudaMemcpyAsync(sums, h->scal, 6 * 8, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    host_scalars(h->g, sums, out);
+    return NFGS_OK;
+}
+
+template <typename T>
+static int iterate_end_t(Handle* h, NfgsIterResult* res, double* hist, int hist_rows) {
+    if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
+    CK(cudaEventRecord(h->ev1, h->s));
+    CK(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    const DevCtl& c = *h->ctl_h;
+    NfgsIterResult r{};
+    r.n_hist = c.n_hist;
+    r.best_iter = c.best_iter;
+    r.final_iter = c.final_iter;
+    r.stop_reason = c.stop_reason;
+    r.rollbacks = c.rollbacks;
+    r.best_sigma = c.best_sigma;
+    r.final_sigma = c.cur_sigma;
+    r.sigma0 = c.sigma0;
+    r.divB0 = c.divb0;
+    r.energy0 = c.e0;
+    r.last_sigma_improvement = c.have_last_imp ? c.last_imp : std::nan("");
+    r.init_source_zero_mode_ratio = h->init_zr;
+    r.device_ms = ms;
+    if (hist && hist_rows > 0) {
+        int n = std::min(hist_rows, c.n_hist);
+        if (n > 0) CK(cudaMemcpy(hist, h->hist, (size_t)n * NFGS_HCOLS * 8, cudaMemcpyDeviceToHost));
+    }
+    h->iter_active = 0;
+    h->solution = c.best;
+    h->cur_host = c.cur;
+    // final-vs-best relative B difference (nfgs_solver.py:3820-3824)
+    if (c.cur != c.best) {
+        const long long V3 = 3 * h->g.V;
+        if (!h->bscratch) TRY(alloc(h, &h->bscratch, V3 * h->esz));
+        TRY(run_stencil<T>(h, &h->consts[c.best], nullptr, 0, 0));
+        CK(cudaMemcpyAsync(h->bscratch, h->B, V3 * h->esz, cudaMemcpyDeviceToDevice, h->s));
+        TRY(run_stencil<T>(h, &h->consts[c.cur], nullptr, 0, 0));
+        k_diff_sums<T><<<1, 1024, 0, h->s>>>((const T*)h->B, (const T*)h->bscratch, V3, h->scal);
+        CK(cudaGetLastError());
+        double sums[2];
+        CK(cudaMemcpyAsync(sums, h->scal, 16, cudaMemcpyDeviceToHost, h->s));
+        CK(cudaStreamSynchronize(h->s));
+        r.final_vs_best_B_relative = std::sqrt(sums[0] / V3) / std::max(std::sqrt(sums[1] / V3), 1e-30);
+        h->launches += 5;
+    } else {
+        r.final_vs_best_B_relative = 0.0;
+    }
+    r.kernel_launches = h->launches;
+    if (res) *res = r;
+    if (c.policy_error) {
+        // the row that failed is the next step's source (nfgs_solver.py:5457-5476)
+        char b[256];
+        snprintf(b, sizeof b,
+                 "The Phi_c nonlinear source has an incompatible zero mode ratio=%.6e exceeds tolerance=%.6e.",
+                 c.zero_ratio_last, h->prm.source_zero_mode_tolerance);
+        return fail(NFGS_EPOLICY, b);
+    }
+    return NFGS_OK;
+}
+
+template <typename T>
+static int fields_t(Handle* h, int which, int crop, double* out, int32_t* dims) {
+    int idx;
+    TRY(resolve_state(h, which, &idx));
+    TRY(run_stencil<T>(h, &h->consts[idx], nullptr, 0, 0, 1));
+    int nzc = h->g.nz, y0 = 0, x0 = 0, nyc = h->g.ny, nxc = h->g.nx;
+    if (crop) {
+        nzc = h->nzo_crop; y0 = h->fov_y0; x0 = h->fov_x0; nyc = h->nyo; nxc = h->nxo;
+    }
+    long long n = (long long)nzc * nyc * nxc;
+    double* dout;
+    TRY(alloc(h, &dout, 6 * n * 8));
+    k_gather_fields<T><<<(unsigned)((n + 255) / 256), 256, 0, h->s>>>(h->g, (const T*)h->B, (const T*)h->jz,
+                                                                      (const T*)h->jpf, nzc, y0, nyc, x0, nxc, dout);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, dout, 6 * n * 8, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    for (auto it = h->owned.begin(); it != h->owned.end();) {
+        if (it->p == dout) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+    }
+    if (dims) { dims[0] = nzc; dims[1] = nyc; dims[2] = nxc; }
+    return NFGS_OK;
+}
+
+template <typename T>
+static int get_state_t(Handle* h, int which, double* phi, double* az, double* sc) {
+    int idx;
+    TRY(resolve_state(h, which, &idx));
+    const long long V = h->g.V;
+    if (!h->dscratch) TRY(alloc(h, &h->dscratch, V * 8));
+    if (phi) {
+        TRY(from_storage(h, h->st.phi[idx], h->dscratch, V));
+        CK(cudaMemcpyAsync(phi, h->dscratch, V * 8, cudaMemcpyDeviceToHost, h->s));
+    }
+    if (az) {
+        CK(cudaStreamSynchronize(h->s));
+        TRY(from_storage(h, h->st.az[idx], h->dscratch, V));
+        CK(cudaMemcpyAsync(az, h->dscratch, V * 8, cudaMemcpyDeviceToHost, h->s));
+    }
+    CK(cudaStreamSynchronize(h->s));
+    if (sc) TRY(state_scalars<T>(h, idx, sc));
+    return NFGS_OK;
+}
+
+template <typename T>
+static int step_t(Handle* h, double mu, int polarity) {
+    if (!h->boundary_set) return fail(NFGS_ESTATE, "NFGS boundary is not configured");
+    const int cur = h->cur_host;
+    const int cand = (cur + 1) % 3 == h->solution ? (cur + 2) % 3 : (cur + 1) % 3;
+    TRY(run_stencil<T>(h, &h->consts[cur], nullptr, 1, polarity));
+    TRY(run_solve<T>(h, nullptr, &h->consts[cand], 0));
+    const long long P = h->g.P;
+    k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(h->g, h->st, nullptr, 0, mu, &h->consts[cand],
+                                                                &h->consts[cur], (const T*)h->phiab_t,
+                                                                (const T*)h->dphi_t, h->prm.projection_weight, 1);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->s));
+    h->cur_host = cand;
+    return NFGS_OK;
+}
+
+// B^> on z = 0 (nfgs_solver.py:4921-4946) and the harmonic-style gradient.
+static int gaussian_above_impl(Handle* h, double* out) {
+    if (!h->boundary_set) return fail(NFGS_ESTATE, "NFGS Gaussian separation is not configured");
+    const Geo& g = h->g;
+    const int nx = g.nx, ny = g.ny, nxi = nx - 2, nyi = ny - 2;
+    const long long P = g.P;
+    cudaStream_t s = h->s;
+    double* w;
+    TRY(alloc(h, &w, 6 * P * 8));
+    CK(cudaMemsetAsync(w, 0, 6 * P * 8, s));
+    double *t1 = w, *t2 = w + P, *gx = w + 2 * P, *gy = w + 3 * P, *dph = w + 4 * P;
+    double *kN = h->kN, *pah = h->phi_above_hat, *alx = h->alx, *aly = h->aly;
+    double dx = g.dx, dy = g.dy;
+    CK(launch_map(P, s, [=] __device__(long long q) { dph[q] = kN[q] * pah[q]; }));
+    if (h->prm.gaussian_spectral) {
+        CK(launch_map(P, s, [=] __device__(long long q) { t1[q] = -alx[q % nx] * dph[q]; }));
+        TRY(apply_y<double>(h, h->idcty, t1, nx, P, t2, nx, P, ny, ny, nx, 1));
+        TRY(apply_x<double>(h, h->idstx, t2 + 1, nx, P, gx + 1, nx, P, ny, nxi, nxi, 1));
+        CK(launch_map(P, s, [=] __device__(long long q) { t1[q] = -aly[q / nx] * dph[q]; }));
+        TRY(apply_x<double>(h, h->idctx, t1, nx, P, t2, nx, P, ny, nx, nx, 1));
+        TRY(apply_y<double>(h, h->idsty, t2 + nx, nx, P, gy + nx, nx, P, nyi, nyi, nx, 1));
+    } else {
+        TRY(idct2_d(h, dph, t1, t2));
+        CK(launch_map(P, s, [=] __device__(long long q) {
+            int j = (int)(q / nx), i = (int)(q % nx);
+            gx[q] = d2d(t1, nx, ny, j, i, 0, dx);
+            gy[q] = d2d(t1, nx, ny, j, i, 1, dy);
+        }));
+    }
+    std::vector<double> a = d2h(h, gx, P), b = d2h(h, gy, P), c = d2h(h, h->bz_above, P);
+    for (long long q = 0; q < P; ++q) {
+        out[q] = -a[q];
+        out[P + q] = -b[q];
+        out[2 * P + q] = c[q];
+    }
+    for (auto it = h->owned.begin(); it != h->owned.end();) {
+        if (it->p == w) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+    }
+    return NFGS_OK;
+}
+
+// Post-solve source diagnostics (nfgs_solver.py:7014-7100, scalar keys).
+template <typename T>
+static int source_diag_t(Handle* h, double* out) {
+    int idx;
+    TRY(resolve_state(h, 0, &idx));
+    const Geo& g = h->g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const long long P = g.P, V = g.V;
+    cudaStream_t s = h->s;
+    TRY(run_stencil<T>(h, &h->consts[idx], nullptr, 0, 0));
+    double* w;
+    const int NW = 29;
+    TRY(alloc(h, &w, NW * P * 8));
+    CK(cudaMemsetAsync(w, 0, NW * P * 8, s));
+    // plane map: bc 0..5, bx0 6, by0 7, hat 8..13, dct scratch 14..19,
+    // rob 20, prob 21, upw 22, ph1 23, ph2 24, sp 25, sp2 26, o 27, scratch 28
+    double* bc = w;  // Bc_z = B_z - B_bg,z on planes 0,1,2 and nz-3, nz-2, nz-1
+    const T* Bt = (const T*)h->B;
+    const T* bgt = (const T*)h->bbg;
+    CK(launch_map(6 * P, s, [=] __device__(long long q) {
+        int p = (int)(q / P);
+        long long m = q % P;
+        int k = p < 3 ? p : nz - 6 + p;
+        bc[q] = (double)(Bt[2 * V + (long long)k * P + m] - bgt[2 * V + (long long)k * P + m]);
+    }));
+    double *bx0 = w + 6 * P, *by0 = w + 7 * P;
+    CK(launch_map(P, s, [=] __device__(long long q) {
+        bx0[q] = (double)Bt[q];
+        by0[q] = (double)Bt[V + q];
+    }));
+    double* hat = w + 8 * P;
+    TRY(dct2_d(h, bc, hat, w + 14 * P, 6));
+    double* lamN = h->lamN;
+    double* kN = h->kN;
+    const double dz = g.dz;
+    double *rob = w + 20 * P, *prob = w + 21 * P, *upw = w + 22 * P, *ph1 = w + 23 * P, *ph2 = w + 24 * P;
+    double *sp = w + 25 * P, *sp2 = w + 26 * P, *o = w + 27 * P, *scr = w + 28 * P;
+    CK(launch_map(P, s, [=] __device__(long long q) {
+        double h3 = hat[3 * P + q], h4 = hat[4 * P + q], h5 = hat[5 * P + q];
+        double der = (3.0 * h5 - 4.0 * h4 + h3) / (2.0 * dz);
+        double ls = q == 0 ? 1.0 : lamN[q];
+        double p3 = q == 0 ? 0.0 : h3 / ls, p4 = q == 0 ? 0.0 : h4 / ls, p5 = q == 0 ? 0.0 : h5 / ls;
+        double pder = (3.0 * p5 - 4.0 * p4 + p3) / (2.0 * dz);
+        double ks = q == 0 ? 1.0 : kN[q];
+        rob[q] = q == 0 ? 0.0 : der + kN[q] * h5;
+        prob[q] = q == 0 ? 0.0 : pder + kN[q] * p5;
+        upw[q] = q == 0 ? 0.0 : 0.5 * (h5 + der / ks);
+        ph1[q] = q == 0 ? 0.0 : hat[P + q] / ls;   // Neumann solves of planes 1, 2
+        ph2[q] = q == 0 ? 0.0 : hat[2 * P + q] / ls;
+    }));
+    double res[NFGS_NSRCDIAG];
+    for (int q = 0; q < NFGS_NSRCDIAG; ++q) res[q] = 0.0;
+    int rc = 0;
+    double r[4];
+    {
+        double *bza = h->bz_above, *bzo = h->bz_obs, *bbgd = h->bbg_d;
+        CK(launch_map(P, s, [=] __device__(long long q) { sp[q] = bbgd[2 * V + q] + bza[q] - bzo[q]; }));
+        TRY(reduce4(h, sp, P, r));
+        res[0] = std::sqrt(r[1] / P);
+        res[1] = r[3];
+        CK(launch_map(P, s, [=] __device__(long long q) { sp[q] = bc[q] - bza[q]; }));
+        res[2] = rms_of(h, sp, P, &rc); TRY(rc);
+    }
+    TRY(idct2_d(h, rob, sp, scr)); res[3] = rms_of(h, sp, P, &rc); TRY(rc);
+    TRY(idct2_d(h, prob, sp, scr)); res[4] = rms_of(h, sp, P, &rc); TRY(rc);
+    TRY(idct2_d(h, upw, sp, scr));
+    double up_rms = rms_of(h, sp, P, &rc); TRY(rc);
+    double top_rms = rms_of(h, bc + 5 * P, P, &rc); TRY(rc);
+    res[5] = up_rms;
+    res[6] = up_rms / std::max(top_rms, 1e-30);
+    {
+        double* d0 = h->d0;
+        double dx = g.dx, dy = g.dy;
+        CK(launch_map(P, s, [=] __device__(long long q) {
+            int j = (int)(q / nx), i = (int)(q % nx);
+            sp[q] = d2d(bx0, nx, ny, j, i, 0, dx) + d2d(by0, nx, ny, j, i, 1, dy) - d0[q];
+        }));
+        double er = rms_of(h, sp, P, &rc); TRY(rc);
+        double ds = rms_of(h, d0, P, &rc); TRY(rc);
+        res[9] = er;
+        res[10] = er / std::max(ds, 1e-30);
+    }
+    {
+        TRY(idct2_d(h, ph1, sp, scr));
+        TRY(idct2_d(h, ph2, sp2, scr));
+        double *pab = h->phi_above, *tg = h->dphi_tgt;
+        CK(launch_map(P, s, [=] __device__(long long q) {
+            double d = (-3.0 * pab[q] + 4.0 * sp[q] - sp2[q]) / (2.0 * dz);
+            o[q] = d - tg[q];
+        }));
+        res[11] = rms_of(h, o, P, &rc); TRY(rc);
+    }
+    std::memcpy(out, res, sizeof res);
+    for (auto it = h->owned.begin(); it != h->owned.end();) {
+        if (it->p == w) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+    }
+    return NFGS_OK;
+}
+
+static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) {
+    if (!geom || !prm || !out) return fail(NFGS_EINVAL, "null argument");
+    if (geom->nx < 3 || geom->ny < 3) return fail(NFGS_EINVAL, "NFGS requires a calculation grid with Nx, Ny >= 3");
+    if (geom->nz < 3) return fail(NFGS_EINVAL, "NFGS requires Nz >= 3");
+    if (geom->dtype != NFGS_F32 && geom->dtype != NFGS_F64) return fail(NFGS_EINVAL, "dtype must be F32 or F64");
+    if (!(geom->dx > 0) || !(geom->dy > 0) || !(geom->dz > 0)) return fail(NFGS_EINVAL, "grid spacing must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(NFGS_ECUDA, "no CUDA device: the NFGS B200 library has no CPU path");
+    Handle* h = new Handle();
+    h->geom = *geom;
+    h->prm = *prm;
+    h->f32 = geom->dtype == NFGS_F32;
+    h->esz = h->f32 ? 4 : 8;
+    Geo& g = h->g;
+    g.nx = geom->nx; g.ny = geom->ny; g.nz = geom->nz;
+    g.P = (long long)g.nx * g.ny;
+    g.V = g.P * g.nz;
+    g.dx = geom->dx; g.dy = geom->dy; g.dz = geom->dz;
+    h->PI = (long long)(g.nx - 2) * (g.ny - 2);
+    auto bail = [&](int r) { free_all(h); delete h; return r; };
+#define TRYC(call) do { int r_ = (call); if (r_ != NFGS_OK) return bail(r_); } while (0)
+#define CKC(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { fail(NFGS_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); return bail(NFGS_ECUDA); } } while (0)
+    CKC(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
+    CKC(cudaEventCreate(&h->ev0));
+    CKC(cudaEventCreate(&h->ev1));
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const long long P = g.P, V = g.V, PI = h->PI;
+    // transforms
+    {
+        auto cx = dct_matrix(nx, false), icx = dct_matrix(nx, true);
+        auto cy = dct_matrix(ny, false), icy = dct_matrix(ny, true);
+        auto sx = dst_matrix(nx - 2, false), isx = dst_matrix(nx - 2, true);
+        auto sy = dst_matrix(ny - 2, false), isy = dst_matrix(ny - 2, true);
+        TRYC(upload(h, &h->dctx, cx)); TRYC(upload(h, &h->idctx, icx));
+        TRYC(upload(h, &h->dcty, cy)); TRYC(upload(h, &h->idcty, icy));
+        TRYC(upload(h, &h->dstx, sx)); TRYC(upload(h, &h->idstx, isx));
+        TRYC(upload(h, &h->dsty, sy)); TRYC(upload(h, &h->idsty, isy));
+        TRYC(upload_t(h, &h->dctx_t, cx)); TRYC(upload_t(h, &h->idctx_t, icx));
+        TRYC(upload_t(h, &h->dcty_t, cy)); TRYC(upload_t(h, &h->idcty_t, icy));
+        TRYC(upload_t(h, &h->dstx_t, sx)); TRYC(upload_t(h, &h->idstx_t, isx));
+        TRYC(upload_t(h, &h->dsty_t, sy)); TRYC(upload_t(h, &h->idsty_t, isy));
+    }
+    // eigenvalues (nfgs_solver.py:1083-1118, 4357-4383, 4811)
+    {
+        std::vector<double> lx(nx), ly(ny), ax(nx), ay(ny), ln(P), kn(P), lns(P), ld(PI);
+        for (int i = 0; i < nx; ++i) {
+            double sn = std::sin(M_PI * i / (2.0 * std::max(nx - 1, 1)));
+            lx[i] = -4.0 * sn * sn / (g.dx * g.dx);
+            ax[i] = 2.0 * sn / g.dx;
+        }
+        for (int j = 0; j < ny; ++j) {
+            double sn = std::sin(M_PI * j / (2.0 * std::max(ny - 1, 1)));
+            ly[j] = -4.0 * sn * sn / (g.dy * g.dy);
+            ay[j] = 2.0 * sn / g.dy;
+        }
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                double l = ly[j] + lx[i];
+                ln[(size_t)j * nx + i] = l;
+                kn[(size_t)j * nx + i] = std::sqrt(std::max(-l, 0.0));
+                lns[(size_t)j * nx + i] = (i == 0 && j == 0) ? 1.0 : l;
+            }
+        for (int j = 0; j < ny - 2; ++j)
+            for (int i = 0; i < nx - 2; ++i) {
+                double sx = std::sin(M_PI * (i + 1) / (2.0 * (nx - 1)));
+                double sy = std::sin(M_PI * (j + 1) / (2.0 * (ny - 1)));
+                ld[(size_t)j * (nx - 2) + i] = -4.0 * sx * sx / (g.dx * g.dx) + -4.0 * sy * sy / (g.dy * g.dy);
+            }
+        TRYC(upload(h, &h->lamN, ln)); TRYC(upload(h, &h->kN, kn)); TRYC(upload(h, &h->lamNs, lns));
+        TRYC(upload(h, &h->lamD, ld)); TRYC(upload(h, &h->alx, ax)); TRYC(upload(h, &h->aly, ay));
+    }
+    // factor tables
+    TRYC(alloc(h, &h->zr_c, (size_t)nz * P * 8)); TRYC(alloc(h, &h->zr_i, (size_t)nz * P * 8));
+    TRYC(alloc(h, &h->zr_il, P * 8)); TRYC(alloc(h, &h->zr_ci, P * 8)); TRYC(alloc(h, &h->zr_ii, P * 8));
+    TRYC(alloc(h, &h->zr_rc, P * 4));
+    TRYC(alloc(h, &h->zd_c, (size_t)nz * PI * 8)); TRYC(alloc(h, &h->zd_i, (size_t)nz * PI * 8));
+    TRYC(alloc(h, &h->zd_il, PI * 8)); TRYC(alloc(h, &h->zd_ci, PI * 8)); TRYC(alloc(h, &h->zd_ii, PI * 8));
+    TRYC(alloc(h, &h->zd_rc, PI * 4));
+    // boundary planes
+    double** planes[] = {&h->bz_obs, &h->bx_obs, &h->by_obs, &h->jz_obs, &h->az_bot, &h->jz_t,
+                         &h->phi_above, &h->bz_above, &h->d0, &h->dphi_tgt, &h->phi_above_hat,
+                         &h->phi_below_hat, &h->phi_bot_hat, &h->der_hat};
+    for (auto pp : planes) { TRYC(alloc(h, pp, P * 8)); CKC(cudaMemset(*pp, 0, P * 8)); }
+    TRYC(alloc(h, &h->az_bot_hat, PI * 8));
+    TRYC(alloc(h, &h->bbg_d, 3 * V * 8));
+    TRYC(alloc(h, &h->bbg, 3 * V * h->esz));
+    TRYC(alloc(h, &h->bzobs_t, P * h->esz)); TRYC(alloc(h, &h->jzt_t, P * h->esz));
+    TRYC(alloc(h, &h->phiab_t, P * h->esz)); TRYC(alloc(h, &h->dphi_t, P * h->esz));
+    // buffer window (nfgs_solver.py:1569-1591)
+    if (prm->buffer_thickness > 0) {
+        const int t = prm->buffer_thickness;
+        auto bell = [&](int n) {
+            std::vector<double> w(n);
+            int tt = std::min(t, std::max(1, (n - 1) / 2));
+            for (int q = 0; q < n; ++q) {
+                int d = std::min(q, n - 1 - q);
+                w[q] = d >= tt ? 1.0 : 0.5 * (1.0 - std::cos(M_PI * d / (double)tt));
+            }
+            return w;
+        };
+        std::vector<double> wz(nz, 1.0);
+        if (!prm->buffer_xy_only) {
+            int tz = std::min(t, std::max(1, nz - 1));
+            for (int k = 0; k < nz; ++k) {
+                int d = nz - 1 - k;
+                wz[k] = d >= tz ? 1.0 : 0.5 * (1.0 - std::cos(M_PI * d / (double)tz));
+            }
+            wz[0] = 1.0;
+        }
+        TRYC(upload_t(h, &h->wx, bell(nx)));
+        TRYC(upload_t(h, &h->wy, bell(ny)));
+        TRYC(upload_t(h, &h->wz, wz));
+    }
+    // state and work buffers
+    for (int b = 0; b < 3; ++b) {
+        TRYC(alloc(h, &h->st.phi[b], V * h->esz));
+        TRYC(alloc(h, &h->st.az[b], V * h->esz));
+        CKC(cudaMemset(h->st.phi[b], 0, V * h->esz));
+        CKC(cudaMemset(h->st.az[b], 0, V * h->esz));
+    }
+    TRYC(alloc(h, &h->st_dev, sizeof(StateTab)));
+    CKC(cudaMemcpy(h->st_dev, &h->st, sizeof(StateTab), cudaMemcpyHostToDevice));
+    TRYC(alloc(h, &h->B, 3 * V * h->esz));
+    TRYC(alloc(h, &h->jz, V * h->esz));
+    TRYC(alloc(h, &h->jpf, 3 * (size_t)(nz - 1) * P * h->esz));
+    TRYC(alloc(h, &h->jb, 2 * P * h->esz));
+    TRYC(alloc(h, &h->sb, V * h->esz));
+    TRYC(alloc(h, &h->sj, (size_t)nz * PI * h->esz));
+    TRYC(alloc(h, &h->tmpA, V * h->esz));
+    TRYC(alloc(h, &h->tmpB, (size_t)nz * PI * h->esz));
+    CKC(cudaMemset(h->sj, 0, (size_t)nz * PI * h->esz));
+    CKC(cudaMemset(h->jpf, 0, 3 * (size_t)(nz - 1) * P * h->esz));
+    h->sblock = dim3(32, 4, 1);
+    h->sgrid = dim3((nx + 31) / 32, (ny + 3) / 4, nz);
+    h->nb_face = h->nb_src = (int)(h->sgrid.x * h->sgrid.y * h->sgrid.z);
+    TRYC(alloc(h, &h->pface, (size_t)h->nb_face * 5 * 8));
+    TRYC(alloc(h, &h->psrc, (size_t)h->nb_src * 8));
+    TRYC(alloc(h, &h->s00, (size_t)nz * 8));
+    TRYC(alloc(h, &h->scal, 64 * 8));
+    TRYC(alloc(h, &h->ctl, sizeof(DevCtl)));
+    CKC(cudaMallocHost(&h->ctl_h, sizeof(DevCtl)));
+    std::memset(h->ctl_h, 0, sizeof(DevCtl));
+    TRYC(alloc(h, &h->consts, 4 * sizeof(int)));
+    {
+        int cs[4] = {0, 1, 2, 0};
+        CKC(cudaMemcpy(h->consts, cs, sizeof cs, cudaMemcpyHostToDevice));
+    }
+#undef TRYC
+#undef CKC
+    *out = h;
+    return NFGS_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* nfgs_last_error(void) { return g_err.c_str(); }
+
+const char* nfgs_version(void) { return "nfgs_b200 0.1 (sm_100a)"; }
+
+int nfgs_create(const NfgsGeom* geom, const NfgsParams* params, void** handle_out) {
+    g_err.clear();
+    return create_impl(geom, params, handle_out);
+}
+
+int nfgs_destroy(void* handle) {
+    if (!handle) return NFGS_OK;
+    Handle* h = (Handle*)handle;
+    if (h->s) cudaStreamSynchronize(h->s);
+    free_all(h);
+    delete h;
+    return NFGS_OK;
+}
+
+int nfgs_set_boundary(void* handle, const double* bx, const double* by, const double* bz, const double* jz,
+                      const NfgsBoundaryOpts* opts, double* diag_out) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h || !bx || !by || !bz || !opts) return fail(NFGS_EINVAL, "null argument");
+    if (opts->jz_mode == NFGS_JZ_PROVIDED && !jz) return fail(NFGS_EINVAL, "jz is required when provided");
+    if (opts->copy_ny <= 0 || opts->copy_nx <= 0 || opts->fov_y0 < 0 || opts->fov_x0 < 0 ||
+        opts->fov_y0 + opts->copy_ny > h->g.ny || opts->fov_x0 + opts->copy_nx > h->g.nx ||
+        opts->src_y0 < 0 || opts->src_x0 < 0 || opts->src_y0 + opts->copy_ny > opts->ny_obs ||
+        opts->src_x0 + opts->copy_nx > opts->nx_obs)
+        return fail(NFGS_EINVAL, "inconsistent boundary placement");
+    if (opts->nzo < 1 || opts->nzo > h->g.nz) return fail(NFGS_EINVAL, "observed height out of range");
+    h->fov_y0 = opts->fov_y0;
+    h->fov_x0 = opts->fov_x0;
+    h->nyo = opts->copy_ny;
+    h->nxo = opts->copy_nx;
+    h->nzo_crop = opts->nzo;
+    // cwsin box on the face grid (nfgs_solver.py:2656-2676)
+    {
+        const int nzf = h->g.nz - 1, ny = h->g.ny, nx = h->g.nx;
+        const int nzo = opts->nzo;
+        const int bfz = std::max(0, nzf - nzo);
+        const int ax = opts->nx_obs / 8 + opts->fov_x0;
+        const int ay = opts->ny_obs / 8 + opts->fov_y0;
+        const int az = nzo / 4 + bfz;
+        Box b;
+        b.z0 = 1; b.z1 = std::max(1, nzf - 1 - az + 1);
+        b.y0 = ay; b.y1 = std::max(ay + 1, ny - 1 - ay + 1);
+        b.x0 = ax; b.x1 = std::max(ax + 1, nx - 1 - ax + 1);
+        b.z1 = std::min(b.z1, nzf); b.y1 = std::min(b.y1, ny); b.x1 = std::min(b.x1, nx);
+        h->box = b;
+    }
+    h->launches = 0;
+    int r = setup_boundary(h, bx, by, bz, jz, opts, diag_out);
+    if (r != NFGS_OK) h->boundary_set = 0;
+    return r;
+}
+
+int nfgs_iterate_begin(void* handle, const NfgsStop* stop) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h || !stop) return fail(NFGS_EINVAL, "null argument");
+    return h->f32 ? iterate_begin_t<float>(h, stop) : iterate_begin_t<double>(h, stop);
+}
+
+int nfgs_iterate_initial(void* handle, double* scalars3) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h || !scalars3) return fail(NFGS_EINVAL, "null argument");
+    if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
+    CK(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    scalars3[0] = h->ctl_h->sigma0;
+    scalars3[1] = h->ctl_h->divb0;
+    scalars3[2] = h->ctl_h->e0;
+    return NFGS_OK;
+}
+
+int nfgs_iterate_advance(void* handle, int32_t max_steps, int32_t* stop_reason, int32_t* n_done) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(NFGS_EINVAL, "null argument");
+    return h->f32 ? iterate_advance_t<float>(h, max_steps, stop_reason, n_done)
+                  : iterate_advance_t<double>(h, max_steps, stop_reason, n_done);
+}
+
+int nfgs_iterate_end(void* handle, NfgsIterResult* result, double* hist, int32_t hist_rows) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(NFGS_EINVAL, "null argument");
+    return h->f32 ? iterate_end_t<float>(h, result, hist, hist_rows) : iterate_end_t<double>(h, result, hist, hist_rows);
+}
+
+int nfgs_get_history(void* handle, int32_t first, int32_t n, double* out, int32_t* n_total) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(NFGS_EINVAL, "null argument");
+    if (!h->hist) { if (n_total) *n_total = 0; return NFGS_OK; }
+    CK(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    int tot = h->ctl_h->n_hist;
+    if (n_total) *n_total = tot;
+    if (out && n > 0 && first >= 0 && first < tot) {
+        int m = std::min(n, tot - first);
+        CK(cudaMemcpy(out, h->hist + (size_t)first * NFGS_HCOLS, (size_t)m * NFGS_HCOLS * 8, cudaMemcpyDeviceToHost));
+    }
+    return NFGS_OK;
+}
+
+int nfgs_iterate(void* handle, const NfgsStop* stop, NfgsIterResult* result, double* hist, int32_t hist_rows) {
+    TRY(nfgs_iterate_begin(handle, stop));
+    int32_t reason = 0, n = 0;
+    TRY(nfgs_iterate_advance(handle, stop->max_iter + 1, &reason, &n));
+    return nfgs_iterate_end(handle, result, hist, hist_rows);
+}
+
+int nfgs_fields(void* handle, int32_t which, int32_t crop, double* out, int32_t* dims_out) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h || !out) return fail(NFGS_EINVAL, "null argument");
+    return h->f32 ? fields_t<float>(h, which, crop, out, dims_out) : fields_t<double>(h, which, crop, out, dims_out);
+}
+
+int nfgs_get_scalars_state(void* handle, int32_t which, double* phi, double* az, double* scalars3) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(NFGS_EINVAL, "null argument");
+    return h->f32 ? get_state_t<float>(h, which, phi, az, scalars3) : get_state_t<double>(h, which, phi, az, scalars3);
+}
+
+int nfgs_step(void* handle, double mu, int32_t polarity_mask) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(NFGS_EINVAL, "null argument");
+    return h->f32 ? step_t<float>(h, mu, polarity_mask) : step_t<double>(h, mu, polarity_mask);
+}
+
+int nfgs_gaussian_above(void* handle, double* out) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h || !out) return fail(NFGS_EINVAL, "null argument");
+    return gaussian_above_impl(h, out);
+}
+
+int nfgs_get_plane(void* handle, int32_t which, double* out) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h || !out) return fail(NFGS_EINVAL, "null argument");
+    if (!h->boundary_set) return fail(NFGS_ESTATE, "boundary is not set");
+    const double* src[] = {h->bz_obs, h->bx_obs, h->by_obs, h->jz_obs, h->az_bot,
+                           h->jz_t, h->phi_above, h->bz_above, h->d0, h->dphi_tgt};
+    if (which < 0 || which > 9) return fail(NFGS_EINVAL, "plane index out of range");
+    CK(cudaMemcpyAsync(out, src[which], h->g.P * 8, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    return NFGS_OK;
+}
+
+int nfgs_get_background(void* handle, double* out) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h || !out) return fail(NFGS_EINVAL, "null argument");
+    if (!h->boundary_set) return fail(NFGS_ESTATE, "boundary is not set");
+    CK(cudaMemcpyAsync(out, h->bbg_d, 3 * h->g.V * 8, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    return NFGS_OK;
+}
+
+int nfgs_source_diagnostics(void* handle, double* out) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h || !out) return fail(NFGS_EINVAL, "null argument");
+    return h->f32 ? source_diag_t<float>(h, out) : source_diag_t<double>(h, out);
+}
+
+}  // extern "C"
