@@ -1,0 +1,377 @@
+#!/usr/bin/env python3
+"""Benchmark of the NFGS reconstruction hot path on B200.
+
+Workload (one GPU): a seeded Titov-Demoulin-type flux rope on a 256x256x128
+grid (calculation grid 258x258x129), rho = 0.5, FP32 storage, gs_cfcf
+start.  One *step* is one NFGSSolverGPU.iterate() call of ITERS NFPT
+iterations with the stop rule disabled, on a boundary that is already
+resident on the device.  The metric is Gcell-iter/s on the calculation
+grid (cells x iterations / device seconds, CUDA events on the solver's
+stream, max over ranks).
+
+  python bench.py [--gpus N --steps K --warmup W]            # B200 path
+  python bench.py --impl reference [--steps K --warmup W]    # CPU reference arm
+
+The reference arm times the CPU restatement of the reference algorithm
+(the oracle: NumPy/SciPy FP64) on the host cores for the same workload and
+metric, one NFPT iteration per step.  Under torchrun (N > 1) every rank
+solves its own replica (the path does not shard); rank 0 prints the line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gcell-iter/s (NFGS NFPT iterations, calc grid 258x258x129, TD-type flux rope 256x256x128)"
+NX, NY, NZ = 256, 256, 128
+EXTENT = 8.0
+RHO = 0.5
+# per calculation-grid cell and iteration: 19 volume passes x 4 B on the
+# minimal data flow (stencil 5R+2W, forward 2R+2W, z-solves 2R+2W,
+# inverse 2R+2W)
+ALG_BYTES_PER_CELL_ITER = 76.0
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def boundary():
+    from nfgs_b200.synthetic import td_bottom
+
+    return td_bottom(NX, NY, seed=1, extent=EXTENT)
+
+
+def solver_kwargs():
+    return dict(bottom_divergence_robin_weight=RHO, horizontal_zero_mode_policy="frozen_linear_harmonic",
+                vertical_current_operator="staggered_face", d0_zero_mode_policy="project",
+                source_zero_mode_policy="project")
+
+
+def spacing():
+    h = 2 * EXTENT / (NX - 1)
+    return h, h, h
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_{index}.csv"
+
+    def start(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier_sync(pg, local):
+    import torch
+
+    if torch.cuda.is_available():
+        torch.cuda.synchronize(local)
+    if pg is not None:
+        pg.barrier()
+        torch.cuda.synchronize(local)
+
+
+def max_over_ranks(pg, value: float, local: int) -> float:
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference_rate(iters: int = 2, threads: int | None = None) -> dict:
+    """Oracle (CPU restatement of the reference) Gcell-iter/s on this workload."""
+    from oracle.nfgs_oracle import OracleNFGS
+
+    bx, by, bz = boundary()
+    dx, dy, dz = spacing()
+    o = OracleNFGS(NX, NY, NZ, dx, dy, dz, **{k: v for k, v in solver_kwargs().items()
+                                               if k != "vertical_current_operator"})
+    o.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+    st = o.compute_initial_conditions()
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        st = o.iteration_step(*st)
+        o.compute_sigma(st[0], st[1])
+        o.compute_divB(st[0])
+        o.compute_energy(st[0])
+    dt = time.perf_counter() - t0
+    cells = o.Nx * o.Ny * o.Nz
+    return {"value": cells * iters / dt / 1e9, "unit": "Gcell-iter/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{iters} NFPT iterations (+ sigma/divB/energy) of the FP64 NumPy/SciPy oracle on the "
+                      f"same {o.Nx}x{o.Ny}x{o.Nz} workload after its gs_cfcf start; {dt:.1f} s; transforms on "
+                      f"{os.cpu_count()} threads, element-wise work on one"}
+
+
+def run_reference(args):
+    world, rank, local, pg = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0, None
+    if rank != 0:
+        return 0
+    from oracle.nfgs_oracle import OracleNFGS
+
+    bx, by, bz = boundary()
+    dx, dy, dz = spacing()
+    o = OracleNFGS(NX, NY, NZ, dx, dy, dz, **{k: v for k, v in solver_kwargs().items()
+                                               if k != "vertical_current_operator"})
+    o.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+    st = o.compute_initial_conditions()
+    cells = o.Nx * o.Ny * o.Nz
+    for _ in range(args.warmup):
+        st = o.iteration_step(*st)
+        o.compute_sigma(st[0], st[1])
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st = o.iteration_step(*st)
+        o.compute_sigma(st[0], st[1])
+        o.compute_divB(st[0])
+        o.compute_energy(st[0])
+    dt = time.perf_counter() - t0
+    value = cells * args.steps / dt / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "Gcell-iter/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded TD-type flux rope)",
+        "config": {"workload": "td_flux_rope 256x256x128 -> calc 258x258x129, rho=0.5, one NFPT iteration per step",
+                   "grid": [NX, NY, NZ], "calc_grid": [o.Nx, o.Ny, o.Nz]},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "Gcell-iter/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": f"{args.steps} timed NFPT iterations of the FP64 NumPy/SciPy restatement of the "
+                                   f"reference algorithm; transforms on {os.cpu_count()} threads"},
+        "e2e": {"value": value, "unit": "Gcell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    world, rank, local, pg = dist_setup()
+    import torch  # noqa: F401  (device plumbing and synchronisation only)
+
+    from nfgs_b200 import NFGSSolverGPU
+
+    bx, by, bz = boundary()
+    dx, dy, dz = spacing()
+    dev = f"cuda:{local}"
+    s = NFGSSolverGPU(NX, NY, NZ, dx, dy, dz, device=dev, dtype="float32", **solver_kwargs())
+    cells = s.Nx * s.Ny * s.Nz
+    s.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+    it_kw = dict(max_iter=args.iters, tol=1e-30, patience=0, sigma_improvement_tol=None, verbose=False,
+                 check_every=args.check_every)
+    for _ in range(args.warmup):
+        s.iterate(**it_kw)
+    clocks = Clocks(local)
+    barrier_sync(pg, local)
+    clocks.start()
+    dev_ms = 0.0
+    launches = 0
+    for _ in range(args.steps):
+        h = s.iterate(**it_kw)
+        dev_ms += h["device_ms"]
+        launches += h["kernel_launches"]
+    barrier_sync(pg, local)
+    ck = clocks.stop()
+    dev_ms = max_over_ranks(pg, dev_ms, local)
+    total_iters = args.iters * args.steps
+    value = cells * total_iters * world / (dev_ms / 1e3) / 1e9
+
+    # end to end through the public API with host buffers: boundary H2D,
+    # set-up, iterate, fields D2H, every step
+    e2e_times = []
+    fields_bytes = 0
+    for _ in range(max(1, min(args.steps, 3))):
+        barrier_sync(pg, local)
+        t0 = time.perf_counter()
+        s2 = NFGSSolverGPU(NX, NY, NZ, dx, dy, dz, device=dev, dtype="float32", **solver_kwargs())
+        s2.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+        s2.iterate(**it_kw)
+        f = s2.fields_to_numpy()
+        barrier_sync(pg, local)
+        e2e_times.append(time.perf_counter() - t0)
+        fields_bytes = 6 * f["Bx"].size * 8
+        del s2
+    e2e_s = max_over_ranks(pg, statistics.median(e2e_times), local)
+    e2e_value = cells * args.iters * world / e2e_s / 1e9
+
+    # phase breakdown of the iteration (CUDA events on the solver stream)
+    s.iterate(max_iter=0, verbose=False)
+    ph = s._time_phases(args.phase_iters)
+    ph_ms = ph / args.phase_iters
+    names = ["stencil", "forward_transforms", "z_solves", "inverse_transforms", "finalize"]
+    dom = int(np.argmax(ph_ms))
+    hbm_gbs, bf16_tf, peak_src = load_peaks()
+    # algorithmic bytes / flops per launch group (per iteration)
+    alg_bytes = {"stencil": 28.0 * cells, "forward_transforms": 16.0 * cells, "z_solves": 16.0 * cells,
+                 "inverse_transforms": 16.0 * cells, "finalize": 4.0 * s.Nx * s.Ny}
+    tr_flops = 2.0 * cells * (s.Nx + s.Ny) * 2  # two chains x (x and y) x 2N per output element
+    dname = names[dom]
+    if dname in ("forward_transforms", "inverse_transforms"):
+        achieved = tr_flops / (ph_ms[dom] / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": bf16_tf, "unit": "TFLOP/s",
+                "frac": achieved / bf16_tf, "traffic": None, "kernel": dname,
+                "note": f"peak = {peak_src} bf16 dense; dense FP32-equivalent transform flops"}
+    else:
+        achieved = alg_bytes[dname] / (ph_ms[dom] / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_gbs, "unit": "GB/s", "frac": achieved / hbm_gbs,
+                "traffic": None, "kernel": dname, "note": f"peak = {peak_src} HBM copy bandwidth"}
+    iter_ms = float(ph_ms.sum())
+    whole = {"achieved_gbs": ALG_BYTES_PER_CELL_ITER * cells / (iter_ms / 1e3) / 1e9,
+             "frac_of_hbm": ALG_BYTES_PER_CELL_ITER * cells / (iter_ms / 1e3) / 1e9 / hbm_gbs,
+             "iteration_ms": iter_ms, "phase_ms": {n: float(v) for n, v in zip(names, ph_ms)}}
+
+    # time to the sigma_J stop with the production stop rule
+    t_stop = None
+    if args.stop_run:
+        h = s.iterate(max_iter=3000, tol=1e-5, patience=40, sigma_improvement_tol=1e-5, verbose=False,
+                      check_every=args.check_every)
+        t_stop = {"seconds": h["device_ms"] / 1e3, "iterations": len(h["sigma"]), "best_iter": h["best_iter"],
+                  "best_sigma": h["best_sigma"], "stop_reason": h["stop_reason"]}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_reference_rate(iters=args.cpu_iters)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gcell-iter/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded TD-type flux rope, seed 1)",
+            "config": {"workload": f"td_flux_rope 256x256x128 -> calc {s.Nx}x{s.Ny}x{s.Nz}, rho=0.5, fp32 storage, "
+                                   f"gs_cfcf + {args.iters} NFPT iterations per step, stop rule off",
+                       "grid": [NX, NY, NZ], "calc_grid": [s.Nx, s.Ny, s.Nz], "iters_per_step": args.iters,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "working set > L2: each iteration streams phi, A_z and the 103 MB background"},
+            "e2e": {"value": e2e_value, "unit": "Gcell-iter/s", "h2d_bytes_per_step": 3 * NX * NY * 8,
+                    "d2h_bytes_per_step": fields_bytes, "seconds_per_step": e2e_s},
+            "roofline": roof,
+            "iteration_roofline": whole,
+            "gpu_launches": launches,
+            "clocks": ck,
+            "time_to_sigma_stop": t_stop,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def run_window(args):
+    import torch
+
+    from nfgs_b200 import NFGSSolverGPU
+
+    bx, by, bz = boundary()
+    dx, dy, dz = spacing()
+    s = NFGSSolverGPU(NX, NY, NZ, dx, dy, dz, device="cuda:0", dtype="float32", **solver_kwargs())
+    s.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+    s.iterate(max_iter=0, verbose=False)
+    s._time_phases(1)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    ms = s._time_phases(args.phase_iters)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"phase_ms_per_iter": (ms / args.phase_iters).tolist()}))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--iters", type=int, default=100)
+    ap.add_argument("--check-every", type=int, default=50)
+    ap.add_argument("--phase-iters", type=int, default=10)
+    ap.add_argument("--cpu-iters", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-stop-run", dest="stop_run", action="store_false")
+    ap.add_argument("--ncu-window", action="store_true",
+                    help="profile window only: set-up, then --phase-iters iterations between "
+                         "cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    args = ap.parse_args()
+    if args.ncu_window:
+        return run_window(args)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

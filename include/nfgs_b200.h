@@ -71,6 +71,7 @@ typedef struct NfgsGeom {
     int32_t input_nx, input_ny, input_nz; /* constructor grid */
     int32_t pad_x, pad_y;        /* calculation_pad_xy */
     int32_t dtype;               /* NFGS_F32 or NFGS_F64 */
+    int32_t device;              /* CUDA device ordinal */
 } NfgsGeom;
 
 /* NFGS policy (constructor keywords, nfgs_solver.py:3925-4349). */
@@ -215,6 +216,14 @@ int nfgs_get_background(void* handle, double* out);
  * the order documented in nfgs_b200/solver.py (NFGS_NSRCDIAG doubles). */
 #define NFGS_NSRCDIAG 12
 int nfgs_source_diagnostics(void* handle, double* out);
+
+/* Per-phase device time of n_iters NFPT iterations from the current
+ * state (no stop rule), CUDA events on the handle's stream.  ms_out[5]:
+ * 0 stencil passes (reconstruction, face current, sources, reductions),
+ * 1 forward DCT-I/DST-I transforms, 2 modal z-solves, 3 inverse
+ * transforms, 4 finalisation/control.  Instrumentation for roofline
+ * reporting; the state advances as in nfgs_step. */
+int nfgs_time_phases(void* handle, int32_t n_iters, double* ms_out);
 
 int nfgs_destroy(void* handle);
 

@@ -42,7 +42,7 @@ class NfgsGeom(C.Structure):
     _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
                 ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
                 ("input_nx", C.c_int32), ("input_ny", C.c_int32), ("input_nz", C.c_int32),
-                ("pad_x", C.c_int32), ("pad_y", C.c_int32), ("dtype", C.c_int32)]
+                ("pad_x", C.c_int32), ("pad_y", C.c_int32), ("dtype", C.c_int32), ("device", C.c_int32)]
 
 
 class NfgsParams(C.Structure):
@@ -101,6 +101,7 @@ SIGNATURES = {
     "nfgs_get_plane": (C.c_int, [_P, C.c_int32, _DP]),
     "nfgs_get_background": (C.c_int, [_P, _DP]),
     "nfgs_source_diagnostics": (C.c_int, [_P, _DP]),
+    "nfgs_time_phases": (C.c_int, [_P, C.c_int32, _DP]),
     "nfgs_destroy": (C.c_int, [_P]),
     "nfgs_last_error": (C.c_char_p, []),
     "nfgs_version": (C.c_char_p, []),

@@ -1535,6 +1535,74 @@ static int source_diag_t(Handle* h, double* out) {
     return NFGS_OK;
 }
 
+template <typename T>
+static int time_phases_t(Handle* h, int n_iters, double* ms_out) {
+    if (!h->boundary_set) return fail(NFGS_ESTATE, "boundary is not set");
+    cudaEvent_t ev[6];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    double acc[5] = {0, 0, 0, 0, 0};
+    const Geo& g = h->g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const long long P = g.P, PI = h->PI;
+    const int nxi = nx - 2, nyi = ny - 2;
+    for (int it = 0; it < n_iters; ++it) {
+        const int cur = h->cur_host;
+        const int cand = (cur + 1) % 3 == h->solution ? (cur + 2) % 3 : (cur + 1) % 3;
+        CK(cudaEventRecord(ev[0], h->s));
+        TRY(run_stencil<T>(h, &h->consts[cur], nullptr, 1, 0));
+        k_sum_partials<<<6, 256, 0, h->s>>>(h->pface, h->nb_face, h->psrc, h->nb_src, h->scal);
+        CK(cudaEventRecord(ev[1], h->s));
+        TRY(apply_x<T>(h, h->dctx_t, h->sb, nx, P, h->tmpA, nx, P, ny * nz, nx, nx, 1));
+        TRY(apply_y<T>(h, h->dcty_t, h->tmpA, nx, P, h->sb, nx, P, ny, ny, nx, nz));
+        {
+            const char* sjp = (const char*)h->sj + (size_t)PI * h->esz;
+            char* tbp = (char*)h->tmpB + (size_t)PI * h->esz;
+            TRY(apply_x<T>(h, h->dstx_t, sjp, nxi, PI, tbp, nxi, PI, nyi * (nz - 2), nxi, nxi, 1));
+            TRY(apply_y<T>(h, h->dsty_t, tbp, nxi, PI, (void*)sjp, nxi, PI, nyi, nyi, nxi, nz - 2));
+        }
+        CK(cudaEventRecord(ev[2], h->s));
+        {
+            ZTab tr{h->zr_c, h->zr_i, h->zr_il, h->zr_ci, h->zr_ii, h->zr_rc};
+            ZTab td{h->zd_c, h->zd_i, h->zd_il, h->zd_ci, h->zd_ii, h->zd_rc};
+            int nbr = (int)((P + 255) / 256);
+            int nbd = (int)((PI + 255) / 256);
+            k_zsolve<T><<<nbr + nbd, 256, 0, h->s>>>(g, nullptr, (T*)h->sb, tr, h->lamNs, h->phi_bot_hat, h->der_hat,
+                                                     h->prm.robin_weight, h->s00, (T*)h->sj, td, h->lamD,
+                                                     h->az_bot_hat, nbr);
+            CK(cudaGetLastError());
+        }
+        CK(cudaEventRecord(ev[3], h->s));
+        {
+            const char* shp = (const char*)h->sb + (size_t)P * h->esz;
+            char* tap = (char*)h->tmpA + (size_t)P * h->esz;
+            TRY(apply_y<T>(h, h->idcty_t, shp, nx, P, tap, nx, P, ny, ny, nx, nz - 1));
+            TRY(apply_x<T>(h, h->idctx_t, tap, nx, P, (void*)(intptr_t)(P * h->esz), nx, P, ny * (nz - 1), nx, nx, 1,
+                           (void* const*)h->st_dev->phi, &h->consts[cand]));
+            const char* sjp = (const char*)h->sj + (size_t)PI * h->esz;
+            char* tbp = (char*)h->tmpB + (size_t)PI * h->esz;
+            TRY(apply_y<T>(h, h->idsty_t, sjp, nxi, PI, tbp, nxi, PI, nyi, nyi, nxi, nz - 2));
+            TRY(apply_x<T>(h, h->idstx_t, tbp, nxi, PI, (void*)(intptr_t)((P + nx + 1) * h->esz), nx, P, nyi, nxi,
+                           nxi, nz - 2, (void* const*)h->st_dev->az, &h->consts[cand]));
+        }
+        CK(cudaEventRecord(ev[4], h->s));
+        k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(h->g, h->st, nullptr, 0, 1.0, &h->consts[cand],
+                                                                    &h->consts[cur], (const T*)h->phiab_t,
+                                                                    (const T*)h->dphi_t, h->prm.projection_weight, 1);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ev[5], h->s));
+        CK(cudaEventSynchronize(ev[5]));
+        for (int q = 0; q < 5; ++q) {
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, ev[q], ev[q + 1]));
+            acc[q] += ms;
+        }
+        h->cur_host = cand;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int q = 0; q < 5; ++q) ms_out[q] = acc[q];
+    return NFGS_OK;
+}
+
 static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) {
     if (!geom || !prm || !out) return fail(NFGS_EINVAL, "null argument");
     if (geom->nx < 3 || geom->ny < 3) return fail(NFGS_EINVAL, "NFGS requires a calculation grid with Nx, Ny >= 3");
@@ -1544,6 +1612,8 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(NFGS_ECUDA, "no CUDA device: the NFGS B200 library has no CPU path");
+    if (geom->device < 0 || geom->device >= ndev) return fail(NFGS_EINVAL, "device ordinal out of range");
+    if (cudaSetDevice(geom->device) != cudaSuccess) return fail(NFGS_ECUDA, "cudaSetDevice failed");
     Handle* h = new Handle();
     h->geom = *geom;
     h->prm = *prm;
@@ -1718,6 +1788,7 @@ int nfgs_set_boundary(void* handle, const double* bx, const double* by, const do
                       const NfgsBoundaryOpts* opts, double* diag_out) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h || !bx || !by || !bz || !opts) return fail(NFGS_EINVAL, "null argument");
     if (opts->jz_mode == NFGS_JZ_PROVIDED && !jz) return fail(NFGS_EINVAL, "jz is required when provided");
     if (opts->copy_ny <= 0 || opts->copy_nx <= 0 || opts->fov_y0 < 0 || opts->fov_x0 < 0 ||
@@ -1755,6 +1826,7 @@ int nfgs_set_boundary(void* handle, const double* bx, const double* by, const do
 int nfgs_iterate_begin(void* handle, const NfgsStop* stop) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h || !stop) return fail(NFGS_EINVAL, "null argument");
     return h->f32 ? iterate_begin_t<float>(h, stop) : iterate_begin_t<double>(h, stop);
 }
@@ -1762,6 +1834,7 @@ int nfgs_iterate_begin(void* handle, const NfgsStop* stop) {
 int nfgs_iterate_initial(void* handle, double* scalars3) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h || !scalars3) return fail(NFGS_EINVAL, "null argument");
     if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
     CK(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->s));
@@ -1775,6 +1848,7 @@ int nfgs_iterate_initial(void* handle, double* scalars3) {
 int nfgs_iterate_advance(void* handle, int32_t max_steps, int32_t* stop_reason, int32_t* n_done) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h) return fail(NFGS_EINVAL, "null argument");
     return h->f32 ? iterate_advance_t<float>(h, max_steps, stop_reason, n_done)
                   : iterate_advance_t<double>(h, max_steps, stop_reason, n_done);
@@ -1783,6 +1857,7 @@ int nfgs_iterate_advance(void* handle, int32_t max_steps, int32_t* stop_reason, 
 int nfgs_iterate_end(void* handle, NfgsIterResult* result, double* hist, int32_t hist_rows) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h) return fail(NFGS_EINVAL, "null argument");
     return h->f32 ? iterate_end_t<float>(h, result, hist, hist_rows) : iterate_end_t<double>(h, result, hist, hist_rows);
 }
@@ -1790,6 +1865,7 @@ int nfgs_iterate_end(void* handle, NfgsIterResult* result, double* hist, int32_t
 int nfgs_get_history(void* handle, int32_t first, int32_t n, double* out, int32_t* n_total) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h) return fail(NFGS_EINVAL, "null argument");
     if (!h->hist) { if (n_total) *n_total = 0; return NFGS_OK; }
     CK(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->s));
@@ -1813,6 +1889,7 @@ int nfgs_iterate(void* handle, const NfgsStop* stop, NfgsIterResult* result, dou
 int nfgs_fields(void* handle, int32_t which, int32_t crop, double* out, int32_t* dims_out) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h || !out) return fail(NFGS_EINVAL, "null argument");
     return h->f32 ? fields_t<float>(h, which, crop, out, dims_out) : fields_t<double>(h, which, crop, out, dims_out);
 }
@@ -1820,6 +1897,7 @@ int nfgs_fields(void* handle, int32_t which, int32_t crop, double* out, int32_t*
 int nfgs_get_scalars_state(void* handle, int32_t which, double* phi, double* az, double* scalars3) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h) return fail(NFGS_EINVAL, "null argument");
     return h->f32 ? get_state_t<float>(h, which, phi, az, scalars3) : get_state_t<double>(h, which, phi, az, scalars3);
 }
@@ -1827,6 +1905,7 @@ int nfgs_get_scalars_state(void* handle, int32_t which, double* phi, double* az,
 int nfgs_step(void* handle, double mu, int32_t polarity_mask) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h) return fail(NFGS_EINVAL, "null argument");
     return h->f32 ? step_t<float>(h, mu, polarity_mask) : step_t<double>(h, mu, polarity_mask);
 }
@@ -1834,6 +1913,7 @@ int nfgs_step(void* handle, double mu, int32_t polarity_mask) {
 int nfgs_gaussian_above(void* handle, double* out) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h || !out) return fail(NFGS_EINVAL, "null argument");
     return gaussian_above_impl(h, out);
 }
@@ -1841,6 +1921,7 @@ int nfgs_gaussian_above(void* handle, double* out) {
 int nfgs_get_plane(void* handle, int32_t which, double* out) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h || !out) return fail(NFGS_EINVAL, "null argument");
     if (!h->boundary_set) return fail(NFGS_ESTATE, "boundary is not set");
     const double* src[] = {h->bz_obs, h->bx_obs, h->by_obs, h->jz_obs, h->az_bot,
@@ -1854,6 +1935,7 @@ int nfgs_get_plane(void* handle, int32_t which, double* out) {
 int nfgs_get_background(void* handle, double* out) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h || !out) return fail(NFGS_EINVAL, "null argument");
     if (!h->boundary_set) return fail(NFGS_ESTATE, "boundary is not set");
     CK(cudaMemcpyAsync(out, h->bbg_d, 3 * h->g.V * 8, cudaMemcpyDeviceToHost, h->s));
@@ -1861,9 +1943,18 @@ int nfgs_get_background(void* handle, double* out) {
     return NFGS_OK;
 }
 
+int nfgs_time_phases(void* handle, int32_t n_iters, double* ms_out) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
+    if (!h || !ms_out) return fail(NFGS_EINVAL, "null argument");
+    return h->f32 ? time_phases_t<float>(h, n_iters, ms_out) : time_phases_t<double>(h, n_iters, ms_out);
+}
+
 int nfgs_source_diagnostics(void* handle, double* out) {
     g_err.clear();
     Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
     if (!h || !out) return fail(NFGS_EINVAL, "null argument");
     return h->f32 ? source_diag_t<float>(h, out) : source_diag_t<double>(h, out);
 }

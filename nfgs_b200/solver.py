@@ -48,6 +48,8 @@ def _dtype_code(dtype) -> tuple[int, np.dtype]:
 
 
 def _check_device(device) -> None:
+    if hasattr(device, "type") and hasattr(device, "index"):  # torch.device
+        device = f"{device.type}:{device.index}" if device.index is not None else device.type
     name = str(device)
     if not name.startswith("cuda"):
         raise ValueError(
@@ -305,8 +307,10 @@ class NFGSSolverGPU:
         self._have_solution = False
         self._lib = L.lib()
         am = self.alpha_max()
+        dev = str(device)
+        self._device_index = int(dev.split(":")[1]) if ":" in dev else 0
         geom = L.NfgsGeom(self.Nx, self.Ny, self.Nz, self.dx, self.dy, self.dz, int(Nx), int(Ny), int(Nz),
-                          g["pad_xy"][0], g["pad_xy"][1], self._dtype_code)
+                          g["pad_xy"][0], g["pad_xy"][1], self._dtype_code, self._device_index)
         prm = L.NfgsParams(
             robin_weight=rho, projection_weight=proj_w,
             alpha_max=(am if (am is not None and math.isfinite(am)) else -1.0),
@@ -767,3 +771,9 @@ class NFGSSolverGPU:
 
     def _step(self, mu: float = 1.0, polarity_mask: str = "both"):
         L.check(self._lib.nfgs_step(self._h, float(mu), _POLARITY[polarity_mask]))
+
+    def _time_phases(self, n_iters: int) -> np.ndarray:
+        """Device ms per phase over n_iters iterations (see nfgs_time_phases)."""
+        ms = np.zeros(5)
+        L.check(self._lib.nfgs_time_phases(self._h, int(n_iters), L.dptr(ms)))
+        return ms

@@ -29,6 +29,9 @@ from typing import Callable, Optional
 import numpy as np
 from scipy import fft as _sfft
 
+# SciPy FFT worker threads (batch-parallel transforms give identical results)
+_WORKERS = -1
+
 __all__ = [
     "mudpack_axis_size",
     "fortran_grid",
@@ -79,7 +82,7 @@ def dct1(x: np.ndarray, axis: int) -> np.ndarray:
     """Unnormalised DCT-I along ``axis`` (nfgs_solver.py:1052-1074)."""
     if x.shape[axis] == 1:
         return x.copy()
-    return _sfft.dct(x, type=1, axis=axis)
+    return _sfft.dct(x, type=1, axis=axis, workers=_WORKERS)
 
 
 def idct1(x: np.ndarray, axis: int) -> np.ndarray:
@@ -92,7 +95,7 @@ def idct1(x: np.ndarray, axis: int) -> np.ndarray:
 
 def dst1(x: np.ndarray, axis: int) -> np.ndarray:
     """Unnormalised DST-I along ``axis`` (nfgs_solver.py:1019-1045)."""
-    return _sfft.dst(x, type=1, axis=axis)
+    return _sfft.dst(x, type=1, axis=axis, workers=_WORKERS)
 
 
 def idst1(x: np.ndarray, axis: int) -> np.ndarray:
