@@ -204,6 +204,21 @@ int nfgs_step(void* handle, double mu, int32_t polarity_mask);
  * out is (3, ny, nx) FP64. */
 int nfgs_gaussian_above(void* handle, double* out);
 
+/* Allocation-free variant of nfgs_gaussian_above; no counterpart in the
+ * reference.  For callers that cannot allocate device memory while they
+ * run: applications whose own pool allocator holds the free HBM, and
+ * applications sharing the GPU with latency-critical work (cudaMalloc and
+ * cudaFree synchronise the device).  The handle must have been created and
+ * given a boundary beforehand.  Writes (3, ny, nx) FP64 to the caller's
+ * device buffer out_dev, enqueued on `stream` (a cudaStream_t; NULL is the
+ * default stream) without synchronising; scratch comes from one static
+ * 16 MiB device array that this library reserves on every GPU it loads on,
+ * so the calculation plane may hold at most 419,430 cells (NFGS_EINVAL
+ * beyond that).  The first call on a device looks the array up, and should
+ * come before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race. */
+int nfgs_gaussian_above_noalloc(void* handle, double* out_dev, void* stream);
+
 /* Fixed 2-D products of the boundary set-up (FP64, calc grid, (ny, nx)):
  * which = 0 Bz_obs, 1 Bx_obs, 2 By_obs, 3 Jz_obs, 4 Az_bottom, 5 Jz_T,
  * 6 Phi_above_bottom, 7 Bz_above, 8 D0, 9 bottom_dphi_c_target. */

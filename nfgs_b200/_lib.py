@@ -98,6 +98,7 @@ SIGNATURES = {
     "nfgs_get_scalars_state": (C.c_int, [_P, C.c_int32, _DP, _DP, _DP]),
     "nfgs_step": (C.c_int, [_P, C.c_double, C.c_int32]),
     "nfgs_gaussian_above": (C.c_int, [_P, _DP]),
+    "nfgs_gaussian_above_noalloc": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "nfgs_get_plane": (C.c_int, [_P, C.c_int32, _DP]),
     "nfgs_get_background": (C.c_int, [_P, _DP]),
     "nfgs_source_diagnostics": (C.c_int, [_P, _DP]),

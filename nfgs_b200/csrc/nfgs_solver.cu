@@ -10,6 +10,7 @@
 #include "nfgs_setup.cuh"
 
 #include <cmath>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -1762,6 +1763,115 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
 }  // namespace
 
 // ===========================================================================
+// Allocation-free B^> (variant of gaussian_above_impl)
+//
+// Callers that cannot allocate device memory at run time use this path:
+// host programs whose own pool allocator already holds the free HBM (a
+// fresh cudaMalloc from inside this library would fail or fragment it),
+// and programs sharing the GPU with latency-critical streams (cudaMalloc and
+// cudaFree synchronise the whole device).  The scratch planes live in one
+// file-scope device array, reserved on every GPU that loads this library
+// until the process exits.
+// ===========================================================================
+namespace {
+
+// 2^21 doubles = 16 MiB; five scratch planes -> at most 419,430 cells per
+// calculation-grid plane (e.g. 646 x 646).
+constexpr long long kNoAllocScratchDoubles = 1LL << 21;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+constexpr int kMaxDevices = 128;
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array for `dev`, looked up once per device
+// with that device current (the array's name is only a host-side stand-in).
+static int noalloc_scratch(int dev, double** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (dev < 0 || dev >= kMaxDevices) return fail(NFGS_EINVAL, "device ordinal out of range");
+    if (g_noalloc_ptr[dev] == nullptr) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr)
+            return fail(NFGS_ECUDA, std::string("cudaGetSymbolAddress(scratch) failed: ") + cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = (double*)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return NFGS_OK;
+}
+
+// out(r, c) = sum_m M[c][m] in(r, m), rows of pitch `pitch`, on `st`
+static int noalloc_gemm_x(cudaStream_t st, const double* M, const double* in, double* out, long long pitch, int rows,
+                          int K, int N) {
+    GemmArgs a{};
+    a.A = in; a.a_rs = pitch; a.a_cs = 1; a.a_bs = 0;
+    a.B = M; a.b_rs = 1; a.b_cs = K; a.b_bs = 0;
+    a.C = out; a.c_rs = pitch; a.c_cs = 1; a.c_bs = 0;
+    a.M = rows; a.N = N; a.K = K; a.batch = 1;
+    CK(launch_gemm<double>(a, st));
+    return NFGS_OK;
+}
+
+// out(r, c) = sum_m M[r][m] in(m, c), on `st`
+static int noalloc_gemm_y(cudaStream_t st, const double* M, const double* in, double* out, long long pitch, int K,
+                          int N, int cols) {
+    GemmArgs a{};
+    a.A = M; a.a_rs = K; a.a_cs = 1; a.a_bs = 0;
+    a.B = in; a.b_rs = pitch; a.b_cs = 1; a.b_bs = 0;
+    a.C = out; a.c_rs = pitch; a.c_cs = 1; a.c_bs = 0;
+    a.M = N; a.N = cols; a.K = K; a.batch = 1;
+    CK(launch_gemm<double>(a, st));
+    return NFGS_OK;
+}
+
+static int gaussian_above_noalloc_impl(Handle* h, double* out, cudaStream_t st) {
+    const Geo& g = h->g;
+    const int nx = g.nx, ny = g.ny, nxi = nx - 2, nyi = ny - 2;
+    const long long P = g.P;
+    if (5 * P > kNoAllocScratchDoubles) {
+        char b[200];
+        snprintf(b, sizeof b,
+                 "calculation plane of %lld cells exceeds the static scratch limit of %lld cells per plane",
+                 P, kNoAllocScratchDoubles / 5);
+        return fail(NFGS_EINVAL, b);
+    }
+    if (!h->boundary_set) return fail(NFGS_ESTATE, "NFGS Gaussian separation is not configured");
+    double* w = nullptr;
+    TRY(noalloc_scratch(h->geom.device, &w));
+    double *t1 = w, *t2 = w + P, *gx = w + 2 * P, *gy = w + 3 * P, *dph = w + 4 * P;
+    double *kN = h->kN, *pah = h->phi_above_hat, *alx = h->alx, *aly = h->aly, *bza = h->bz_above;
+    const double dx = g.dx, dy = g.dy;
+    // the scratch keeps the previous call's data; the gradient borders are
+    // never written by the transforms and must start at zero
+    CK(cudaMemsetAsync(gx, 0, 2 * P * sizeof(double), st));
+    CK(launch_map(P, st, [=] __device__(long long q) { dph[q] = kN[q] * pah[q]; }));
+    if (h->prm.gaussian_spectral) {
+        CK(launch_map(P, st, [=] __device__(long long q) { t1[q] = -alx[q % nx] * dph[q]; }));
+        TRY(noalloc_gemm_y(st, h->idcty, t1, t2, nx, ny, ny, nx));
+        TRY(noalloc_gemm_x(st, h->idstx, t2 + 1, gx + 1, nx, ny, nxi, nxi));
+        CK(launch_map(P, st, [=] __device__(long long q) { t1[q] = -aly[q / nx] * dph[q]; }));
+        TRY(noalloc_gemm_x(st, h->idctx, t1, t2, nx, ny, nx, nx));
+        TRY(noalloc_gemm_y(st, h->idsty, t2 + nx, gy + nx, nx, nyi, nyi, nx));
+    } else {
+        TRY(noalloc_gemm_x(st, h->idctx, dph, t2, nx, ny, nx, nx));
+        TRY(noalloc_gemm_y(st, h->idcty, t2, t1, nx, ny, ny, nx));
+        CK(launch_map(P, st, [=] __device__(long long q) {
+            int j = (int)(q / nx), i = (int)(q % nx);
+            gx[q] = d2d(t1, nx, ny, j, i, 0, dx);
+            gy[q] = d2d(t1, nx, ny, j, i, 1, dy);
+        }));
+    }
+    CK(launch_map(P, st, [=] __device__(long long q) {
+        out[q] = -gx[q];
+        out[P + q] = -gy[q];
+        out[2 * P + q] = bza[q];
+    }));
+    return NFGS_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
 // C ABI
 // ===========================================================================
 extern "C" {
@@ -1916,6 +2026,14 @@ int nfgs_gaussian_above(void* handle, double* out) {
     if (h) cudaSetDevice(h->geom.device);
     if (!h || !out) return fail(NFGS_EINVAL, "null argument");
     return gaussian_above_impl(h, out);
+}
+
+int nfgs_gaussian_above_noalloc(void* handle, double* out_dev, void* stream) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h || !out_dev) return fail(NFGS_EINVAL, "null argument");
+    if (cudaSetDevice(h->geom.device) != cudaSuccess) return fail(NFGS_ECUDA, "cudaSetDevice failed");
+    return gaussian_above_noalloc_impl(h, out_dev, (cudaStream_t)stream);
 }
 
 int nfgs_get_plane(void* handle, int32_t which, double* out) {
