@@ -240,6 +240,16 @@ int nfgs_source_diagnostics(void* handle, double* out);
  * reporting; the state advances as in nfgs_step. */
 int nfgs_time_phases(void* handle, int32_t n_iters, double* ms_out);
 
+/* The 2-D transforms of one iteration applied to host data (instrumentation
+ * for transform parity tests; uses the handle's work buffers and its third
+ * state buffer).  chain 0: DCT-I in x then y of an (nz, ny, nx) volume
+ * (nfgs_solver.py:4354-4355, 4445-4446); chain 1: DST-I of the interior
+ * (nz, ny-2, nx-2) volume (nfgs_solver.py:1019-1050).  inverse != 0 applies
+ * the inverse transforms.  Forward: all planes of chain 0, planes 1..nz-2 of
+ * chain 1; inverse: planes 1..nz-1 (chain 0) and 1..nz-2 (chain 1); other
+ * planes of out are left unspecified. */
+int nfgs_apply_transform(void* handle, int32_t chain, int32_t inverse, const double* in, double* out);
+
 int nfgs_destroy(void* handle);
 
 /* Message for the last failing call on this thread ("" if none). */

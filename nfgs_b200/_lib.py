@@ -103,6 +103,7 @@ SIGNATURES = {
     "nfgs_get_background": (C.c_int, [_P, _DP]),
     "nfgs_source_diagnostics": (C.c_int, [_P, _DP]),
     "nfgs_time_phases": (C.c_int, [_P, C.c_int32, _DP]),
+    "nfgs_apply_transform": (C.c_int, [_P, C.c_int32, C.c_int32, _DP, _DP]),
     "nfgs_destroy": (C.c_int, [_P]),
     "nfgs_last_error": (C.c_char_p, []),
     "nfgs_version": (C.c_char_p, []),

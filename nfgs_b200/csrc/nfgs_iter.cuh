@@ -39,8 +39,11 @@ __device__ __forceinline__ T lap1(F f, int i, int n) {
 }
 
 // ---------------------------------------------------------------------------
-// k_recon: B = B_background + (Bc_x + H_x, Bc_y + H_y, Bc_z), B_z(0) = Bz_obs,
-// state J_z = -lap_xy A_z with zero walls/top and J_z(0) = Jz_T.
+// k_recon: carrier C = B - B_background = (Bc_x + H_x, Bc_y + H_y, Bc_z) with
+// C_z(0) = Bz_obs - B_background,z(0) (B_z(0) = Bz_obs), and the state
+// J_z = -lap_xy A_z with zero walls/top and J_z(0) = Jz_T.  The carrier is
+// formed directly: the reference forms it as (B_bg + B_c + H) - B_bg
+// (nfgs_solver.py:5759), which in FP32 cancels where B_c << B_bg.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(128) k_recon(Geo g, StateTab st, const int* sel, const int* skip,
@@ -73,14 +76,12 @@ __global__ void __launch_bounds__(128) k_recon(Geo g, StateTab st, const int* se
     T bcy = -dydz - dxa;
     T bcz = lap1<T>([&](int q) { return PH(k, j, q); }, i, nx) * idx2 +
             lap1<T>([&](int q) { return PH(k, q, i); }, j, ny) * idy2;
-    T bx = ldg(bbg, c) + bcx;
-    T by = ldg(bbg, g.V + c) + bcy;
-    T bz = ldg(bbg, 2 * g.V + c) + bcz;
-    if (use_h) { bx = bx + hx; by = by + hy; }
-    if (k == 0) bz = ldg(bzobs, (long long)j * nx + i);
-    Bout[c] = bx;
-    Bout[g.V + c] = by;
-    Bout[2 * g.V + c] = bz;
+    T cx = bcx, cy = bcy, cz = bcz;
+    if (use_h) { cx = cx + hx; cy = cy + hy; }
+    if (k == 0) cz = ldg(bzobs, (long long)j * nx + i) - ldg(bbg, 2 * g.V + c);
+    Bout[c] = cx;
+    Bout[g.V + c] = cy;
+    Bout[2 * g.V + c] = cz;
     T jz;
     if (k == 0) jz = ldg(jzt, (long long)j * nx + i);
     else if (k == nz - 1 || i == 0 || i == nx - 1 || j == 0 || j == ny - 1) jz = T(0);
@@ -112,9 +113,19 @@ __global__ void __launch_bounds__(128) k_face(Geo g, const int* skip, const T* _
         const long long c = k * P + (long long)j * nx + i;
         const T i2dx = T(1.0 / (2.0 * g.dx)), i2dy = T(1.0 / (2.0 * g.dy)), i2dz = T(1.0 / (2.0 * g.dz));
         const T idz = T(1.0 / g.dz);
-        auto BX = [&](int kk, int jj, int ii) -> T { return ldg(B, kk * P + (long long)jj * nx + ii); };
-        auto BY = [&](int kk, int jj, int ii) -> T { return ldg(B, V + kk * P + (long long)jj * nx + ii); };
-        auto BZ = [&](int kk, int jj, int ii) -> T { return ldg(B, 2 * V + kk * P + (long long)jj * nx + ii); };
+        // B holds the carrier C; the field is B_background + C
+        auto BX = [&](int kk, int jj, int ii) -> T {
+            long long q = kk * P + (long long)jj * nx + ii;
+            return ldg(bbg, q) + ldg(B, q);
+        };
+        auto BY = [&](int kk, int jj, int ii) -> T {
+            long long q = V + kk * P + (long long)jj * nx + ii;
+            return ldg(bbg, q) + ldg(B, q);
+        };
+        auto BZ = [&](int kk, int jj, int ii) -> T {
+            long long q = 2 * V + kk * P + (long long)jj * nx + ii;
+            return ldg(bbg, q) + ldg(B, q);
+        };
         T bx = BX(k, j, i), by = BY(k, j, i), bz = BZ(k, j, i);
         T div = d1<T>([&](int q) { return BX(k, j, q); }, i, nx, i2dx) +
                 d1<T>([&](int q) { return BY(k, q, i); }, j, ny, i2dy) +
@@ -125,16 +136,14 @@ __global__ void __launch_bounds__(128) k_face(Geo g, const int* skip, const T* _
         red[4] = (double)(bx * bx + by * by + bz * bz);
         if (k < nz - 1) {
             const long long c1 = c + P;
-            T bx1 = ldg(B, c1), by1 = ldg(B, V + c1), bz1 = ldg(B, 2 * V + c1);
+            T bx1 = BX(k + 1, j, i), by1 = BY(k + 1, j, i), bz1 = BZ(k + 1, j, i);
             T bfx = T(0.5) * (bx1 + bx), bfy = T(0.5) * (by1 + by), bfz = T(0.5) * (bz1 + bz);
             auto CZF = [&](int jj, int ii) -> T {
-                long long q0 = k * P + (long long)jj * nx + ii;
-                T a = ldg(B, 2 * V + q0) - ldg(bbg, 2 * V + q0);
-                T b = ldg(B, 2 * V + q0 + P) - ldg(bbg, 2 * V + q0 + P);
-                return T(0.5) * (b + a);
+                long long q0 = 2 * V + k * P + (long long)jj * nx + ii;
+                return T(0.5) * (ldg(B, q0 + P) + ldg(B, q0));
             };
-            T cx0 = bx - ldg(bbg, c), cx1 = bx1 - ldg(bbg, c1);
-            T cy0 = by - ldg(bbg, V + c), cy1 = by1 - ldg(bbg, V + c1);
+            T cx0 = ldg(B, c), cx1 = ldg(B, c1);
+            T cy0 = ldg(B, V + c), cy1 = ldg(B, V + c1);
             T dbx = (cx1 - cx0) * idz;
             T dby = (cy1 - cy0) * idz;
             T jxf = d1<T>([&](int q) { return CZF(q, i); }, j, ny, i2dy) - dby;
@@ -174,8 +183,9 @@ __global__ void __launch_bounds__(128) k_face(Geo g, const int* skip, const T* _
     block_reduce<5>(red, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+        const long long nb = (long long)gridDim.x * gridDim.y * gridDim.z;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) partials[b * 5 + q] = red[q];
+        for (int q = 0; q < 5; ++q) partials[q * nb + b] = red[q];
     }
 }
 
@@ -264,6 +274,9 @@ __global__ void __launch_bounds__(128) k_src(Geo g, const int* skip, const T* __
 // both values equal their converged limits (checked bitwise when the
 // tables are built), which are kept in registers instead of being re-read.
 // ---------------------------------------------------------------------------
+// rows per batch of independent loads in the z-solves
+#define ZB 8
+
 struct ZTab {
     const double* c;      // [rows][modes]
     const double* inv;    // [rows][modes]
@@ -303,24 +316,47 @@ __device__ void zsolve_robin_mode(Geo g, long long m, T* __restrict__ hat, ZTab 
     double d = rhs0 * t.inv[m];
     hat[P + m] = (T)d;
     double s_last = s1;  // source of plane nz-2 (used again by the Robin row)
-    for (int r = 1; r <= n - 2; ++r) {
-        const long long q = (long long)(r + 1) * P + m;
-        double s = (double)hat[q] * ils;
-        s_last = s;
-        double iv = (r < rc) ? t.inv[(long long)r * P + m] : iinf;
-        d = (s - low * d) * iv;
-        hat[q] = (T)d;
+    // interior rows in batches: the loads of a batch are issued together
+    for (int r0 = 1; r0 <= n - 2; r0 += ZB) {
+        double sv[ZB];
+#pragma unroll
+        for (int u = 0; u < ZB; ++u) {
+            const int r = r0 + u;
+            sv[u] = (r <= n - 2) ? (double)hat[(long long)(r + 1) * P + m] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < ZB; ++u) {
+            const int r = r0 + u;
+            if (r <= n - 2) {
+                double s = sv[u] * ils;
+                s_last = s;
+                double iv = (r < rc) ? t.inv[(long long)r * P + m] : iinf;
+                d = (s - low * d) * iv;
+                hat[(long long)(r + 1) * P + m] = (T)d;
+            }
+        }
     }
     // Robin row after eliminating u_{N-2} (top_robin_hat = 0)
     const double rl = -ls * dz2 - 2.0;
     const double rr = -s_last * dz2;
     double u = (rr - rl * d) * t.inv_last[m];
     hat[(long long)nz * P - P + m] = (T)u;
-    for (int r = n - 2; r >= 0; --r) {
-        const long long q = (long long)(r + 1) * P + m;
-        double cr = (r < rc) ? t.c[(long long)r * P + m] : cinf;
-        u = (double)hat[q] - cr * u;
-        hat[q] = (T)u;
+    for (int r0 = n - 2; r0 >= 0; r0 -= ZB) {
+        double dv[ZB];
+#pragma unroll
+        for (int q = 0; q < ZB; ++q) {
+            const int r = r0 - q;
+            dv[q] = (r >= 0) ? (double)hat[(long long)(r + 1) * P + m] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < ZB; ++q) {
+            const int r = r0 - q;
+            if (r >= 0) {
+                double cr = (r < rc) ? t.c[(long long)r * P + m] : cinf;
+                u = dv[q] - cr * u;
+                hat[(long long)(r + 1) * P + m] = (T)u;
+            }
+        }
     }
 }
 
@@ -345,12 +381,23 @@ __device__ void zsolve_dir_mode(Geo g, long long m, long long PI, T* __restrict_
     }
     d = (r1 - a * bot_hat[m]) * t.inv[m];
     hat[PI + m] = (T)d;
-    for (int r = 1; r <= n - 2; ++r) {
-        const long long q = (long long)(r + 1) * PI + m;
-        double s = (double)hat[q] * ilam;
-        double iv = (r < rc) ? t.inv[(long long)r * PI + m] : iinf;
-        d = (s - a * d) * iv;
-        hat[q] = (T)d;
+    for (int r0 = 1; r0 <= n - 2; r0 += ZB) {
+        double sv[ZB];
+#pragma unroll
+        for (int u = 0; u < ZB; ++u) {
+            const int r = r0 + u;
+            sv[u] = (r <= n - 2) ? (double)hat[(long long)(r + 1) * PI + m] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < ZB; ++u) {
+            const int r = r0 + u;
+            if (r <= n - 2) {
+                double s = sv[u] * ilam;
+                double iv = (r < rc) ? t.inv[(long long)r * PI + m] : iinf;
+                d = (s - a * d) * iv;
+                hat[(long long)(r + 1) * PI + m] = (T)d;
+            }
+        }
     }
     {
         const long long q = (long long)n * PI + m;
@@ -359,11 +406,22 @@ __device__ void zsolve_dir_mode(Geo g, long long m, long long PI, T* __restrict_
         hat[q] = (T)d;
     }
     double u = d;
-    for (int r = n - 2; r >= 0; --r) {
-        const long long q = (long long)(r + 1) * PI + m;
-        double cr = (r < rc) ? t.c[(long long)r * PI + m] : cinf;
-        u = (double)hat[q] - cr * u;
-        hat[q] = (T)u;
+    for (int r0 = n - 2; r0 >= 0; r0 -= ZB) {
+        double dv[ZB];
+#pragma unroll
+        for (int q = 0; q < ZB; ++q) {
+            const int r = r0 - q;
+            dv[q] = (r >= 0) ? (double)hat[(long long)(r + 1) * PI + m] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < ZB; ++q) {
+            const int r = r0 - q;
+            if (r >= 0) {
+                double cr = (r < rc) ? t.c[(long long)r * PI + m] : cinf;
+                u = dv[q] - cr * u;
+                hat[(long long)(r + 1) * PI + m] = (T)u;
+            }
+        }
     }
 }
 

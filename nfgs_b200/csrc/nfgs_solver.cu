@@ -8,6 +8,8 @@
 #include "nfgs_gemm.cuh"
 #include "nfgs_iter.cuh"
 #include "nfgs_setup.cuh"
+#include "nfgs_tc.cuh"
+#include <cuda_fp16.h>
 
 #include <cmath>
 #include <mutex>
@@ -116,6 +118,11 @@ struct Handle {
     void* bscratch = nullptr;  // 3V storage-type scratch (final-vs-best)
     double* dscratch = nullptr; // V FP64 scratch for host transfers
     int nzo_crop = 0;
+    // tensor-core transform plan (FP32 storage, even N with (N-2)/2 <= 128)
+    bool tc_on = false;
+    void* tc_img[4] = {nullptr, nullptr, nullptr, nullptr};  // dct_x, dct_y, dst_x, dst_y
+    int tc_px = 0, tc_py = 0, tc_nsm = 0;
+    int* tc_err = nullptr;
     std::vector<void*> setup_scratch;  // freed at the end of a boundary set-up
 };
 
@@ -283,6 +290,178 @@ static int upload_t(Handle* h, void** dp, const std::vector<double>& v) {
     return NFGS_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Tensor-core transform plan
+// ---------------------------------------------------------------------------
+// Operand image of one transform: four fp16 matrices [half A hi | half A lo |
+// half B hi | half B lo], each 128 modes x 128 pairs in the no-swizzle
+// K-major UMMA layout (j/8)*2048 + (k/8)*128 + (j%8)*16 + (k%8)*2 bytes.
+static std::vector<uint16_t> tc_image(int kind, int n, int P) {
+    std::vector<uint16_t> img(4 * 128 * 128, 0);
+    const int period = kind == 0 ? n - 1 : n + 1;  // DCT: N-1, DST: n+1
+    for (int h = 0; h < 2; ++h)
+        for (int j = 0; j < 128; ++j)
+            for (int k = 0; k < 128; ++k) {
+                double val = 0.0;
+                if (j < P && k < P) {
+                    const long long m = k + 1;
+                    long long kk;
+                    if (kind == 0) kk = (h == 0) ? 2 * j + 2 : 2 * j + 1;
+                    else kk = (h == 0) ? 2 * j + 1 : 2 * j + 2;
+                    const long long a = (kk * m) % (2LL * period);
+                    val = kind == 0 ? 2.0 * std::cos(M_PI * (double)a / period)
+                                    : 2.0 * std::sin(M_PI * (double)a / period);
+                }
+                __half hi = __float2half_rn((float)val);
+                __half lo = __float2half_rn((float)(val - (double)__half2float(hi)));
+                const size_t off = ((size_t)(j / 8) * 2048 + (size_t)(k / 8) * 128 + (j % 8) * 16 + (k % 8) * 2) / 2;
+                img[(size_t)(2 * h) * 16384 + off] = *(uint16_t*)&hi;
+                img[(size_t)(2 * h + 1) * 16384 + off] = *(uint16_t*)&lo;
+            }
+    return img;
+}
+
+static int tc_setup(Handle* h) {
+    const int nx = h->g.nx, ny = h->g.ny;
+    if (!h->f32 || (nx % 2) || (ny % 2)) return NFGS_OK;
+    const int px = (nx - 2) / 2, py = (ny - 2) / 2;
+    if (px < 1 || py < 1 || px > tc::PP || py > tc::PP) return NFGS_OK;
+    if (getenv("NFGS_DISABLE_TC") != nullptr) return NFGS_OK;
+    int dev = 0, nsm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaFuncSetAttribute(tc::k_tc_transform, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_TOTAL));
+    const int kinds[4] = {0, 0, 1, 1};
+    const int lens[4] = {nx, ny, nx - 2, ny - 2};
+    const int ps[4] = {px, py, px, py};
+    for (int q = 0; q < 4; ++q) {
+        auto img = tc_image(kinds[q], lens[q], ps[q]);
+        TRY(alloc(h, &h->tc_img[q], img.size() * 2));
+        CK(cudaMemcpy(h->tc_img[q], img.data(), img.size() * 2, cudaMemcpyHostToDevice));
+    }
+    TRY(alloc(h, &h->tc_err, sizeof(int)));
+    CK(cudaMemset(h->tc_err, 0, sizeof(int)));
+    h->tc_px = px;
+    h->tc_py = py;
+    h->tc_nsm = nsm;
+    h->tc_on = true;
+    return NFGS_OK;
+}
+
+static int tc_launch(Handle* h, int which, int inverse, const float* in, tc::Addr ia, float* out,
+                     void* const* otab, const int* osel, tc::Addr oa, int nvec, const int* skip) {
+    if (nvec <= 0) return NFGS_OK;
+    tc::Args a{};
+    a.in = in;
+    a.out = out;
+    a.out_table = otab;
+    a.out_sel = osel;
+    a.ia = ia;
+    a.oa = oa;
+    a.nvec = nvec;
+    const int kinds[4] = {0, 0, 1, 1};
+    const int lens[4] = {h->g.nx, h->g.ny, h->g.nx - 2, h->g.ny - 2};
+    a.kind = kinds[which];
+    a.axis = which & 1;
+    a.N = lens[which];
+    a.P = (which & 1) ? h->tc_py : h->tc_px;
+    a.norm = inverse ? (float)(1.0 / (2.0 * (a.kind == 0 ? a.N - 1 : a.N + 1))) : 1.0f;
+    a.mat = (const uint4*)h->tc_img[which];
+    a.skip = skip;
+    a.err = h->tc_err;
+    const int ntiles = (nvec + tc::TV - 1) / tc::TV;
+    const int grid = std::min(ntiles, h->tc_nsm);
+    tc::k_tc_transform<<<grid, tc::NTHREADS, tc::SMEM_TOTAL, h->s>>>(a);
+    CK(cudaGetLastError());
+    h->launches++;
+    return NFGS_OK;
+}
+
+static tc::Addr rows(long long off, long long nvec, long long pitch) { return tc::Addr{off, nvec, 0, pitch, 1}; }
+static tc::Addr cols(long long off, long long ncols, long long plane, long long pitch) {
+    return tc::Addr{off, ncols, plane, 1, pitch};
+}
+
+// Forward 2-D transforms of S_B (DCT-I, all planes) and S_J (DST-I,
+// interior, planes 1..nz-2), in place through tmpA / tmpB.
+template <typename T>
+static int forward_transforms(Handle* h, const DevCtl* ctl) {
+    const Geo& g = h->g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const long long P = g.P, PI = h->PI;
+    const int nxi = nx - 2, nyi = ny - 2;
+    const int* skip = ctl ? &ctl->stopped : nullptr;
+    if (h->tc_on) {
+        float *sb = (float*)h->sb, *ta = (float*)h->tmpA, *sj = (float*)h->sj, *tb = (float*)h->tmpB;
+        const long long nr = (long long)nz * ny, nc = (long long)nz * nx;
+        TRY(tc_launch(h, 0, 0, sb, rows(0, nr, nx), ta, nullptr, nullptr, rows(0, nr, nx), (int)nr, skip));
+        TRY(tc_launch(h, 1, 0, ta, cols(0, nx, P, nx), sb, nullptr, nullptr, cols(0, nx, P, nx), (int)nc, skip));
+        if (nz > 2) {
+            const long long nri = (long long)(nz - 2) * nyi, nci = (long long)(nz - 2) * nxi;
+            TRY(tc_launch(h, 2, 0, sj, rows(PI, nri, nxi), tb, nullptr, nullptr, rows(PI, nri, nxi), (int)nri, skip));
+            TRY(tc_launch(h, 3, 0, tb, cols(PI, nxi, PI, nxi), sj, nullptr, nullptr, cols(PI, nxi, PI, nxi), (int)nci,
+                          skip));
+        }
+        return NFGS_OK;
+    }
+    TRY(apply_x<T>(h, h->dctx_t, h->sb, nx, P, h->tmpA, nx, P, ny * nz, nx, nx, 1, nullptr, nullptr, ctl));
+    TRY(apply_y<T>(h, h->dcty_t, h->tmpA, nx, P, h->sb, nx, P, ny, ny, nx, nz, ctl));
+    if (nz > 2) {
+        const char* sjp = (const char*)h->sj + (size_t)PI * h->esz;
+        char* tbp = (char*)h->tmpB + (size_t)PI * h->esz;
+        TRY(apply_x<T>(h, h->dstx_t, sjp, nxi, PI, tbp, nxi, PI, nyi * (nz - 2), nxi, nxi, 1, nullptr, nullptr, ctl));
+        TRY(apply_y<T>(h, h->dsty_t, tbp, nxi, PI, (void*)sjp, nxi, PI, nyi, nyi, nxi, nz - 2, ctl));
+    }
+    return NFGS_OK;
+}
+
+// Inverse 2-D transforms: Robin-chain planes 1..nz-1 into phi[*cand_sel]
+// planes 1..nz-1; Dirichlet-chain planes 1..nz-2 into the interior of
+// az[*cand_sel].
+template <typename T>
+static int inverse_transforms(Handle* h, const DevCtl* ctl, const int* cand_sel) {
+    const Geo& g = h->g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const long long P = g.P, PI = h->PI;
+    const int nxi = nx - 2, nyi = ny - 2;
+    const int* skip = ctl ? &ctl->stopped : nullptr;
+    void* const* ptab = (void* const*)h->st_dev->phi;
+    void* const* atab = (void* const*)h->st_dev->az;
+    if (h->tc_on) {
+        float *sb = (float*)h->sb, *ta = (float*)h->tmpA, *sj = (float*)h->sj, *tb = (float*)h->tmpB;
+        const long long nc = (long long)(nz - 1) * nx, nr = (long long)(nz - 1) * ny;
+        TRY(tc_launch(h, 1, 1, sb, cols(P, nx, P, nx), ta, nullptr, nullptr, cols(P, nx, P, nx), (int)nc, skip));
+        TRY(tc_launch(h, 0, 1, ta, rows(P, nr, nx), nullptr, ptab, cand_sel, rows(P, nr, nx), (int)nr, skip));
+        if (nz > 2) {
+            const long long nci = (long long)(nz - 2) * nxi, nri = (long long)(nz - 2) * nyi;
+            TRY(tc_launch(h, 3, 1, sj, cols(PI, nxi, PI, nxi), tb, nullptr, nullptr, cols(PI, nxi, PI, nxi), (int)nci,
+                          skip));
+            TRY(tc_launch(h, 2, 1, tb, rows(PI, nri, nxi), nullptr, atab, cand_sel,
+                          tc::Addr{P + nx + 1, nyi, P, nx, 1}, (int)nri, skip));
+        }
+        return NFGS_OK;
+    }
+    {
+        const char* shp = (const char*)h->sb + (size_t)P * h->esz;
+        char* tap = (char*)h->tmpA + (size_t)P * h->esz;
+        TRY(apply_y<T>(h, h->idcty_t, shp, nx, P, tap, nx, P, ny, ny, nx, nz - 1, ctl));
+        TRY(apply_x<T>(h, h->idctx_t, tap, nx, P, (void*)(intptr_t)(P * h->esz), nx, P, ny * (nz - 1), nx, nx, 1,
+                       ptab, cand_sel, ctl));
+    }
+    if (nz > 2) {
+        const char* sjp = (const char*)h->sj + (size_t)PI * h->esz;
+        char* tbp = (char*)h->tmpB + (size_t)PI * h->esz;
+        TRY(apply_y<T>(h, h->idsty_t, sjp, nxi, PI, tbp, nxi, PI, nyi, nyi, nxi, nz - 2, ctl));
+        TRY(apply_x<T>(h, h->idstx_t, tbp, nxi, PI, (void*)(intptr_t)((P + nx + 1) * h->esz), nx, P, nyi, nxi, nxi,
+                       nz - 2, atab, cand_sel, ctl));
+    }
+    return NFGS_OK;
+}
+
+template <typename T>
+static int zsolve_launch(Handle* h, const int* skip);
+
 // ---------------------------------------------------------------------------
 // Stencil pass launchers
 // ---------------------------------------------------------------------------
@@ -311,31 +490,31 @@ static int run_stencil(Handle* h, const int* sel, const int* skip, int with_src,
     return NFGS_OK;
 }
 
-// Forward transforms of S_B (all planes, DCT-I) and S_J (planes 1..nz-2,
-// interior DST-I), z-solves, inverse transforms into the candidate state.
+// Sources -> modal solves -> candidate state (transforms, z-solves, inverse).
 template <typename T>
 static int run_solve(Handle* h, const DevCtl* ctl, const int* cand_sel, int zero_sources) {
     const Geo& g = h->g;
-    const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const long long P = g.P, PI = h->PI;
-    const int nxi = nx - 2, nyi = ny - 2;
-    const int* skip = ctl ? &ctl->stopped : nullptr;
     if (!zero_sources) {
-        {
-            TRY(apply_x<T>(h, h->dctx_t, h->sb, nx, P, h->tmpA, nx, P, ny * nz, nx, nx, 1, nullptr, nullptr, ctl));
-            TRY(apply_y<T>(h, h->dcty_t, h->tmpA, nx, P, h->sb, nx, P, ny, ny, nx, nz, ctl));
-            if (nz > 2) {
-                const char* sjp = (const char*)h->sj + (size_t)PI * h->esz;
-                char* tbp = (char*)h->tmpB + (size_t)PI * h->esz;
-                TRY(apply_x<T>(h, h->dstx_t, sjp, nxi, PI, tbp, nxi, PI, nyi * (nz - 2), nxi, nxi, 1, nullptr, nullptr,
-                               ctl));
-                TRY(apply_y<T>(h, h->dsty_t, tbp, nxi, PI, (void*)sjp, nxi, PI, nyi, nyi, nxi, nz - 2, ctl));
-            }
-        }
+        TRY(forward_transforms<T>(h, ctl));
     } else {
         CK(cudaMemsetAsync(h->sb, 0, g.V * h->esz, h->s));
-        CK(cudaMemsetAsync(h->sj, 0, (size_t)nz * PI * h->esz, h->s));
+        CK(cudaMemsetAsync(h->sj, 0, (size_t)g.nz * h->PI * h->esz, h->s));
     }
+    TRY(zsolve_launch<T>(h, ctl ? &ctl->stopped : nullptr));
+    if (ctl != nullptr) {
+        k_zero_mode<<<1, 32, 0, h->s>>>(g, (DevCtl*)ctl, h->s00);
+        CK(cudaGetLastError());
+        h->launches++;
+    }
+    TRY(inverse_transforms<T>(h, ctl, cand_sel));
+    return NFGS_OK;
+}
+
+template <typename T>
+static int zsolve_launch(Handle* h, const int* skip) {
+    const Geo& g = h->g;
+    const long long P = g.P, PI = h->PI;
+    const int nz = g.nz;
     ZTab tr{h->zr_c, h->zr_i, h->zr_il, h->zr_ci, h->zr_ii, h->zr_rc};
     ZTab td{h->zd_c, h->zd_i, h->zd_il, h->zd_ci, h->zd_ii, h->zd_rc};
     int nbr = (int)((P + 255) / 256);
@@ -345,48 +524,25 @@ static int run_solve(Handle* h, const DevCtl* ctl, const int* cand_sel, int zero
                                              h->az_bot_hat, nbr);
     CK(cudaGetLastError());
     h->launches++;
-    if (ctl != nullptr) {
-        k_zero_mode<<<1, 32, 0, h->s>>>(g, (DevCtl*)ctl, h->s00);
-        CK(cudaGetLastError());
-        h->launches++;
-    }
-    // inverse: planes 1..nz-1 of the Robin chain into phi[cand]
-    {
-        const char* shp = (const char*)h->sb + (size_t)P * h->esz;
-        char* tap = (char*)h->tmpA + (size_t)P * h->esz;
-        void* const* ptab = (void* const*)h->st_dev->phi;
-        {
-            TRY(apply_y<T>(h, h->idcty_t, shp, nx, P, tap, nx, P, ny, ny, nx, nz - 1, ctl));
-            TRY(apply_x<T>(h, h->idctx_t, tap, nx, P, (void*)(intptr_t)(P * h->esz), nx, P, ny * (nz - 1), nx, nx, 1,
-                           ptab, cand_sel, ctl));
-        }
-    }
-    if (nz > 2) {
-        const char* sjp = (const char*)h->sj + (size_t)PI * h->esz;
-        char* tbp = (char*)h->tmpB + (size_t)PI * h->esz;
-        void* const* atab = (void* const*)h->st_dev->az;
-        {
-            TRY(apply_y<T>(h, h->idsty_t, sjp, nxi, PI, tbp, nxi, PI, nyi, nyi, nxi, nz - 2, ctl));
-            // output: interior rows/cols of planes 1..nz-2 (offset P + nx + 1)
-            TRY(apply_x<T>(h, h->idstx_t, tbp, nxi, PI, (void*)(intptr_t)((P + nx + 1) * h->esz), nx, P, nyi, nxi, nxi,
-                           nz - 2, atab, cand_sel, ctl));
-        }
-    }
     return NFGS_OK;
 }
 
 // ---------------------------------------------------------------------------
 // Control kernels
 // ---------------------------------------------------------------------------
-// Deterministic column sums of block partials by one warp per column.
-__global__ void k_sum_partials(const double* pf, int nbf, const double* ps, int nbs, double* out6) {
-    const int col = blockIdx.x;  // 0..4 face columns, 5 source column
-    const double* base = col < 5 ? pf : ps;
-    const int stride = col < 5 ? 5 : 1;
-    const int off = col < 5 ? col : 0;
+// Deterministic column sums of the block partials (column-major: face
+// columns 0..4 of length nbf, the source column of length nbs): stage 1
+// reduces contiguous chunks into 6 x NCHUNK values, stage 2 sums those in a
+// fixed order.
+#define NCHUNK 64
+__global__ void k_sum_stage1(const double* pf, int nbf, const double* ps, int nbs, double* mid) {
+    const int col = blockIdx.y;
+    const double* base = col < 5 ? pf + (long long)col * nbf : ps;
     const int nb = col < 5 ? nbf : nbs;
+    const int per = (nb + NCHUNK - 1) / NCHUNK;
+    const int b0 = blockIdx.x * per, b1 = min(nb, b0 + per);
     double acc = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) acc += base[(long long)b * stride + off];
+    for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x) acc += base[b];
     __shared__ double sh[32];
     acc = warp_sum(acc);
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
@@ -394,8 +550,15 @@ __global__ void k_sum_partials(const double* pf, int nbf, const double* ps, int 
     if (threadIdx.x < 32) {
         double t = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
         t = warp_sum(t);
-        if (threadIdx.x == 0) out6[col] = t;
+        if (threadIdx.x == 0) mid[col * NCHUNK + blockIdx.x] = t;
     }
+}
+
+__global__ void k_sum_stage2(const double* mid, double* out6) {
+    const int col = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double t = mid[col * NCHUNK + lane] + mid[col * NCHUNK + 32 + lane];
+    t = warp_sum(t);
+    if (lane == 0) out6[col] = t;
 }
 
 __device__ __forceinline__ void scal_from_sums(Geo g, const double* s, double& sigma, double& divb, double& energy) {
@@ -486,6 +649,12 @@ __global__ void k_ctl_step(Geo g, DevCtl* c, const double* sums, double* hist) {
 __global__ void k_ctl_rollback_sources(DevCtl* c, const double* sums) {
     if (c->not_rollback) return;
     c->sumsb2 = sums[5];
+}
+
+static void sum_partials(Handle* h) {
+    k_sum_stage1<<<dim3(NCHUNK, 6), 256, 0, h->s>>>(h->pface, h->nb_face, h->psrc, h->nb_src, h->scal + 8);
+    k_sum_stage2<<<1, 192, 0, h->s>>>(h->scal + 8, h->scal);
+    h->launches += 2;
 }
 
 // ---------------------------------------------------------------------------
@@ -1071,14 +1240,14 @@ static int enqueue_iteration(Handle* h) {
         h->launches++;
     }
     TRY(run_stencil<T>(h, &c->cand, &c->stopped, 1, h->stop.polarity_mask));
-    k_sum_partials<<<6, 256, 0, h->s>>>(h->pface, h->nb_face, h->psrc, h->nb_src, h->scal);
+    sum_partials(h);
     CK(cudaGetLastError());
     k_ctl_step<<<1, 1, 0, h->s>>>(h->g, c, h->scal, h->hist);
     CK(cudaGetLastError());
     h->launches += 2;
     if (h->stop.adaptive_mu) {
         TRY(run_stencil<T>(h, &c->cur, &c->not_rollback, 1, h->stop.polarity_mask));
-        k_sum_partials<<<6, 256, 0, h->s>>>(h->pface, h->nb_face, h->psrc, h->nb_src, h->scal);
+        sum_partials(h);
         k_ctl_rollback_sources<<<1, 1, 0, h->s>>>(c, h->scal);
         CK(cudaGetLastError());
         h->launches += 2;
@@ -1135,7 +1304,7 @@ static int iterate_begin_t(Handle* h, const NfgsStop* stop) {
         h->launches++;
     }
     TRY(run_stencil<T>(h, &h->consts[0], nullptr, 1, stop->polarity_mask));
-    k_sum_partials<<<6, 256, 0, h->s>>>(h->pface, h->nb_face, h->psrc, h->nb_src, h->scal);
+    sum_partials(h);
     k_ctl_init<<<1, 1, 0, h->s>>>(h->g, h->ctl, h->scal, h->hist);
     CK(cudaGetLastError());
     h->launches += 2;
@@ -1200,8 +1369,9 @@ namespace {
 // J_x,y = vertical faces mapped to centres with zero walls and top
 // (nfgs_solver.py:5780-5794, 5935-5941).
 template <typename T>
-__global__ void k_gather_fields(Geo g, const T* __restrict__ B, const T* __restrict__ jz, const T* __restrict__ jf,
-                                int nzc, int y0, int ny_c, int x0, int nx_c, double* __restrict__ out) {
+__global__ void k_gather_fields(Geo g, const T* __restrict__ B, const T* __restrict__ bbg, const T* __restrict__ jz,
+                                const T* __restrict__ jf, int nzc, int y0, int ny_c, int x0, int nx_c,
+                                double* __restrict__ out) {
     long long n = (long long)nzc * ny_c * nx_c;
     long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
@@ -1211,9 +1381,10 @@ __global__ void k_gather_fields(Geo g, const T* __restrict__ B, const T* __restr
     const long long P = g.P, V = g.V, FV = (long long)(g.nz - 1) * P;
     const long long c = (long long)k * P + (long long)j * g.nx + i;
     const long long pq = (long long)j * g.nx + i;
-    out[q] = (double)B[c];
-    out[n + q] = (double)B[V + c];
-    out[2 * n + q] = (double)B[2 * V + c];
+    // B holds the carrier; the field is B_background + carrier
+    out[q] = (double)(bbg[c] + B[c]);
+    out[n + q] = (double)(bbg[V + c] + B[V + c]);
+    out[2 * n + q] = (double)(bbg[2 * V + c] + B[2 * V + c]);
     bool wall = (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1 || k == g.nz - 1);
     double jx = 0.0, jy = 0.0;
     if (!wall) {
@@ -1233,12 +1404,14 @@ __global__ void k_gather_fields(Geo g, const T* __restrict__ B, const T* __restr
     out[5 * n + q] = (double)jz[c];
 }
 
+// sum (B_a - B_b)^2 and sum B_b^2 with B = bg + carrier
 template <typename T>
-__global__ void k_diff_sums(const T* __restrict__ a, const T* __restrict__ b, long long n, double* out) {
+__global__ void k_diff_sums(const T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ bg, long long n,
+                            double* out) {
     __shared__ double sh[2 * 32];
     double v[2] = {0, 0};
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        double x = (double)a[q], y = (double)b[q];
+        double x = (double)(bg[q] + a[q]), y = (double)(bg[q] + b[q]);
         v[0] += (x - y) * (x - y);
         v[1] += y * y;
     }
@@ -1266,7 +1439,7 @@ static void host_scalars(const Geo& g, const double* s, double out[3]) {
 template <typename T>
 static int state_scalars(Handle* h, int idx, double out[3]) {
     TRY(run_stencil<T>(h, &h->consts[idx], nullptr, 0, 0));
-    k_sum_partials<<<6, 256, 0, h->s>>>(h->pface, h->nb_face, h->psrc, h->nb_src, h->scal);
+    sum_partials(h);
     CK(cudaGetLastError());
     double sums[6];
     CK(cudaMemcpyAsync(sums, h->scal, 6 * 8, cudaMemcpyDeviceToHost, h->s));
@@ -1312,7 +1485,7 @@ static int iterate_end_t(Handle* h, NfgsIterResult* res, double* hist, int hist_
         TRY(run_stencil<T>(h, &h->consts[c.best], nullptr, 0, 0));
         CK(cudaMemcpyAsync(h->bscratch, h->B, V3 * h->esz, cudaMemcpyDeviceToDevice, h->s));
         TRY(run_stencil<T>(h, &h->consts[c.cur], nullptr, 0, 0));
-        k_diff_sums<T><<<1, 1024, 0, h->s>>>((const T*)h->B, (const T*)h->bscratch, V3, h->scal);
+        k_diff_sums<T><<<1, 1024, 0, h->s>>>((const T*)h->B, (const T*)h->bscratch, (const T*)h->bbg, V3, h->scal);
         CK(cudaGetLastError());
         double sums[2];
         CK(cudaMemcpyAsync(sums, h->scal, 16, cudaMemcpyDeviceToHost, h->s));
@@ -1347,8 +1520,8 @@ static int fields_t(Handle* h, int which, int crop, double* out, int32_t* dims) 
     long long n = (long long)nzc * nyc * nxc;
     double* dout;
     TRY(alloc(h, &dout, 6 * n * 8));
-    k_gather_fields<T><<<(unsigned)((n + 255) / 256), 256, 0, h->s>>>(h->g, (const T*)h->B, (const T*)h->jz,
-                                                                      (const T*)h->jpf, nzc, y0, nyc, x0, nxc, dout);
+    k_gather_fields<T><<<(unsigned)((n + 255) / 256), 256, 0, h->s>>>(
+        h->g, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz, (const T*)h->jpf, nzc, y0, nyc, x0, nxc, dout);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, dout, 6 * n * 8, cudaMemcpyDeviceToHost, h->s));
     CK(cudaStreamSynchronize(h->s));
@@ -1460,12 +1633,12 @@ static int source_diag_t(Handle* h, double* out) {
         int p = (int)(q / P);
         long long m = q % P;
         int k = p < 3 ? p : nz - 6 + p;
-        bc[q] = (double)(Bt[2 * V + (long long)k * P + m] - bgt[2 * V + (long long)k * P + m]);
+        bc[q] = (double)Bt[2 * V + (long long)k * P + m];  // carrier = B_z - B_bg,z
     }));
     double *bx0 = w + 6 * P, *by0 = w + 7 * P;
     CK(launch_map(P, s, [=] __device__(long long q) {
-        bx0[q] = (double)Bt[q];
-        by0[q] = (double)Bt[V + q];
+        bx0[q] = (double)(bgt[q] + Bt[q]);
+        by0[q] = (double)(bgt[V + q] + Bt[V + q]);
     }));
     double* hat = w + 8 * P;
     TRY(dct2_d(h, bc, hat, w + 14 * P, 6));
@@ -1551,40 +1724,13 @@ static int time_phases_t(Handle* h, int n_iters, double* ms_out) {
         const int cand = (cur + 1) % 3 == h->solution ? (cur + 2) % 3 : (cur + 1) % 3;
         CK(cudaEventRecord(ev[0], h->s));
         TRY(run_stencil<T>(h, &h->consts[cur], nullptr, 1, 0));
-        k_sum_partials<<<6, 256, 0, h->s>>>(h->pface, h->nb_face, h->psrc, h->nb_src, h->scal);
+        sum_partials(h);
         CK(cudaEventRecord(ev[1], h->s));
-        TRY(apply_x<T>(h, h->dctx_t, h->sb, nx, P, h->tmpA, nx, P, ny * nz, nx, nx, 1));
-        TRY(apply_y<T>(h, h->dcty_t, h->tmpA, nx, P, h->sb, nx, P, ny, ny, nx, nz));
-        {
-            const char* sjp = (const char*)h->sj + (size_t)PI * h->esz;
-            char* tbp = (char*)h->tmpB + (size_t)PI * h->esz;
-            TRY(apply_x<T>(h, h->dstx_t, sjp, nxi, PI, tbp, nxi, PI, nyi * (nz - 2), nxi, nxi, 1));
-            TRY(apply_y<T>(h, h->dsty_t, tbp, nxi, PI, (void*)sjp, nxi, PI, nyi, nyi, nxi, nz - 2));
-        }
+        TRY(forward_transforms<T>(h, nullptr));
         CK(cudaEventRecord(ev[2], h->s));
-        {
-            ZTab tr{h->zr_c, h->zr_i, h->zr_il, h->zr_ci, h->zr_ii, h->zr_rc};
-            ZTab td{h->zd_c, h->zd_i, h->zd_il, h->zd_ci, h->zd_ii, h->zd_rc};
-            int nbr = (int)((P + 255) / 256);
-            int nbd = (int)((PI + 255) / 256);
-            k_zsolve<T><<<nbr + nbd, 256, 0, h->s>>>(g, nullptr, (T*)h->sb, tr, h->lamNs, h->phi_bot_hat, h->der_hat,
-                                                     h->prm.robin_weight, h->s00, (T*)h->sj, td, h->lamD,
-                                                     h->az_bot_hat, nbr);
-            CK(cudaGetLastError());
-        }
+        TRY(zsolve_launch<T>(h, nullptr));
         CK(cudaEventRecord(ev[3], h->s));
-        {
-            const char* shp = (const char*)h->sb + (size_t)P * h->esz;
-            char* tap = (char*)h->tmpA + (size_t)P * h->esz;
-            TRY(apply_y<T>(h, h->idcty_t, shp, nx, P, tap, nx, P, ny, ny, nx, nz - 1));
-            TRY(apply_x<T>(h, h->idctx_t, tap, nx, P, (void*)(intptr_t)(P * h->esz), nx, P, ny * (nz - 1), nx, nx, 1,
-                           (void* const*)h->st_dev->phi, &h->consts[cand]));
-            const char* sjp = (const char*)h->sj + (size_t)PI * h->esz;
-            char* tbp = (char*)h->tmpB + (size_t)PI * h->esz;
-            TRY(apply_y<T>(h, h->idsty_t, sjp, nxi, PI, tbp, nxi, PI, nyi, nyi, nxi, nz - 2));
-            TRY(apply_x<T>(h, h->idstx_t, tbp, nxi, PI, (void*)(intptr_t)((P + nx + 1) * h->esz), nx, P, nyi, nxi,
-                           nxi, nz - 2, (void* const*)h->st_dev->az, &h->consts[cand]));
-        }
+        TRY(inverse_transforms<T>(h, nullptr, &h->consts[cand]));
         CK(cudaEventRecord(ev[4], h->s));
         k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(h->g, h->st, nullptr, 0, 1.0, &h->consts[cand],
                                                                     &h->consts[cur], (const T*)h->phiab_t,
@@ -1601,6 +1747,55 @@ static int time_phases_t(Handle* h, int n_iters, double* ms_out) {
     }
     for (auto& e : ev) cudaEventDestroy(e);
     for (int q = 0; q < 5; ++q) ms_out[q] = acc[q];
+    return NFGS_OK;
+}
+
+template <typename T>
+static int apply_transform_t(Handle* h, int chain, int inverse, const double* in, double* out) {
+    const Geo& g = h->g;
+    const long long P = g.P, PI = h->PI, V = g.V;
+    const long long n = chain == 0 ? V : (long long)g.nz * PI;
+    if (!h->dscratch) TRY(alloc(h, &h->dscratch, V * 8));
+    CK(cudaMemcpyAsync(h->dscratch, in, n * 8, cudaMemcpyHostToDevice, h->s));
+    CK(cudaMemsetAsync(h->sb, 0, V * h->esz, h->s));
+    CK(cudaMemsetAsync(h->sj, 0, (size_t)g.nz * PI * h->esz, h->s));
+    TRY(to_storage(h, h->dscratch, chain == 0 ? h->sb : h->sj, n));
+    const int* sel = &h->consts[2];
+    if (!inverse) {
+        TRY(forward_transforms<T>(h, nullptr));
+        TRY(from_storage(h, chain == 0 ? h->sb : h->sj, h->dscratch, n));
+    } else {
+        CK(cudaMemsetAsync(h->st.phi[2], 0, V * h->esz, h->s));
+        CK(cudaMemsetAsync(h->st.az[2], 0, V * h->esz, h->s));
+        TRY(inverse_transforms<T>(h, nullptr, sel));
+        if (chain == 0) {
+            TRY(from_storage(h, h->st.phi[2], h->dscratch, V));
+        } else {
+            // interior of az[2] back to the compact (nz, ny-2, nx-2) layout
+            TRY(from_storage(h, h->st.az[2], h->dscratch, V));
+            double* tmp;
+            TRY(alloc(h, &tmp, n * 8));
+            const int nx = g.nx, nxi = g.nx - 2, nyi = g.ny - 2;
+            double* src = h->dscratch;
+            CK(launch_map(n, h->s, [=] __device__(long long q) {
+                long long k = q / PI, r = q % PI, j = r / nxi, i = r % nxi;
+                tmp[q] = src[k * P + (j + 1) * nx + (i + 1)];
+            }));
+            CK(cudaMemcpyAsync(out, tmp, n * 8, cudaMemcpyDeviceToHost, h->s));
+            CK(cudaStreamSynchronize(h->s));
+            for (auto it = h->owned.begin(); it != h->owned.end();) {
+                if (it->p == tmp) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+            }
+            return NFGS_OK;
+        }
+    }
+    CK(cudaMemcpyAsync(out, h->dscratch, n * 8, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    int err = 0;
+    if (h->tc_err) {
+        CK(cudaMemcpy(&err, h->tc_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) return fail(NFGS_ETIMEDOUT, "tensor-core transform wait ran out");
+    }
     return NFGS_OK;
 }
 
@@ -1745,7 +1940,7 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
     TRYC(alloc(h, &h->pface, (size_t)h->nb_face * 5 * 8));
     TRYC(alloc(h, &h->psrc, (size_t)h->nb_src * 8));
     TRYC(alloc(h, &h->s00, (size_t)nz * 8));
-    TRYC(alloc(h, &h->scal, 64 * 8));
+    TRYC(alloc(h, &h->scal, (8 + 6 * NCHUNK) * 8));
     TRYC(alloc(h, &h->ctl, sizeof(DevCtl)));
     CKC(cudaMallocHost(&h->ctl_h, sizeof(DevCtl)));
     std::memset(h->ctl_h, 0, sizeof(DevCtl));
@@ -1754,6 +1949,7 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
         int cs[4] = {0, 1, 2, 0};
         CKC(cudaMemcpy(h->consts, cs, sizeof cs, cudaMemcpyHostToDevice));
     }
+    TRYC(tc_setup(h));
 #undef TRYC
 #undef CKC
     *out = h;
@@ -2067,6 +2263,16 @@ int nfgs_time_phases(void* handle, int32_t n_iters, double* ms_out) {
     if (h) cudaSetDevice(h->geom.device);
     if (!h || !ms_out) return fail(NFGS_EINVAL, "null argument");
     return h->f32 ? time_phases_t<float>(h, n_iters, ms_out) : time_phases_t<double>(h, n_iters, ms_out);
+}
+
+int nfgs_apply_transform(void* handle, int32_t chain, int32_t inverse, const double* in, double* out) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
+    if (!h || !in || !out) return fail(NFGS_EINVAL, "null argument");
+    if (chain != 0 && chain != 1) return fail(NFGS_EINVAL, "chain must be 0 or 1");
+    return h->f32 ? apply_transform_t<float>(h, chain, inverse, in, out)
+                  : apply_transform_t<double>(h, chain, inverse, in, out);
 }
 
 int nfgs_source_diagnostics(void* handle, double* out) {
