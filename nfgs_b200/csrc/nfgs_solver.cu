@@ -9,6 +9,7 @@
 #include "nfgs_iter.cuh"
 #include "nfgs_setup.cuh"
 #include "nfgs_tc.cuh"
+#include "nfgs_stencil.cuh"
 #include <cuda_fp16.h>
 
 #include <cmath>
@@ -99,6 +100,13 @@ struct Handle {
     double *pface = nullptr, *psrc = nullptr, *s00 = nullptr, *scal = nullptr;
     int nb_face = 0, nb_src = 0;
     dim3 sgrid, sblock;
+    // fused stencil plan (source-producing passes)
+    bool fs_on = false;
+    dim3 fs_grid;
+    int fs_nb = 0;
+    // partial-sum layout of the last stencil pass
+    const double *sum_pf = nullptr, *sum_ps = nullptr;
+    int sum_nbf = 0, sum_nbs = 0;
 
     // iteration control
     DevCtl* ctl = nullptr;
@@ -322,6 +330,40 @@ static std::vector<uint16_t> tc_image(int kind, int n, int P) {
     return img;
 }
 
+// Fused stencil plan: 32 x 8 column tiles and z segments of about 16
+// planes.  A CTA is latency-bound on its plane-to-plane chain, so more
+// resident and queued CTAs raise throughput until the three halo planes each
+// segment re-marches (3/16 here) cost more than they hide.
+static int fs_setup(Handle* h) {
+    const int nx = h->g.nx, ny = h->g.ny, nz = h->g.nz;
+    if (nz < 3 || nx < 3 || ny < 3 || getenv("NFGS_DISABLE_FUSED_STENCIL") != nullptr) return NFGS_OK;
+    const size_t smem = h->f32 ? fs::smem_bytes<float>() : fs::smem_bytes<double>();
+    int per_sm = 0;
+    if (h->f32) {
+        CK(cudaFuncSetAttribute(fs::k_stencil<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs::k_stencil<float>, fs::NT, smem));
+    } else {
+        CK(cudaFuncSetAttribute(fs::k_stencil<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs::k_stencil<double>, fs::NT, smem));
+    }
+    if (per_sm < 1) return NFGS_OK;
+    const int gx = fs::ntiles(nx, fs::TX), gy = fs::ntiles(ny, fs::TY);
+    const long long tiles = (long long)gx * gy;
+    int best = std::max(1, std::min(16, nz / 16));
+    if (const char* e = getenv("NFGS_STENCIL_NSEG")) {
+        const int v = atoi(e);
+        if (v >= 1 && v <= nz) best = v;
+    }
+    {
+        const int per = (nz + best - 1) / best;
+        best = (nz + per - 1) / per;  // no empty segments
+    }
+    h->fs_grid = dim3((unsigned)gx, (unsigned)gy, (unsigned)best);
+    h->fs_nb = (int)(tiles * best);
+    h->fs_on = true;
+    return NFGS_OK;
+}
+
 static int tc_setup(Handle* h) {
     const int nx = h->g.nx, ny = h->g.ny;
     if (!h->f32 || (nx % 2) || (ny % 2)) return NFGS_OK;
@@ -466,8 +508,49 @@ static int zsolve_launch(Handle* h, const int* skip);
 // Stencil pass launchers
 // ---------------------------------------------------------------------------
 template <typename T>
+static int run_fused(Handle* h, const int* sel, const int* skip, int polarity) {
+    fs::Args a{};
+    a.g = h->g;
+    a.st = h->st;
+    a.sel = sel;
+    a.skip = skip;
+    a.bbg = h->bbg;
+    a.bzobs = h->bzobs_t;
+    a.jzt = h->jzt_t;
+    a.hx = h->hx;
+    a.hy = h->hy;
+    a.use_h = h->use_h;
+    a.box = h->box;
+    const double am = h->prm.alpha_max;
+    a.alpha_max = (am > 0 && std::isfinite(am)) ? am : -1.0;
+    a.floor_b2 = h->prm.weak_field_floor_b2;
+    a.o = SrcOpts{polarity, h->prm.face_parallel_exact_jz, h->wx != nullptr};
+    a.wx = h->wx;
+    a.wy = h->wy;
+    a.wz = h->wz;
+    a.sb = h->sb;
+    a.sj = h->sj;
+    a.partials = h->pface;
+    a.nseg = (int)h->fs_grid.z;
+    a.gx = (int)h->fs_grid.x;
+    a.gy = (int)h->fs_grid.y;
+    fs::k_stencil<T><<<h->fs_grid, fs::NT, fs::smem_bytes<T>(), h->s>>>(a);
+    CK(cudaGetLastError());
+    h->launches++;
+    h->sum_pf = h->pface;
+    h->sum_nbf = h->fs_nb;
+    h->sum_ps = h->pface + 5 * (size_t)h->fs_nb;
+    h->sum_nbs = h->fs_nb;
+    return NFGS_OK;
+}
+
+// Stencil pass.  Source-producing passes run the fused z-march; passes that
+// only reconstruct (fields, diagnostics) run the three-pass kernels, which
+// leave B, J_z and the face currents in HBM for their callers.
+template <typename T>
 static int run_stencil(Handle* h, const int* sel, const int* skip, int with_src, int polarity, int raw_j = 0) {
     const Geo& g = h->g;
+    if (with_src && !raw_j && h->fs_on) return run_fused<T>(h, sel, skip, polarity);
     k_recon<T><<<h->sgrid, h->sblock, 0, h->s>>>(g, h->st, sel, skip, (const T*)h->bbg, (const T*)h->bzobs_t,
                                                  (const T*)h->jzt_t, (T)h->hx, (T)h->hy, h->use_h, (T*)h->B,
                                                  (T*)h->jz);
@@ -479,6 +562,10 @@ static int run_stencil(Handle* h, const int* sel, const int* skip, int with_src,
                                                 raw_j);
     CK(cudaGetLastError());
     h->launches += 2;
+    h->sum_pf = h->pface;
+    h->sum_nbf = h->nb_face;
+    h->sum_ps = h->psrc;
+    h->sum_nbs = h->nb_src;
     if (with_src) {
         SrcOpts o{polarity, h->prm.face_parallel_exact_jz, h->wx != nullptr};
         k_src<T><<<h->sgrid, h->sblock, 0, h->s>>>(g, skip, (const T*)h->jpf, (const T*)h->jb, (const T*)h->jzt_t,
@@ -652,7 +739,7 @@ __global__ void k_ctl_rollback_sources(DevCtl* c, const double* sums) {
 }
 
 static void sum_partials(Handle* h) {
-    k_sum_stage1<<<dim3(NCHUNK, 6), 256, 0, h->s>>>(h->pface, h->nb_face, h->psrc, h->nb_src, h->scal + 8);
+    k_sum_stage1<<<dim3(NCHUNK, 6), 256, 0, h->s>>>(h->sum_pf, h->sum_nbf, h->sum_ps, h->sum_nbs, h->scal + 8);
     k_sum_stage2<<<1, 192, 0, h->s>>>(h->scal + 8, h->scal);
     h->launches += 2;
 }
@@ -1937,7 +2024,8 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
     h->sblock = dim3(32, 4, 1);
     h->sgrid = dim3((nx + 31) / 32, (ny + 3) / 4, nz);
     h->nb_face = h->nb_src = (int)(h->sgrid.x * h->sgrid.y * h->sgrid.z);
-    TRYC(alloc(h, &h->pface, (size_t)h->nb_face * 5 * 8));
+    TRYC(fs_setup(h));
+    TRYC(alloc(h, &h->pface, (size_t)std::max(h->nb_face * 5, h->fs_nb * NFGS_NRED) * 8));
     TRYC(alloc(h, &h->psrc, (size_t)h->nb_src * 8));
     TRYC(alloc(h, &h->s00, (size_t)nz * 8));
     TRYC(alloc(h, &h->scal, (8 + 6 * NCHUNK) * 8));
