@@ -17,10 +17,20 @@
 // likewise; three products hi*hi + hi*lo + lo*hi per K step give ~2^-21
 // relative error per product against the vector's maximum.
 //
-// One persistent CTA per SM: the four matrix operands (two halves, hi and
-// lo; 128 KB) stay resident in shared memory; the 64-vector data tile
-// (64 KB) is rebuilt per tile by all threads; one thread issues the MMAs;
-// completion is signalled through an mbarrier with bounded waits.
+// One persistent CTA per SM, warp-specialised and pipelined:
+//   * the four matrix operands (two halves, hi and lo; 128 KB) stay resident
+//     in shared memory;
+//   * producer warps 0-3 prefetch raw input tiles (16 vectors, FP32) two
+//     tiles ahead with cp.async into a double-buffered staging area
+//     (coalesced: vector rows on axis 0, 16-column rows on axis 1), then
+//     form the FP16 hi/lo pair sums and differences of tile i in K-major
+//     operand layout (double-buffered, 16 KB each);
+//   * warp 8 issues the MMAs of tile i into one of two TMEM accumulators;
+//   * epilogue warps 4-7 drain tile i-1: TMEM -> registers -> the consumed
+//     operand buffer (transposed for axis 1) -> row-contiguous global stores.
+// Hand-offs are mbarriers (operands full, MMA done, accumulator free) with
+// bounded waits; the producer and epilogue roles decide failures with a
+// barrier-reduction so that their named barriers stay uniform.
 #pragma once
 #include <cuda_fp16.h>
 #include "nfgs_common.cuh"
@@ -28,15 +38,18 @@
 namespace tc {
 
 constexpr int PP = 128;          // padded pair count (K) and modes per half (M)
-constexpr int TV = 64;           // vectors per tile (N of the MMA)
-constexpr int NTHREADS = 256;
+constexpr int TV = 16;           // vectors per tile (N of the MMA)
+constexpr int NTHREADS = 288;    // 4 producer warps, 4 epilogue warps, 1 MMA warp
 constexpr int MAT_BYTES = PP * PP * 2;        // one fp16 matrix operand: 32 KB
-constexpr int DAT_BYTES = PP * TV * 2;        // one fp16 data operand: 16 KB
+constexpr int DAT_BYTES = PP * TV * 2;        // one fp16 data operand: 4 KB
 constexpr int SMEM_MAT = 4 * MAT_BYTES;       // 128 KB
-constexpr int SMEM_DAT = 4 * DAT_BYTES;       // 64 KB
-constexpr int SMEM_AUX = 8 * 1024;            // per-vector scalars, partial sums, barrier
-constexpr int SMEM_TOTAL = SMEM_MAT + SMEM_DAT + SMEM_AUX;
-constexpr long long WAIT_LIMIT = 1LL << 26;   // mbarrier polls before giving up
+constexpr int SMEM_DAT = 8 * DAT_BYTES;       // two buffers of four operands: 32 KB
+constexpr int STG_PITCH = 2 * PP + 10;        // axis-0 staging row pitch (floats; 8-byte rows, 16 rows on distinct banks)
+constexpr int STG_FLOATS = TV * STG_PITCH;    // one raw tile: 16 rows (axis 0) or 2PP+2 rows of 16 (axis 1)
+constexpr int SMEM_STG = 2 * STG_FLOATS * 4;  // double-buffered raw tiles: 33.9 KB
+constexpr int SMEM_AUX = 8 * 1024;            // per-vector scalars, partial sums, barriers
+constexpr int SMEM_TOTAL = SMEM_MAT + SMEM_DAT + SMEM_STG + SMEM_AUX;
+constexpr long long WAIT_LIMIT = 1LL << 22;   // mbarrier polls before giving up
 
 // Vector / element addressing: addr(v, m) = (v / vpb) * bstride + (v % vpb) * vstride + m * estride
 struct Addr {
@@ -119,16 +132,61 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+
+template <int B>
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(src), "n"(B) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 __device__ __forceinline__ long long vaddr(const Addr& a, long long v) {
     return a.off + (v / a.vpb) * a.bstride + (v % a.vpb) * a.vstride;
 }
 
 // byte offset of (vec, pair) in a data operand
 //   axis 0 (K-major):  (v/8)*2048 + (k/8)*128 + (v%8)*16 + (k%8)*2
-//   axis 1 (MN-major): (k/8)*1024 + (v/8)*128 + (k%8)*16 + (v%8)*2
+//   axis 1 (MN-major): (k/8)*(TV*16) + (v/8)*128 + (k%8)*16 + (v%8)*2
 __device__ __forceinline__ uint32_t dat_off(int axis, int v, int k) {
     return axis == 0 ? (uint32_t)((v >> 3) * 2048 + (k >> 3) * 128 + (v & 7) * 16 + (k & 7) * 2)
-                     : (uint32_t)((k >> 3) * 1024 + (v >> 3) * 128 + (k & 7) * 16 + (v & 7) * 2);
+                     : (uint32_t)((k >> 3) * (TV * 16) + (v >> 3) * 128 + (k & 7) * 16 + (v & 7) * 2);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+// barrier among the 128 producer threads only
+__device__ __forceinline__ void producer_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+// barrier among the 128 epilogue threads only
+__device__ __forceinline__ void epilogue_sync() { asm volatile("bar.sync 2, 128;" ::: "memory"); }
+// barrier of one 128-thread role (id 1 producers, 2 epilogue) that also ORs a flag
+template <int ID>
+__device__ __forceinline__ bool role_any(bool x) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)x), "n"(ID)
+        : "memory");
+    return r != 0;
 }
 
 __device__ __forceinline__ void split_h(float x, __half& hi, __half& lo) {
@@ -141,151 +199,168 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     if (g.skip != nullptr && *g.skip) return;
     unsigned char* smat = smem;
     unsigned char* sdat = smem + SMEM_MAT;
-    float* aux = (float*)(smem + SMEM_MAT + SMEM_DAT);
-    // aux layout (floats): e0[64] e1[64] sp0[64] sp1[64] part[4][64][2] red[16]
-    float* e0 = aux;
-    float* e1 = aux + 64;
-    float* sp0 = aux + 128;
-    float* sp1 = aux + 192;
-    float* part = aux + 256;          // [4][64][2]
-    float* red = aux + 256 + 512;     // [16]
-    uint64_t* mbar = (uint64_t*)(aux + 256 + 512 + 16);
-    uint32_t* tslot = (uint32_t*)(aux + 256 + 512 + 16 + 4);
-    long long* ibase = (long long*)(aux + 256 + 512 + 16 + 8);   // [64] input base of each tile vector
-    long long* obase = ibase + TV;                               // [64] output base
-    int* vexp = (int*)(obase + TV);                              // [64] per-vector scale exponent
-    float* vmax = (float*)(vexp + TV);                           // [4][64] partial maxima (axis 0)
+    float* stg = (float*)(smem + SMEM_MAT + SMEM_DAT);   // [2][STG_FLOATS]
+    unsigned char* saux = smem + SMEM_MAT + SMEM_DAT + SMEM_STG;
+    // per-buffer tile scalars (written by producers, read by the epilogue)
+    long long* obase = (long long*)saux;          // [2][TV]
+    int* vexp = (int*)(obase + 2 * TV);           // [2][TV]
+    float* e0 = (float*)(vexp + 2 * TV);          // [2][TV]
+    float* e1 = e0 + 2 * TV;
+    float* sp0 = e1 + 2 * TV;
+    float* sp1 = sp0 + 2 * TV;
+    float* vdown = sp1 + 2 * TV;                  // [2][TV] output scale norm * 2^-vexp
+    // producer scratch
+    float* part = vdown + 2 * TV;                 // [8][TV][2]
+    float* vmax = part + 16 * TV;                 // [8][TV]
+    long long* ibase = (long long*)(vmax + 8 * TV);  // [2][TV] input base of each vector (staging buffer)
+    uint64_t* bars = (uint64_t*)(ibase + 2 * TV);  // full[2] mmad[2] afree[2]
+    uint32_t* tslot = (uint32_t*)(bars + 6);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ntiles = (g.nvec + TV - 1) / TV;
-    // resident matrices
+    const int nlocal = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     {
         uint4* d = (uint4*)smat;
         for (int q = tid; q < SMEM_MAT / 16; q += NTHREADS) d[q] = g.mat[q];
     }
+    const uint32_t full0 = smem_u32(bars), mmad0 = smem_u32(bars + 2), afree0 = smem_u32(bars + 4);
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(full0 + 8 * b, 128);
+            mbar_init(mmad0 + 8 * b, 1);
+            mbar_init(afree0 + 8 * b, 128);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(smem_u32(tslot)));
+    if (warp == 8) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(tslot)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tbase = *tslot;
-    const uint32_t mb = smem_u32(mbar);
-    const uint32_t mat0 = smem_u32(smat), dat0 = smem_u32(sdat);
-    const uint32_t idesc = (1u << 4) | ((uint32_t)g.axis << 16) | ((uint32_t)(TV >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
     const int P = g.P, N = g.N;
     const bool dct = g.kind == 0;
     bool failed = false;
-    uint32_t phase = 0;
 
     float* outp = g.out;
     if (g.out_table != nullptr) outp = (float*)((char*)g.out_table[*g.out_sel]);
 
-    for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-        const long long v0 = (long long)tile * TV;
-        if (tid < TV) {
-            const long long v = v0 + tid;
-            ibase[tid] = v < g.nvec ? vaddr(g.ia, v) : 0;
-            obase[tid] = v < g.nvec ? vaddr(g.oa, v) : -1;
-        }
-        __syncthreads();
-        // ---------------- build the data operands
-        float sv[32], dv[32];
-        int myv;            // the tile vector this thread works on
-        float psum_s = 0.f, psum_d = 0.f;
-        float lmax = 0.f;
-        if (g.axis == 0) {
-            // units (row r, k-group kg): r fixed per thread, kg = tid/64 + 4 i
-            myv = (tid & 7) + 8 * ((tid >> 3) & 7);
-            const long long v = v0 + myv;
-            const bool ok = v < g.nvec;
-            const long long base = ibase[myv];
+    if (warp < 4) {
+        // ================= producers
+        const int t = tid;
+        const uint32_t stg0 = smem_u32(stg);
+        // raw tile of local index i into staging buffer i&1; one commit group
+        // per call (possibly empty) keeps the group accounting uniform
+        // input bases of the vectors of local tile i (into ibase[i & 1]);
+        // written by threads 0..TV-1 ahead of a producer barrier
+        auto bases = [&](int i) {
+            if (t < TV) {
+                const long long v = (long long)(blockIdx.x + (long long)i * gridDim.x) * TV + t;
+                ibase[(i & 1) * TV + t] = (i < nlocal && v < g.nvec) ? vaddr(g.ia, v) : -1;
+            }
+        };
+        // 8-byte copies when every axis-0 row starts on an 8-byte boundary
+        const bool pairs8 = g.axis == 0 && g.ia.estride == 1 && ((uintptr_t)g.in & 7) == 0 &&
+                            (g.ia.off & 1) == 0 && (g.ia.bstride & 1) == 0 && (g.ia.vstride & 1) == 0;
+        auto prefetch = [&](int i) {
+            if (i < nlocal) {
+                const uint32_t dst = stg0 + (uint32_t)((i & 1) * STG_FLOATS * 4);
+                const long long* ib = ibase + (i & 1) * TV;
+                if (g.axis == 0) {
+                    // warp w: rows 4w..4w+3, lanes along the row
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int kg = (tid >> 6) + 4 * i;
-#pragma unroll
-                for (int t = 0; t < 8; ++t) {
-                    const int k = 8 * kg + t;  // pair index, m = k + 1
-                    float a = 0.f, b = 0.f;
-                    if (ok && k < P) {
-                        const int ia = dct ? k + 1 : k;             // element index of x_m
-                        const int ib = dct ? N - 2 - k : N - 1 - k; // element index of the partner
-                        a = g.in[base + (long long)ia * g.ia.estride];
-                        b = g.in[base + (long long)ib * g.ia.estride];
+                    for (int rr = 0; rr < 4; ++rr) {
+                        const int r = 4 * warp + rr;
+                        const long long base = ib[r];
+                        if (base < 0) continue;
+                        const float* src = g.in + base;
+                        const uint32_t drow = dst + (uint32_t)(r * STG_PITCH * 4);
+                        if (pairs8) {
+                            for (int m2 = lane; 2 * m2 < N; m2 += 32) cp_async4<8>(drow + 8u * m2, src + 2 * m2);
+                        } else {
+                            for (int m = lane; m < N; m += 32)
+                                cp_async4<4>(drow + 4u * m, src + (long long)m * g.ia.estride);
+                        }
                     }
-                    const float s = a + b, d = a - b;
-                    sv[8 * i + t] = s;
-                    dv[8 * i + t] = d;
+                } else {
+                    // lanes 0-15: vectors, lanes 16-31: the next element row
+                    const int vl = lane & 15;
+                    const long long base = ib[vl];
+                    if (base >= 0) {
+                        const float* src = g.in + base + (long long)(2 * warp + (lane >> 4)) * g.ia.estride;
+                        const long long step = 8 * g.ia.estride;
+                        uint32_t d = dst + (uint32_t)(((2 * warp + (lane >> 4)) * TV + vl) * 4);
+                        for (int m = 2 * warp + (lane >> 4); m < N; m += 8, src += step, d += 8 * TV * 4)
+                            cp_async4<4>(d, src);
+                    }
+                }
+            }
+            cp_commit();
+        };
+        bases(0);
+        bases(1);
+        producer_sync();
+        prefetch(0);
+        prefetch(1);
+        const int vl = t & 15, kq = t >> 4;
+        for (int i = 0; i < nlocal && !failed; ++i) {
+            const int b = i & 1, u = i >> 1;
+            const long long v0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * TV;
+            const bool ok_free = u < 1 || mbar_wait(afree0 + 8 * b, (u - 1) & 1);
+            if (role_any<1>(!ok_free)) { failed = true; break; }
+            cp_wait1();          // the group of tile i has landed (tile i+1 may be in flight)
+            producer_sync();
+            const float* raw = stg + b * STG_FLOATS;
+            const bool okv = v0 + vl < g.nvec;
+            auto X = [&](int m) -> float {
+                return g.axis == 0 ? raw[vl * STG_PITCH + m] : raw[m * TV + vl];
+            };
+            // pair sums / differences: vector vl, pair groups kg = kq + 8 i2
+            float sv[16], dv[16];
+            float psum_s = 0.f, psum_d = 0.f, lmax = 0.f;
+#pragma unroll
+            for (int i2 = 0; i2 < 2; ++i2) {
+                const int kg = kq + 8 * i2;
+#pragma unroll
+                for (int tt = 0; tt < 8; ++tt) {
+                    const int k = 8 * kg + tt;  // pair index, m = k + 1 (DCT)
+                    float a = 0.f, c = 0.f;
+                    if (okv && k < P) {
+                        a = X(dct ? k + 1 : k);
+                        c = X(dct ? N - 2 - k : N - 1 - k);
+                    }
+                    const float s = a + c, d = a - c;
+                    sv[8 * i2 + tt] = s;
+                    dv[8 * i2 + tt] = d;
                     psum_s += s;
                     psum_d += ((k + 1) & 1) ? -d : d;   // (-1)^m d_m, m = k + 1
                     lmax = fmaxf(lmax, fmaxf(fabsf(s), fabsf(d)));
                 }
             }
-            part[((tid >> 6) * 64 + myv) * 2 + 0] = psum_s;
-            part[((tid >> 6) * 64 + myv) * 2 + 1] = psum_d;
-            if (dct && (tid >> 6) == 0) {
-                float x0 = 0.f, xn = 0.f;
-                if (ok) {
-                    x0 = g.in[base];
-                    xn = g.in[base + (long long)(N - 1) * g.ia.estride];
-                }
-                e0[myv] = x0 + xn;
-                e1[myv] = x0 - xn;
+            part[(kq * TV + vl) * 2 + 0] = psum_s;
+            part[(kq * TV + vl) * 2 + 1] = psum_d;
+            vmax[kq * TV + vl] = lmax;
+            if (dct && kq == 0) {
+                const float x0 = okv ? X(0) : 0.f, xn = okv ? X(N - 1) : 0.f;
+                e0[b * TV + vl] = x0 + xn;
+                e1[b * TV + vl] = x0 - xn;
             }
-        } else {
-            // elements (vec, pair): vec = 8*warp + lane%8, pair = 4 i + lane/8
-            myv = 8 * warp + (lane & 7);
-            const long long v = v0 + myv;
-            const bool ok = v < g.nvec;
-            const long long base = ibase[myv];
-#pragma unroll
-            for (int i = 0; i < 32; ++i) {
-                const int k = 4 * i + (lane >> 3);
-                float a = 0.f, b = 0.f;
-                if (ok && k < P) {
-                    const int ia = dct ? k + 1 : k;
-                    const int ib = dct ? N - 2 - k : N - 1 - k;
-                    a = g.in[base + (long long)ia * g.ia.estride];
-                    b = g.in[base + (long long)ib * g.ia.estride];
-                }
-                const float s = a + b, d = a - b;
-                sv[i] = s;
-                dv[i] = d;
-                psum_s += s;
-                psum_d += ((k + 1) & 1) ? -d : d;
-                lmax = fmaxf(lmax, fmaxf(fabsf(s), fabsf(d)));
+            if (t < TV) {
+                const long long v = v0 + t;
+                obase[b * TV + t] = v < g.nvec ? vaddr(g.oa, v) : -1;
             }
-            // combine the four lanes that share a vector (lane%8 equal)
-            psum_s += __shfl_xor_sync(0xffffffffu, psum_s, 8);
-            psum_s += __shfl_xor_sync(0xffffffffu, psum_s, 16);
-            psum_d += __shfl_xor_sync(0xffffffffu, psum_d, 8);
-            psum_d += __shfl_xor_sync(0xffffffffu, psum_d, 16);
-            if (lane < 8) {
-                part[myv * 2 + 0] = psum_s;
-                part[myv * 2 + 1] = psum_d;
-                if (dct) {
-                    float x0 = 0.f, xn = 0.f;
-                    if (ok) {
-                        x0 = g.in[base];
-                        xn = g.in[base + (long long)(N - 1) * g.ia.estride];
-                    }
-                    e0[myv] = x0 + xn;
-                    e1[myv] = x0 - xn;
+            bases(i + 2);
+            producer_sync();     // raw buffer b consumed, bases of tile i+2 ready
+            prefetch(i + 2);
+            if (t < TV) {
+                float m = 0.f, ss = 0.f, sd = 0.f;
+                for (int q = 0; q < 8; ++q) {
+                    m = fmaxf(m, vmax[q * TV + t]);
+                    ss += part[(q * TV + t) * 2 + 0];
+                    sd += part[(q * TV + t) * 2 + 1];
                 }
-            }
-        }
-        // per-vector maximum -> power-of-two scale of each vector
-        int myex = 0;
-        if (g.axis == 0) {
-            vmax[(tid >> 6) * 64 + myv] = lmax;
-            __syncthreads();
-            if (tid < TV) {
-                float m = fmaxf(fmaxf(vmax[tid], vmax[64 + tid]), fmaxf(vmax[128 + tid], vmax[192 + tid]));
                 int ex = 0;
                 if (m > 0.f) {
                     int e2;
@@ -294,156 +369,154 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                     // decayed modes hold subnormal maxima: keep 2^ex finite
                     ex = ex > 100 ? 100 : (ex < -100 ? -100 : ex);
                 }
-                vexp[tid] = ex;
+                const int vv = b * TV + t;
+                vexp[vv] = ex;
+                vdown[vv] = ldexpf(g.norm, -ex);
+                if (dct) {
+                    sp0[vv] = (e0[vv] + 2.f * ss) * g.norm;
+                    sp1[vv] = (e1[vv] + 2.f * sd) * g.norm;
+                    e0[vv] *= g.norm;
+                    e1[vv] *= g.norm;
+                }
             }
-            __syncthreads();
-            myex = vexp[myv];
-        } else {
-            lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, 8));
-            lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, 16));
-            if (lmax > 0.f) {
-                int e2;
-                frexpf(lmax, &e2);
-                myex = 14 - e2;
-                myex = myex > 100 ? 100 : (myex < -100 ? -100 : myex);
-            }
-            if (lane < 8) vexp[myv] = myex;
-        }
-        const float up = ldexpf(1.f, myex);
-        // convert and store
-        if (g.axis == 0) {
+            producer_sync();
+            const float up = ldexpf(1.f, vexp[b * TV + vl]);
+            unsigned char* db = sdat + b * 4 * DAT_BYTES;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int kg = (tid >> 6) + 4 * i;
+            for (int i2 = 0; i2 < 2; ++i2) {
+                const int kg = kq + 8 * i2;
                 uint32_t hs[4], ls[4], hd[4], ld[4];
 #pragma unroll
-                for (int t = 0; t < 4; ++t) {
-                    __half a0, a1, b0, b1;
-                    split_h(sv[8 * i + 2 * t] * up, a0, b0);
-                    split_h(sv[8 * i + 2 * t + 1] * up, a1, b1);
-                    hs[t] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
-                    ls[t] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
-                    split_h(dv[8 * i + 2 * t] * up, a0, b0);
-                    split_h(dv[8 * i + 2 * t + 1] * up, a1, b1);
-                    hd[t] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
-                    ld[t] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
-                }
-                const uint32_t o = dat_off(0, myv, 8 * kg);
-                *(uint4*)(sdat + 0 * DAT_BYTES + o) = make_uint4(hs[0], hs[1], hs[2], hs[3]);
-                *(uint4*)(sdat + 1 * DAT_BYTES + o) = make_uint4(ls[0], ls[1], ls[2], ls[3]);
-                *(uint4*)(sdat + 2 * DAT_BYTES + o) = make_uint4(hd[0], hd[1], hd[2], hd[3]);
-                *(uint4*)(sdat + 3 * DAT_BYTES + o) = make_uint4(ld[0], ld[1], ld[2], ld[3]);
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < 32; ++i) {
-                const int k = 4 * i + (lane >> 3);
-                __half hs, ls, hd, ld;
-                split_h(sv[i] * up, hs, ls);
-                split_h(dv[i] * up, hd, ld);
-                const uint32_t o = dat_off(1, myv, k);
-                *(__half*)(sdat + 0 * DAT_BYTES + o) = hs;
-                *(__half*)(sdat + 1 * DAT_BYTES + o) = ls;
-                *(__half*)(sdat + 2 * DAT_BYTES + o) = hd;
-                *(__half*)(sdat + 3 * DAT_BYTES + o) = ld;
-            }
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        // ---------------- MMAs: half A (pair sums), half B (pair differences)
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t dsbo = g.axis == 0 ? 2048u : 128u;
-            const uint32_t dlbo = g.axis == 0 ? 128u : 1024u;
-            const uint32_t dstep = g.axis == 0 ? 256u : 2048u;
-#pragma unroll 1
-            for (int h = 0; h < 2; ++h) {
-                const uint32_t acc = tbase + (uint32_t)(h * TV);
-                const uint32_t mh = mat0 + (uint32_t)(2 * h) * MAT_BYTES, ml = mh + MAT_BYTES;
-                const uint32_t dh = dat0 + (uint32_t)(2 * h) * DAT_BYTES, dl = dh + DAT_BYTES;
-#pragma unroll 1
-                for (int ks = 0; ks < PP / 16; ++ks) {
-                    const uint64_t a_hi = sdesc(mh + 256u * ks, 128u, 2048u);
-                    const uint64_t a_lo = sdesc(ml + 256u * ks, 128u, 2048u);
-                    const uint64_t b_hi = sdesc(dh + dstep * ks, dlbo, dsbo);
-                    const uint64_t b_lo = sdesc(dl + dstep * ks, dlbo, dsbo);
-                    mma_f16(acc, a_hi, b_hi, idesc, ks > 0 ? 1u : 0u);
-                    mma_f16(acc, a_hi, b_lo, idesc, 1u);
-                    mma_f16(acc, a_lo, b_hi, idesc, 1u);
-                }
-            }
-            mma_commit(mb);
-        }
-        // specials and endpoint terms (DCT), per vector, while the MMAs run
-        if (dct && tid < TV) {
-            float ss = 0.f, sd = 0.f;
-            if (g.axis == 0) {
-#pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    ss += part[(q * 64 + tid) * 2 + 0];
-                    sd += part[(q * 64 + tid) * 2 + 1];
+                    __half a0, a1, b0, b1;
+                    split_h(sv[8 * i2 + 2 * q] * up, a0, b0);
+                    split_h(sv[8 * i2 + 2 * q + 1] * up, a1, b1);
+                    hs[q] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
+                    ls[q] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
+                    split_h(dv[8 * i2 + 2 * q] * up, a0, b0);
+                    split_h(dv[8 * i2 + 2 * q + 1] * up, a1, b1);
+                    hd[q] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
+                    ld[q] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
+                }
+                const uint32_t o = dat_off(0, vl, 8 * kg);
+                *(uint4*)(db + 0 * DAT_BYTES + o) = make_uint4(hs[0], hs[1], hs[2], hs[3]);
+                *(uint4*)(db + 1 * DAT_BYTES + o) = make_uint4(ls[0], ls[1], ls[2], ls[3]);
+                *(uint4*)(db + 2 * DAT_BYTES + o) = make_uint4(hd[0], hd[1], hd[2], hd[3]);
+                *(uint4*)(db + 3 * DAT_BYTES + o) = make_uint4(ld[0], ld[1], ld[2], ld[3]);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(full0 + 8 * b);
+        }
+        cp_wait0();
+    } else if (warp == 8) {
+        // ================= MMA issuer (both axes: K-major data operands)
+        const uint32_t mat0 = smem_u32(smat), dat0 = smem_u32(sdat);
+        const uint32_t idesc = (1u << 4) | ((uint32_t)(TV >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+        int issued[2] = {0, 0};
+        for (int i = 0; i < nlocal && !failed; ++i) {
+            const int b = i & 1, u = i >> 1;
+            bool ok = mbar_wait(full0 + 8 * b, u & 1);
+            ok = ok && (u < 1 || mbar_wait(afree0 + 8 * b, (u - 1) & 1));
+            if (!__all_sync(0xffffffffu, ok)) { failed = true; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (lane == 0) {
+#pragma unroll 1
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t acc = tbase + (uint32_t)(b * 2 * TV + h * TV);
+                    const uint32_t mh = mat0 + (uint32_t)(2 * h) * MAT_BYTES, ml = mh + MAT_BYTES;
+                    const uint32_t dh = dat0 + (uint32_t)(b * 4 + 2 * h) * DAT_BYTES, dl = dh + DAT_BYTES;
+#pragma unroll 1
+                    for (int ks = 0; ks < PP / 16; ++ks) {
+                        const uint64_t a_hi = sdesc(mh + 256u * ks, 128u, 2048u);
+                        const uint64_t a_lo = sdesc(ml + 256u * ks, 128u, 2048u);
+                        const uint64_t b_hi = sdesc(dh + 256u * ks, 128u, 2048u);
+                        const uint64_t b_lo = sdesc(dl + 256u * ks, 128u, 2048u);
+                        mma_f16(acc, a_hi, b_hi, idesc, ks > 0 ? 1u : 0u);
+                        mma_f16(acc, a_hi, b_lo, idesc, 1u);
+                        mma_f16(acc, a_lo, b_hi, idesc, 1u);
+                    }
+                }
+                mma_commit(mmad0 + 8 * b);
+            }
+            __syncwarp();
+            issued[b]++;
+        }
+        // outstanding MMAs must finish before the accumulator columns are released
+        for (int b = 0; b < 2; ++b)
+            if (issued[b] > 0) mbar_wait(mmad0 + 8 * b, (issued[b] - 1) & 1);
+    } else {
+        // ================= epilogue (warps 4-7: TMEM lanes 32*(warp-4) ...)
+        // Outputs go through the just-consumed operand buffer of the tile so
+        // that global stores are row-contiguous: axis 0 stages S[c][k - koff]
+        // (vector rows), axis 1 stages S[k - koff][c ^ ((k - koff)/2 % 16)]
+        // (output rows across the tile's 16 vector columns).
+        const int q = warp - 4;
+        const int j = 32 * q + lane;  // mode index within a half
+        const uint32_t lanebits = (uint32_t)(32 * q) << 16;
+        const int koff = dct ? 1 : 0, nk = 2 * P;
+        for (int i = 0; i < nlocal && !failed; ++i) {
+            const int b = i & 1, u = i >> 1;
+            const bool ok = mbar_wait(full0 + 8 * b, u & 1) && mbar_wait(mmad0 + 8 * b, u & 1);
+            if (role_any<2>(!ok)) { failed = true; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            float va[TV], vb[TV];
+            tmem_ld16(tbase + lanebits + (uint32_t)(b * 2 * TV), va);
+            tmem_ld16(tbase + lanebits + (uint32_t)(b * 2 * TV + TV), vb);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float* S = (float*)(sdat + b * 4 * DAT_BYTES);
+            if (j < P) {
+                const int ia = (dct ? 2 * j + 2 : 2 * j) - koff, ib = 2 * j + 1 - koff;
+#pragma unroll
+                for (int c = 0; c < TV; ++c) {
+                    const float down = vdown[b * TV + c];
+                    float av = va[c] * down, bv = vb[c] * down;
+                    if (dct) { av += e0[b * TV + c]; bv += e1[b * TV + c]; }
+                    if (g.axis == 0) {
+                        S[c * (2 * PP) + ia] = av;
+                        S[c * (2 * PP) + ib] = bv;
+                    } else {
+                        S[ia * TV + (c ^ ((ia >> 1) & 15))] = av;
+                        S[ib * TV + (c ^ ((ib >> 1) & 15))] = bv;
+                    }
+                }
+            }
+            epilogue_sync();
+            if (g.axis == 0) {
+                for (int c = q; c < TV; c += 4) {
+                    const long long ob = obase[b * TV + c];
+                    if (ob < 0) continue;
+                    const float* sr = S + c * (2 * PP);
+                    float* op = outp + ob + (long long)(lane + koff) * g.oa.estride;
+                    const long long ostep = 32 * g.oa.estride;
+                    for (int k = lane; k < nk; k += 32, op += ostep) *op = sr[k];
                 }
             } else {
-                ss = part[tid * 2 + 0];
-                sd = part[tid * 2 + 1];
-            }
-            sp0[tid] = (e0[tid] + 2.f * ss) * g.norm;
-            sp1[tid] = (e1[tid] + 2.f * sd) * g.norm;
-            e0[tid] *= g.norm;
-            e1[tid] *= g.norm;
-        }
-        __syncthreads();
-        const bool ok = mbar_wait(mb, phase);
-        failed = __syncthreads_or(!ok) != 0;
-        if (failed && tid == 0 && g.err != nullptr) atomicExch(g.err, 1);
-        phase ^= 1u;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // ---------------- epilogue: TMEM -> global
-        if (!failed) {
-            const int q = warp & 3, ch = warp >> 2;
-            const int j = 32 * q + lane;  // mode index within the half
-            float va[32], vb[32];
-            const uint32_t lanebits = (uint32_t)(32 * q) << 16;
-            tmem_ld32(tbase + lanebits + (uint32_t)(32 * ch), va);
-            tmem_ld32(tbase + lanebits + (uint32_t)(TV + 32 * ch), vb);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-
-            if (j < P) {
-                // output element indices of the two halves
-                const int ka = dct ? 2 * j + 2 : 2 * j;
-                const int kb = dct ? 2 * j + 1 : 2 * j + 1;
-#pragma unroll
-                for (int c = 0; c < 32; ++c) {
-                    const int tv = 32 * ch + c;
-                    const long long ob = obase[tv];
-                    if (ob < 0) continue;
-                    const float down = ldexpf(g.norm, -vexp[tv]);
-                    float a = va[c] * down, b = vb[c] * down;
-                    if (dct) { a += e0[tv]; b += e1[tv]; }
-                    outp[ob + (long long)ka * g.oa.estride] = a;
-                    outp[ob + (long long)kb * g.oa.estride] = b;
-                }
-            }
-            if (dct && tid < TV) {
-                const long long ob = obase[tid];
+                const int c = lane & 15;
+                const long long ob = obase[b * TV + c];
                 if (ob >= 0) {
-                    outp[ob] = sp0[tid];
-                    outp[ob + (long long)(N - 1) * g.oa.estride] = sp1[tid];
+                    const int k0 = 2 * q + (lane >> 4);
+                    float* op = outp + ob + (long long)(k0 + koff) * g.oa.estride;
+                    const long long ostep = 8 * g.oa.estride;
+                    for (int k = k0; k < nk; k += 8, op += ostep) *op = S[k * TV + (c ^ ((k >> 1) & 15))];
                 }
             }
+            if (dct && q == 0 && lane < TV) {
+                const long long ob = obase[b * TV + lane];
+                if (ob >= 0) {
+                    outp[ob] = sp0[b * TV + lane];
+                    outp[ob + (long long)(N - 1) * g.oa.estride] = sp1[b * TV + lane];
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(afree0 + 8 * b);
         }
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     }
-    if (failed) {
-        // a completion never arrived: give the outstanding MMAs one more
-        // bounded wait before the accumulator columns are released
-        mbar_wait(mb, phase ^ 1u);
-    }
+    if (failed && g.err != nullptr) atomicExch(g.err, 1);
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tbase));
+    if (warp == 8) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tbase));
+    }
 }
 
 }  // namespace tc
