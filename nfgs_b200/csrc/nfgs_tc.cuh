@@ -17,16 +17,17 @@
 // likewise; three products hi*hi + hi*lo + lo*hi per K step give ~2^-21
 // relative error per product against the vector's maximum.
 //
-// One persistent CTA per SM, warp-specialised and pipelined:
+// One persistent CTA per SM, warp-specialised and pipelined (NB = 3 tiles
+// between operand build and epilogue):
 //   * the four matrix operands (two halves, hi and lo; 128 KB) stay resident
 //     in shared memory;
-//   * producer warps 0-3 prefetch raw input tiles (16 vectors, FP32) two
+//   * the producer warps prefetch raw input tiles (16 vectors, FP32) two
 //     tiles ahead with cp.async into a double-buffered staging area
 //     (coalesced: vector rows on axis 0, 16-column rows on axis 1), then
 //     form the FP16 hi/lo pair sums and differences of tile i in K-major
-//     operand layout (double-buffered, 16 KB each);
-//   * warp 8 issues the MMAs of tile i into one of two TMEM accumulators;
-//   * epilogue warps 4-7 drain tile i-1: TMEM -> registers -> the consumed
+//     operand layout (NB buffers, 16 KB each);
+//   * the last warp issues the MMAs of tile i into one of NB TMEM accumulators;
+//   * the epilogue warps drain earlier tiles: TMEM -> registers -> the consumed
 //     operand buffer (transposed for axis 1) -> row-contiguous global stores.
 // Hand-offs are mbarriers (operands full, MMA done, accumulator free) with
 // bounded waits; the producer and epilogue roles decide failures with a
@@ -39,11 +40,14 @@ namespace tc {
 
 constexpr int PP = 128;          // padded pair count (K) and modes per half (M)
 constexpr int TV = 16;           // vectors per tile (N of the MMA)
-constexpr int NTHREADS = 288;    // 4 producer warps, 4 epilogue warps, 1 MMA warp
+constexpr int NPW = 8, NEW = 8;  // producer and epilogue warps
+constexpr int NPROD = 32 * NPW, NEPI = 32 * NEW;
+constexpr int NTHREADS = NPROD + NEPI + 32;  // + 1 MMA warp
 constexpr int MAT_BYTES = PP * PP * 2;        // one fp16 matrix operand: 32 KB
 constexpr int DAT_BYTES = PP * TV * 2;        // one fp16 data operand: 4 KB
 constexpr int SMEM_MAT = 4 * MAT_BYTES;       // 128 KB
-constexpr int SMEM_DAT = 8 * DAT_BYTES;       // two buffers of four operands: 32 KB
+constexpr int NB = 3;                         // operand buffers / accumulators in flight
+constexpr int SMEM_DAT = NB * 4 * DAT_BYTES;  // NB buffers of four operands: 48 KB
 constexpr int STG_PITCH = 2 * PP + 10;        // axis-0 staging row pitch (floats; 8-byte rows, 16 rows on distinct banks)
 constexpr int STG_FLOATS = TV * STG_PITCH;    // one raw tile: 16 rows (axis 0) or 2PP+2 rows of 16 (axis 1)
 constexpr int SMEM_STG = 2 * STG_FLOATS * 4;  // double-buffered raw tiles: 33.9 KB
@@ -132,6 +136,15 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
 }
 
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = __uint_as_float(r[q]);
+}
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     uint32_t r[16];
     asm volatile(
@@ -170,21 +183,21 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
 __device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
 }
-// barrier among the 128 producer threads only
-__device__ __forceinline__ void producer_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
-// barrier among the 128 epilogue threads only
-__device__ __forceinline__ void epilogue_sync() { asm volatile("bar.sync 2, 128;" ::: "memory"); }
-// barrier of one 128-thread role (id 1 producers, 2 epilogue) that also ORs a flag
+// barrier among the producer threads only
+__device__ __forceinline__ void producer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(NPROD) : "memory"); }
+// barrier among the epilogue threads only
+__device__ __forceinline__ void epilogue_sync() { asm volatile("bar.sync 2, %0;" ::"n"(NEPI) : "memory"); }
+// barrier of one role (id 1 producers, 2 epilogue; NPROD == NEPI threads) that also ORs a flag
 template <int ID>
 __device__ __forceinline__ bool role_any(bool x) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred p, q;\n\t"
         "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, %2, 128, p;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
         "selp.u32 %0, 1, 0, q;\n\t}\n"
         : "=r"(r)
-        : "r"((uint32_t)x), "n"(ID)
+        : "r"((uint32_t)x), "n"(ID), "n"(NPROD)
         : "memory");
     return r != 0;
 }
@@ -202,19 +215,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     float* stg = (float*)(smem + SMEM_MAT + SMEM_DAT);   // [2][STG_FLOATS]
     unsigned char* saux = smem + SMEM_MAT + SMEM_DAT + SMEM_STG;
     // per-buffer tile scalars (written by producers, read by the epilogue)
-    long long* obase = (long long*)saux;          // [2][TV]
-    int* vexp = (int*)(obase + 2 * TV);           // [2][TV]
-    float* e0 = (float*)(vexp + 2 * TV);          // [2][TV]
-    float* e1 = e0 + 2 * TV;
-    float* sp0 = e1 + 2 * TV;
-    float* sp1 = sp0 + 2 * TV;
-    float* vdown = sp1 + 2 * TV;                  // [2][TV] output scale norm * 2^-vexp
+    long long* obase = (long long*)saux;          // [NB][TV]
+    int* vexp = (int*)(obase + NB * TV);          // [NB][TV]
+    float* e0 = (float*)(vexp + NB * TV);         // [NB][TV]
+    float* e1 = e0 + NB * TV;
+    float* sp0 = e1 + NB * TV;
+    float* sp1 = sp0 + NB * TV;
+    float* vdown = sp1 + NB * TV;                 // [NB][TV] output scale norm * 2^-vexp
     // producer scratch
-    float* part = vdown + 2 * TV;                 // [8][TV][2]
-    float* vmax = part + 16 * TV;                 // [8][TV]
-    long long* ibase = (long long*)(vmax + 8 * TV);  // [2][TV] input base of each vector (staging buffer)
-    uint64_t* bars = (uint64_t*)(ibase + 2 * TV);  // full[2] mmad[2] afree[2]
-    uint32_t* tslot = (uint32_t*)(bars + 6);
+    float* part = vdown + NB * TV;                // [16][TV][2]
+    float* vmax = part + 32 * TV;                 // [16][TV]
+    long long* ibase = (long long*)(vmax + 16 * TV);  // [2][TV] input base of each vector (staging buffer)
+    uint64_t* bars = (uint64_t*)(ibase + 2 * TV);  // full[NB] mmad[NB] afree[NB]
+    uint32_t* tslot = (uint32_t*)(bars + 3 * NB);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ntiles = (g.nvec + TV - 1) / TV;
@@ -223,17 +236,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
         uint4* d = (uint4*)smat;
         for (int q = tid; q < SMEM_MAT / 16; q += NTHREADS) d[q] = g.mat[q];
     }
-    const uint32_t full0 = smem_u32(bars), mmad0 = smem_u32(bars + 2), afree0 = smem_u32(bars + 4);
+    const uint32_t full0 = smem_u32(bars), mmad0 = smem_u32(bars + NB), afree0 = smem_u32(bars + 2 * NB);
     if (tid == 0) {
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(full0 + 8 * b, 128);
+        for (int b = 0; b < NB; ++b) {
+            mbar_init(full0 + 8 * b, NPROD);
             mbar_init(mmad0 + 8 * b, 1);
-            mbar_init(afree0 + 8 * b, 128);
+            mbar_init(afree0 + 8 * b, NEPI);
         }
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    if (warp == 8) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(tslot)));
+    if (warp == NPW + NEW) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(smem_u32(tslot)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -247,7 +260,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     float* outp = g.out;
     if (g.out_table != nullptr) outp = (float*)((char*)g.out_table[*g.out_sel]);
 
-    if (warp < 4) {
+    if (warp < NPW) {
         // ================= producers
         const int t = tid;
         const uint32_t stg0 = smem_u32(stg);
@@ -269,10 +282,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                 const uint32_t dst = stg0 + (uint32_t)((i & 1) * STG_FLOATS * 4);
                 const long long* ib = ibase + (i & 1) * TV;
                 if (g.axis == 0) {
-                    // warp w: rows 4w..4w+3, lanes along the row
+                    // warp w: rows (TV/NPW) w ..., lanes along the row
 #pragma unroll
-                    for (int rr = 0; rr < 4; ++rr) {
-                        const int r = 4 * warp + rr;
+                    for (int rr = 0; rr < TV / NPW; ++rr) {
+                        const int r = (TV / NPW) * warp + rr;
                         const long long base = ib[r];
                         if (base < 0) continue;
                         const float* src = g.in + base;
@@ -289,10 +302,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                     const int vl = lane & 15;
                     const long long base = ib[vl];
                     if (base >= 0) {
-                        const float* src = g.in + base + (long long)(2 * warp + (lane >> 4)) * g.ia.estride;
-                        const long long step = 8 * g.ia.estride;
-                        uint32_t d = dst + (uint32_t)(((2 * warp + (lane >> 4)) * TV + vl) * 4);
-                        for (int m = 2 * warp + (lane >> 4); m < N; m += 8, src += step, d += 8 * TV * 4)
+                        const int m0 = 2 * warp + (lane >> 4);
+                        const float* src = g.in + base + (long long)m0 * g.ia.estride;
+                        const long long step = 2 * NPW * g.ia.estride;
+                        uint32_t d = dst + (uint32_t)((m0 * TV + vl) * 4);
+                        for (int m = m0; m < N; m += 2 * NPW, src += step, d += 2 * NPW * TV * 4)
                             cp_async4<4>(d, src);
                     }
                 }
@@ -306,38 +320,34 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
         prefetch(1);
         const int vl = t & 15, kq = t >> 4;
         for (int i = 0; i < nlocal && !failed; ++i) {
-            const int b = i & 1, u = i >> 1;
+            const int b = i % NB, u = i / NB;
             const long long v0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * TV;
             const bool ok_free = u < 1 || mbar_wait(afree0 + 8 * b, (u - 1) & 1);
             if (role_any<1>(!ok_free)) { failed = true; break; }
             cp_wait1();          // the group of tile i has landed (tile i+1 may be in flight)
             producer_sync();
-            const float* raw = stg + b * STG_FLOATS;
+            const float* raw = stg + (i & 1) * STG_FLOATS;
             const bool okv = v0 + vl < g.nvec;
             auto X = [&](int m) -> float {
                 return g.axis == 0 ? raw[vl * STG_PITCH + m] : raw[m * TV + vl];
             };
-            // pair sums / differences: vector vl, pair groups kg = kq + 8 i2
-            float sv[16], dv[16];
+            // pair sums / differences: vector vl, pair group kg = kq (8 pairs)
+            float sv[8], dv[8];
             float psum_s = 0.f, psum_d = 0.f, lmax = 0.f;
 #pragma unroll
-            for (int i2 = 0; i2 < 2; ++i2) {
-                const int kg = kq + 8 * i2;
-#pragma unroll
-                for (int tt = 0; tt < 8; ++tt) {
-                    const int k = 8 * kg + tt;  // pair index, m = k + 1 (DCT)
-                    float a = 0.f, c = 0.f;
-                    if (okv && k < P) {
-                        a = X(dct ? k + 1 : k);
-                        c = X(dct ? N - 2 - k : N - 1 - k);
-                    }
-                    const float s = a + c, d = a - c;
-                    sv[8 * i2 + tt] = s;
-                    dv[8 * i2 + tt] = d;
-                    psum_s += s;
-                    psum_d += ((k + 1) & 1) ? -d : d;   // (-1)^m d_m, m = k + 1
-                    lmax = fmaxf(lmax, fmaxf(fabsf(s), fabsf(d)));
+            for (int tt = 0; tt < 8; ++tt) {
+                const int k = 8 * kq + tt;  // pair index, m = k + 1 (DCT)
+                float a = 0.f, c = 0.f;
+                if (okv && k < P) {
+                    a = X(dct ? k + 1 : k);
+                    c = X(dct ? N - 2 - k : N - 1 - k);
                 }
+                const float s = a + c, d = a - c;
+                sv[tt] = s;
+                dv[tt] = d;
+                psum_s += s;
+                psum_d += ((k + 1) & 1) ? -d : d;   // (-1)^m d_m, m = k + 1
+                lmax = fmaxf(lmax, fmaxf(fabsf(s), fabsf(d)));
             }
             part[(kq * TV + vl) * 2 + 0] = psum_s;
             part[(kq * TV + vl) * 2 + 1] = psum_d;
@@ -356,7 +366,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             prefetch(i + 2);
             if (t < TV) {
                 float m = 0.f, ss = 0.f, sd = 0.f;
-                for (int q = 0; q < 8; ++q) {
+                for (int q = 0; q < NPROD / TV; ++q) {
                     m = fmaxf(m, vmax[q * TV + t]);
                     ss += part[(q * TV + t) * 2 + 0];
                     sd += part[(q * TV + t) * 2 + 1];
@@ -382,23 +392,21 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             producer_sync();
             const float up = ldexpf(1.f, vexp[b * TV + vl]);
             unsigned char* db = sdat + b * 4 * DAT_BYTES;
-#pragma unroll
-            for (int i2 = 0; i2 < 2; ++i2) {
-                const int kg = kq + 8 * i2;
+            {
                 uint32_t hs[4], ls[4], hd[4], ld[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     __half a0, a1, b0, b1;
-                    split_h(sv[8 * i2 + 2 * q] * up, a0, b0);
-                    split_h(sv[8 * i2 + 2 * q + 1] * up, a1, b1);
+                    split_h(sv[2 * q] * up, a0, b0);
+                    split_h(sv[2 * q + 1] * up, a1, b1);
                     hs[q] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
                     ls[q] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
-                    split_h(dv[8 * i2 + 2 * q] * up, a0, b0);
-                    split_h(dv[8 * i2 + 2 * q + 1] * up, a1, b1);
+                    split_h(dv[2 * q] * up, a0, b0);
+                    split_h(dv[2 * q + 1] * up, a1, b1);
                     hd[q] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
                     ld[q] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
                 }
-                const uint32_t o = dat_off(0, vl, 8 * kg);
+                const uint32_t o = dat_off(0, vl, 8 * kq);
                 *(uint4*)(db + 0 * DAT_BYTES + o) = make_uint4(hs[0], hs[1], hs[2], hs[3]);
                 *(uint4*)(db + 1 * DAT_BYTES + o) = make_uint4(ls[0], ls[1], ls[2], ls[3]);
                 *(uint4*)(db + 2 * DAT_BYTES + o) = make_uint4(hd[0], hd[1], hd[2], hd[3]);
@@ -408,13 +416,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             mbar_arrive(full0 + 8 * b);
         }
         cp_wait0();
-    } else if (warp == 8) {
+    } else if (warp == NPW + NEW) {
         // ================= MMA issuer (both axes: K-major data operands)
         const uint32_t mat0 = smem_u32(smat), dat0 = smem_u32(sdat);
         const uint32_t idesc = (1u << 4) | ((uint32_t)(TV >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-        int issued[2] = {0, 0};
+        int issued[NB] = {0, 0, 0};
         for (int i = 0; i < nlocal && !failed; ++i) {
-            const int b = i & 1, u = i >> 1;
+            const int b = i % NB, u = i / NB;
             bool ok = mbar_wait(full0 + 8 * b, u & 1);
             ok = ok && (u < 1 || mbar_wait(afree0 + 8 * b, (u - 1) & 1));
             if (!__all_sync(0xffffffffu, ok)) { failed = true; break; }
@@ -442,34 +450,36 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             issued[b]++;
         }
         // outstanding MMAs must finish before the accumulator columns are released
-        for (int b = 0; b < 2; ++b)
+        for (int b = 0; b < NB; ++b)
             if (issued[b] > 0) mbar_wait(mmad0 + 8 * b, (issued[b] - 1) & 1);
     } else {
-        // ================= epilogue (warps 4-7: TMEM lanes 32*(warp-4) ...)
+        // ================= epilogue (warps NPW .. NPW+7): warp e reads TMEM
+        // lanes 32*(e%4) (modes) and columns 8*(e/4) .. +8 (vectors) of each half.
         // Outputs go through the just-consumed operand buffer of the tile so
         // that global stores are row-contiguous: axis 0 stages S[c][k - koff]
         // (vector rows), axis 1 stages S[k - koff][c ^ ((k - koff)/2 % 16)]
         // (output rows across the tile's 16 vector columns).
-        const int q = warp - 4;
+        const int e = warp - NPW, q = e & 3, ch = e >> 2;
         const int j = 32 * q + lane;  // mode index within a half
         const uint32_t lanebits = (uint32_t)(32 * q) << 16;
         const int koff = dct ? 1 : 0, nk = 2 * P;
         for (int i = 0; i < nlocal && !failed; ++i) {
-            const int b = i & 1, u = i >> 1;
+            const int b = i % NB, u = i / NB;
             const bool ok = mbar_wait(full0 + 8 * b, u & 1) && mbar_wait(mmad0 + 8 * b, u & 1);
             if (role_any<2>(!ok)) { failed = true; break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            float va[TV], vb[TV];
-            tmem_ld16(tbase + lanebits + (uint32_t)(b * 2 * TV), va);
-            tmem_ld16(tbase + lanebits + (uint32_t)(b * 2 * TV + TV), vb);
+            float va[8], vb[8];
+            tmem_ld8(tbase + lanebits + (uint32_t)(b * 2 * TV + 8 * ch), va);
+            tmem_ld8(tbase + lanebits + (uint32_t)(b * 2 * TV + TV + 8 * ch), vb);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             float* S = (float*)(sdat + b * 4 * DAT_BYTES);
             if (j < P) {
                 const int ia = (dct ? 2 * j + 2 : 2 * j) - koff, ib = 2 * j + 1 - koff;
 #pragma unroll
-                for (int c = 0; c < TV; ++c) {
+                for (int cc = 0; cc < 8; ++cc) {
+                    const int c = 8 * ch + cc;
                     const float down = vdown[b * TV + c];
-                    float av = va[c] * down, bv = vb[c] * down;
+                    float av = va[cc] * down, bv = vb[cc] * down;
                     if (dct) { av += e0[b * TV + c]; bv += e1[b * TV + c]; }
                     if (g.axis == 0) {
                         S[c * (2 * PP) + ia] = av;
@@ -482,7 +492,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             }
             epilogue_sync();
             if (g.axis == 0) {
-                for (int c = q; c < TV; c += 4) {
+                for (int c = e; c < TV; c += NEW) {
                     const long long ob = obase[b * TV + c];
                     if (ob < 0) continue;
                     const float* sr = S + c * (2 * PP);
@@ -494,13 +504,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                 const int c = lane & 15;
                 const long long ob = obase[b * TV + c];
                 if (ob >= 0) {
-                    const int k0 = 2 * q + (lane >> 4);
+                    const int k0 = 2 * e + (lane >> 4);
                     float* op = outp + ob + (long long)(k0 + koff) * g.oa.estride;
-                    const long long ostep = 8 * g.oa.estride;
-                    for (int k = k0; k < nk; k += 8, op += ostep) *op = S[k * TV + (c ^ ((k >> 1) & 15))];
+                    const long long ostep = 2 * NEW * g.oa.estride;
+                    for (int k = k0; k < nk; k += 2 * NEW, op += ostep) *op = S[k * TV + (c ^ ((k >> 1) & 15))];
                 }
             }
-            if (dct && q == 0 && lane < TV) {
+            if (dct && e == 0 && lane < TV) {
                 const long long ob = obase[b * TV + lane];
                 if (ob >= 0) {
                     outp[ob] = sp0[b * TV + lane];
@@ -513,9 +523,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     }
     if (failed && g.err != nullptr) atomicExch(g.err, 1);
     __syncthreads();
-    if (warp == 8) {
+    if (warp == NPW + NEW) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tbase));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tbase));
     }
 }
 
