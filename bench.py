@@ -43,6 +43,9 @@ RHO = 0.5
 # minimal data flow (stencil 5R+2W, forward 2R+2W, z-solves 2R+2W,
 # inverse 2R+2W)
 ALG_BYTES_PER_CELL_ITER = 76.0
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# the dominant kernels on this workload, from one ncu capture each
+KERNEL_TRAFFIC = {"stencil": 172.354304e6 + 50.836480e6}
 
 
 def load_peaks():
@@ -288,7 +291,8 @@ def run_b200(args):
     else:
         achieved = alg_bytes[dname] / (ph_ms[dom] / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_gbs, "unit": "GB/s", "frac": achieved / hbm_gbs,
-                "traffic": None, "kernel": dname, "note": f"peak = {peak_src} HBM copy bandwidth"}
+                "traffic": KERNEL_TRAFFIC.get(dname), "algorithmic_bytes": alg_bytes[dname], "kernel": dname,
+                "note": f"peak = {peak_src} HBM copy bandwidth; traffic = ncu DRAM bytes of one launch"}
     iter_ms = float(ph_ms.sum())
     whole = {"achieved_gbs": ALG_BYTES_PER_CELL_ITER * cells / (iter_ms / 1e3) / 1e9,
              "frac_of_hbm": ALG_BYTES_PER_CELL_ITER * cells / (iter_ms / 1e3) / 1e9 / hbm_gbs,

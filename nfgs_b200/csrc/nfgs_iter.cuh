@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(128) k_src(Geo g, const int* skip, const T* __
 // tables are built), which are kept in registers instead of being re-read.
 // ---------------------------------------------------------------------------
 // rows per batch of independent loads in the z-solves
-#define ZB 8
+#define ZB 16
 
 struct ZTab {
     const double* c;      // [rows][modes]
@@ -318,20 +318,21 @@ __device__ void zsolve_robin_mode(Geo g, long long m, T* __restrict__ hat, ZTab 
     double s_last = s1;  // source of plane nz-2 (used again by the Robin row)
     // interior rows in batches: the loads of a batch are issued together
     for (int r0 = 1; r0 <= n - 2; r0 += ZB) {
-        double sv[ZB];
+        T sv[ZB];
+        double ivb[ZB];
 #pragma unroll
         for (int u = 0; u < ZB; ++u) {
             const int r = r0 + u;
-            sv[u] = (r <= n - 2) ? (double)hat[(long long)(r + 1) * P + m] : 0.0;
+            sv[u] = (r <= n - 2) ? hat[(long long)(r + 1) * P + m] : T(0);
+            ivb[u] = (r <= n - 2 && r < rc) ? t.inv[(long long)r * P + m] : iinf;
         }
 #pragma unroll
         for (int u = 0; u < ZB; ++u) {
             const int r = r0 + u;
             if (r <= n - 2) {
-                double s = sv[u] * ils;
+                double s = (double)sv[u] * ils;
                 s_last = s;
-                double iv = (r < rc) ? t.inv[(long long)r * P + m] : iinf;
-                d = (s - low * d) * iv;
+                d = (s - low * d) * ivb[u];
                 hat[(long long)(r + 1) * P + m] = (T)d;
             }
         }
@@ -342,18 +343,19 @@ __device__ void zsolve_robin_mode(Geo g, long long m, T* __restrict__ hat, ZTab 
     double u = (rr - rl * d) * t.inv_last[m];
     hat[(long long)nz * P - P + m] = (T)u;
     for (int r0 = n - 2; r0 >= 0; r0 -= ZB) {
-        double dv[ZB];
+        T dv[ZB];
+        double crb[ZB];
 #pragma unroll
         for (int q = 0; q < ZB; ++q) {
             const int r = r0 - q;
-            dv[q] = (r >= 0) ? (double)hat[(long long)(r + 1) * P + m] : 0.0;
+            dv[q] = (r >= 0) ? hat[(long long)(r + 1) * P + m] : T(0);
+            crb[q] = (r >= 0 && r < rc) ? t.c[(long long)r * P + m] : cinf;
         }
 #pragma unroll
         for (int q = 0; q < ZB; ++q) {
             const int r = r0 - q;
             if (r >= 0) {
-                double cr = (r < rc) ? t.c[(long long)r * P + m] : cinf;
-                u = dv[q] - cr * u;
+                u = (double)dv[q] - crb[q] * u;
                 hat[(long long)(r + 1) * P + m] = (T)u;
             }
         }
@@ -382,19 +384,20 @@ __device__ void zsolve_dir_mode(Geo g, long long m, long long PI, T* __restrict_
     d = (r1 - a * bot_hat[m]) * t.inv[m];
     hat[PI + m] = (T)d;
     for (int r0 = 1; r0 <= n - 2; r0 += ZB) {
-        double sv[ZB];
+        T sv[ZB];
+        double ivb[ZB];
 #pragma unroll
         for (int u = 0; u < ZB; ++u) {
             const int r = r0 + u;
-            sv[u] = (r <= n - 2) ? (double)hat[(long long)(r + 1) * PI + m] : 0.0;
+            sv[u] = (r <= n - 2) ? hat[(long long)(r + 1) * PI + m] : T(0);
+            ivb[u] = (r <= n - 2 && r < rc) ? t.inv[(long long)r * PI + m] : iinf;
         }
 #pragma unroll
         for (int u = 0; u < ZB; ++u) {
             const int r = r0 + u;
             if (r <= n - 2) {
-                double s = sv[u] * ilam;
-                double iv = (r < rc) ? t.inv[(long long)r * PI + m] : iinf;
-                d = (s - a * d) * iv;
+                double s = (double)sv[u] * ilam;
+                d = (s - a * d) * ivb[u];
                 hat[(long long)(r + 1) * PI + m] = (T)d;
             }
         }
@@ -407,18 +410,19 @@ __device__ void zsolve_dir_mode(Geo g, long long m, long long PI, T* __restrict_
     }
     double u = d;
     for (int r0 = n - 2; r0 >= 0; r0 -= ZB) {
-        double dv[ZB];
+        T dv[ZB];
+        double crb[ZB];
 #pragma unroll
         for (int q = 0; q < ZB; ++q) {
             const int r = r0 - q;
-            dv[q] = (r >= 0) ? (double)hat[(long long)(r + 1) * PI + m] : 0.0;
+            dv[q] = (r >= 0) ? hat[(long long)(r + 1) * PI + m] : T(0);
+            crb[q] = (r >= 0 && r < rc) ? t.c[(long long)r * PI + m] : cinf;
         }
 #pragma unroll
         for (int q = 0; q < ZB; ++q) {
             const int r = r0 - q;
             if (r >= 0) {
-                double cr = (r < rc) ? t.c[(long long)r * PI + m] : cinf;
-                u = dv[q] - cr * u;
+                u = (double)dv[q] - crb[q] * u;
                 hat[(long long)(r + 1) * PI + m] = (T)u;
             }
         }
