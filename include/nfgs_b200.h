@@ -191,6 +191,14 @@ int nfgs_iterate(void* handle, const NfgsStop* stop, NfgsIterResult* result, dou
  * the output shape. */
 int nfgs_fields(void* handle, int32_t which, int32_t crop, double* out, int32_t* dims_out);
 
+/* NFGSSolverGPU.fields_to_numpy (nfgs_solver.py:2881-2903) in the dtype the
+ * reference returns there (the solver dtype, `B[0].cpu().numpy()`):
+ * as nfgs_fields, with out holding 6 blocks of out_dtype (NFGS_F32 or
+ * NFGS_F64) in host memory of any kind.  The gather buffer on the device is
+ * kept by the handle between calls; the copy to the host goes through two
+ * pinned 32 MB chunks. */
+int nfgs_fields_into(void* handle, int32_t which, int32_t crop, void* out, int32_t out_dtype, int32_t* dims_out);
+
 /* Single-step access used by parity tests and by per_step_callback:
  * reconstructs the state of `which` and returns phi_c, A_z (FP64, full
  * calc grid), and its sigma/divB/energy. */

@@ -95,6 +95,7 @@ SIGNATURES = {
     "nfgs_get_history": (C.c_int, [_P, C.c_int32, C.c_int32, _DP, _IP]),
     "nfgs_iterate": (C.c_int, [_P, C.POINTER(NfgsStop), C.POINTER(NfgsIterResult), _DP, C.c_int32]),
     "nfgs_fields": (C.c_int, [_P, C.c_int32, C.c_int32, _DP, _IP]),
+    "nfgs_fields_into": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, _IP]),
     "nfgs_get_scalars_state": (C.c_int, [_P, C.c_int32, _DP, _DP, _DP]),
     "nfgs_step": (C.c_int, [_P, C.c_double, C.c_int32]),
     "nfgs_gaussian_above": (C.c_int, [_P, _DP]),

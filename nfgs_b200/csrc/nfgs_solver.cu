@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 static thread_local std::string g_err;
@@ -132,6 +133,11 @@ struct Handle {
     int tc_px = 0, tc_py = 0, tc_nsm = 0;
     int* tc_err = nullptr;
     std::vector<void*> setup_scratch;  // freed at the end of a boundary set-up
+    // field export: persistent device gather buffer and two pinned chunks
+    void* fbuf = nullptr;
+    size_t fbuf_bytes = 0;
+    void* pin[2] = {nullptr, nullptr};
+    cudaEvent_t pin_ev[2] = {nullptr, nullptr};
 };
 
 template <typename T>
@@ -151,6 +157,10 @@ static void free_all(Handle* h) {
     for (auto& b : h->owned) cudaFree(b.p);
     h->owned.clear();
     if (h->ctl_h) cudaFreeHost(h->ctl_h);
+    for (int q = 0; q < 2; ++q) {
+        if (h->pin[q]) cudaFreeHost(h->pin[q]);
+        if (h->pin_ev[q]) cudaEventDestroy(h->pin_ev[q]);
+    }
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->s) cudaStreamDestroy(h->s);
@@ -1455,10 +1465,10 @@ namespace {
 // Fields of a state (nfgs_solver.py:2881-2903): B from k_recon, J_z state,
 // J_x,y = vertical faces mapped to centres with zero walls and top
 // (nfgs_solver.py:5780-5794, 5935-5941).
-template <typename T>
+template <typename T, typename O>
 __global__ void k_gather_fields(Geo g, const T* __restrict__ B, const T* __restrict__ bbg, const T* __restrict__ jz,
                                 const T* __restrict__ jf, int nzc, int y0, int ny_c, int x0, int nx_c,
-                                double* __restrict__ out) {
+                                O* __restrict__ out) {
     long long n = (long long)nzc * ny_c * nx_c;
     long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
@@ -1469,9 +1479,9 @@ __global__ void k_gather_fields(Geo g, const T* __restrict__ B, const T* __restr
     const long long c = (long long)k * P + (long long)j * g.nx + i;
     const long long pq = (long long)j * g.nx + i;
     // B holds the carrier; the field is B_background + carrier
-    out[q] = (double)(bbg[c] + B[c]);
-    out[n + q] = (double)(bbg[V + c] + B[V + c]);
-    out[2 * n + q] = (double)(bbg[2 * V + c] + B[2 * V + c]);
+    out[q] = (O)(bbg[c] + B[c]);
+    out[n + q] = (O)(bbg[V + c] + B[V + c]);
+    out[2 * n + q] = (O)(bbg[2 * V + c] + B[2 * V + c]);
     bool wall = (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1 || k == g.nz - 1);
     double jx = 0.0, jy = 0.0;
     if (!wall) {
@@ -1479,16 +1489,14 @@ __global__ void k_gather_fields(Geo g, const T* __restrict__ B, const T* __restr
             jx = (double)jf[pq];
             jy = (double)jf[FV + pq];
         } else {
-            jx = 0.5 * ((double)jf[(long long)(k - 1) * P + pq] + (double)jf[(long long)k * P + pq]);
-            jy = 0.5 * ((double)jf[FV + (long long)(k - 1) * P + pq] + (double)jf[FV + (long long)k * P + pq]);
-            // match the storage-type average of the reference (0.5 * (a + b) in T)
+            // the storage-type average of the reference (0.5 * (a + b) in T)
             jx = (double)(T(0.5) * (jf[(long long)(k - 1) * P + pq] + jf[(long long)k * P + pq]));
             jy = (double)(T(0.5) * (jf[FV + (long long)(k - 1) * P + pq] + jf[FV + (long long)k * P + pq]));
         }
     }
-    out[3 * n + q] = jx;
-    out[4 * n + q] = jy;
-    out[5 * n + q] = (double)jz[c];
+    out[3 * n + q] = (O)jx;
+    out[4 * n + q] = (O)jy;
+    out[5 * n + q] = (O)jz[c];
 }
 
 // sum (B_a - B_b)^2 and sum B_b^2 with B = bg + carrier
@@ -1595,8 +1603,48 @@ static int iterate_end_t(Handle* h, NfgsIterResult* res, double* hist, int hist_
     return NFGS_OK;
 }
 
+// Host copy of one chunk on up to 8 threads (a fresh pageable destination
+// costs a page fault per page; the threads take those in parallel).
+static void host_copy(char* dst, const char* src, size_t len) {
+    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const size_t per = ((len + hw - 1) / hw + 4095) & ~(size_t)4095;
+    if (hw == 1 || len <= per) {
+        std::memcpy(dst, src, len);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (size_t off = per; off < len; off += per)
+        th.emplace_back([=] { std::memcpy(dst + off, src + off, std::min(per, len - off)); });
+    std::memcpy(dst, src, std::min(per, len));
+    for (auto& t : th) t.join();
+}
+
+// Copy n bytes from device memory to pageable host memory through two pinned
+// chunks: the DMA of chunk k overlaps the host copy of chunk k-1.
+static int d2h_chunked(Handle* h, void* host, const void* dev, size_t n) {
+    const size_t CH = (size_t)32 << 20;
+    for (int q = 0; q < 2; ++q) {
+        if (!h->pin[q]) CK(cudaHostAlloc(&h->pin[q], CH, cudaHostAllocDefault));
+        if (!h->pin_ev[q]) CK(cudaEventCreateWithFlags(&h->pin_ev[q], cudaEventDisableTiming));
+    }
+    const size_t nch = (n + CH - 1) / CH;
+    for (size_t k = 0; k <= nch; ++k) {
+        if (k < nch) {
+            const size_t off = k * CH, len = std::min(CH, n - off);
+            CK(cudaMemcpyAsync(h->pin[k & 1], (const char*)dev + off, len, cudaMemcpyDeviceToHost, h->s));
+            CK(cudaEventRecord(h->pin_ev[k & 1], h->s));
+        }
+        if (k >= 1) {
+            const size_t kp = k - 1, off = kp * CH, len = std::min(CH, n - off);
+            CK(cudaEventSynchronize(h->pin_ev[kp & 1]));
+            host_copy((char*)host + off, (const char*)h->pin[kp & 1], len);
+        }
+    }
+    return NFGS_OK;
+}
+
 template <typename T>
-static int fields_t(Handle* h, int which, int crop, double* out, int32_t* dims) {
+static int fields_t(Handle* h, int which, int crop, void* out, int odtype, int32_t* dims) {
     int idx;
     TRY(resolve_state(h, which, &idx));
     TRY(run_stencil<T>(h, &h->consts[idx], nullptr, 0, 0, 1));
@@ -1604,17 +1652,29 @@ static int fields_t(Handle* h, int which, int crop, double* out, int32_t* dims) 
     if (crop) {
         nzc = h->nzo_crop; y0 = h->fov_y0; x0 = h->fov_x0; nyc = h->nyo; nxc = h->nxo;
     }
-    long long n = (long long)nzc * nyc * nxc;
-    double* dout;
-    TRY(alloc(h, &dout, 6 * n * 8));
-    k_gather_fields<T><<<(unsigned)((n + 255) / 256), 256, 0, h->s>>>(
-        h->g, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz, (const T*)h->jpf, nzc, y0, nyc, x0, nxc, dout);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(out, dout, 6 * n * 8, cudaMemcpyDeviceToHost, h->s));
-    CK(cudaStreamSynchronize(h->s));
-    for (auto it = h->owned.begin(); it != h->owned.end();) {
-        if (it->p == dout) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+    const long long n = (long long)nzc * nyc * nxc;
+    const size_t osz = odtype == NFGS_F32 ? 4 : 8;
+    const size_t bytes = 6 * (size_t)n * osz;
+    if (bytes > h->fbuf_bytes) {
+        if (h->fbuf) {
+            for (auto it = h->owned.begin(); it != h->owned.end();) {
+                if (it->p == h->fbuf) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+            }
+            h->fbuf = nullptr;
+            h->fbuf_bytes = 0;
+        }
+        TRY(alloc(h, &h->fbuf, bytes));
+        h->fbuf_bytes = bytes;
     }
+    const unsigned grid = (unsigned)((n + 255) / 256);
+    if (odtype == NFGS_F32)
+        k_gather_fields<T, float><<<grid, 256, 0, h->s>>>(h->g, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz,
+                                                          (const T*)h->jpf, nzc, y0, nyc, x0, nxc, (float*)h->fbuf);
+    else
+        k_gather_fields<T, double><<<grid, 256, 0, h->s>>>(h->g, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz,
+                                                           (const T*)h->jpf, nzc, y0, nyc, x0, nxc, (double*)h->fbuf);
+    CK(cudaGetLastError());
+    TRY(d2h_chunked(h, out, h->fbuf, bytes));
     if (dims) { dims[0] = nzc; dims[1] = nyc; dims[2] = nxc; }
     return NFGS_OK;
 }
@@ -2285,7 +2345,18 @@ int nfgs_fields(void* handle, int32_t which, int32_t crop, double* out, int32_t*
     Handle* h = (Handle*)handle;
     if (h) cudaSetDevice(h->geom.device);
     if (!h || !out) return fail(NFGS_EINVAL, "null argument");
-    return h->f32 ? fields_t<float>(h, which, crop, out, dims_out) : fields_t<double>(h, which, crop, out, dims_out);
+    return h->f32 ? fields_t<float>(h, which, crop, out, NFGS_F64, dims_out)
+                  : fields_t<double>(h, which, crop, out, NFGS_F64, dims_out);
+}
+
+int nfgs_fields_into(void* handle, int32_t which, int32_t crop, void* out, int32_t out_dtype, int32_t* dims_out) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
+    if (!h || !out) return fail(NFGS_EINVAL, "null argument");
+    if (out_dtype != NFGS_F32 && out_dtype != NFGS_F64) return fail(NFGS_EINVAL, "out_dtype must be NFGS_F32 or NFGS_F64");
+    return h->f32 ? fields_t<float>(h, which, crop, out, out_dtype, dims_out)
+                  : fields_t<double>(h, which, crop, out, out_dtype, dims_out);
 }
 
 int nfgs_get_scalars_state(void* handle, int32_t which, double* phi, double* az, double* scalars3) {

@@ -700,10 +700,12 @@ class NFGSSolverGPU:
             shape = (nzo, sy.stop - sy.start, sx.stop - sx.start)
         else:
             shape = (self.Nz, self.Ny, self.Nx)
-        out = np.empty(6 * int(np.prod(shape)))
+        out = np.empty(6 * int(np.prod(shape)), dtype=self._np_dtype)
         dims = (L.C.c_int32 * 3)()
-        L.check(self._lib.nfgs_fields(self._h, 0, int(bool(crop_to_observed_fov)), L.dptr(out), dims))
-        f = out.reshape((6,) + shape).astype(self._np_dtype)
+        code = L.NFGS_F32 if out.dtype == np.float32 else L.NFGS_F64
+        L.check(self._lib.nfgs_fields_into(self._h, 0, int(bool(crop_to_observed_fov)),
+                                           out.ctypes.data_as(L.C.c_void_p), code, dims))
+        f = out.reshape((6,) + shape)
         return {"Bx": f[0], "By": f[1], "Bz": f[2], "Jx": f[3], "Jy": f[4], "Jz": f[5]}
 
     def compute_source_diagnostics(self) -> dict:

@@ -175,3 +175,36 @@ def test_deterministic_reductions():
     h2 = s2.iterate(max_iter=8, patience=40, verbose=False)
     assert h1["sigma"] == h2["sigma"]
     assert h1["energy"] == h2["energy"]
+
+
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_fields_into_matches_fp64_export(dtype):
+    """nfgs_fields_into (solver dtype, pinned chunked copy) returns exactly
+    the FP64 export of nfgs_fields rounded to the solver dtype, cropped and
+    uncropped, and on a second call into fresh host memory."""
+    import ctypes as C
+
+    from nfgs_b200 import _lib as L
+
+    meta, data = load("small_rho03_buffer")
+    s, _ = build(meta, data, dtype)
+    s.iterate(max_iter=6, patience=40, verbose=False)
+    lib = L.lib()
+    for crop in (1, 0):
+        dims = (C.c_int32 * 3)()
+        n_full = 6 * s.Nz * s.Ny * s.Nx
+        ref = np.zeros(n_full)
+        L.check(lib.nfgs_fields(s._h, 0, crop, L.dptr(ref), dims))
+        n = 6 * dims[0] * dims[1] * dims[2]
+        want = ref[:n].astype(np.dtype(dtype))
+        for _ in range(2):
+            got = np.full(n, np.nan, dtype=np.dtype(dtype))
+            dims2 = (C.c_int32 * 3)()
+            code = L.NFGS_F32 if dtype == "float32" else L.NFGS_F64
+            L.check(lib.nfgs_fields_into(s._h, 0, crop, got.ctypes.data_as(C.c_void_p), code, dims2))
+            assert tuple(dims2) == tuple(dims)
+            np.testing.assert_array_equal(got, want)
+    f = s.fields_to_numpy()
+    assert f["Bx"].dtype == np.dtype(dtype)
+    with pytest.raises(ValueError):
+        L.check(lib.nfgs_fields_into(s._h, 0, 1, np.zeros(4).ctypes.data_as(C.c_void_p), 7, None))
