@@ -266,6 +266,61 @@ const char* nfgs_last_error(void);
 /* Library build identification (sm arch, version). */
 const char* nfgs_version(void);
 
+/* Learned warm start (no reference counterpart; the reference always starts
+ * from the zero-source state, nfgs_solver.py:6613-6645).
+ * nfgs_iterate_start_state: device views (storage type, (nz, ny, nx)) of the
+ * gs_cfcf start state that nfgs_iterate_begin prepared; valid until the first
+ * nfgs_iterate_advance.
+ * nfgs_iterate_restart_from: phi, az are device arrays of the same shape and
+ * type; the supplied state becomes the start when its sigma_J is lower than
+ * the gs_cfcf start's (or always, fallback == 0).  out3 = {sigma of the
+ * supplied state, sigma of the gs_cfcf start, 1 if accepted}.  Must come
+ * before the first nfgs_iterate_advance (NFGS_ESTATE otherwise). */
+int nfgs_iterate_start_state(void* handle, void** phi_out, void** az_out);
+int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int32_t fallback, double* out3);
+
+/* ------------------------------------------------------------------------
+ * Learned warm start: operator kernels of a 3-D neural operator on a
+ * truncated cosine basis.  No reference counterpart (the reference starts
+ * every solve from the zero-source state, nfgs_solver.py:6613-6645).
+ * All pointers are device pointers; activations are FP32, channel-major
+ * (C, Nz, Ny, Nx); stream is a cudaStream_t (NULL = legacy stream).
+ * Reductions are fixed-order (bitwise repeatable).
+ * ------------------------------------------------------------------------ */
+const char* nfgs_nn_last_error(void);
+/* y[o,v] (+)= sum_i W[o*ci + i] x[i,v] + b[o] (b may be NULL) */
+int nfgs_nn_pointwise(const float* x, const float* W, const float* b, float* y, int32_t ci, int32_t co, int64_t nvox,
+                      int32_t accumulate, void* stream);
+/* gx (+)= W^T gy (gx may be NULL); gW += gy x^T; gb += sum_v gy (gb may be NULL).
+ * scratch holds ceil(nvox/1024) * (co*ci + co) floats. */
+int nfgs_nn_pointwise_bwd(const float* x, const float* W, const float* gy, float* gx, float* gW, float* gb, int32_t ci,
+                          int32_t co, int64_t nvox, int32_t accumulate_gx, float* scratch, int64_t scratch_len,
+                          void* stream);
+int nfgs_nn_gelu(const float* x, float* y, int64_t n, void* stream);
+int nfgs_nn_gelu_bwd(const float* x, const float* gy, float* gx, int64_t n, int32_t accumulate, void* stream);
+/* out[c,kz,ky,kx] = sum Mz[kz,z] My[ky,y] Mx[kx,x] in[c,z,y,x]; bases row-major (K, N), kx <= 32.
+ * t1: C*nz*ny*kx floats, t2: C*nz*ky*kx floats. */
+int nfgs_nn_reduce3(const float* in, float* out, int32_t C, int32_t nz, int32_t ny, int32_t nx, const float* Mz,
+                    const float* My, const float* Mx, int32_t kz, int32_t ky, int32_t kx, float* t1, float* t2,
+                    void* stream);
+/* out[c,z,y,x] (+)= sum Mz[kz,z] My[ky,y] Mx[kx,x] in[c,kz,ky,kx].
+ * t1: C*nz*ky*kx floats, t2: C*nz*ny*kx floats. */
+int nfgs_nn_expand3(const float* in, float* out, int32_t C, int32_t nz, int32_t ny, int32_t nx, const float* Mz,
+                    const float* My, const float* Mx, int32_t kz, int32_t ky, int32_t kx, int32_t accumulate,
+                    float* t1, float* t2, void* stream);
+/* yh[o,k] = sum_i W[(k*ci + i)*co + o] xh[i,k] */
+int nfgs_nn_modemix(const float* xh, const float* W, float* yh, int32_t ci, int32_t co, int32_t nm, void* stream);
+/* gxh = W^T gyh per mode; gW += xh gyh^T per mode */
+int nfgs_nn_modemix_bwd(const float* xh, const float* W, const float* gyh, float* gxh, float* gW, int32_t ci,
+                        int32_t co, int32_t nm, void* stream);
+/* loss_out (device double) = sum mask (pred - target)^2 / count; grad = 2 mask (pred - target) / count.
+ * part: device doubles, at least ceil(n/256). mask may be NULL. */
+int nfgs_nn_mse(const float* pred, const float* target, const float* mask, float* grad, int64_t n, double count,
+                double* part, double* loss_out, void* stream);
+/* Adam with decoupled weight decay, step >= 1 */
+int nfgs_nn_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
+                 float wd, int32_t step, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -108,6 +108,24 @@ SIGNATURES = {
     "nfgs_destroy": (C.c_int, [_P]),
     "nfgs_last_error": (C.c_char_p, []),
     "nfgs_version": (C.c_char_p, []),
+    "nfgs_iterate_start_state": (C.c_int, [_P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "nfgs_iterate_restart_from": (C.c_int, [_P, _P, _P, C.c_int32, _DP]),
+    # learned warm start operator kernels (device pointers)
+    "nfgs_nn_last_error": (C.c_char_p, []),
+    "nfgs_nn_pointwise": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, C.c_int64, C.c_int32, _P]),
+    "nfgs_nn_pointwise_bwd": (C.c_int, [_P, _P, _P, _P, _P, _P, C.c_int32, C.c_int32, C.c_int64, C.c_int32, _P,
+                                        C.c_int64, _P]),
+    "nfgs_nn_gelu": (C.c_int, [_P, _P, C.c_int64, _P]),
+    "nfgs_nn_gelu_bwd": (C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, _P]),
+    "nfgs_nn_reduce3": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32,
+                                  C.c_int32, C.c_int32, _P, _P, _P]),
+    "nfgs_nn_expand3": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32,
+                                  C.c_int32, C.c_int32, C.c_int32, _P, _P, _P]),
+    "nfgs_nn_modemix": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, C.c_int32, _P]),
+    "nfgs_nn_modemix_bwd": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, C.c_int32, C.c_int32, _P]),
+    "nfgs_nn_mse": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.c_double, _P, _P, _P]),
+    "nfgs_nn_adam": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                               C.c_int32, _P]),
 }
 
 

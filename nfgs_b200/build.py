@@ -10,7 +10,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libnfgs_b200.so"
-SOURCES = ["nfgs_solver.cu"]
+SOURCES = ["nfgs_solver.cu", "nfgs_nn.cu"]
 
 
 def nvcc() -> str:

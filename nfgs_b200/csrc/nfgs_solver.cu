@@ -136,6 +136,8 @@ struct Handle {
     // field export: persistent device gather buffer and two pinned chunks
     void* fbuf = nullptr;
     size_t fbuf_bytes = 0;
+    double* dsmall = nullptr;  // small device scratch for host decisions
+    int advanced = 0;          // the current iteration has taken a step
     void* pin[2] = {nullptr, nullptr};
     cudaEvent_t pin_ev[2] = {nullptr, nullptr};
 };
@@ -1407,14 +1409,73 @@ static int iterate_begin_t(Handle* h, const NfgsStop* stop) {
     h->launches += 2;
     h->init_zr = 0.0;
     h->iter_active = 1;
+    h->advanced = 0;
     h->solution = -1;
     h->total_ms = 0.0f;
+    return NFGS_OK;
+}
+
+// sigma, divB and energy of a set of partial sums (for host decisions)
+__global__ void k_scal_out(Geo g, const double* sums, double* out3) {
+    double sigma, divb, energy;
+    scal_from_sums(g, sums, sigma, divb, energy);
+    out3[0] = sigma;
+    out3[1] = divb;
+    out3[2] = energy;
+}
+
+// Start state prepared by iterate_begin (buffer 0).
+static int start_state(Handle* h, void** phi, void** az) {
+    if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
+    if (h->advanced) return fail(NFGS_ESTATE, "the iteration has already advanced");
+    *phi = h->st.phi[0];
+    *az = h->st.az[0];
+    return NFGS_OK;
+}
+
+// Replace the gs_cfcf start by a supplied state (device, storage type) when
+// its sigma_J is lower (or unconditionally when fallback == 0).  Buffer 2 is
+// free right after iterate_begin (current = best = 0, candidate = 1).
+template <typename T>
+static int restart_from_t(Handle* h, const void* phi, const void* az, int fallback, double* out) {
+    if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
+    if (h->advanced) return fail(NFGS_ESTATE, "the iteration has already advanced");
+    const size_t vb = (size_t)h->g.V * h->esz;
+    if (!h->dsmall) TRY(alloc(h, &h->dsmall, 8 * sizeof(double)));
+    CK(cudaMemcpyAsync(h->st.phi[2], phi, vb, cudaMemcpyDeviceToDevice, h->s));
+    CK(cudaMemcpyAsync(h->st.az[2], az, vb, cudaMemcpyDeviceToDevice, h->s));
+    TRY(run_stencil<T>(h, &h->consts[2], nullptr, 1, h->stop.polarity_mask));
+    sum_partials(h);
+    k_scal_out<<<1, 1, 0, h->s>>>(h->g, h->scal, h->dsmall);
+    CK(cudaGetLastError());
+    double sc[3];
+    CK(cudaMemcpyAsync(sc, h->dsmall, sizeof sc, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    const double s_gs = h->ctl_h->sigma0;
+    const bool accept = std::isfinite(sc[0]) && (!fallback || sc[0] < s_gs);
+    if (accept) {
+        // the sources and sums of the supplied state are current: make it state 0
+        CK(cudaMemcpyAsync(h->st.phi[0], h->st.phi[2], vb, cudaMemcpyDeviceToDevice, h->s));
+        CK(cudaMemcpyAsync(h->st.az[0], h->st.az[2], vb, cudaMemcpyDeviceToDevice, h->s));
+        k_ctl_init<<<1, 1, 0, h->s>>>(h->g, h->ctl, h->scal, h->hist);
+        CK(cudaGetLastError());
+    } else {
+        // restore the sources of the gs_cfcf start
+        TRY(run_stencil<T>(h, &h->consts[0], nullptr, 1, h->stop.polarity_mask));
+        sum_partials(h);
+    }
+    CK(cudaStreamSynchronize(h->s));
+    out[0] = sc[0];
+    out[1] = s_gs;
+    out[2] = accept ? 1.0 : 0.0;
     return NFGS_OK;
 }
 
 template <typename T>
 static int iterate_advance_t(Handle* h, int max_steps, int32_t* stop_reason, int32_t* n_done) {
     if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
+    h->advanced = 1;
     CK(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->s));
     CK(cudaStreamSynchronize(h->s));
     int done = 0;
@@ -2283,6 +2344,22 @@ int nfgs_iterate_begin(void* handle, const NfgsStop* stop) {
     if (h) cudaSetDevice(h->geom.device);
     if (!h || !stop) return fail(NFGS_EINVAL, "null argument");
     return h->f32 ? iterate_begin_t<float>(h, stop) : iterate_begin_t<double>(h, stop);
+}
+
+int nfgs_iterate_start_state(void* handle, void** phi_out, void** az_out) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
+    if (!h || !phi_out || !az_out) return fail(NFGS_EINVAL, "null argument");
+    return start_state(h, phi_out, az_out);
+}
+
+int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int32_t fallback, double* out3) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
+    if (!h || !phi || !az || !out3) return fail(NFGS_EINVAL, "null argument");
+    return h->f32 ? restart_from_t<float>(h, phi, az, fallback, out3) : restart_from_t<double>(h, phi, az, fallback, out3);
 }
 
 int nfgs_iterate_initial(void* handle, double* scalars3) {

@@ -543,12 +543,14 @@ class NFGSSolverGPU:
                 fixed_point_update_tol=None, fixed_point_pde_tol: float = 1.0e-8,
                 fixed_point_observable_tol=None, fixed_point_patience: int = 10,
                 auto_rbsl_improvement_grace: int = 20, check_every: int = 32, use_graph: bool = True,
-                **_auto_rbsl_kwargs):
+                warm_start=None, **_auto_rbsl_kwargs):
         mode = str(init_mode).lower().replace("-", "_")
         if mode == "yi_soft":
             mode = "soft_cfcf"
-        if mode not in ("gs_cfcf", "cfcf", "curl_free_current", "soft_cfcf"):
+        if mode not in ("gs_cfcf", "cfcf", "curl_free_current", "soft_cfcf", "learned"):
             raise ValueError("NFGS supports init_mode='gs_cfcf', 'cfcf', or 'soft_cfcf'")
+        if mode == "learned" and warm_start is None:
+            raise ValueError("init_mode='learned' needs warm_start (a learned.NeuralOperator or a callable)")
         stop_mode = str(stop_mode).lower().replace("-", "_")
         if stop_mode == "fixed_point" and not self.record_iteration_diagnostics:
             raise ValueError("stop_mode='fixed_point' requires record_iteration_diagnostics=True")
@@ -560,7 +562,7 @@ class NFGSSolverGPU:
             raise ValueError("fixed-point tolerances must be positive")
         if int(fixed_point_patience) < 1:
             raise ValueError("fixed_point_patience must be >= 1")
-        if mode != "gs_cfcf":
+        if mode not in ("gs_cfcf", "learned"):
             raise NotImplementedError(f"init_mode={init_mode!r}: only the gs_cfcf start is built for B200")
         if polarity_mask not in _POLARITY:
             raise ValueError("polarity_mask must be 'positive', 'negative', or 'both'")
@@ -580,6 +582,11 @@ class NFGSSolverGPU:
             use_graph=int(bool(use_graph)))
         lib = self._lib
         L.check(lib.nfgs_iterate_begin(self._h, L.C.byref(stop)))
+        self.learned_start_info = None
+        if mode == "learned":
+            from . import learned as _learned
+
+            self.learned_start_info = _learned.learned_start(self, warm_start, fallback=True)
         rows_seen = 0
         if verbose:
             sc = np.zeros(3)
@@ -677,6 +684,7 @@ class NFGSSolverGPU:
             "initial_sigma": float(res.sigma0), "initial_divB": float(res.divB0),
             "initial_energy": float(res.energy0),
             "device_ms": float(res.device_ms), "kernel_launches": int(res.kernel_launches),
+            "learned_start": self.learned_start_info,
         }
         history["source_diagnostics"] = self.compute_source_diagnostics()
         return history
