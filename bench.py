@@ -222,6 +222,27 @@ def run_reference(args):
     return 0
 
 
+def learned_vs_plain(seeds=(1_000_000, 1_000_001, 1_000_002), eps=1e-3):
+    """Time to sigma* (1 + eps) from the gs_cfcf start and from the learned
+    start on held-out sunspot magnetograms at 256x256x128 (the network was
+    trained at 128x128x64); sigma* is the plain run's best sigma_J."""
+    from nfgs_b200 import learned as LN
+    from nfgs_b200 import warmstart_train as W
+
+    model = LN.NeuralOperator.load(ROOT / "nfgs_b200" / "weights" / "warmstart_sunspots_130x130x65.npz")
+    rows = W.evaluate(model, list(seeds), 256, 128, eps=(eps,), log=lambda m: None)
+    tag = f"eps{eps:g}"
+    tp = sum(r[tag]["plain_s"] for r in rows)
+    tl = sum(r[tag]["learned_s"] for r in rows)
+    return {"workload": "held-out seeded sunspot magnetograms 256x256x128 (calc 258x258x129), FP32, rho=0.5",
+            "target": f"sigma <= sigma_plain_best * (1 + {eps:g}), same stop rule",
+            "plain_s": tp, "learned_s": tl, "speedup": tp / tl if tl > 0 else None,
+            "accepted": sum(int(r[tag]["learned_accepted"]) for r in rows), "solves": len(rows),
+            "rows": [{"seed": r["seed"], "plain_s": r[tag]["plain_s"], "plain_iterations": r[tag]["plain_iterations"],
+                      "learned_s": r[tag]["learned_s"], "learned_iterations": r[tag]["learned_iterations"],
+                      "accepted": r[tag]["learned_accepted"]} for r in rows]}
+
+
 def run_b200(args):
     world, rank, local, pg = dist_setup()
     import torch  # noqa: F401  (device plumbing and synchronisation only)
@@ -305,6 +326,9 @@ def run_b200(args):
                       check_every=args.check_every)
         t_stop = {"seconds": h["device_ms"] / 1e3, "iterations": len(h["sigma"]), "best_iter": h["best_iter"],
                   "best_sigma": h["best_sigma"], "stop_reason": h["stop_reason"]}
+    lvp = None
+    if world == 1 and args.learned:
+        lvp = learned_vs_plain()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_reference_rate(iters=args.cpu_iters)
@@ -325,6 +349,7 @@ def run_b200(args):
             "gpu_launches": launches,
             "clocks": ck,
             "time_to_sigma_stop": t_stop,
+            "learned_vs_plain": lvp,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -366,6 +391,8 @@ def main():
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-stop-run", dest="stop_run", action="store_false")
+    ap.add_argument("--no-learned", dest="learned", action="store_false",
+                    help="skip the learned-vs-plain time-to-sigma measurement")
     ap.add_argument("--ncu-window", action="store_true",
                     help="profile window only: set-up, then --phase-iters iterations between "
                          "cudaProfilerStart/Stop (for ncu --profile-from-start off)")

@@ -269,15 +269,18 @@ const char* nfgs_version(void);
 /* Learned warm start (no reference counterpart; the reference always starts
  * from the zero-source state, nfgs_solver.py:6613-6645).
  * nfgs_iterate_start_state: device views (storage type, (nz, ny, nx)) of the
- * gs_cfcf start state that nfgs_iterate_begin prepared; valid until the first
- * nfgs_iterate_advance.
+ * gs_cfcf start state that nfgs_iterate_begin prepared; the library's stream
+ * is synchronised, so the views are complete for any stream; valid until the
+ * first nfgs_iterate_advance.
  * nfgs_iterate_restart_from: phi, az are device arrays of the same shape and
- * type; the supplied state becomes the start when its sigma_J is lower than
- * the gs_cfcf start's (or always, fallback == 0).  out3 = {sigma of the
- * supplied state, sigma of the gs_cfcf start, 1 if accepted}.  Must come
- * before the first nfgs_iterate_advance (NFGS_ESTATE otherwise). */
+ * type, complete when called (the library reads them on its own stream).
+ * mode 0: only evaluate their sigma_J; 1: make them the start when their
+ * sigma_J is lower than the gs_cfcf start's; 2: make them the start.
+ * out3 = {sigma of the supplied state, sigma of the gs_cfcf start, 1 if it
+ * became the start}.  Must come before the first nfgs_iterate_advance
+ * (NFGS_ESTATE otherwise). */
 int nfgs_iterate_start_state(void* handle, void** phi_out, void** az_out);
-int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int32_t fallback, double* out3);
+int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int32_t mode, double* out3);
 
 /* ------------------------------------------------------------------------
  * Learned warm start: operator kernels of a 3-D neural operator on a

@@ -1428,16 +1428,18 @@ __global__ void k_scal_out(Geo g, const double* sums, double* out3) {
 static int start_state(Handle* h, void** phi, void** az) {
     if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
     if (h->advanced) return fail(NFGS_ESTATE, "the iteration has already advanced");
+    CK(cudaStreamSynchronize(h->s));  // the views are complete for any stream
     *phi = h->st.phi[0];
     *az = h->st.az[0];
     return NFGS_OK;
 }
 
-// Replace the gs_cfcf start by a supplied state (device, storage type) when
-// its sigma_J is lower (or unconditionally when fallback == 0).  Buffer 2 is
-// free right after iterate_begin (current = best = 0, candidate = 1).
+// sigma_J of a supplied state (device, storage type), and optionally make it
+// the start: mode 0 evaluates only, 1 replaces the gs_cfcf start when the
+// supplied sigma_J is lower, 2 replaces it unconditionally.  Buffer 2 is free
+// right after iterate_begin (current = best = 0, candidate = 1).
 template <typename T>
-static int restart_from_t(Handle* h, const void* phi, const void* az, int fallback, double* out) {
+static int restart_from_t(Handle* h, const void* phi, const void* az, int mode, double* out) {
     if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
     if (h->advanced) return fail(NFGS_ESTATE, "the iteration has already advanced");
     const size_t vb = (size_t)h->g.V * h->esz;
@@ -1453,7 +1455,7 @@ static int restart_from_t(Handle* h, const void* phi, const void* az, int fallba
     CK(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->s));
     CK(cudaStreamSynchronize(h->s));
     const double s_gs = h->ctl_h->sigma0;
-    const bool accept = std::isfinite(sc[0]) && (!fallback || sc[0] < s_gs);
+    const bool accept = mode == 2 || (mode == 1 && std::isfinite(sc[0]) && sc[0] < s_gs);
     if (accept) {
         // the sources and sums of the supplied state are current: make it state 0
         CK(cudaMemcpyAsync(h->st.phi[0], h->st.phi[2], vb, cudaMemcpyDeviceToDevice, h->s));
@@ -1461,9 +1463,13 @@ static int restart_from_t(Handle* h, const void* phi, const void* az, int fallba
         k_ctl_init<<<1, 1, 0, h->s>>>(h->g, h->ctl, h->scal, h->hist);
         CK(cudaGetLastError());
     } else {
-        // restore the sources of the gs_cfcf start
+        // restore the sources of the gs_cfcf start, and overwrite the rejected
+        // state: the modal solves never write some boundary entries of a
+        // candidate buffer, so nothing of it may outlive this call
         TRY(run_stencil<T>(h, &h->consts[0], nullptr, 1, h->stop.polarity_mask));
         sum_partials(h);
+        CK(cudaMemcpyAsync(h->st.phi[2], h->st.phi[0], vb, cudaMemcpyDeviceToDevice, h->s));
+        CK(cudaMemcpyAsync(h->st.az[2], h->st.az[0], vb, cudaMemcpyDeviceToDevice, h->s));
     }
     CK(cudaStreamSynchronize(h->s));
     out[0] = sc[0];
@@ -2354,12 +2360,13 @@ int nfgs_iterate_start_state(void* handle, void** phi_out, void** az_out) {
     return start_state(h, phi_out, az_out);
 }
 
-int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int32_t fallback, double* out3) {
+int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int32_t mode, double* out3) {
     g_err.clear();
     Handle* h = (Handle*)handle;
     if (h) cudaSetDevice(h->geom.device);
     if (!h || !phi || !az || !out3) return fail(NFGS_EINVAL, "null argument");
-    return h->f32 ? restart_from_t<float>(h, phi, az, fallback, out3) : restart_from_t<double>(h, phi, az, fallback, out3);
+    if (mode < 0 || mode > 2) return fail(NFGS_EINVAL, "mode must be 0, 1 or 2");
+    return h->f32 ? restart_from_t<float>(h, phi, az, mode, out3) : restart_from_t<double>(h, phi, az, mode, out3);
 }
 
 int nfgs_iterate_initial(void* handle, double* scalars3) {

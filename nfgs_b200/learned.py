@@ -70,6 +70,14 @@ class Config:
     hidden: int = 32
     cout: int = 2
     seed: int = 0
+    # per-channel scales of (phi_c, A_z): inputs are divided by in_scale,
+    # outputs multiplied by out_scale (training-set RMS after the field and
+    # length scaling of each sample)
+    in_scale: tuple = (1.0, 1.0)
+    out_scale: tuple = (1.0, 1.0)
+    # the output is band-limited to these cosine modes per axis (z, y, x),
+    # capped by the grid; (0, 0, 0) leaves it unfiltered
+    out_modes: tuple = (24, 24, 24)
 
     def param_shapes(self) -> list[tuple[str, tuple]]:
         w, nm = self.width, int(np.prod(self.modes))
@@ -130,6 +138,17 @@ class Grid:
         nvox = nz * ny * nx
         npair = w * w + w
         self.pw_scratch = torch.empty(((nvox + 1023) // 1024) * npair, device=dev)
+        # band-limiting output filter
+        self.ko = None
+        if all(k > 0 for k in cfg.out_modes):
+            ko = tuple(min(k, n) for k, n in zip(cfg.out_modes, (nz, ny, nx)))
+            self.ko = ko
+            self.Ao = [torch.from_numpy(cosine_bases(n, k)[0]).to(dev) for n, k in zip((nz, ny, nx), ko)]
+            self.So = [torch.from_numpy(cosine_bases(n, k)[1]).to(dev) for n, k in zip((nz, ny, nx), ko)]
+            co = cfg.cout
+            self.big_o = torch.empty(co * nz * ny * ko[2], device=dev)
+            self.small_o = torch.empty(co * nz * ko[1] * ko[2], device=dev)
+            self.coef_o = torch.empty(co * ko[0] * ko[1] * ko[2], device=dev)
 
 
 class NeuralOperator:
@@ -179,7 +198,9 @@ class NeuralOperator:
     def load(cls, path: str | Path, device="cuda") -> "NeuralOperator":
         d = np.load(path, allow_pickle=False)
         c = json.loads(str(d["config"]))
-        c["modes"] = tuple(c["modes"])
+        for key in ("modes", "in_scale", "out_scale", "out_modes"):
+            if key in c:
+                c[key] = tuple(c[key])
         cfg = Config(**c)
         params = {k: d[k].astype(np.float32) for k in d.files if k != "config"}
         return cls(cfg, params, device)
@@ -213,6 +234,19 @@ class NeuralOperator:
                                      kz, ky, kx, 1, _p(g.small), _p(g.big), self._stream()))
         return a
 
+    def _band_limit(self, g: Grid, y, first, second):
+        """second^T (first y) over the output modes (the filter, or with the
+        bases swapped its transpose)."""
+        torch = _torch()
+        kz, ky, kx = g.ko
+        co = self.cfg.cout
+        out = torch.empty_like(y)
+        _ck(self.lib.nfgs_nn_reduce3(_p(y), _p(g.coef_o), co, g.nz, g.ny, g.nx, _p(first[0]), _p(first[1]),
+                                     _p(first[2]), kz, ky, kx, _p(g.big_o), _p(g.small_o), self._stream()))
+        _ck(self.lib.nfgs_nn_expand3(_p(g.coef_o), _p(out), co, g.nz, g.ny, g.nx, _p(second[0]), _p(second[1]),
+                                     _p(second[2]), kz, ky, kx, 0, _p(g.small_o), _p(g.big_o), self._stream()))
+        return out
+
     def forward(self, x, cache: bool = False):
         """x: (cin, nz, ny, nx) float32 device tensor -> (cout, nz, ny, nx)."""
         torch = _torch()
@@ -244,6 +278,8 @@ class NeuralOperator:
         _ck(self.lib.nfgs_nn_gelu(_p(p1), _p(q1), p1.numel(), self._stream()))
         y = torch.empty((cfg.cout, nz, ny, nx), device=self.device)
         self._pointwise(q1, self.P["proj2_W"], self.P["proj2_b"], y, cfg.hidden, cfg.cout, nvox)
+        if g.ko is not None:
+            y = self._band_limit(g, y, g.Ao, g.So)
         if cache:
             self._cache = dict(x=x, hs=hs, zs=zs, As=As, p1=p1, q1=q1, grid=g)
         return y
@@ -261,6 +297,9 @@ class NeuralOperator:
         nm = kz * ky * kx
         st = self._stream()
         sl = len(g.pw_scratch)
+        gy = gy.contiguous()
+        if g.ko is not None:
+            gy = self._band_limit(g, gy, g.So, g.Ao)
         gq = torch.empty_like(c["q1"])
         _ck(self.lib.nfgs_nn_pointwise_bwd(_p(c["q1"]), _p(self.P["proj2_W"]), _p(gy.contiguous()), _p(gq),
                                            _p(self.G["proj2_W"]), _p(self.G["proj2_b"]), cfg.hidden, cfg.cout,
@@ -365,7 +404,7 @@ def masks(nz, ny, nx, device):
     return m
 
 
-def features(solver, phi, az):
+def features(solver, phi, az, in_scale=(1.0, 1.0)):
     """(6, nz, ny, nx) float32 features: phi_c, A_z of the start state, the
     bottom (Bx, By, Bz) broadcast in height, and the height fraction."""
     torch = _torch()
@@ -373,37 +412,58 @@ def features(solver, phi, az):
     nz, ny, nx = solver.Nz, solver.Ny, solver.Nx
     dev = phi.device
     x = torch.empty((6, nz, ny, nx), device=dev)
-    x[0] = phi.float() / (bs * ls)
-    x[1] = az.float() / (bs * ls)
+    x[0] = phi.float() / (bs * ls * in_scale[0])
+    x[1] = az.float() / (bs * ls * in_scale[1])
     for c, plane in ((2, 1), (3, 2), (4, 0)):
         x[c] = torch.from_numpy((solver._plane(plane) / bs).astype(np.float32)).to(dev).view(1, ny, nx)
     x[5] = torch.linspace(0.0, 1.0, nz, device=dev).view(nz, 1, 1)
     return x
 
 
-def learned_start(solver, model, fallback: bool = True) -> dict:
-    """After nfgs_iterate_begin: predict the correction, hand the corrected
-    state to the solver, which keeps it only if its sigma_J is lower.
+def learned_start(solver, model, fallback: bool = True, scales_tried=(1.0, 0.6, 0.35, 0.2)) -> dict:
+    """After nfgs_iterate_begin: hand a predicted start to the solver.
 
     model: a NeuralOperator, or a callable (solver, phi, az) -> (phi, az)
-    returning a candidate start state as device tensors of the solver dtype."""
+    returning a candidate start state as device tensors of the solver dtype.
+    For the network, the predicted correction is tried at the given scales
+    and the one with the lowest sigma_J is kept when it beats the gs_cfcf
+    start (fallback) -- the plain iteration then runs unchanged."""
     torch = _torch()
     phi, az = start_state_views(solver)
-    if isinstance(model, NeuralOperator):
-        x = features(solver, phi, az)
-        bs, ls = scales(solver)
-        with torch.no_grad():
-            y = model.forward(x)
-            m = masks(solver.Nz, solver.Ny, solver.Nx, x.device)
-            corr = (y * m) * (bs * ls)
-            cand_phi = (phi.double() + corr[0].double()).to(phi.dtype).contiguous()
-            cand_az = (az.double() + corr[1].double()).to(az.dtype).contiguous()
-    else:
+    lib = solver._lib
+    out = np.zeros(3)
+
+    def evaluate(cp, ca, mode):
+        torch.cuda.current_stream().synchronize()  # the library reads them on its own stream
+        L.check(lib.nfgs_iterate_restart_from(solver._h, C.c_void_p(cp.data_ptr()), C.c_void_p(ca.data_ptr()),
+                                              mode, L.dptr(out)))
+        return float(out[0]), float(out[1]), bool(out[2])
+
+    if not isinstance(model, NeuralOperator):
         cand_phi, cand_az = model(solver, phi, az)
         cand_phi = cand_phi.to(device=phi.device, dtype=phi.dtype).contiguous()
         cand_az = cand_az.to(device=az.device, dtype=az.dtype).contiguous()
-    out = np.zeros(3)
-    L.check(solver._lib.nfgs_iterate_restart_from(solver._h, C.c_void_p(cand_phi.data_ptr()),
-                                                   C.c_void_p(cand_az.data_ptr()), int(bool(fallback)),
-                                                   L.dptr(out)))
-    return {"sigma_learned": float(out[0]), "sigma_gs_cfcf": float(out[1]), "accepted": bool(out[2])}
+        s_new, s_gs, acc = evaluate(cand_phi, cand_az, 1 if fallback else 2)
+        return {"sigma_learned": s_new, "sigma_gs_cfcf": s_gs, "accepted": acc}
+
+    x = features(solver, phi, az, model.cfg.in_scale)
+    bs, ls = scales(solver)
+    with torch.no_grad():
+        y = model.forward(x)
+        m = masks(solver.Nz, solver.Ny, solver.Nx, x.device)
+        osc = torch.tensor(model.cfg.out_scale, device=x.device, dtype=torch.float32).view(2, 1, 1, 1)
+        corr = ((y * m) * osc * (bs * ls)).double()
+    tried = []
+    best = None
+    for lam in scales_tried:
+        cp = (phi.double() + lam * corr[0]).to(phi.dtype).contiguous()
+        ca = (az.double() + lam * corr[1]).to(az.dtype).contiguous()
+        s_new, s_gs, _ = evaluate(cp, ca, 0)
+        tried.append((lam, s_new))
+        if np.isfinite(s_new) and (best is None or s_new < best[1]):
+            best = (lam, s_new, cp, ca)
+    accepted = False
+    if best is not None and (not fallback or best[1] < s_gs):
+        _, _, accepted = evaluate(best[2], best[3], 2)
+    return {"sigma_learned": best[1] if best else float("nan"), "sigma_gs_cfcf": s_gs, "accepted": accepted,
+            "scale": best[0] if best else None, "tried": tried}

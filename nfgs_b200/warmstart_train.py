@@ -1,0 +1,254 @@
+"""Training and evaluation of the learned warm start.
+
+    python -m nfgs_b200.warmstart_train --samples 2000 --epochs 6 --out warmstart.npz
+
+1. Data: seeded synthetic magnetograms (2-6 Gaussian spots, sigma 4-16 cells,
+   |Bz| <= 1, random twist, zero net flux) at 128 x 128 x 64 (calculation grid
+   130 x 130 x 65); each is solved by the plain NFGS iteration in FP32 to its
+   sigma_best stop.  A sample is (gs_cfcf start state, bottom maps) -> the
+   correction from the start to the best state, all scaled by the field and
+   length scales of the sample.
+2. Training: masked MSE on the correction, Adam, gradient accumulation over a
+   few samples, cosine learning-rate decay; every operator runs on the
+   project's nfgs_nn_* kernels.
+3. Evaluation: held-out seeds at 256 x 256 x 128.  The plain gs_cfcf run gives
+   sigma* (its best sigma_J); both the plain and the learned start are then run
+   with tol = sigma* (1 + eps) under the same stop rule and timed until they
+   reach it (inference included for the learned start).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+
+import numpy as np
+
+from . import learned as LN
+from .solver import NFGSSolverGPU
+from .synthetic import sunspot_magnetogram
+
+SOLVER_KW = dict(dtype="float32", bottom_divergence_robin_weight=0.5,
+                 horizontal_zero_mode_policy="frozen_linear_harmonic", vertical_current_operator="staggered_face",
+                 d0_zero_mode_policy="project", source_zero_mode_policy="project")
+STOP = dict(tol=1e-5, patience=40, sigma_improvement_tol=1e-5)
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def solve_sample(solver: NFGSSolverGPU, seed: int, n: int, max_iter: int):
+    """Set the boundary of `seed`, run the plain iteration, return the
+    gs_cfcf start state (device copies), the best state (device) and the history."""
+    torch = _torch()
+    bx, by, bz = sunspot_magnetogram(n, seed)
+    solver.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+    keep = {}
+
+    def grab(s, phi, az):
+        keep["phi"], keep["az"] = phi.clone(), az.clone()
+        return phi, az
+
+    h = solver.iterate(max_iter=max_iter, verbose=False, init_mode="learned", warm_start=grab, **STOP)
+    phi_b, az_b, _ = solver._get_state(0)
+    best = (torch.from_numpy(phi_b.astype(np.float32)).cuda(), torch.from_numpy(az_b.astype(np.float32)).cuda())
+    return keep["phi"], keep["az"], best, h
+
+
+def generate(n_samples: int, seed0: int = 0, n: int = 128, nz: int = 64, max_iter: int = 600, log=print):
+    torch = _torch()
+    solver = NFGSSolverGPU(n, n, nz, 1.0, 1.0, 1.0, **SOLVER_KW)
+    Nz, Ny, Nx = solver.Nz, solver.Ny, solver.Nx
+    X = torch.empty((n_samples, 2, Nz, Ny, Nx), device="cuda")
+    PL = torch.empty((n_samples, 3, Ny, Nx), device="cuda")
+    Y = torch.empty((n_samples, 2, Nz, Ny, Nx), device="cuda")
+    iters = []
+    t0 = time.perf_counter()
+    for i in range(n_samples):
+        phi, az, (pb, ab), h = solve_sample(solver, seed0 + i, n, max_iter)
+        bs, ls = LN.scales(solver)
+        k = bs * ls
+        X[i, 0] = phi / k
+        X[i, 1] = az / k
+        for c, plane in ((0, 1), (1, 2), (2, 0)):
+            PL[i, c] = torch.from_numpy((solver._plane(plane) / bs).astype(np.float32)).cuda()
+        Y[i, 0] = (pb - phi) / k
+        Y[i, 1] = (ab - az) / k
+        iters.append(len(h["sigma"]))
+        if (i + 1) % max(1, n_samples // 10) == 0:
+            log(f"  generated {i + 1}/{n_samples} ({time.perf_counter() - t0:.1f} s, mean iterations "
+                f"{np.mean(iters):.1f})")
+    return dict(X=X, PL=PL, Y=Y, shape=(Nz, Ny, Nx), iters=iters)
+
+
+def _features(ds, i, out):
+    torch = _torch()
+    Nz, Ny, Nx = ds["shape"]
+    out[0:2] = ds["X"][i]
+    out[2:5] = ds["PL"][i].view(3, 1, Ny, Nx)
+    out[5] = torch.linspace(0.0, 1.0, Nz, device=out.device).view(Nz, 1, 1)
+    return out
+
+
+def normalise(ds, val_frac: float):
+    """Per-channel RMS scales of the inputs and targets over the training
+    samples; the dataset is scaled in place.  Returns (in_scale, out_scale)."""
+    torch = _torch()
+    n = ds["X"].shape[0]
+    nval = max(1, int(n * val_frac))
+    Nz, Ny, Nx = ds["shape"]
+    mask = LN.masks(Nz, Ny, Nx, torch.device("cuda"))
+    ins, outs = [], []
+    for c in range(2):
+        xs = ds["X"][nval:, c]
+        ys = ds["Y"][nval:, c] * mask[c]
+        ins.append(float(xs.pow(2).mean().sqrt().item()) or 1.0)
+        outs.append(float((ys.pow(2).sum() / (mask[c].sum() * (n - nval))).sqrt().item()) or 1.0)
+        ds["X"][:, c] /= ins[-1]
+        ds["Y"][:, c] /= outs[-1]
+    return tuple(ins), tuple(outs)
+
+
+def train(ds, cfg: LN.Config, epochs: int, lr: float = 1e-3, batch: int = 4, val_frac: float = 0.05, log=print):
+    torch = _torch()
+    cfg.in_scale, cfg.out_scale = normalise(ds, val_frac)
+    log(f"  channel scales: inputs {cfg.in_scale}, targets {cfg.out_scale}")
+    model = LN.NeuralOperator(cfg)
+    n = ds["X"].shape[0]
+    nval = max(1, int(n * val_frac))
+    idx_train = np.arange(nval, n)
+    Nz, Ny, Nx = ds["shape"]
+    mask = LN.masks(Nz, Ny, Nx, torch.device("cuda"))
+    x = torch.empty((cfg.cin, Nz, Ny, Nx), device="cuda")
+    steps_total = epochs * math.ceil(len(idx_train) / batch)
+    rng = np.random.default_rng(cfg.seed + 1)
+    step = 0
+    hist = []
+
+    def val_loss():
+        tot = 0.0
+        for i in range(nval):
+            y = model.forward(_features(ds, i, x))
+            loss, _ = model.mse(y, ds["Y"][i], mask)
+            tot += loss.item()
+        return tot / nval
+
+    def zero_loss():
+        tot = 0.0
+        for i in range(nval):
+            t = ds["Y"][i] * mask
+            tot += float((t * t).sum().item() / mask.sum().item())
+        return tot / nval
+
+    base = zero_loss()
+    log(f"  validation loss of the zero correction (gs_cfcf start): {base:.4e}")
+    t0 = time.perf_counter()
+    for ep in range(epochs):
+        perm = rng.permutation(idx_train)
+        run = 0.0
+        for b0 in range(0, len(perm), batch):
+            model.zero_grad()
+            for i in perm[b0:b0 + batch]:
+                y = model.forward(_features(ds, int(i), x), cache=True)
+                loss, g = model.mse(y, ds["Y"][int(i)], mask)
+                model.backward(g * (1.0 / len(perm[b0:b0 + batch])))
+                run += loss.item()
+            cur = lr * 0.5 * (1 + math.cos(math.pi * step / steps_total)) + 1e-5
+            model.adam_step(lr=cur)
+            step += 1
+        v = val_loss()
+        hist.append(dict(epoch=ep + 1, train=run / len(perm), val=v, val_rel=v / base))
+        log(f"  epoch {ep + 1}: train {run / len(perm):.4e}  val {v:.4e} ({v / base:.3f} of the zero correction)"
+            f"  {time.perf_counter() - t0:.1f} s")
+    return model, dict(history=hist, zero_correction_val=base, seconds=time.perf_counter() - t0)
+
+
+def evaluate(model, seeds, n: int = 256, nz: int = 128, eps=(1e-4, 1e-3), max_iter: int = 3000, log=print):
+    torch = _torch()
+    solver = NFGSSolverGPU(n, n, nz, 1.0, 1.0, 1.0, **SOLVER_KW)
+    # bases and scratch of this grid are built once, outside the timed runs
+    model.forward(torch.zeros((model.cfg.cin, solver.Nz, solver.Ny, solver.Nx), device="cuda"))
+    torch.cuda.synchronize()
+    rows = []
+    for sd in seeds:
+        bx, by, bz = sunspot_magnetogram(n, sd)
+        solver.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+        plain = solver.iterate(max_iter=max_iter, verbose=False, **STOP)
+        sstar = float(plain["best_sigma"])
+        row = dict(seed=sd, sigma_star=sstar, plain_best_iter=int(plain["best_iter"]),
+                   plain_iterations=len(plain["sigma"]), plain_device_ms=float(plain["device_ms"]))
+        for e in eps:
+            target = sstar * (1 + e)
+            kw = dict(STOP, tol=target)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            hp = solver.iterate(max_iter=max_iter, verbose=False, **kw)
+            torch.cuda.synchronize()
+            tp = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            hl = solver.iterate(max_iter=max_iter, verbose=False, init_mode="learned", warm_start=model, **kw)
+            torch.cuda.synchronize()
+            tl = time.perf_counter() - t0
+            tag = f"eps{e:g}"
+            row[tag] = dict(
+                plain_s=tp, plain_iterations=len(hp["sigma"]), plain_reached=hp["stop_reason"] == "tol",
+                learned_s=tl, learned_iterations=len(hl["sigma"]), learned_reached=hl["stop_reason"] == "tol",
+                learned_best_sigma=float(hl["best_sigma"]), learned_accepted=hl["learned_start"]["accepted"],
+                sigma_learned_start=hl["learned_start"]["sigma_learned"],
+                sigma_gs_start=hl["learned_start"]["sigma_gs_cfcf"],
+                speedup=tp / tl if tl > 0 else None)
+        rows.append(row)
+        log("  " + json.dumps(row))
+    return rows
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--samples", type=int, default=2000)
+    ap.add_argument("--epochs", type=int, default=6)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--nz", type=int, default=64)
+    ap.add_argument("--gen-max-iter", type=int, default=600)
+    ap.add_argument("--eval-seeds", type=int, default=6)
+    ap.add_argument("--eval-n", type=int, default=256)
+    ap.add_argument("--eval-nz", type=int, default=128)
+    ap.add_argument("--out", default="warmstart.npz")
+    ap.add_argument("--report", default=None)
+    ap.add_argument("--load", default=None, help="skip training: evaluate this model")
+    args = ap.parse_args(argv)
+    report = {}
+    if args.load:
+        model = LN.NeuralOperator.load(args.load)
+    else:
+        print(f"generating {args.samples} reconstructions at {args.n}x{args.n}x{args.nz}", flush=True)
+        t0 = time.perf_counter()
+        ds = generate(args.samples, 0, args.n, args.nz, args.gen_max_iter,
+                      log=lambda m: print(m, flush=True))
+        report["generation_s"] = time.perf_counter() - t0
+        report["generation_mean_iterations"] = float(np.mean(ds["iters"]))
+        cfg = LN.Config()
+        print(f"training ({sum(int(np.prod(s)) for _, s in cfg.param_shapes())} parameters)", flush=True)
+        model, tr = train(ds, cfg, args.epochs, args.lr, args.batch, log=lambda m: print(m, flush=True))
+        report["training"] = tr
+        model.save(args.out)
+        del ds
+    seeds = [1_000_000 + i for i in range(args.eval_seeds)]
+    print(f"evaluating held-out seeds at the training size {args.n}x{args.n}x{args.nz}", flush=True)
+    report["evaluation_train_size"] = evaluate(model, seeds, args.n, args.nz, log=lambda m: print(m, flush=True))
+    print(f"evaluating held-out seeds at {args.eval_n}x{args.eval_n}x{args.eval_nz}", flush=True)
+    report["evaluation"] = evaluate(model, seeds, args.eval_n, args.eval_nz, log=lambda m: print(m, flush=True))
+    if args.report:
+        with open(args.report, "w") as f:
+            json.dump(report, f, indent=1)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

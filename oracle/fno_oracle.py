@@ -76,7 +76,14 @@ def forward(params, cfg, x):
     p1 = pointwise(h, params["proj1_W"], params["proj1_b"])
     q1 = gelu(p1)
     y = pointwise(q1, params["proj2_W"], params["proj2_b"])
-    cache = dict(x=x, hs=hs, zs=zs, As=As, p1=p1, q1=q1, bases=(Az, Ay, Ax, Sz, Sy, Sx))
+    out_bases = None
+    ko = cfg.get("out_modes", (0, 0, 0))
+    if all(k > 0 for k in ko):
+        kz2, ky2, kx2 = (min(k, n) for k, n in zip(ko, (nz, ny, nx)))
+        (Aoz, Soz), (Aoy, Soy), (Aox, Sox) = cosine_bases(nz, kz2), cosine_bases(ny, ky2), cosine_bases(nx, kx2)
+        out_bases = (Aoz, Aoy, Aox, Soz, Soy, Sox)
+        y = expand3(reduce3(y, Aoz, Aoy, Aox), Soz, Soy, Sox)
+    cache = dict(x=x, hs=hs, zs=zs, As=As, p1=p1, q1=q1, bases=(Az, Ay, Ax, Sz, Sy, Sx), out_bases=out_bases)
     return y, cache
 
 
@@ -93,6 +100,9 @@ def backward(params, cfg, cache, gy):
         g[name + "_b"] = gyy.sum(axis=tuple(range(1, x.ndim)))
         return np.tensordot(W, gyy, axes=([0], [0]))
 
+    if cache.get("out_bases") is not None:
+        Aoz, Aoy, Aox, Soz, Soy, Sox = cache["out_bases"]
+        gy = expand3(reduce3(gy, Soz, Soy, Sox), Aoz, Aoy, Aox)
     gq = pw_back(cache["q1"], params["proj2_W"], gy, "proj2")
     gp = gq * gelu_grad(cache["p1"])
     gh = pw_back(cache["hs"][-1], params["proj1_W"], gp, "proj1")

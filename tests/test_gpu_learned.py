@@ -149,7 +149,7 @@ def test_network_forward_backward_against_oracle():
     parameter gradient within FP32 tolerance of the FP64 oracle."""
     from nfgs_b200.learned import Config, NeuralOperator, init_params
 
-    cfg = Config(cin=6, width=32, layers=3, modes=(3, 4, 4), hidden=32, cout=2, seed=5)
+    cfg = Config(cin=6, width=32, layers=3, modes=(3, 4, 4), hidden=32, cout=2, seed=5, out_modes=(5, 6, 7))
     rng = np.random.default_rng(6)
     params = init_params(cfg)
     params["proj2_W"] = (0.2 * rng.standard_normal(params["proj2_W"].shape)).astype(np.float32)
@@ -162,7 +162,7 @@ def test_network_forward_backward_against_oracle():
     y = net.forward(dev(x), cache=True)
     net.zero_grad()
     gx = net.backward(dev(gy))
-    ocfg = dict(cin=6, width=32, layers=3, modes=(3, 4, 4), hidden=32, cout=2)
+    ocfg = dict(cin=6, width=32, layers=3, modes=(3, 4, 4), hidden=32, cout=2, out_modes=(5, 6, 7))
     p64 = {k: v.astype(np.float64) for k, v in params.items()}
     yo, cache = O.forward(p64, ocfg, x)
     go, gxo = O.backward(p64, ocfg, cache, gy)
@@ -178,7 +178,7 @@ def test_training_reduces_loss():
     into a working optimiser)."""
     from nfgs_b200.learned import Config, NeuralOperator
 
-    cfg = Config(cin=6, width=32, layers=2, modes=(4, 4, 4), hidden=32, cout=2, seed=7)
+    cfg = Config(cin=6, width=32, layers=2, modes=(4, 4, 4), hidden=32, cout=2, seed=7, out_modes=(6, 6, 6))
     net = NeuralOperator(cfg)
     rng = np.random.default_rng(8)
     x = dev(rng.standard_normal((6, 9, 10, 11)))

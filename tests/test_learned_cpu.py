@@ -6,13 +6,13 @@ import pytest
 
 from oracle import fno_oracle as O
 
-CFG = dict(cin=3, width=4, layers=2, modes=(2, 3, 3), hidden=3, cout=2)
+CFG = dict(cin=3, width=4, layers=2, modes=(2, 3, 3), hidden=3, cout=2, out_modes=(3, 4, 4))
 
 
 def _params(rng):
     from nfgs_b200.learned import Config, init_params
 
-    cfg = Config(cin=3, width=4, layers=2, modes=(2, 3, 3), hidden=3, cout=2, seed=3)
+    cfg = Config(cin=3, width=4, layers=2, modes=(2, 3, 3), hidden=3, cout=2, seed=3, out_modes=(3, 4, 4))
     p = {k: v.astype(np.float64) for k, v in init_params(cfg).items()}
     # non-zero output layer and biases so every path carries gradient
     for k in p:
