@@ -266,6 +266,18 @@ const char* nfgs_last_error(void);
 /* Library build identification (sm arch, version). */
 const char* nfgs_version(void);
 
+/* Batched scan (the reference runs its weight x rho sweeps as a serial loop
+ * of solves, run_nfgs_td_robin_weight_sweep.py:510-660): handles that have
+ * each been through nfgs_iterate_begin (graph mode) are advanced together.
+ * nfgs_scan_create builds one CUDA graph holding `iters` iterations of every
+ * handle (independent chains, so the solves run concurrently); each
+ * nfgs_scan_launch launches it once, waits, and returns how many solves have
+ * not stopped (stopped solves skip their work on the device).  Finish each
+ * handle with nfgs_iterate_end.  All handles must be on one device. */
+int nfgs_scan_create(void* const* handles, int32_t n, int32_t iters, void** scan_out);
+int nfgs_scan_launch(void* scan, int32_t* n_active_out);
+int nfgs_scan_destroy(void* scan);
+
 /* Learned warm start (no reference counterpart; the reference always starts
  * from the zero-source state, nfgs_solver.py:6613-6645).
  * nfgs_iterate_start_state: device views (storage type, (nz, ny, nx)) of the

@@ -13,7 +13,9 @@
 #include <cuda_fp16.h>
 
 #include <cmath>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -137,6 +139,8 @@ struct Handle {
     void* fbuf = nullptr;
     size_t fbuf_bytes = 0;
     double* dsmall = nullptr;  // small device scratch for host decisions
+    int fs_tuned = 0;          // the fused-stencil segment count has been tuned
+    long long pface_len = 0;   // doubles in pface
     int advanced = 0;          // the current iteration has taken a step
     void* pin[2] = {nullptr, nullptr};
     cudaEvent_t pin_ev[2] = {nullptr, nullptr};
@@ -1354,6 +1358,66 @@ static int enqueue_iteration(Handle* h) {
     return NFGS_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Tile autotuner: the z-segment count of the fused stencil is chosen per grid
+// shape by timing candidates on live data (the gs_cfcf start state) the
+// first time a shape is iterated; the choice is cached for the process.
+// NFGS_STENCIL_NSEG fixes it; NFGS_AUTOTUNE=0 keeps the built-in heuristic.
+// ---------------------------------------------------------------------------
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int, int>, int> g_tune_nseg;
+
+template <typename T>
+static int autotune_stencil(Handle* h, int polarity) {
+    if (!h->fs_on || h->fs_tuned) return NFGS_OK;
+    h->fs_tuned = 1;
+    if (getenv("NFGS_STENCIL_NSEG") != nullptr) return NFGS_OK;
+    if (const char* e = getenv("NFGS_AUTOTUNE"))
+        if (e[0] == '0') return NFGS_OK;
+    const int nz = h->g.nz;
+    const auto key = std::make_tuple(h->g.nx, h->g.ny, nz, (int)h->f32);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_nseg.find(key);
+        if (it != g_tune_nseg.end()) {
+            const int per = (nz + it->second - 1) / it->second;
+            h->fs_grid.z = (unsigned)((nz + per - 1) / per);
+            h->fs_nb = (int)(h->fs_grid.x * h->fs_grid.y * h->fs_grid.z);
+            return NFGS_OK;
+        }
+    }
+    const int cands[] = {1, 2, 4, 8, 12, 16};
+    const unsigned gz0 = h->fs_grid.z;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    float best_ms = -1.0f;
+    unsigned best = gz0;
+    for (int c : cands) {
+        if (c > nz / 4 && c != 1) continue;
+        const int per = (nz + c - 1) / c;
+        const unsigned gz = (unsigned)((nz + per - 1) / per);
+        if ((long long)h->fs_grid.x * h->fs_grid.y * gz * NFGS_NRED > h->pface_len) continue;
+        h->fs_grid.z = gz;
+        h->fs_nb = (int)(h->fs_grid.x * h->fs_grid.y * gz);
+        TRY(run_fused<T>(h, &h->consts[0], nullptr, polarity));
+        CK(cudaEventRecord(a, h->s));
+        for (int r = 0; r < 3; ++r) TRY(run_fused<T>(h, &h->consts[0], nullptr, polarity));
+        CK(cudaEventRecord(b, h->s));
+        CK(cudaEventSynchronize(b));
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        if (best_ms < 0 || ms < best_ms) { best_ms = ms; best = gz; }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    h->fs_grid.z = best;
+    h->fs_nb = (int)(h->fs_grid.x * h->fs_grid.y * best);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_nseg[key] = (int)best;
+    return NFGS_OK;
+}
+
 template <typename T>
 static int iterate_begin_t(Handle* h, const NfgsStop* stop) {
     if (!h->boundary_set)
@@ -1402,6 +1466,7 @@ static int iterate_begin_t(Handle* h, const NfgsStop* stop) {
         CK(cudaGetLastError());
         h->launches++;
     }
+    TRY(autotune_stencil<T>(h, stop->polarity_mask));
     TRY(run_stencil<T>(h, &h->consts[0], nullptr, 1, stop->polarity_mask));
     sum_partials(h);
     k_ctl_init<<<1, 1, 0, h->s>>>(h->g, h->ctl, h->scal, h->hist);
@@ -1478,6 +1543,35 @@ static int restart_from_t(Handle* h, const void* phi, const void* az, int mode, 
     return NFGS_OK;
 }
 
+// Capture the per-iteration launch sequence of a handle into its CUDA graph
+// (once per iterate call; the graph holds device-side indices only).
+template <typename T>
+static int ensure_graph_t(Handle* h) {
+    if (h->gexec) return NFGS_OK;
+    CK(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+    int before = h->launches;
+    int r = enqueue_iteration<T>(h);
+    cudaGraph_t gr = nullptr;
+    cudaError_t e = cudaStreamEndCapture(h->s, &gr);
+    if (r != NFGS_OK) { if (gr) cudaGraphDestroy(gr); return r; }
+    CK(e);
+    h->graph = gr;
+    CK(cudaGraphInstantiate(&h->gexec, h->graph, 0));
+    h->launches = before;  // counted per graph launch
+    size_t nn = 0;
+    CK(cudaGraphGetNodes(h->graph, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    CK(cudaGraphGetNodes(h->graph, nodes.data(), &nn));
+    int kn = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        CK(cudaGraphNodeGetType(nd, &t));
+        kn += (t == cudaGraphNodeTypeKernel);
+    }
+    h->graph_kernels = kn;
+    return NFGS_OK;
+}
+
 template <typename T>
 static int iterate_advance_t(Handle* h, int max_steps, int32_t* stop_reason, int32_t* n_done) {
     if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
@@ -1488,29 +1582,7 @@ static int iterate_advance_t(Handle* h, int max_steps, int32_t* stop_reason, int
     while (!h->ctl_h->stopped && done < max_steps) {
         int k = std::min(h->stop.check_every, max_steps - done);
         if (h->stop.use_graph) {
-            if (!h->gexec) {
-                CK(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
-                int before = h->launches;
-                int r = enqueue_iteration<T>(h);
-                cudaGraph_t gr = nullptr;
-                cudaError_t e = cudaStreamEndCapture(h->s, &gr);
-                if (r != NFGS_OK) { if (gr) cudaGraphDestroy(gr); return r; }
-                CK(e);
-                h->graph = gr;
-                CK(cudaGraphInstantiate(&h->gexec, h->graph, 0));
-                h->launches = before;  // counted per graph launch below
-                size_t nn = 0;
-                CK(cudaGraphGetNodes(h->graph, nullptr, &nn));
-                std::vector<cudaGraphNode_t> nodes(nn);
-                CK(cudaGraphGetNodes(h->graph, nodes.data(), &nn));
-                int kn = 0;
-                for (auto nd : nodes) {
-                    cudaGraphNodeType t;
-                    CK(cudaGraphNodeGetType(nd, &t));
-                    kn += (t == cudaGraphNodeTypeKernel);
-                }
-                h->graph_kernels = kn;
-            }
+            TRY(ensure_graph_t<T>(h));
             for (int q = 0; q < k; ++q) CK(cudaGraphLaunch(h->gexec, h->s));
             h->launches += k * h->graph_kernels;
         } else {
@@ -2152,7 +2224,12 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
     h->sgrid = dim3((nx + 31) / 32, (ny + 3) / 4, nz);
     h->nb_face = h->nb_src = (int)(h->sgrid.x * h->sgrid.y * h->sgrid.z);
     TRYC(fs_setup(h));
-    TRYC(alloc(h, &h->pface, (size_t)std::max(h->nb_face * 5, h->fs_nb * NFGS_NRED) * 8));
+    {
+        // room for the tuner's largest candidate (16 z segments)
+        const long long fs_max = (long long)h->fs_grid.x * h->fs_grid.y * std::max(16u, h->fs_grid.z) * NFGS_NRED;
+        h->pface_len = std::max((long long)h->nb_face * 5, fs_max);
+        TRYC(alloc(h, &h->pface, (size_t)h->pface_len * 8));
+    }
     TRYC(alloc(h, &h->psrc, (size_t)h->nb_src * 8));
     TRYC(alloc(h, &h->s00, (size_t)nz * 8));
     TRYC(alloc(h, &h->scal, (8 + 6 * NCHUNK) * 8));
@@ -2367,6 +2444,91 @@ int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int
     if (!h || !phi || !az || !out3) return fail(NFGS_EINVAL, "null argument");
     if (mode < 0 || mode > 2) return fail(NFGS_EINVAL, "mode must be 0, 1 or 2");
     return h->f32 ? restart_from_t<float>(h, phi, az, mode, out3) : restart_from_t<double>(h, phi, az, mode, out3);
+}
+
+// ---------------------------------------------------------------------------
+// Batched scan: many begun iterations advanced together by one graph launch.
+// ---------------------------------------------------------------------------
+struct NfgsScanObj {
+    std::vector<Handle*> hs;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t s = nullptr;
+    int iters = 0;
+    int device = 0;
+};
+
+int nfgs_scan_create(void* const* handles, int32_t n, int32_t iters, void** scan_out) {
+    g_err.clear();
+    if (!handles || n <= 0 || iters <= 0 || !scan_out) return fail(NFGS_EINVAL, "scan: bad arguments");
+    Handle* h0 = (Handle*)handles[0];
+    if (!h0) return fail(NFGS_EINVAL, "scan: null handle");
+    cudaSetDevice(h0->geom.device);
+    auto* sc = new NfgsScanObj();
+    sc->iters = iters;
+    sc->device = h0->geom.device;
+    auto bail = [&](int code) {
+        if (sc->exec) cudaGraphExecDestroy(sc->exec);
+        if (sc->graph) cudaGraphDestroy(sc->graph);
+        if (sc->s) cudaStreamDestroy(sc->s);
+        delete sc;
+        return code;
+    };
+    if (cudaGraphCreate(&sc->graph, 0) != cudaSuccess) return bail(fail(NFGS_ECUDA, "scan: graph create"));
+    for (int i = 0; i < n; ++i) {
+        Handle* h = (Handle*)handles[i];
+        if (!h || h->geom.device != sc->device) return bail(fail(NFGS_EINVAL, "scan: handles must share a device"));
+        if (!h->iter_active) return bail(fail(NFGS_ESTATE, "scan: every handle needs nfgs_iterate_begin"));
+        if (!h->stop.use_graph) return bail(fail(NFGS_EINVAL, "scan: handles must iterate with use_graph"));
+        int r = h->f32 ? ensure_graph_t<float>(h) : ensure_graph_t<double>(h);
+        if (r != NFGS_OK) return bail(r);
+        // the begin work (gs_cfcf start) ran on the handle's stream
+        if (cudaStreamSynchronize(h->s) != cudaSuccess) return bail(fail(NFGS_ECUDA, "scan: sync"));
+        h->advanced = 1;
+        cudaGraphNode_t prev = nullptr;
+        for (int k = 0; k < iters; ++k) {
+            cudaGraphNode_t nd;
+            if (cudaGraphAddChildGraphNode(&nd, sc->graph, prev ? &prev : nullptr, prev ? 1 : 0, h->graph) !=
+                cudaSuccess)
+                return bail(fail(NFGS_ECUDA, "scan: add child graph"));
+            prev = nd;
+        }
+        sc->hs.push_back(h);
+    }
+    if (cudaGraphInstantiate(&sc->exec, sc->graph, 0) != cudaSuccess) return bail(fail(NFGS_ECUDA, "scan: instantiate"));
+    if (cudaStreamCreateWithFlags(&sc->s, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(NFGS_ECUDA, "scan: stream"));
+    *scan_out = sc;
+    return NFGS_OK;
+}
+
+int nfgs_scan_launch(void* scan, int32_t* n_active_out) {
+    g_err.clear();
+    auto* sc = (NfgsScanObj*)scan;
+    if (!sc) return fail(NFGS_EINVAL, "null scan");
+    cudaSetDevice(sc->device);
+    CK(cudaGraphLaunch(sc->exec, sc->s));
+    CK(cudaStreamSynchronize(sc->s));
+    int active = 0;
+    for (Handle* h : sc->hs) {
+        CK(cudaMemcpy(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost));
+        h->launches += sc->iters * h->graph_kernels;
+        active += h->ctl_h->stopped ? 0 : 1;
+    }
+    if (n_active_out) *n_active_out = active;
+    return NFGS_OK;
+}
+
+int nfgs_scan_destroy(void* scan) {
+    auto* sc = (NfgsScanObj*)scan;
+    if (!sc) return NFGS_OK;
+    cudaSetDevice(sc->device);
+    if (sc->s) cudaStreamSynchronize(sc->s);
+    if (sc->exec) cudaGraphExecDestroy(sc->exec);
+    if (sc->graph) cudaGraphDestroy(sc->graph);
+    if (sc->s) cudaStreamDestroy(sc->s);
+    delete sc;
+    return NFGS_OK;
 }
 
 int nfgs_iterate_initial(void* handle, double* scalars3) {

@@ -1,0 +1,136 @@
+"""Batched weight x rho scan: many NFGS solves advanced together.
+
+The reference runs its TD weight x rho sweeps as a serial loop of solves
+(run_nfgs_td_robin_weight_sweep.py:510-660).  Here every solve of the scan is
+begun on its own handle (gs_cfcf start, per-iteration CUDA graph captured),
+and one CUDA graph holding `iters` iterations of every solve -- independent
+chains, so solves of different sizes fill the GPU together -- is launched
+until every solve has met its stop rule.  Solves that stopped skip their work
+on the device; the results are those of the same solves run one by one.
+The fused stencil's z-segment count is autotuned per grid shape.
+
+    python -m nfgs_b200.scan --boundaries 33 --report scan.json
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import time
+
+import numpy as np
+
+from . import _lib as L
+from .solver import NFGSSolverGPU
+from .synthetic import td_bottom
+
+GRIDS = ((128, 64), (160, 80), (192, 96), (224, 112), (256, 128))
+RHOS = (0.0, 0.3, 0.5, 0.7, 1.0)
+KW = dict(dtype="float32", horizontal_zero_mode_policy="frozen_linear_harmonic",
+          vertical_current_operator="staggered_face", d0_zero_mode_policy="project",
+          source_zero_mode_policy="project")
+STOP = dict(tol=1e-5, patience=40, sigma_improvement_tol=1e-5)
+
+
+def td_scan_cases(n_boundaries: int = 33, rhos=RHOS, seed: int = 0, grids=GRIDS, extent: float = 8.0):
+    """Seeded TD-type boundaries (R in [2,4], a in [0.6,1.2], d in [1,2],
+    twist from the seeded current) on grids drawn from `grids`, each at
+    every rho."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for b in range(n_boundaries):
+        R, a, d = rng.uniform(2.0, 4.0), rng.uniform(0.6, 1.2), rng.uniform(1.0, 2.0)
+        n, nz = grids[int(rng.integers(len(grids)))]
+        bx, by, bz = td_bottom(n, n, seed=seed * 1000 + b, extent=extent, R=R, a=a, d=d)
+        h = 2 * extent / (n - 1)
+        for rho in rhos:
+            cases.append(dict(boundary=b, n=n, nz=nz, rho=float(rho), R=R, a=a, d=d, h=h, bx=bx, by=by, bz=bz))
+    return cases
+
+
+def _solver(case):
+    s = NFGSSolverGPU(case["n"], case["n"], case["nz"], case["h"], case["h"], case["h"],
+                      bottom_divergence_robin_weight=case["rho"], **KW)
+    s.set_bottom_vector_boundary(case["bx"], case["by"], case["bz"], zero_net_current=False, smooth_passes=0,
+                                 ijzbcor=3)
+    return s
+
+
+def run_scan(cases, iters: int = 8, max_iter: int = 3000, stop=STOP):
+    """All cases in one batched run; returns (histories, timings)."""
+    import torch
+
+    t0 = time.perf_counter()
+    solvers, ctxs = [], []
+    for c in cases:
+        s = _solver(c)
+        ctxs.append(s._iterate_begin(max_iter=max_iter, verbose=False, use_graph=True, **stop))
+        solvers.append(s)
+    lib = L.lib()
+    arr = (C.c_void_p * len(solvers))(*[s._h.value if isinstance(s._h, C.c_void_p) else s._h for s in solvers])
+    scan = C.c_void_p()
+    L.check(lib.nfgs_scan_create(arr, len(solvers), iters, C.byref(scan)))
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    launches = 0
+    active = C.c_int32(len(solvers))
+    try:
+        while active.value > 0 and launches * iters < max_iter + iters:
+            L.check(lib.nfgs_scan_launch(scan, C.byref(active)))
+            launches += 1
+    finally:
+        t2 = time.perf_counter()
+        L.check(lib.nfgs_scan_destroy(scan))
+    hists = [s._iterate_finish(ctx) for s, ctx in zip(solvers, ctxs)]
+    cells_iters = sum(s.Nx * s.Ny * s.Nz * len(h["sigma"]) for s, h in zip(solvers, hists))
+    timing = dict(setup_s=t1 - t0, scan_s=t2 - t1, graph_launches=launches, iters_per_launch=iters,
+                  cell_iterations=cells_iters, gcell_iter_per_s=cells_iters / (t2 - t1) / 1e9)
+    del solvers
+    return hists, timing
+
+
+def run_serial(cases, max_iter: int = 3000, stop=STOP):
+    """The same solves one after another (each its own iterate call)."""
+    import torch
+
+    hists, t_iter = [], 0.0
+    for c in cases:
+        s = _solver(c)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        hists.append(s.iterate(max_iter=max_iter, verbose=False, **stop))
+        torch.cuda.synchronize()
+        t_iter += time.perf_counter() - t
+        del s
+    return hists, dict(serial_iterate_s=t_iter)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--boundaries", type=int, default=33)
+    ap.add_argument("--iters", type=int, default=8)
+    ap.add_argument("--max-iter", type=int, default=3000)
+    ap.add_argument("--serial", action="store_true", help="also run the solves one by one and compare")
+    ap.add_argument("--report", default=None)
+    args = ap.parse_args(argv)
+    cases = td_scan_cases(args.boundaries)
+    hists, timing = run_scan(cases, args.iters, args.max_iter)
+    out = dict(solves=len(cases), timing=timing,
+               results=[dict(boundary=c["boundary"], n=c["n"], nz=c["nz"], rho=c["rho"],
+                             best_sigma=h["best_sigma"], best_iter=h["best_iter"], iterations=len(h["sigma"]),
+                             stop_reason=h["stop_reason"]) for c, h in zip(cases, hists)])
+    if args.serial:
+        sh, st = run_serial(cases, args.max_iter)
+        out["serial"] = st
+        out["identical_histories"] = all(a["sigma"] == b["sigma"] for a, b in zip(hists, sh))
+        out["speedup_vs_serial_iterate"] = st["serial_iterate_s"] / timing["scan_s"]
+    print(json.dumps({k: v for k, v in out.items() if k != "results"}), flush=True)
+    if args.report:
+        with open(args.report, "w") as f:
+            json.dump(out, f, indent=1)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

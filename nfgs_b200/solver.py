@@ -544,6 +544,29 @@ class NFGSSolverGPU:
                 fixed_point_observable_tol=None, fixed_point_patience: int = 10,
                 auto_rbsl_improvement_grace: int = 20, check_every: int = 32, use_graph: bool = True,
                 warm_start=None, **_auto_rbsl_kwargs):
+        """Run the NFGS iteration to its stop rule (nfgs_solver.py:6937-7009 ->
+        3522-3850) and return the reference's history dict."""
+        ctx = self._iterate_begin(
+            max_iter=max_iter, tol=tol, mu=mu, patience=patience, verbose=verbose, polarity_mask=polarity_mask,
+            init_mode=init_mode, sigma_improvement_tol=sigma_improvement_tol, per_step_callback=per_step_callback,
+            adaptive_mu=adaptive_mu, mu_min=mu_min, mu_max=mu_max, mu_backoff=mu_backoff, mu_growth=mu_growth,
+            growth_streak=growth_streak, divergence_factor=divergence_factor, max_rollbacks=max_rollbacks,
+            stop_mode=stop_mode, fixed_point_update_tol=fixed_point_update_tol,
+            fixed_point_pde_tol=fixed_point_pde_tol, fixed_point_observable_tol=fixed_point_observable_tol,
+            fixed_point_patience=fixed_point_patience, auto_rbsl_improvement_grace=auto_rbsl_improvement_grace,
+            check_every=check_every, use_graph=use_graph, warm_start=warm_start, **_auto_rbsl_kwargs)
+        self._iterate_loop(ctx)
+        return self._iterate_finish(ctx)
+
+    def _iterate_begin(self, max_iter=200, tol=1e-5, mu=1.0, patience=1, verbose=True, polarity_mask="both", *,
+                init_mode="gs_cfcf", sigma_improvement_tol: Optional[float] = 1e-5,
+                per_step_callback: Optional[Callable] = None, adaptive_mu: bool = False, mu_min: float = 0.02,
+                mu_max: float = 1.0, mu_backoff: float = 0.5, mu_growth: float = 1.1, growth_streak: int = 5,
+                divergence_factor: float = 2.0, max_rollbacks: int = 12, stop_mode: str = "sigma_best",
+                fixed_point_update_tol=None, fixed_point_pde_tol: float = 1.0e-8,
+                fixed_point_observable_tol=None, fixed_point_patience: int = 10,
+                auto_rbsl_improvement_grace: int = 20, check_every: int = 32, use_graph: bool = True,
+                warm_start=None, **_auto_rbsl_kwargs):
         mode = str(init_mode).lower().replace("-", "_")
         if mode == "yi_soft":
             mode = "soft_cfcf"
@@ -587,7 +610,6 @@ class NFGSSolverGPU:
             from . import learned as _learned
 
             self.learned_start_info = _learned.learned_start(self, warm_start, fallback=True)
-        rows_seen = 0
         if verbose:
             sc = np.zeros(3)
             L.check(lib.nfgs_iterate_initial(self._h, L.dptr(sc)))
@@ -595,6 +617,15 @@ class NFGSSolverGPU:
             am_text = f"{am:.3e}" if am is not None else "off"
             print(f"Initial  sigma={sc[0]:.4e}  divB={sc[1]:.4e}  E={sc[2]:.4e} "
                   f"(mu0={mu}, adaptive={adaptive_mu}, alpha_max={am_text}, toroidal_bc=True)")
+        return dict(lib=lib, verbose=verbose, per_step_callback=per_step_callback, step_by_step=step_by_step,
+                    check_every=check_every, max_iter=max_iter, stop_mode=stop_mode, update_tol=update_tol,
+                    observable_tol=observable_tol, fixed_point_pde_tol=fixed_point_pde_tol,
+                    fixed_point_patience=fixed_point_patience, eps=eps, use_imp=use_imp)
+
+    def _iterate_loop(self, ctx):
+        lib, per_step_callback, check_every = ctx["lib"], ctx["per_step_callback"], ctx["check_every"]
+        step_by_step, verbose = ctx["step_by_step"], ctx["verbose"]
+        rows_seen = 0
         reason = L.C.c_int32(0)
         ndone = L.C.c_int32(0)
         while True:
@@ -620,6 +651,12 @@ class NFGSSolverGPU:
                             print(f"Iter {n:4d} | sigma={r[0]:.4e} DIVERGED -> rollback, mu={r[3]:.3f}")
             if reason.value != 0:
                 break
+
+    def _iterate_finish(self, ctx):
+        lib, verbose, max_iter, stop_mode = ctx["lib"], ctx["verbose"], ctx["max_iter"], ctx["stop_mode"]
+        update_tol, observable_tol = ctx["update_tol"], ctx["observable_tol"]
+        fixed_point_pde_tol, fixed_point_patience = ctx["fixed_point_pde_tol"], ctx["fixed_point_patience"]
+        eps, use_imp = ctx["eps"], ctx["use_imp"]
         res = L.NfgsIterResult()
         hist = np.zeros((max(max_iter, 0) + 1, L.NFGS_HIST_COLS))
         code = lib.nfgs_iterate_end(self._h, L.C.byref(res), L.dptr(hist), hist.shape[0])
