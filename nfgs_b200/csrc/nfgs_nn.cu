@@ -380,7 +380,14 @@ int nfgs_nn_reduce3(const float* in, float* out, int32_t C, int32_t nz, int32_t 
     cudaStream_t s = (cudaStream_t)stream;
     const long long rows = (long long)C * nz * ny;
     const size_t shm = (size_t)kx * nx * sizeof(float);
-    if (shm > 48 * 1024) return nn_fail(NFGS_EINVAL, "reduce3: x basis too large");
+    if (shm > 200 * 1024) return nn_fail(NFGS_EINVAL, "reduce3: x basis too large");
+    if (shm > 48 * 1024) {
+        static int raised = 0;  // the attribute is per device function; raise it once to the cap
+        if (!raised) {
+            NNCK(cudaFuncSetAttribute(k_contract_x, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            raised = 1;
+        }
+    }
     k_contract_x<<<nblk(rows, 8), 256, shm, s>>>(in, Mx, t1, rows, nx, kx);
     NNCK(cudaGetLastError());
     long long n2 = (long long)C * nz * ky * kx;
