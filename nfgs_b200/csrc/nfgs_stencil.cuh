@@ -97,11 +97,13 @@ __device__ __forceinline__ void cp_async(unsigned dst, const void* src) {
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <typename T>
-__global__ void __launch_bounds__(NT, min_blocks<T>()) k_stencil(Args a) {
-    extern __shared__ __align__(16) unsigned char sm_raw[];
-    __shared__ double shred[NFGS_NRED * 32];
-    if (a.skip != nullptr && *a.skip) return;
+// Body of the z-march.  EDGE = false is the version of tiles none of whose
+// cells (levels 0-2) lies on a lateral wall: every x/y stencil takes the
+// interior form, so the one-sided wall code is dead and warps never diverge
+// on it; the bottom and top planes keep their one-sided z forms (a branch
+// uniform over the CTA).
+template <typename T, bool EDGE>
+__device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_raw, double* shred) {
     T* const sm = (T*)sm_raw;
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(sm_raw);
 
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(NT, min_blocks<T>()) k_stencil(Args a) {
         return sm[O_JC + ((c % 3) * 3 + comp) * CAP(1) + OF(1, jj, ii)];
     };
     auto win = [&](int c, int jj, int ii) -> T { return (wz[c] * wy[jj]) * wx[ii]; };
-    auto xy_in = [&](int jj, int ii) { return ii > 0 && ii < nx - 1 && jj > 0 && jj < ny - 1; };
+    auto xy_in = [&](int jj, int ii) { return !EDGE || (ii > 0 && ii < nx - 1 && jj > 0 && jj < ny - 1); };
 
     double red[NFGS_NRED] = {0, 0, 0, 0, 0, 0};
 
@@ -496,6 +498,21 @@ __global__ void __launch_bounds__(NT, min_blocks<T>()) k_stencil(Args a) {
 #pragma unroll
         for (int q = 0; q < NFGS_NRED; ++q) a.partials[q * nb + b] = red[q];
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NT, min_blocks<T>()) k_stencil(Args a) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    __shared__ double shred[NFGS_NRED * 32];
+    if (a.skip != nullptr && *a.skip) return;
+    const int nx = a.g.nx, ny = a.g.ny;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int tw = ((int)blockIdx.x == a.gx - 1) ? nx - x0 : TX;
+    const int th = ((int)blockIdx.y == a.gy - 1) ? ny - y0 : TY;
+    // the level-2 box [x0-2, x0+tw+2) x [y0-2, y0+th+2) stays off the walls
+    const bool interior = x0 - 2 >= 1 && x0 + tw + 1 <= nx - 2 && y0 - 2 >= 1 && y0 + th + 1 <= ny - 2;
+    if (interior) stencil_body<T, false>(a, sm_raw, shred);
+    else stencil_body<T, true>(a, sm_raw, shred);
 }
 
 }  // namespace fs
