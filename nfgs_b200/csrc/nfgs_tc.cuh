@@ -106,7 +106,10 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
 }
 
 // Bounded wait on an mbarrier phase; returns false if the limit ran out.
+// After a few immediate polls the waiting warp sleeps between polls (up to
+// 256 ns) so that it leaves the issue slots to the warps doing the work.
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    unsigned ns = 0;
     for (long long it = 0; it < WAIT_LIMIT; ++it) {
         uint32_t done;
         asm volatile(
@@ -117,6 +120,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
             : "r"(mbar), "r"(parity)
             : "memory");
         if (done) return true;
+        if (it >= 4) {
+            ns = ns == 0 ? 16 : (ns < 256 ? 2 * ns : 256);
+            __nanosleep(ns);
+        }
     }
     return false;
 }

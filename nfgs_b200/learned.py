@@ -152,7 +152,12 @@ class Grid:
 
 
 class NeuralOperator:
-    """The warm-start network with its forward and backward pass."""
+    """The warm-start network with its forward and backward pass.
+
+    start_filters: the band limits (cosine modes per axis, or None for the
+    unfiltered correction) that learned_start tries by default."""
+
+    start_filters: tuple = (None,)
 
     def __init__(self, cfg: Config, params: dict[str, np.ndarray] | None = None, device="cuda"):
         torch = _torch()
@@ -420,14 +425,38 @@ def features(solver, phi, az, in_scale=(1.0, 1.0)):
     return x
 
 
-def learned_start(solver, model, fallback: bool = True, scales_tried=(1.0, 0.6, 0.35, 0.2)) -> dict:
+def band_limit(model: NeuralOperator, field, modes):
+    """Project a (C, nz, ny, nx) device field onto its first `modes` cosine
+    modes per axis (nfgs_nn_reduce3 then nfgs_nn_expand3)."""
+    torch = _torch()
+    C_, nz, ny, nx = field.shape
+    kz, ky, kx = (min(k, n) for k, n in zip(modes, (nz, ny, nx)))
+    A = [torch.from_numpy(cosine_bases(n, k)[0]).to(field.device) for n, k in ((nz, kz), (ny, ky), (nx, kx))]
+    S = [torch.from_numpy(cosine_bases(n, k)[1]).to(field.device) for n, k in ((nz, kz), (ny, ky), (nx, kx))]
+    f = field.float().contiguous()
+    coef = torch.empty(C_ * kz * ky * kx, device=field.device)
+    big = torch.empty(C_ * nz * ny * kx, device=field.device)
+    small = torch.empty(C_ * nz * ky * kx, device=field.device)
+    out = torch.empty_like(f)
+    st = model._stream()
+    _ck(model.lib.nfgs_nn_reduce3(_p(f), _p(coef), C_, nz, ny, nx, _p(A[0]), _p(A[1]), _p(A[2]), kz, ky, kx,
+                                  _p(big), _p(small), st))
+    _ck(model.lib.nfgs_nn_expand3(_p(coef), _p(out), C_, nz, ny, nx, _p(S[0]), _p(S[1]), _p(S[2]), kz, ky, kx, 0,
+                                  _p(small), _p(big), st))
+    return out
+
+
+def learned_start(solver, model, fallback: bool = True, scales_tried=(1.0, 0.6, 0.35, 0.2),
+                  filters_tried=None) -> dict:
     """After nfgs_iterate_begin: hand a predicted start to the solver.
 
     model: a NeuralOperator, or a callable (solver, phi, az) -> (phi, az)
     returning a candidate start state as device tensors of the solver dtype.
     For the network, the predicted correction is tried at the given scales
     and the one with the lowest sigma_J is kept when it beats the gs_cfcf
-    start (fallback) -- the plain iteration then runs unchanged."""
+    start (fallback) -- the plain iteration then runs unchanged.  Each band
+    limit of filters_tried (default model.start_filters) is tried with every
+    scale."""
     torch = _torch()
     phi, az = start_state_views(solver)
     lib = solver._lib
@@ -455,15 +484,17 @@ def learned_start(solver, model, fallback: bool = True, scales_tried=(1.0, 0.6, 
         corr = ((y * m) * osc * (bs * ls)).double()
     tried = []
     best = None
-    for lam in scales_tried:
-        cp = (phi.double() + lam * corr[0]).to(phi.dtype).contiguous()
-        ca = (az.double() + lam * corr[1]).to(az.dtype).contiguous()
-        s_new, s_gs, _ = evaluate(cp, ca, 0)
-        tried.append((lam, s_new))
-        if np.isfinite(s_new) and (best is None or s_new < best[1]):
-            best = (lam, s_new, cp, ca)
+    for flt in (model.start_filters if filters_tried is None else filters_tried):
+        cf = corr if flt is None else (band_limit(model, corr, flt) * m).double()
+        for lam in scales_tried:
+            cp = (phi.double() + lam * cf[0]).to(phi.dtype).contiguous()
+            ca = (az.double() + lam * cf[1]).to(az.dtype).contiguous()
+            s_new, s_gs, _ = evaluate(cp, ca, 0)
+            tried.append((flt, lam, s_new))
+            if np.isfinite(s_new) and (best is None or s_new < best[1]):
+                best = (lam, s_new, cp, ca, flt)
     accepted = False
     if best is not None and (not fallback or best[1] < s_gs):
         _, _, accepted = evaluate(best[2], best[3], 2)
     return {"sigma_learned": best[1] if best else float("nan"), "sigma_gs_cfcf": s_gs, "accepted": accepted,
-            "scale": best[0] if best else None, "tried": tried}
+            "scale": best[0] if best else None, "filter": best[4] if best else None, "tried": tried}

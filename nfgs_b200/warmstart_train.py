@@ -207,6 +207,15 @@ def evaluate(model, seeds, n: int = 256, nz: int = 128, eps=(1e-4, 1e-3), max_it
     return rows
 
 
+def parse_filters(text: str) -> tuple:
+    """'none;10,10,10' -> (None, (10, 10, 10))."""
+    out = []
+    for part in text.split(";"):
+        part = part.strip().lower()
+        out.append(None if part in ("", "none") else tuple(int(v) for v in part.split(",")))
+    return tuple(out)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--samples", type=int, default=2000)
@@ -222,6 +231,9 @@ def main(argv=None):
     ap.add_argument("--out", default="warmstart.npz")
     ap.add_argument("--report", default=None)
     ap.add_argument("--load", default=None, help="skip training: evaluate this model")
+    ap.add_argument("--skip-train-size", action="store_true", help="evaluate at --eval-n/--eval-nz only")
+    ap.add_argument("--start-filters", default="none",
+                    help="band limits the learned start tries, e.g. 'none;10,10,10' (none = unfiltered)")
     args = ap.parse_args(argv)
     report = {}
     if args.load:
@@ -239,9 +251,11 @@ def main(argv=None):
         report["training"] = tr
         model.save(args.out)
         del ds
+    model.start_filters = parse_filters(args.start_filters)
     seeds = [1_000_000 + i for i in range(args.eval_seeds)]
-    print(f"evaluating held-out seeds at the training size {args.n}x{args.n}x{args.nz}", flush=True)
-    report["evaluation_train_size"] = evaluate(model, seeds, args.n, args.nz, log=lambda m: print(m, flush=True))
+    if not args.skip_train_size:
+        print(f"evaluating held-out seeds at the training size {args.n}x{args.n}x{args.nz}", flush=True)
+        report["evaluation_train_size"] = evaluate(model, seeds, args.n, args.nz, log=lambda m: print(m, flush=True))
     print(f"evaluating held-out seeds at {args.eval_n}x{args.eval_n}x{args.eval_nz}", flush=True)
     report["evaluation"] = evaluate(model, seeds, args.eval_n, args.eval_nz, log=lambda m: print(m, flush=True))
     if args.report:

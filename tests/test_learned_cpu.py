@@ -83,3 +83,13 @@ def test_masks_keep_boundary_values():
     assert not m[1, 0].any() and not m[1, -1].any()
     assert not m[1, :, 0].any() and not m[1, :, :, -1].any()
     assert m[1, 1:-1, 1:-1, 1:-1].all()
+
+
+def test_start_filter_option_parses():
+    from nfgs_b200.learned import NeuralOperator
+    from nfgs_b200.warmstart_train import parse_filters
+
+    assert parse_filters("none") == (None,)
+    assert parse_filters("none;10,10,10") == (None, (10, 10, 10))
+    assert parse_filters("16,12,12") == ((16, 12, 12),)
+    assert NeuralOperator.start_filters == (None,)
