@@ -199,6 +199,13 @@ int nfgs_fields(void* handle, int32_t which, int32_t crop, double* out, int32_t*
  * pinned 32 MB chunks. */
 int nfgs_fields_into(void* handle, int32_t which, int32_t crop, void* out, int32_t out_dtype, int32_t* dims_out);
 
+/* The same six fields gathered into caller-owned DEVICE memory (no host
+ * copy), for evaluation on the GPU: out_dev holds 6 * nz_out * ny_out *
+ * nx_out values of out_dtype.  out_dev == NULL only reports dims_out.
+ * Returns after the gather has been queued on the solver's stream and that
+ * stream has completed it. */
+int nfgs_fields_device(void* handle, int32_t which, int32_t crop, void* out_dev, int32_t out_dtype, int32_t* dims_out);
+
 /* Single-step access used by parity tests and by per_step_callback:
  * reconstructs the state of `which` and returns phi_c, A_z (FP64, full
  * calc grid), and its sigma/divB/energy. */
@@ -293,6 +300,42 @@ int nfgs_scan_destroy(void* scan);
  * (NFGS_ESTATE otherwise). */
 int nfgs_iterate_start_state(void* handle, void** phi_out, void** az_out);
 int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int32_t mode, double* out3);
+
+/* ------------------------------------------------------------------------
+ * Evaluation metrics of a solution on a region of interest, in one FP64-
+ * accumulating pass on the GPU.  Replaces the NumPy metrics the reference
+ * runs on host copies of the fields:
+ *   compute_reference_metrics   nfgs/_backend/util/metrics.py:123-178
+ *   compute_metrics             nfgs/_backend/scripts/recompute_td_referee_diagnostics.py:344-400
+ *   roi_cwsin / fortran_cwsin   nfgs/_backend/util/metrics.py:64-120
+ *   curl, divergence, sigma_j   nfgs/diagnostics/common_fd2.py:21-78
+ * ref, sol, cur: device pointers to component-major (3, nz, ny, nx) volumes
+ * of dtype (NFGS_F32 or NFGS_F64); ref and cur may be NULL.  spacing3 =
+ * {dx, dy, dz}.  roi6 = {z0, z1, y0, y1, x0, x1}, half-open, non-empty and
+ * inside the volume.  The finite-difference curl and divergence are those
+ * of the full volume (one-sided at its walls), evaluated on the region.
+ * out (host, NFGS_MET_COUNT doubles) gets the metrics below; those that need
+ * ref (or cur) are NaN when it is NULL.  stream is a cudaStream_t; the call
+ * returns when the result is on the host.
+ * ------------------------------------------------------------------------ */
+enum {
+    NFGS_MET_C_VEC = 0,        /* sum b.B / sqrt(sum |B|^2 sum |b|^2) */
+    NFGS_MET_C_CS,             /* mean b.B / (|B||b|) */
+    NFGS_MET_EPRIME_N,         /* 1 - sum |b - B| / sum |B| */
+    NFGS_MET_EPRIME_M,         /* 1 - mean |b - B| / |B| */
+    NFGS_MET_EPSILON,          /* sum |b|^2 / sum |B|^2 */
+    NFGS_MET_SIGMA_J,          /* on cur: sum |J x b| / max(|b|, 1e-10) / sum |J| */
+    NFGS_MET_SIGMA_J_FD2,      /* the same on the second-order curl of sol */
+    NFGS_MET_DIVB_NORM,        /* mean |div b| / (6 mean |b| / h_eff), h_eff = 3 / (1/dx + 1/dy + 1/dz) */
+    NFGS_MET_CELLS,            /* cells in the region */
+    NFGS_MET_SUM_B2,           /* sum |b|^2 */
+    NFGS_MET_SUM_REF2,         /* sum |B|^2 */
+    NFGS_MET_NONFINITE_B,      /* cells with a non-finite b or B component */
+    NFGS_MET_NONFINITE_J,      /* cells with a non-finite cur component */
+    NFGS_MET_COUNT
+};
+int nfgs_field_metrics(const void* ref, const void* sol, const void* cur, int32_t dtype, int32_t nz, int32_t ny,
+                       int32_t nx, const double* spacing3, const int32_t* roi6, double* out, void* stream);
 
 /* ------------------------------------------------------------------------
  * Learned warm start: operator kernels of a 3-D neural operator on a

@@ -26,6 +26,7 @@ NFGS_F32, NFGS_F64 = 0, 1
 NFGS_NDIAG = 40
 NFGS_NSRCDIAG = 12
 NFGS_HIST_COLS = 8
+NFGS_MET_COUNT = 13
 
 STOP_REASONS = {
     0: "running",
@@ -96,6 +97,9 @@ SIGNATURES = {
     "nfgs_iterate": (C.c_int, [_P, C.POINTER(NfgsStop), C.POINTER(NfgsIterResult), _DP, C.c_int32]),
     "nfgs_fields": (C.c_int, [_P, C.c_int32, C.c_int32, _DP, _IP]),
     "nfgs_fields_into": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, _IP]),
+    "nfgs_fields_device": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, _IP]),
+    "nfgs_field_metrics": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                     _DP, _IP, _DP, C.c_void_p]),
     "nfgs_get_scalars_state": (C.c_int, [_P, C.c_int32, _DP, _DP, _DP]),
     "nfgs_step": (C.c_int, [_P, C.c_double, C.c_int32]),
     "nfgs_gaussian_above": (C.c_int, [_P, _DP]),

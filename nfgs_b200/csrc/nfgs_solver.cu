@@ -10,6 +10,7 @@
 #include "nfgs_setup.cuh"
 #include "nfgs_tc.cuh"
 #include "nfgs_stencil.cuh"
+#include "nfgs_metrics.cuh"
 #include <cuda_fp16.h>
 
 #include <cmath>
@@ -1782,15 +1783,39 @@ static int d2h_chunked(Handle* h, void* host, const void* dev, size_t n) {
     return NFGS_OK;
 }
 
+// Region of the exported fields: the observed field of view (crop) or the
+// whole calculation grid.
+static void export_region(const Handle* h, int crop, int* nzc, int* y0, int* nyc, int* x0, int* nxc) {
+    *nzc = h->g.nz; *y0 = 0; *x0 = 0; *nyc = h->g.ny; *nxc = h->g.nx;
+    if (crop) {
+        *nzc = h->nzo_crop; *y0 = h->fov_y0; *x0 = h->fov_x0; *nyc = h->nyo; *nxc = h->nxo;
+    }
+}
+
+// Reconstruct the state `which` and gather its six fields into dst (device).
 template <typename T>
-static int fields_t(Handle* h, int which, int crop, void* out, int odtype, int32_t* dims) {
+static int gather_t(Handle* h, int which, int crop, void* dst, int odtype) {
     int idx;
     TRY(resolve_state(h, which, &idx));
     TRY(run_stencil<T>(h, &h->consts[idx], nullptr, 0, 0, 1));
-    int nzc = h->g.nz, y0 = 0, x0 = 0, nyc = h->g.ny, nxc = h->g.nx;
-    if (crop) {
-        nzc = h->nzo_crop; y0 = h->fov_y0; x0 = h->fov_x0; nyc = h->nyo; nxc = h->nxo;
-    }
+    int nzc, y0, nyc, x0, nxc;
+    export_region(h, crop, &nzc, &y0, &nyc, &x0, &nxc);
+    const long long n = (long long)nzc * nyc * nxc;
+    const unsigned grid = (unsigned)((n + 255) / 256);
+    if (odtype == NFGS_F32)
+        k_gather_fields<T, float><<<grid, 256, 0, h->s>>>(h->g, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz,
+                                                          (const T*)h->jpf, nzc, y0, nyc, x0, nxc, (float*)dst);
+    else
+        k_gather_fields<T, double><<<grid, 256, 0, h->s>>>(h->g, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz,
+                                                           (const T*)h->jpf, nzc, y0, nyc, x0, nxc, (double*)dst);
+    CK(cudaGetLastError());
+    return NFGS_OK;
+}
+
+template <typename T>
+static int fields_t(Handle* h, int which, int crop, void* out, int odtype, int32_t* dims) {
+    int nzc, y0, nyc, x0, nxc;
+    export_region(h, crop, &nzc, &y0, &nyc, &x0, &nxc);
     const long long n = (long long)nzc * nyc * nxc;
     const size_t osz = odtype == NFGS_F32 ? 4 : 8;
     const size_t bytes = 6 * (size_t)n * osz;
@@ -1805,16 +1830,75 @@ static int fields_t(Handle* h, int which, int crop, void* out, int odtype, int32
         TRY(alloc(h, &h->fbuf, bytes));
         h->fbuf_bytes = bytes;
     }
-    const unsigned grid = (unsigned)((n + 255) / 256);
-    if (odtype == NFGS_F32)
-        k_gather_fields<T, float><<<grid, 256, 0, h->s>>>(h->g, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz,
-                                                          (const T*)h->jpf, nzc, y0, nyc, x0, nxc, (float*)h->fbuf);
-    else
-        k_gather_fields<T, double><<<grid, 256, 0, h->s>>>(h->g, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz,
-                                                           (const T*)h->jpf, nzc, y0, nyc, x0, nxc, (double*)h->fbuf);
-    CK(cudaGetLastError());
+    TRY(gather_t<T>(h, which, crop, h->fbuf, odtype));
     TRY(d2h_chunked(h, out, h->fbuf, bytes));
     if (dims) { dims[0] = nzc; dims[1] = nyc; dims[2] = nxc; }
+    return NFGS_OK;
+}
+
+template <typename T>
+static int fields_device_t(Handle* h, int which, int crop, void* out_dev, int odtype, int32_t* dims) {
+    int nzc, y0, nyc, x0, nxc;
+    export_region(h, crop, &nzc, &y0, &nyc, &x0, &nxc);
+    if (dims) { dims[0] = nzc; dims[1] = nyc; dims[2] = nxc; }
+    if (!out_dev) return NFGS_OK;
+    TRY(gather_t<T>(h, which, crop, out_dev, odtype));
+    CK(cudaStreamSynchronize(h->s));
+    return NFGS_OK;
+}
+
+// Metrics of one region (nfgs_metrics.cuh); out gets NFGS_MET_COUNT values.
+template <typename T>
+static int field_metrics_t(const met::Args& a, cudaStream_t s, double* out) {
+    int dev = 0, nsm = 148;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const long long cells = (long long)a.cz * a.cy * a.cx;
+    const int gx = (a.cx + 31) / 32, gy = (a.cy + met::NT / 32 - 1) / (met::NT / 32);
+    const long long gxy = (long long)gx * gy;
+    const int gz = (int)std::max<long long>(1, std::min<long long>(a.cz, ((long long)nsm * 8 + gxy - 1) / gxy));
+    if (gy > 65535) return fail(NFGS_EINVAL, "field metrics: region too tall");
+    const int nblocks = (int)(gxy * gz);
+    double* part = nullptr;
+    CK(cudaMallocAsync((void**)&part, ((size_t)nblocks + 1) * met::NS * sizeof(double), s));
+    const dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)gz);
+    if (a.ref && a.cur) met::k_metrics<T, true, true><<<grid, met::NT, 0, s>>>(a, part);
+    else if (a.ref) met::k_metrics<T, true, false><<<grid, met::NT, 0, s>>>(a, part);
+    else if (a.cur) met::k_metrics<T, false, true><<<grid, met::NT, 0, s>>>(a, part);
+    else met::k_metrics<T, false, false><<<grid, met::NT, 0, s>>>(a, part);
+    cudaError_t e = cudaGetLastError();
+    double sums[met::NS];
+    if (e == cudaSuccess) {
+        met::k_metrics_sum<<<1, 32 * met::NS, 0, s>>>(part, nblocks, part + (size_t)nblocks * met::NS);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(sums, part + (size_t)nblocks * met::NS, sizeof(sums), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(part, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(NFGS_ECUDA, std::string("field metrics: ") + cudaGetErrorString(e));
+    using namespace met;
+    const double nan = std::nan("");
+    const double cnt = (double)cells, cm = std::max(cnt, 1.0);
+    for (int q = 0; q < NFGS_MET_COUNT; ++q) out[q] = nan;
+    if (a.ref) {
+        out[NFGS_MET_C_VEC] = sums[S_DOT] / (std::sqrt(sums[S_REF2] * sums[S_SOL2]) + 1.0e-12);
+        out[NFGS_MET_C_CS] = sums[S_COS] / cm;
+        out[NFGS_MET_EPRIME_N] = 1.0 - sums[S_ERR] / (sums[S_REFN] + 1.0e-12);
+        out[NFGS_MET_EPRIME_M] = 1.0 - sums[S_ERRR] / cm;
+        out[NFGS_MET_EPSILON] = sums[S_SOL2] / (sums[S_REF2] + 1.0e-12);
+        out[NFGS_MET_SUM_REF2] = sums[S_REF2];
+    }
+    if (a.cur) {
+        out[NFGS_MET_SIGMA_J] = sums[S_SJN] / std::max(sums[S_SJD], 1.0e-30);
+        out[NFGS_MET_NONFINITE_J] = sums[S_NFJ];
+    }
+    out[NFGS_MET_SIGMA_J_FD2] = sums[S_FDN] / std::max(sums[S_FDD], 1.0e-30);
+    const double h_eff = 3.0 / (1.0 / a.dx + 1.0 / a.dy + 1.0 / a.dz);
+    out[NFGS_MET_DIVB_NORM] = (sums[S_DIV] / cm) / (6.0 * (sums[S_BN] / cm) / h_eff + 1.0e-12);
+    out[NFGS_MET_CELLS] = cnt;
+    out[NFGS_MET_SUM_B2] = sums[S_SOL2];
+    out[NFGS_MET_NONFINITE_B] = sums[S_NFB];
     return NFGS_OK;
 }
 
@@ -2603,6 +2687,41 @@ int nfgs_fields_into(void* handle, int32_t which, int32_t crop, void* out, int32
     if (out_dtype != NFGS_F32 && out_dtype != NFGS_F64) return fail(NFGS_EINVAL, "out_dtype must be NFGS_F32 or NFGS_F64");
     return h->f32 ? fields_t<float>(h, which, crop, out, out_dtype, dims_out)
                   : fields_t<double>(h, which, crop, out, out_dtype, dims_out);
+}
+
+int nfgs_fields_device(void* handle, int32_t which, int32_t crop, void* out_dev, int32_t out_dtype,
+                       int32_t* dims_out) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
+    if (!h) return fail(NFGS_EINVAL, "null argument");
+    if (out_dtype != NFGS_F32 && out_dtype != NFGS_F64) return fail(NFGS_EINVAL, "out_dtype must be F32 or F64");
+    if (out_dev && !h->boundary_set) return fail(NFGS_ESTATE, "boundary not set");
+    return h->f32 ? fields_device_t<float>(h, which, crop, out_dev, out_dtype, dims_out)
+                  : fields_device_t<double>(h, which, crop, out_dev, out_dtype, dims_out);
+}
+
+int nfgs_field_metrics(const void* ref, const void* sol, const void* cur, int32_t dtype, int32_t nz, int32_t ny,
+                       int32_t nx, const double* spacing3, const int32_t* roi6, double* out, void* stream) {
+    g_err.clear();
+    if (!sol || !spacing3 || !roi6 || !out) return fail(NFGS_EINVAL, "null argument");
+    if (dtype != NFGS_F32 && dtype != NFGS_F64) return fail(NFGS_EINVAL, "dtype must be F32 or F64");
+    if (nz < 1 || ny < 1 || nx < 1) return fail(NFGS_EINVAL, "volume dimensions must be positive");
+    const int lo[3] = {roi6[0], roi6[2], roi6[4]}, hi[3] = {roi6[1], roi6[3], roi6[5]}, n[3] = {nz, ny, nx};
+    for (int d = 0; d < 3; ++d)
+        if (!(0 <= lo[d] && lo[d] < hi[d] && hi[d] <= n[d]))
+            return fail(NFGS_EINVAL, "Scoring box is outside the field or is empty");
+    for (int d = 0; d < 3; ++d)
+        if (!(spacing3[d] > 0.0) || !std::isfinite(spacing3[d]))
+            return fail(NFGS_EINVAL, "spacing must be positive: a scalar or (dx, dy, dz)");
+    met::Args a;
+    a.ref = ref; a.sol = sol; a.cur = cur;
+    a.nz = nz; a.ny = ny; a.nx = nx;
+    a.z0 = lo[0]; a.y0 = lo[1]; a.x0 = lo[2];
+    a.cz = hi[0] - lo[0]; a.cy = hi[1] - lo[1]; a.cx = hi[2] - lo[2];
+    a.dx = spacing3[0]; a.dy = spacing3[1]; a.dz = spacing3[2];
+    cudaStream_t s = (cudaStream_t)stream;
+    return dtype == NFGS_F32 ? field_metrics_t<float>(a, s, out) : field_metrics_t<double>(a, s, out);
 }
 
 int nfgs_get_scalars_state(void* handle, int32_t which, double* phi, double* az, double* scalars3) {

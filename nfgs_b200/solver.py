@@ -753,6 +753,24 @@ class NFGSSolverGPU:
         f = out.reshape((6,) + shape)
         return {"Bx": f[0], "By": f[1], "Bz": f[2], "Jx": f[3], "Jy": f[4], "Jz": f[5]}
 
+    def fields_to_torch(self, *, crop_to_observed_fov: bool = True):
+        """The fields of fields_to_numpy as one CUDA tensor (6, nz, ny, nx) of
+        the solver dtype -- Bx, By, Bz, Jx, Jy, Jz -- gathered on the device
+        (nfgs_fields_device); nothing is copied to the host."""
+        import torch
+
+        if not self._have_solution:
+            raise RuntimeError("No solution stored; call iterate() first.")
+        dims = (L.C.c_int32 * 3)()
+        crop = int(bool(crop_to_observed_fov))
+        code = L.NFGS_F32 if self._np_dtype == np.float32 else L.NFGS_F64
+        L.check(self._lib.nfgs_fields_device(self._h, 0, crop, None, code, dims))
+        dt = torch.float32 if code == L.NFGS_F32 else torch.float64
+        out = torch.empty((6, dims[0], dims[1], dims[2]), dtype=dt, device=f"cuda:{self._device_index}")
+        torch.cuda.current_stream(out.device).synchronize()  # the solver writes it on its own stream
+        L.check(self._lib.nfgs_fields_device(self._h, 0, crop, L.C.c_void_p(out.data_ptr()), code, dims))
+        return out
+
     def compute_source_diagnostics(self) -> dict:
         """Source-attribution diagnostics of the stored solution (nfgs_solver.py:7014-7196)."""
         if self.gaussian_separation_diagnostics is None:

@@ -129,3 +129,35 @@ def test_oracle_transforms_are_the_dense_matrices():
         np.testing.assert_allclose(S @ x, O.dst1(x, 0), rtol=1e-12, atol=1e-12)
         np.testing.assert_allclose(O.idct1(O.dct1(x, 0), 0), x, atol=1e-12)
         np.testing.assert_allclose(O.idst1(O.dst1(x, 0), 0), x, atol=1e-12)
+
+
+def test_metric_enum_matches_python_names(tmp_path):
+    from nfgs_b200.metrics import METRIC_NAMES
+
+    src = tmp_path / "met.c"
+    src.write_text('#include <stdio.h>\n#include "nfgs_b200.h"\nint main(void){printf("%d %d %d %d\\n", '
+                   'NFGS_MET_SIGMA_J_FD2, NFGS_MET_DIVB_NORM, NFGS_MET_NONFINITE_J, NFGS_MET_COUNT); return 0;}\n')
+    exe = tmp_path / "met"
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert out == [METRIC_NAMES.index("sigma_J_common_fd2"), METRIC_NAMES.index("divB_normalized"),
+                   METRIC_NAMES.index("nonfinite_J"), len(METRIC_NAMES)]
+    assert L.NFGS_MET_COUNT == len(METRIC_NAMES)
+
+
+def test_metric_regions_match_reference_helpers():
+    from nfgs_b200 import metrics as M
+    from oracle import metrics_oracle as MO
+
+    g = np.load(ROOT / "tests" / "golden" / "metrics_golden.npz")
+    assert M.flux_rope_center_from_bottom_jz(g["rope/jz0"]) == tuple(int(v) for v in g["rope/center"])
+    nz, ny, nx = g["rope/sol"].shape[1:]
+    tx, ty, tz = (int(v) for v in g["rope/test_dims"])
+    iy, ix = (int(v) for v in g["rope/center"])
+    sl = M.test_domain_slices_zyx(nz, ny, nx, iy, ix, tx, ty, tz)
+    assert [v for s in sl for v in (s.start, s.stop)] == [int(v) for v in g["rope/roi"]]
+    assert M._roi(M.fortran_box(16, 14, 12), (16, 14, 12)).tolist() == list(MO.fortran_box(16, 14, 12))
+    with pytest.raises(ValueError):
+        M._roi((slice(0, 3), slice(2, 2), slice(0, 4)), (5, 5, 5))
+    with pytest.raises(ValueError):
+        M._spacing((1.0, -1.0, 1.0))
