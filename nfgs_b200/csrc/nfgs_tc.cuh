@@ -172,8 +172,11 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 __device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// v < 2^31 and vpb < 2^31: the quotient and remainder in 32-bit arithmetic
 __device__ __forceinline__ long long vaddr(const Addr& a, long long v) {
-    return a.off + (v / a.vpb) * a.bstride + (v % a.vpb) * a.vstride;
+    const unsigned uv = (unsigned)v, up = (unsigned)a.vpb;
+    const unsigned q = uv / up, r = uv - q * up;
+    return a.off + (long long)q * a.bstride + (long long)r * a.vstride;
 }
 
 // byte offset of (vec, pair) in a data operand
@@ -230,8 +233,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     float* sp1 = sp0 + NB * TV;
     float* vdown = sp1 + NB * TV;                 // [NB][TV] output scale norm * 2^-vexp
     // producer scratch
-    float* part = vdown + NB * TV;                // [16][TV][2]
-    float* vmax = part + 32 * TV;                 // [16][TV]
+    float* part = vdown + NB * TV;                // [NPW][TV][2] (sized [16][TV][2])
+    float* vmax = part + 32 * TV;                 // [NPW][TV] (sized [16][TV])
     long long* ibase = (long long*)(vmax + 16 * TV);  // [2][TV] input base of each vector (staging buffer)
     uint64_t* bars = (uint64_t*)(ibase + 2 * TV);  // full[NB] mmad[NB] afree[NB]
     uint32_t* tslot = (uint32_t*)(bars + 3 * NB);
@@ -239,10 +242,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int ntiles = (g.nvec + TV - 1) / TV;
     const int nlocal = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-    {
-        uint4* d = (uint4*)smat;
-        for (int q = tid; q < SMEM_MAT / 16; q += NTHREADS) d[q] = g.mat[q];
-    }
     const uint32_t full0 = smem_u32(bars), mmad0 = smem_u32(bars + NB), afree0 = smem_u32(bars + 2 * NB);
     if (tid == 0) {
         for (int b = 0; b < NB; ++b) {
@@ -266,6 +265,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
 
     float* outp = g.out;
     if (g.out_table != nullptr) outp = (float*)((char*)g.out_table[*g.out_sel]);
+
+    // The matrix operands (128 KB) are copied in by the MMA and epilogue
+    // warps, which need them first at the first MMA; the producers start on
+    // the first tiles meanwhile.
+    auto load_matrices = [&]() {
+        const uint32_t d0 = smem_u32(smat);
+        for (int q = tid - NPROD; q < SMEM_MAT / 16; q += NEPI + 32) cp_async4<16>(d0 + 16u * q, g.mat + q);
+        cp_commit();
+        cp_wait0();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("bar.sync 3, %0;" ::"n"(NEPI + 32) : "memory");
+    };
 
     if (warp < NPW) {
         // ================= producers
@@ -356,9 +367,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                 psum_d += ((k + 1) & 1) ? -d : d;   // (-1)^m d_m, m = k + 1
                 lmax = fmaxf(lmax, fmaxf(fabsf(s), fabsf(d)));
             }
-            part[(kq * TV + vl) * 2 + 0] = psum_s;
-            part[(kq * TV + vl) * 2 + 1] = psum_d;
-            vmax[kq * TV + vl] = lmax;
+            // lanes l and l ^ 16 hold the same vector (pair groups kq, kq ^ 1)
+            psum_s += __shfl_xor_sync(0xffffffffu, psum_s, 16);
+            psum_d += __shfl_xor_sync(0xffffffffu, psum_d, 16);
+            lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, 16));
+            if (lane < 16) {
+                part[(warp * TV + vl) * 2 + 0] = psum_s;
+                part[(warp * TV + vl) * 2 + 1] = psum_d;
+                vmax[warp * TV + vl] = lmax;
+            }
             if (dct && kq == 0) {
                 const float x0 = okv ? X(0) : 0.f, xn = okv ? X(N - 1) : 0.f;
                 e0[b * TV + vl] = x0 + xn;
@@ -369,16 +386,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                 obase[b * TV + t] = v < g.nvec ? vaddr(g.oa, v) : -1;
             }
             bases(i + 2);
-            producer_sync();     // raw buffer b consumed, bases of tile i+2 ready
+            producer_sync();     // raw buffer b consumed, partials and bases of tile i+2 ready
             prefetch(i + 2);
-            if (t < TV) {
+            // every thread forms the scale of its own vector from the 8 warp
+            // partials (threads 0..TV-1 also publish it for the epilogue)
+            int ex = 0;
+            {
                 float m = 0.f, ss = 0.f, sd = 0.f;
-                for (int q = 0; q < NPROD / TV; ++q) {
-                    m = fmaxf(m, vmax[q * TV + t]);
-                    ss += part[(q * TV + t) * 2 + 0];
-                    sd += part[(q * TV + t) * 2 + 1];
+#pragma unroll
+                for (int q = 0; q < NPW; ++q) {
+                    m = fmaxf(m, vmax[q * TV + vl]);
+                    ss += part[(q * TV + vl) * 2 + 0];
+                    sd += part[(q * TV + vl) * 2 + 1];
                 }
-                int ex = 0;
                 if (m > 0.f) {
                     int e2;
                     frexpf(m, &e2);
@@ -386,18 +406,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                     // decayed modes hold subnormal maxima: keep 2^ex finite
                     ex = ex > 100 ? 100 : (ex < -100 ? -100 : ex);
                 }
-                const int vv = b * TV + t;
-                vexp[vv] = ex;
-                vdown[vv] = ldexpf(g.norm, -ex);
-                if (dct) {
-                    sp0[vv] = (e0[vv] + 2.f * ss) * g.norm;
-                    sp1[vv] = (e1[vv] + 2.f * sd) * g.norm;
-                    e0[vv] *= g.norm;
-                    e1[vv] *= g.norm;
+                if (t < TV) {
+                    const int vv = b * TV + t;   // t == vl here
+                    vexp[vv] = ex;
+                    vdown[vv] = ldexpf(g.norm, -ex);
+                    if (dct) {
+                        sp0[vv] = (e0[vv] + 2.f * ss) * g.norm;
+                        sp1[vv] = (e1[vv] + 2.f * sd) * g.norm;
+                        e0[vv] *= g.norm;
+                        e1[vv] *= g.norm;
+                    }
                 }
             }
-            producer_sync();
-            const float up = ldexpf(1.f, vexp[b * TV + vl]);
+            const float up = ldexpf(1.f, ex);
             unsigned char* db = sdat + b * 4 * DAT_BYTES;
             {
                 uint32_t hs[4], ls[4], hd[4], ld[4];
@@ -425,6 +446,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
         cp_wait0();
     } else if (warp == NPW + NEW) {
         // ================= MMA issuer (both axes: K-major data operands)
+        load_matrices();
         const uint32_t mat0 = smem_u32(smat), dat0 = smem_u32(sdat);
         const uint32_t idesc = (1u << 4) | ((uint32_t)(TV >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
         int issued[NB] = {0, 0, 0};
@@ -466,6 +488,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
         // that global stores are row-contiguous: axis 0 stages S[c][k - koff]
         // (vector rows), axis 1 stages S[k - koff][c ^ ((k - koff)/2 % 16)]
         // (output rows across the tile's 16 vector columns).
+        load_matrices();
         const int e = warp - NPW, q = e & 3, ch = e >> 2;
         const int j = 32 * q + lane;  // mode index within a half
         const uint32_t lanebits = (uint32_t)(32 * q) << 16;
