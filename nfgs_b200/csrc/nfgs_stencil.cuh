@@ -58,6 +58,17 @@ __device__ __forceinline__ int lift(int q, int row) {
     return q + row * (PW(h2) - PW(h)) + (h2 - h) * (PW(h2) + 1);
 }
 
+// Box geometry of a tile instance: edge tiles (E) may be up to 2 cells wider
+// and taller (the remainder of an axis), interior tiles are exactly TX x TY,
+// so their level-h boxes are (TX + 2h) x (TY + 2h) inside the same slots.
+template <bool E> __host__ __device__ constexpr int pw(int h) { return TX + (E ? 2 : 0) + 2 * h; }
+template <bool E> __host__ __device__ constexpr int rows(int h) { return TY + (E ? 2 : 0) + 2 * h; }
+template <bool E, int h, int h2>
+__device__ __forceinline__ int liftE(int q, int row) {
+    return q + row * (pw<E>(h2) - pw<E>(h)) + (h2 - h) * (pw<E>(h2) + 1);
+}
+static_assert(pw<true>(3) == PW(3) && rows<true>(3) == ROWS(3), "edge boxes fill the slots");
+
 template <typename T> constexpr size_t smem_bytes() { return (size_t)N_TOTAL * sizeof(T); }
 template <typename T> constexpr int min_blocks() { return sizeof(T) == 4 ? 2 : 1; }
 
@@ -141,8 +152,8 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
         for (int k = 0; k < nmax; ++k) {
             const int q = tid + k * NT;
             int v = -1;
-            if (q < PW(h) * ROWS(h)) {
-                const int r = q / PW(h) - h, c = q % PW(h) - h;
+            if (q < pw<EDGE>(h) * rows<EDGE>(h)) {
+                const int r = q / pw<EDGE>(h) - h, c = q % pw<EDGE>(h) - h;
                 const int jj = y0 + r, ii = x0 + c;
                 if (r < th + h && c < tw + h && jj >= 0 && jj < ny && ii >= 0 && ii < nx) v = jj * nx + ii;
             }
@@ -156,7 +167,7 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
 
     // generic accessors by global coordinates (edge cells and edge planes,
     // one-sided stencils of nfgs_solver.py:1361-1419 / 1741-1749)
-    auto OF = [&](int h, int jj, int ii) { return (jj - y0 + h) * PW(h) + (ii - x0 + h); };
+    auto OF = [&](int h, int jj, int ii) { return (jj - y0 + h) * pw<EDGE>(h) + (ii - x0 + h); };
     auto PHI = [&](int pl, int jj, int ii) -> T { return sm[O_PHI + (pl & 3) * CAP(3) + OF(3, jj, ii)]; };
     auto AZ = [&](int pl, int jj, int ii) -> T { return sm[O_AZ + (pl & 1) * CAP(2) + OF(2, jj, ii)]; };
     auto CC = [&](int pl, int comp, int jj, int ii) -> T {
@@ -216,15 +227,15 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
 #pragma unroll
         for (int k = 0; k < NL2; ++k) {
             if (G2[k] < 0) continue;
-            const int q = tid + k * NT, row = q / PW(2);
-            const int jj = y0 + row - 2, ii = x0 + (q - row * PW(2)) - 2;
+            const int q = tid + k * NT, row = q / pw<EDGE>(2);
+            const int jj = y0 + row - 2, ii = x0 + (q - row * pw<EDGE>(2)) - 2;
             T val;
             if (p == 0) {
                 val = bzobs[G2[k]] - bbg[2 * V + G2[k]];
             } else if (xy_in(jj, ii)) {
-                const T* const f = ph0 + lift<2, 3>(q, row);
+                const T* const f = ph0 + liftE<EDGE, 2, 3>(q, row);
                 const T f0 = f[0];
-                val = ((f[1] - T(2) * f0) + f[-1]) * idx2 + ((f[PW(3)] - T(2) * f0) + f[-PW(3)]) * idy2;
+                val = ((f[1] - T(2) * f0) + f[-1]) * idx2 + ((f[pw<EDGE>(3)] - T(2) * f0) + f[-pw<EDGE>(3)]) * idy2;
             } else {
                 val = lap1<T>([&](int t) { return PHI(p, jj, t); }, ii, nx) * idx2 +
                       lap1<T>([&](int t) { return PHI(p, t, ii); }, jj, ny) * idy2;
@@ -257,27 +268,27 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
 #pragma unroll
         for (int k = 0; k < NL1; ++k) {
             if (G1[k] < 0) continue;
-            const int o1 = tid + k * NT, row = o1 / PW(1);
-            const int r = row - 1, c = o1 - row * PW(1) - 1;
+            const int o1 = tid + k * NT, row = o1 / pw<EDGE>(1);
+            const int r = row - 1, c = o1 - row * pw<EDGE>(1) - 1;
             const int jj = y0 + r, ii = x0 + c;
-            const int o2 = lift<1, 2>(o1, row);
+            const int o2 = liftE<EDGE, 1, 2>(o1, row);
             const bool xin = xy_in(jj, ii);
             // carrier x, y and state J_z at plane p
             T cx, cy, jz;
             if (zin && xin) {
-                const int o3 = lift<1, 3>(o1, row);
+                const int o3 = liftE<EDGE, 1, 3>(o1, row);
                 const T* const fp = php + o3;
                 const T* const fm = phm + o3;
                 const T* const A = azs + o2;
                 auto dzp = [&](int d) -> T { return (fp[d] - fm[d]) * i2dz; };
                 T dxdz = (dzp(1) - dzp(-1)) * i2dx;
-                T dydz = (dzp(PW(3)) - dzp(-PW(3))) * i2dy;
-                T dya = (A[PW(2)] - A[-PW(2)]) * i2dy;
+                T dydz = (dzp(pw<EDGE>(3)) - dzp(-pw<EDGE>(3))) * i2dy;
+                T dya = (A[pw<EDGE>(2)] - A[-pw<EDGE>(2)]) * i2dy;
                 T dxa = (A[1] - A[-1]) * i2dx;
                 cx = -dxdz + dya;
                 cy = -dydz - dxa;
                 const T a0 = A[0];
-                jz = -(((A[1] - T(2) * a0) + A[-1]) * idx2 + ((A[PW(2)] - T(2) * a0) + A[-PW(2)]) * idy2);
+                jz = -(((A[1] - T(2) * a0) + A[-1]) * idx2 + ((A[pw<EDGE>(2)] - T(2) * a0) + A[-pw<EDGE>(2)]) * idy2);
             } else {
                 auto dzphi = [&](int j2, int i2) -> T {
                     return d1<T>([&](int kk) { return PHI(kk, j2, i2); }, p, nz, i2dz);
@@ -309,7 +320,7 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
                     const T* const zp = czp + o2;
                     const T* const z0 = czf0 + o2;
                     auto czf = [&](int d) -> T { return T(0.5) * (zp[d] + z0[d]); };
-                    jxf = (czf(PW(2)) - czf(-PW(2))) * i2dy - dby;
+                    jxf = (czf(pw<EDGE>(2)) - czf(-pw<EDGE>(2))) * i2dy - dby;
                     jyf = dbx - (czf(1) - czf(-1)) * i2dx;
                 } else {
                     auto CZF = [&](int j2, int i2) -> T { return T(0.5) * (CC(p, 2, j2, i2) + CC(f, 2, j2, i2)); };
@@ -382,8 +393,8 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
             const int o1 = tid + k * NT;
             T vx = jfx[k], vy = jfy[k], vz = jfz[k];
             if (a.o.window) {
-                const int row = o1 / PW(1);
-                const T w = win(nz - 1, y0 + row - 1, x0 + (o1 - row * PW(1)) - 1);
+                const int row = o1 / pw<EDGE>(1);
+                const T w = win(nz - 1, y0 + row - 1, x0 + (o1 - row * pw<EDGE>(1)) - 1);
                 vx = vx * w; vy = vy * w; vz = vz * w;
             }
             jc[o1] = vx;
@@ -408,7 +419,7 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
             by = bq[CAP(1)] + cq[CAP(1)];
             bz = bq[2 * CAP(1)] + czq[0];
             div = ((bq[1] + cq[1]) - (bq[-1] + cq[-1])) * i2dx +
-                  ((bq[CAP(1) + PW(1)] + cq[CAP(1) + PW(1)]) - (bq[CAP(1) - PW(1)] + cq[CAP(1) - PW(1)])) * i2dy +
+                  ((bq[CAP(1) + pw<EDGE>(1)] + cq[CAP(1) + pw<EDGE>(1)]) - (bq[CAP(1) - pw<EDGE>(1)] + cq[CAP(1) - pw<EDGE>(1)])) * i2dy +
                   ((bzp[0] + czpp[0]) - (bzm[0] + czm[0])) * i2dz;
         } else {
             bx = BB(qd, 0, jj, ii);
@@ -429,7 +440,7 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
         if (xy_in(jj, ii)) {
             const T* const jx = sm + O_JC + (cc % 3) * 3 * CAP(1) + o1;
             const T* const jy = jx + CAP(1);
-            s_b = (jx[PW(1)] - jx[-PW(1)]) * i2dy - (jy[1] - jy[-1]) * i2dx;
+            s_b = (jx[pw<EDGE>(1)] - jx[-pw<EDGE>(1)]) * i2dy - (jy[1] - jy[-1]) * i2dx;
         } else {
             s_b = d1<T>([&](int t) { return JC(cc, 0, t, ii); }, jj, ny, i2dy) -
                   d1<T>([&](int t) { return JC(cc, 1, jj, t); }, ii, nx, i2dx);
@@ -444,18 +455,18 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
         const T* const jp = sm + O_JC + ((cc + 1) % 3) * 3 * CAP(1) + o1;
         const T* const z = sm + O_JC + (cc % 3) * 3 * CAP(1) + 2 * CAP(1) + o1;
         T jz0 = z[0];
-        T lap = ((z[1] - T(2) * jz0) + z[-1]) * idx2 + ((z[PW(1)] - T(2) * jz0) + z[-PW(1)]) * idy2;
+        T lap = ((z[1] - T(2) * jz0) + z[-1]) * idx2 + ((z[pw<EDGE>(1)] - T(2) * jz0) + z[-pw<EDGE>(1)]) * idy2;
         T dxz = (((jp[1] - jm[1]) - jp[-1]) + jm[-1]) * i4xz;
-        T dyz = (((jp[CAP(1) + PW(1)] - jm[CAP(1) + PW(1)]) - jp[CAP(1) - PW(1)]) + jm[CAP(1) - PW(1)]) * i4yz;
+        T dyz = (((jp[CAP(1) + pw<EDGE>(1)] - jm[CAP(1) + pw<EDGE>(1)]) - jp[CAP(1) - pw<EDGE>(1)]) + jm[CAP(1) - pw<EDGE>(1)]) * i4yz;
         sj_out[(long long)cc * FPI + (long long)(jj - 1) * (nx - 2) + (ii - 1)] = lap - dxz - dyz;
     };
     auto loop_e = [&](int p, bool post) {
 #pragma unroll
         for (int k = 0; k < NL0; ++k) {
             if (G0[k] < 0) continue;
-            const int q = tid + k * NT, row = q / PW(0);
-            const int jj = y0 + row, ii = x0 + (q - row * PW(0));
-            const int o1 = lift<0, 1>(q, row), o2 = lift<0, 2>(q, row);
+            const int q = tid + k * NT, row = q / pw<EDGE>(0);
+            const int jj = y0 + row, ii = x0 + (q - row * pw<EDGE>(0));
+            const int o1 = liftE<EDGE, 0, 1>(q, row), o2 = liftE<EDGE, 0, 2>(q, row);
             if (post) {
                 sb_cell(nz - 1, o1, G0[k], jj, ii);
                 sj_cell(nz - 2, o1, jj, ii);
