@@ -24,14 +24,13 @@
 // level (contiguous across a warp: no bank conflicts); entries outside the
 // tile's halo or the domain are idle.
 //
-// Per plane p (three barriers):
-//   B1: plane p staged; stage plane p+1
-//   loop A (level 2): C_z(p)
-//   B2
+// Per plane p (two barriers):
+//   B1: plane p staged, C_z(p) formed; stage plane p+1
 //   loop F (level 1): C_x, C_y, J_z at p; face p-1 (current, sigma terms,
 //           alpha B); centre p-1 from faces p-2, p-1
-//   B3
+//   B2
 //   loop E (level 0): divB/|B|/|B|^2 at p-1, S_B(p-1), S_J(p-2)
+//   loop A (level 2): C_z(p+1)
 #pragma once
 #include "nfgs_iter.cuh"
 
@@ -43,8 +42,8 @@ __host__ __device__ constexpr int ROWS(int h) { return TY + 2 + 2 * h; }
 __host__ __device__ constexpr int CAP(int h) { return PW(h) * ROWS(h); }
 constexpr int O_PHI = 0;                     // 4 planes x CAP(3), slot plane&3
 constexpr int O_AZ = O_PHI + 4 * CAP(3);     // 2 planes x CAP(2), slot plane&1
-constexpr int O_CZ = O_AZ + 2 * CAP(2);      // carrier z, 3 planes x CAP(2), slot plane%3
-constexpr int O_CXY = O_CZ + 3 * CAP(2);     // carrier x,y, 3 planes x 2 x CAP(1), slot (plane%3)*2+comp
+constexpr int O_CZ = O_AZ + 2 * CAP(2);      // carrier z, 4 planes x CAP(2), slot plane&3
+constexpr int O_CXY = O_CZ + 4 * CAP(2);     // carrier x,y, 3 planes x 2 x CAP(1), slot (plane%3)*2+comp
 constexpr int O_BG = O_CXY + 6 * CAP(1);     // background, 4 planes x 3 x CAP(1), slot (plane&3)*3+comp
 constexpr int O_JC = O_BG + 12 * CAP(1);     // centre J_par, 3 x 3 x CAP(1), slot (centre%3)*3+comp
 constexpr int N_TOTAL = O_JC + 9 * CAP(1);
@@ -171,7 +170,7 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
     auto PHI = [&](int pl, int jj, int ii) -> T { return sm[O_PHI + (pl & 3) * CAP(3) + OF(3, jj, ii)]; };
     auto AZ = [&](int pl, int jj, int ii) -> T { return sm[O_AZ + (pl & 1) * CAP(2) + OF(2, jj, ii)]; };
     auto CC = [&](int pl, int comp, int jj, int ii) -> T {
-        return comp == 2 ? sm[O_CZ + (pl % 3) * CAP(2) + OF(2, jj, ii)]
+        return comp == 2 ? sm[O_CZ + (pl & 3) * CAP(2) + OF(2, jj, ii)]
                          : sm[O_CXY + ((pl % 3) * 2 + comp) * CAP(1) + OF(1, jj, ii)];
     };
     auto BG = [&](int pl, int comp, int jj, int ii) -> T {
@@ -223,7 +222,7 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
     // ---- loop A: carrier z of plane p on level 2
     auto loop_a = [&](int p) {
         const T* const ph0 = sm + O_PHI + (p & 3) * CAP(3);
-        T* const cz = sm + O_CZ + (p % 3) * CAP(2);
+        T* const cz = sm + O_CZ + (p & 3) * CAP(2);
 #pragma unroll
         for (int k = 0; k < NL2; ++k) {
             if (G2[k] < 0) continue;
@@ -258,8 +257,8 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
         const T* const phm = sm + O_PHI + ((p + 3) & 3) * CAP(3);
         const T* const php = sm + O_PHI + ((p + 1) & 3) * CAP(3);
         const T* const azs = sm + O_AZ + (p & 1) * CAP(2);
-        const T* const czp = sm + O_CZ + (p % 3) * CAP(2);
-        const T* const czf0 = sm + O_CZ + ((p + 2) % 3) * CAP(2);  // plane p-1
+        const T* const czp = sm + O_CZ + (p & 3) * CAP(2);
+        const T* const czf0 = sm + O_CZ + ((p + 3) & 3) * CAP(2);  // plane p-1
         T* const cxy = sm + O_CXY + (p % 3) * 2 * CAP(1);
         const T* const cxy0 = sm + O_CXY + ((p + 2) % 3) * 2 * CAP(1);
         const T* const bgp = sm + O_BG + ((p & 3) * 3) * CAP(1);
@@ -410,11 +409,11 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
         if (qd > 0 && qd < nz - 1 && xy_in(jj, ii)) {
             const T* const bq = sm + O_BG + ((qd & 3) * 3) * CAP(1) + o1;
             const T* const cq = sm + O_CXY + ((qd % 3) * 2) * CAP(1) + o1;
-            const T* const czq = sm + O_CZ + (qd % 3) * CAP(2) + o2;
+            const T* const czq = sm + O_CZ + (qd & 3) * CAP(2) + o2;
             const T* const bzm = sm + O_BG + (((qd + 3) & 3) * 3 + 2) * CAP(1) + o1;
             const T* const bzp = sm + O_BG + (((qd + 1) & 3) * 3 + 2) * CAP(1) + o1;
-            const T* const czm = sm + O_CZ + ((qd + 2) % 3) * CAP(2) + o2;
-            const T* const czpp = sm + O_CZ + ((qd + 1) % 3) * CAP(2) + o2;
+            const T* const czm = sm + O_CZ + ((qd + 3) & 3) * CAP(2) + o2;
+            const T* const czpp = sm + O_CZ + ((qd + 1) & 3) * CAP(2) + o2;
             bx = bq[0] + cq[0];
             by = bq[CAP(1)] + cq[CAP(1)];
             bz = bq[2 * CAP(1)] + czq[0];
@@ -484,16 +483,21 @@ __device__ __forceinline__ void stencil_body(const Args& a, unsigned char* sm_ra
     };
 
     // ---------------- the z march over planes [pstart, pend]
+    // C_z of plane p + 1 is formed in the same phase as loop E of plane p:
+    // its input Phi(p + 1) is staged with plane p, and the four-slot C_z ring
+    // keeps planes p - 2 .. p (read by loop E) apart from p + 1.
     stage_plane(pstart);
+    cp_wait_all();
+    __syncthreads();
+    loop_a(pstart);
     for (int p = pstart; p <= pend; ++p) {
         cp_wait_all();
-        __syncthreads();  // B1: plane p staged; iteration p-1 finished everywhere
+        __syncthreads();  // B1: plane p staged, C_z(p) complete; iteration p-1 finished everywhere
         if (p < pend) stage_plane(p + 1);
-        loop_a(p);
-        __syncthreads();  // B2
         loop_f(p);
-        __syncthreads();  // B3
+        __syncthreads();  // B2
         loop_e(p, false);
+        if (p < pend) loop_a(p + 1);
     }
     if (pend == nz - 1) {
         __syncthreads();
