@@ -510,13 +510,15 @@ __global__ void k_ztables(Geo g, int chain, double rho, const double* __restrict
 // ---------------------------------------------------------------------------
 __global__ void k_zero_mode(Geo g, DevCtl* ctl, const double* s00) {
     if (ctl->stopped) return;
-    if (threadIdx.x != 0) return;
+    // one warp: lane l sums planes l, l + 32, ...; then a fixed butterfly
     const double norm = 4.0 * (double)(g.nx - 1) * (double)(g.ny - 1);
     double acc = 0.0;
-    for (int p = 0; p < g.nz; ++p) {
+    for (int p = (int)threadIdx.x; p < g.nz; p += 32) {
         double v = s00[p] / norm;
         acc += v * v;
     }
+    acc = warp_sum(acc);
+    if (threadIdx.x != 0) return;
     double zr = sqrt(acc / g.nz);
     double srms = sqrt(ctl->sumsb2 / (double)g.V);
     double ratio = zr / fmax(srms, 1e-30);

@@ -691,7 +691,7 @@ __global__ void k_ctl_init(Geo g, DevCtl* c, const double* sums, double* hist) {
 }
 
 // One step of the stop rule (nfgs_solver.py:3658-3814).
-__global__ void k_ctl_step(Geo g, DevCtl* c, const double* sums, double* hist) {
+__device__ __forceinline__ void ctl_step_body(Geo g, DevCtl* c, const double* sums, double* hist) {
     if (c->stopped) { c->not_rollback = 1; return; }
     double sigma, divb, energy;
     scal_from_sums(g, sums, sigma, divb, energy);
@@ -747,6 +747,19 @@ __global__ void k_ctl_step(Geo g, DevCtl* c, const double* sums, double* hist) {
     if (!c->stopped && n >= c->max_iter) { c->stopped = 1; c->stop_reason = 1; }
     pick_cand(c);
     c->not_rollback = (c->rollback_now && !c->stopped) ? 0 : 1;
+}
+
+__global__ void k_ctl_step(Geo g, DevCtl* c, const double* sums, double* hist) { ctl_step_body(g, c, sums, hist); }
+
+// The second sum stage and the control step in one launch (iteration graph):
+// the six fixed-order sums, then thread 0 steps the controller on them.
+__global__ void k_sum_stage2_ctl(Geo g, const double* mid, double* out6, DevCtl* c, double* hist) {
+    const int col = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double t = mid[col * NCHUNK + lane] + mid[col * NCHUNK + 32 + lane];
+    t = warp_sum(t);
+    if (lane == 0) out6[col] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) ctl_step_body(g, c, out6, hist);
 }
 
 // After a rollback the restored state's sources were recomputed.
@@ -1344,9 +1357,8 @@ static int enqueue_iteration(Handle* h) {
         h->launches++;
     }
     TRY(run_stencil<T>(h, &c->cand, &c->stopped, 1, h->stop.polarity_mask));
-    sum_partials(h);
-    CK(cudaGetLastError());
-    k_ctl_step<<<1, 1, 0, h->s>>>(h->g, c, h->scal, h->hist);
+    k_sum_stage1<<<dim3(NCHUNK, 6), 256, 0, h->s>>>(h->sum_pf, h->sum_nbf, h->sum_ps, h->sum_nbs, h->scal + 8);
+    k_sum_stage2_ctl<<<1, 192, 0, h->s>>>(h->g, h->scal + 8, h->scal, c, h->hist);
     CK(cudaGetLastError());
     h->launches += 2;
     if (h->stop.adaptive_mu) {
