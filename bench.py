@@ -287,7 +287,7 @@ def run_b200(args):
         f = s2.fields_to_numpy()
         barrier_sync(pg, local)
         e2e_times.append(time.perf_counter() - t0)
-        fields_bytes = 6 * f["Bx"].size * 8
+        fields_bytes = 6 * f["Bx"].size * f["Bx"].itemsize
         del s2
     e2e_s = max_over_ranks(pg, statistics.median(e2e_times), local)
     e2e_value = cells * args.iters * world / e2e_s / 1e9

@@ -273,6 +273,17 @@ const char* nfgs_last_error(void);
 /* Library build identification (sm arch, version). */
 const char* nfgs_version(void);
 
+/* Device memory of every solver handle (state, tables, set-up scratch)
+ * comes from one stream-ordered memory pool per device that keeps freed
+ * memory reserved, so creating and destroying solvers does not pay
+ * cudaMalloc / cudaFree after the first one; device-to-host staging uses
+ * pinned chunks shared by the process.  This call hands the reserved device
+ * memory of `device` and the idle pinned chunks back (after a device
+ * synchronisation).  No reference counterpart: the reference's PyTorch
+ * tensors come from torch's caching allocator, whose equivalent is
+ * torch.cuda.empty_cache(). */
+int nfgs_release_cached_memory(int32_t device);
+
 /* Batched scan (the reference runs its weight x rho sweeps as a serial loop
  * of solves, run_nfgs_td_robin_weight_sweep.py:510-660): handles that have
  * each been through nfgs_iterate_begin (graph mode) are advanced together.

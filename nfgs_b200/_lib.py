@@ -112,6 +112,7 @@ SIGNATURES = {
     "nfgs_destroy": (C.c_int, [_P]),
     "nfgs_last_error": (C.c_char_p, []),
     "nfgs_version": (C.c_char_p, []),
+    "nfgs_release_cached_memory": (C.c_int, [C.c_int32]),
     "nfgs_scan_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
     "nfgs_scan_launch": (C.c_int, [_P, _IP]),
     "nfgs_scan_destroy": (C.c_int, [_P]),

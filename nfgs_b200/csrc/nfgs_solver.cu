@@ -143,31 +143,80 @@ struct Handle {
     int fs_tuned = 0;          // the fused-stencil segment count has been tuned
     long long pface_len = 0;   // doubles in pface
     int advanced = 0;          // the current iteration has taken a step
-    void* pin[2] = {nullptr, nullptr};
     cudaEvent_t pin_ev[2] = {nullptr, nullptr};
 };
 
+// Device memory of every handle comes from one stream-ordered pool per
+// device whose release threshold keeps freed memory reserved (as torch's
+// caching allocator does), so creating and destroying solvers and the
+// set-up's scratch buffers cost no cudaMalloc / cudaFree device
+// synchronisation after first use; nfgs_release_cached_memory returns it.
+static std::mutex g_pool_mu;
+static std::map<int, cudaMemPool_t> g_pools;
+
+static int device_pool(int dev, cudaMemPool_t* out) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    auto it = g_pools.find(dev);
+    if (it != g_pools.end()) { *out = it->second; return NFGS_OK; }
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    CK(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pools[dev] = pool;
+    *out = pool;
+    return NFGS_OK;
+}
+
+// Allocation on the handle's stream, complete on return (usable from any
+// stream, including the synchronous copies of the set-up).
 template <typename T>
 static int alloc(Handle* h, T** p, size_t bytes) {
     void* q = nullptr;
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(&q, bytes);
-    if (e != cudaSuccess) return fail(NFGS_ENOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    cudaMemPool_t pool;
+    TRY(device_pool(h->geom.device, &pool));
+    cudaError_t e = cudaMallocFromPoolAsync(&q, bytes, pool, h->s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->s);
+    if (e != cudaSuccess) return fail(NFGS_ENOMEM, std::string("device allocation failed: ") + cudaGetErrorString(e));
     h->owned.push_back({q, bytes});
     *p = (T*)q;
     return NFGS_OK;
 }
 
+// 32 MB pinned host chunks for device-to-host staging, shared by every
+// handle of the process (pinning costs milliseconds per chunk).
+constexpr size_t PIN_CHUNK = (size_t)32 << 20;
+static std::mutex g_pin_mu;
+static std::vector<void*> g_pin_free;
+
+static int pin_acquire(void** p) {
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        if (!g_pin_free.empty()) { *p = g_pin_free.back(); g_pin_free.pop_back(); return NFGS_OK; }
+    }
+    CK(cudaHostAlloc(p, PIN_CHUNK, cudaHostAllocDefault));
+    return NFGS_OK;
+}
+static void pin_release(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_free.push_back(p);
+}
+
 static void free_all(Handle* h) {
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);
-    for (auto& b : h->owned) cudaFree(b.p);
+    for (auto& b : h->owned) cudaFreeAsync(b.p, h->s);
     h->owned.clear();
+    if (h->s) cudaStreamSynchronize(h->s);
     if (h->ctl_h) cudaFreeHost(h->ctl_h);
-    for (int q = 0; q < 2; ++q) {
-        if (h->pin[q]) cudaFreeHost(h->pin[q]);
+    for (int q = 0; q < 2; ++q)
         if (h->pin_ev[q]) cudaEventDestroy(h->pin_ev[q]);
-    }
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->s) cudaStreamDestroy(h->s);
@@ -1263,7 +1312,7 @@ static int setup_boundary(Handle* h, const double* bx_h, const double* by_h, con
         for (auto it = h->owned.begin(); it != h->owned.end();) {
             bool d = false;
             for (void* p : drop) d = d || (it->p == p);
-            if (d) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+            if (d) { cudaFreeAsync(it->p, h->s); it = h->owned.erase(it); } else ++it;
         }
     }
     if (diag) std::memcpy(diag, dg, sizeof dg);
@@ -1334,7 +1383,7 @@ static int build_constants(Handle* h) {
     }
     CK(cudaStreamSynchronize(s));
     for (auto it = h->owned.begin(); it != h->owned.end();) {
-        if (it->p == tmp || it->p == tmp2 || it->p == azb_t) { cudaFree(it->p); it = h->owned.erase(it); }
+        if (it->p == tmp || it->p == tmp2 || it->p == azb_t) { cudaFreeAsync(it->p, h->s); it = h->owned.erase(it); }
         else ++it;
     }
     return NFGS_OK;
@@ -1441,7 +1490,7 @@ static int iterate_begin_t(Handle* h, const NfgsStop* stop) {
     if (rows > h->hist_rows) {
         if (h->hist) {
             for (auto it = h->owned.begin(); it != h->owned.end();) {
-                if (it->p == h->hist) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+                if (it->p == h->hist) { cudaFreeAsync(it->p, h->s); it = h->owned.erase(it); } else ++it;
             }
         }
         TRY(alloc(h, &h->hist, (size_t)rows * NFGS_HCOLS * 8));
@@ -1774,22 +1823,27 @@ static void host_copy(char* dst, const char* src, size_t len) {
 // Copy n bytes from device memory to pageable host memory through two pinned
 // chunks: the DMA of chunk k overlaps the host copy of chunk k-1.
 static int d2h_chunked(Handle* h, void* host, const void* dev, size_t n) {
-    const size_t CH = (size_t)32 << 20;
+    const size_t CH = PIN_CHUNK;
+    struct Pins {
+        void* p[2] = {nullptr, nullptr};
+        ~Pins() { pin_release(p[0]); pin_release(p[1]); }
+    } pins;
     for (int q = 0; q < 2; ++q) {
-        if (!h->pin[q]) CK(cudaHostAlloc(&h->pin[q], CH, cudaHostAllocDefault));
+        TRY(pin_acquire(&pins.p[q]));
         if (!h->pin_ev[q]) CK(cudaEventCreateWithFlags(&h->pin_ev[q], cudaEventDisableTiming));
     }
+    void* const* pin = pins.p;
     const size_t nch = (n + CH - 1) / CH;
     for (size_t k = 0; k <= nch; ++k) {
         if (k < nch) {
             const size_t off = k * CH, len = std::min(CH, n - off);
-            CK(cudaMemcpyAsync(h->pin[k & 1], (const char*)dev + off, len, cudaMemcpyDeviceToHost, h->s));
+            CK(cudaMemcpyAsync(pin[k & 1], (const char*)dev + off, len, cudaMemcpyDeviceToHost, h->s));
             CK(cudaEventRecord(h->pin_ev[k & 1], h->s));
         }
         if (k >= 1) {
             const size_t kp = k - 1, off = kp * CH, len = std::min(CH, n - off);
             CK(cudaEventSynchronize(h->pin_ev[kp & 1]));
-            host_copy((char*)host + off, (const char*)h->pin[kp & 1], len);
+            host_copy((char*)host + off, (const char*)pin[kp & 1], len);
         }
     }
     return NFGS_OK;
@@ -1834,7 +1888,7 @@ static int fields_t(Handle* h, int which, int crop, void* out, int odtype, int32
     if (bytes > h->fbuf_bytes) {
         if (h->fbuf) {
             for (auto it = h->owned.begin(); it != h->owned.end();) {
-                if (it->p == h->fbuf) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+                if (it->p == h->fbuf) { cudaFreeAsync(it->p, h->s); it = h->owned.erase(it); } else ++it;
             }
             h->fbuf = nullptr;
             h->fbuf_bytes = 0;
@@ -1987,7 +2041,7 @@ static int gaussian_above_impl(Handle* h, double* out) {
         out[2 * P + q] = c[q];
     }
     for (auto it = h->owned.begin(); it != h->owned.end();) {
-        if (it->p == w) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+        if (it->p == w) { cudaFreeAsync(it->p, h->s); it = h->owned.erase(it); } else ++it;
     }
     return NFGS_OK;
 }
@@ -2086,7 +2140,7 @@ static int source_diag_t(Handle* h, double* out) {
     }
     std::memcpy(out, res, sizeof res);
     for (auto it = h->owned.begin(); it != h->owned.end();) {
-        if (it->p == w) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+        if (it->p == w) { cudaFreeAsync(it->p, h->s); it = h->owned.erase(it); } else ++it;
     }
     return NFGS_OK;
 }
@@ -2166,7 +2220,7 @@ static int apply_transform_t(Handle* h, int chain, int inverse, const double* in
             CK(cudaMemcpyAsync(out, tmp, n * 8, cudaMemcpyDeviceToHost, h->s));
             CK(cudaStreamSynchronize(h->s));
             for (auto it = h->owned.begin(); it != h->owned.end();) {
-                if (it->p == tmp) { cudaFree(it->p); it = h->owned.erase(it); } else ++it;
+                if (it->p == tmp) { cudaFreeAsync(it->p, h->s); it = h->owned.erase(it); } else ++it;
             }
             return NFGS_OK;
         }
@@ -2463,6 +2517,23 @@ extern "C" {
 const char* nfgs_last_error(void) { return g_err.c_str(); }
 
 const char* nfgs_version(void) { return "nfgs_b200 0.1 (sm_100a)"; }
+
+int nfgs_release_cached_memory(int32_t device) {
+    g_err.clear();
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        auto it = g_pools.find(device);
+        if (it != g_pools.end()) {
+            CK(cudaSetDevice(device));
+            CK(cudaDeviceSynchronize());
+            CK(cudaMemPoolTrimTo(it->second, 0));
+        }
+    }
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    for (void* p : g_pin_free) cudaFreeHost(p);
+    g_pin_free.clear();
+    return NFGS_OK;
+}
 
 int nfgs_create(const NfgsGeom* geom, const NfgsParams* params, void** handle_out) {
     g_err.clear();
