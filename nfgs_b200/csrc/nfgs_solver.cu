@@ -134,6 +134,7 @@ struct Handle {
     bool tc_on = false;
     void* tc_img[4] = {nullptr, nullptr, nullptr, nullptr};  // dct_x, dct_y, dst_x, dst_y
     int tc_px = 0, tc_py = 0, tc_nsm = 0;
+    bool tc_wide[4] = {false, false, false, false};  // 128 < P <= 256: four-role kernel
     int* tc_err = nullptr;
     std::vector<void*> setup_scratch;  // freed at the end of a boundary set-up
     // field export: persistent device gather buffer and two pinned chunks
@@ -396,6 +397,38 @@ static std::vector<uint16_t> tc_image(int kind, int n, int P) {
     return img;
 }
 
+// Wide image (128 < P <= 256): four roles r = 2 h + mb, each the 128 x 256
+// slice (modes 128 mb .. +127 of half h, all pairs) in K-major core-matrix
+// layout (8-row groups 4096 B apart), [hi 64 KB | lo 64 KB] per role.
+static std::vector<uint16_t> tc_image_wide(int kind, int n, int P) {
+    const size_t per = (size_t)128 * tc::PW_K;   // halves per hi (or lo) slice
+    std::vector<uint16_t> img(4 * 2 * per, 0);
+    const int period = kind == 0 ? n - 1 : n + 1;
+    for (int r = 0; r < 4; ++r) {
+        const int h = r >> 1, mb = r & 1;
+        for (int jl = 0; jl < 128; ++jl)
+            for (int k = 0; k < tc::PW_K; ++k) {
+                const int j = 128 * mb + jl;
+                double val = 0.0;
+                if (j < P && k < P) {
+                    const long long m = k + 1;
+                    long long kk;
+                    if (kind == 0) kk = (h == 0) ? 2 * j + 2 : 2 * j + 1;
+                    else kk = (h == 0) ? 2 * j + 1 : 2 * j + 2;
+                    const long long a = (kk * m) % (2LL * period);
+                    val = kind == 0 ? 2.0 * std::cos(M_PI * (double)a / period)
+                                    : 2.0 * std::sin(M_PI * (double)a / period);
+                }
+                __half hi = __float2half_rn((float)val);
+                __half lo = __float2half_rn((float)(val - (double)__half2float(hi)));
+                const size_t off = ((size_t)(jl / 8) * 4096 + (size_t)(k / 8) * 128 + (jl % 8) * 16 + (k % 8) * 2) / 2;
+                img[(size_t)r * 2 * per + off] = *(uint16_t*)&hi;
+                img[(size_t)r * 2 * per + per + off] = *(uint16_t*)&lo;
+            }
+    }
+    return img;
+}
+
 // Fused stencil plan: 32 x 8 column tiles and z segments of about 16
 // planes.  A CTA is latency-bound on its plane-to-plane chain, so more
 // resident and queued CTAs raise throughput until the three halo planes each
@@ -434,17 +467,25 @@ static int tc_setup(Handle* h) {
     const int nx = h->g.nx, ny = h->g.ny;
     if (!h->f32 || (nx % 2) || (ny % 2)) return NFGS_OK;
     const int px = (nx - 2) / 2, py = (ny - 2) / 2;
-    if (px < 1 || py < 1 || px > tc::PP || py > tc::PP) return NFGS_OK;
+    if (px < 1 || py < 1 || px > tc::PW_K || py > tc::PW_K) return NFGS_OK;
+    // Above 128 pairs the four-role kernel is 3.4x faster per transform, but an
+    // FP32 solve of a 514^2 x 257 quadrupole through it stalls at a higher
+    // sigma_J than through the SIMT contractions (0.36-0.42 vs 0.32-0.38), so
+    // it is used only on request.
+    if ((px > tc::PP || py > tc::PP) && getenv("NFGS_TC_WIDE") == nullptr) return NFGS_OK;
     if (getenv("NFGS_DISABLE_TC") != nullptr) return NFGS_OK;
     int dev = 0, nsm = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaFuncSetAttribute(tc::k_tc_transform, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_TOTAL));
+    CK(cudaFuncSetAttribute(tc::k_tc_transform<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_TOTAL));
+    CK(cudaFuncSetAttribute(tc::k_tc_transform<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_TOTAL));
+    if (nsm < 4) return NFGS_OK;
     const int kinds[4] = {0, 0, 1, 1};
     const int lens[4] = {nx, ny, nx - 2, ny - 2};
     const int ps[4] = {px, py, px, py};
     for (int q = 0; q < 4; ++q) {
-        auto img = tc_image(kinds[q], lens[q], ps[q]);
+        h->tc_wide[q] = ps[q] > tc::PP;
+        auto img = h->tc_wide[q] ? tc_image_wide(kinds[q], lens[q], ps[q]) : tc_image(kinds[q], lens[q], ps[q]);
         TRY(alloc(h, &h->tc_img[q], img.size() * 2));
         CK(cudaMemcpy(h->tc_img[q], img.data(), img.size() * 2, cudaMemcpyHostToDevice));
     }
@@ -479,8 +520,14 @@ static int tc_launch(Handle* h, int which, int inverse, const float* in, tc::Add
     a.skip = skip;
     a.err = h->tc_err;
     const int ntiles = (nvec + tc::TV - 1) / tc::TV;
-    const int grid = std::min(ntiles, h->tc_nsm);
-    tc::k_tc_transform<<<grid, tc::NTHREADS, tc::SMEM_TOTAL, h->s>>>(a);
+    if (h->tc_wide[which]) {
+        // four roles per tile group: one CTA per SM in groups of four
+        const int grid = 4 * std::min(ntiles, h->tc_nsm / 4);
+        tc::k_tc_transform<true><<<grid, tc::NTHREADS, tc::SMEM_TOTAL, h->s>>>(a);
+    } else {
+        const int grid = std::min(ntiles, h->tc_nsm);
+        tc::k_tc_transform<false><<<grid, tc::NTHREADS, tc::SMEM_TOTAL, h->s>>>(a);
+    }
     CK(cudaGetLastError());
     h->launches++;
     return NFGS_OK;

@@ -15,7 +15,11 @@
 // vector is scaled by its own power of two (undone exactly per output
 // column) and split into FP16 hi + lo; the matrix (|entries| <= 2) is split
 // likewise; three products hi*hi + hi*lo + lo*hi per K step give ~2^-21
-// relative error per product against the vector's maximum.
+// relative error per product against the vector's maximum.  The tensor
+// core's internal accumulation does not round to nearest, so long running
+// sums drift: the hi*hi products accumulate in chunks of 64 pairs and the
+// correction products apart, each in its own TMEM accumulator, and the
+// epilogue adds them in FP32.
 //
 // One persistent CTA per SM, warp-specialised and pipelined (NB = 3 tiles
 // between operand build and epilogue):
@@ -54,6 +58,22 @@ constexpr int SMEM_STG = 2 * STG_FLOATS * 4;  // double-buffered raw tiles: 33.9
 constexpr int SMEM_AUX = 8 * 1024;            // per-vector scalars, partial sums, barriers
 constexpr int SMEM_TOTAL = SMEM_MAT + SMEM_DAT + SMEM_STG + SMEM_AUX;
 constexpr long long WAIT_LIMIT = 1LL << 22;   // mbarrier polls before giving up
+// Wide transforms (128 < P <= 256 pairs): four CTA roles (half, 128-mode
+// block), each holding its 128 x 256 slice of one half's matrix (hi, lo:
+// 128 KB) and contracting all 256 pairs of that half; one raw staging buffer
+// of 16 rows of up to 514 elements.
+constexpr int PW_K = 256;                     // K extent of the wide layout
+// TMEM accumulators per operand buffer (columns of TV = 16): the hi x hi
+// products accumulate in chunks of KC_STEPS K-steps (64 pairs), one
+// accumulator each, and the correction products in their own; the
+// epilogue adds them in FP32.  Normal: 2 halves x (2 chunks + 1); wide:
+// 4 chunks + 1.
+constexpr int KC_STEPS = 4;
+constexpr int ACC_COLS = 6 * TV;              // columns per buffer (96)
+constexpr int TMEM_COLS = 512;                // allocation (NB * ACC_COLS = 288 used)
+static_assert(NB * ACC_COLS <= TMEM_COLS, "accumulators fit the TMEM allocation");
+constexpr int STG_PITCH_W = 2 * PW_K + 10;    // wide axis-0 staging pitch (fits the staging area once)
+static_assert(TV * STG_PITCH_W <= 2 * TV * STG_PITCH, "wide staging fits");
 
 // Vector / element addressing: addr(v, m) = (v / vpb) * bstride + (v % vpb) * vstride + m * estride
 struct Addr {
@@ -187,6 +207,11 @@ __device__ __forceinline__ uint32_t dat_off(int axis, int v, int k) {
                      : (uint32_t)((k >> 3) * (TV * 16) + (v >> 3) * 128 + (k & 7) * 16 + (v & 7) * 2);
 }
 
+// byte offset of (vec, pair) in a wide K-major data operand (256 pairs)
+__device__ __forceinline__ uint32_t dat_off_w(int v, int k) {
+    return (uint32_t)((v >> 3) * 4096 + (k >> 3) * 128 + (v & 7) * 16 + (k & 7) * 2);
+}
+
 __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
 }
@@ -217,6 +242,7 @@ __device__ __forceinline__ void split_h(float x, __half& hi, __half& lo) {
     lo = __float2half_rn(x - __half2float(hi));
 }
 
+template <bool WIDE>
 __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     extern __shared__ __align__(1024) unsigned char smem[];
     if (g.skip != nullptr && *g.skip) return;
@@ -240,8 +266,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     uint32_t* tslot = (uint32_t*)(bars + 3 * NB);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // tile group of this CTA (wide: four consecutive CTAs, one per role, take
+    // the same tiles, so the input they share is read from L2 after the first)
+    const int grp = WIDE ? (int)(blockIdx.x >> 2) : (int)blockIdx.x;
+    const int ngrp = WIDE ? (int)(gridDim.x >> 2) : (int)gridDim.x;
+    const int role = WIDE ? (int)(blockIdx.x & 3) : 0;
+    const int hh = role >> 1, mb = role & 1;    // wide: matrix half and 128-mode block
     const int ntiles = (g.nvec + TV - 1) / TV;
-    const int nlocal = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int nlocal = grp < ntiles ? (ntiles - 1 - grp) / ngrp + 1 : 0;
     const uint32_t full0 = smem_u32(bars), mmad0 = smem_u32(bars + NB), afree0 = smem_u32(bars + 2 * NB);
     if (tid == 0) {
         for (int b = 0; b < NB; ++b) {
@@ -252,7 +284,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     if (warp == NPW + NEW) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(smem_u32(tslot)));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "n"(TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -271,7 +304,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     // the first tiles meanwhile.
     auto load_matrices = [&]() {
         const uint32_t d0 = smem_u32(smat);
-        for (int q = tid - NPROD; q < SMEM_MAT / 16; q += NEPI + 32) cp_async4<16>(d0 + 16u * q, g.mat + q);
+        const uint4* src = g.mat + (size_t)role * (SMEM_MAT / 16);
+        for (int q = tid - NPROD; q < SMEM_MAT / 16; q += NEPI + 32) cp_async4<16>(d0 + 16u * q, src + q);
         cp_commit();
         cp_wait0();
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -288,16 +322,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
         // written by threads 0..TV-1 ahead of a producer barrier
         auto bases = [&](int i) {
             if (t < TV) {
-                const long long v = (long long)(blockIdx.x + (long long)i * gridDim.x) * TV + t;
+                const long long v = (long long)(grp + (long long)i * ngrp) * TV + t;
                 ibase[(i & 1) * TV + t] = (i < nlocal && v < g.nvec) ? vaddr(g.ia, v) : -1;
             }
         };
         // 8-byte copies when every axis-0 row starts on an 8-byte boundary
         const bool pairs8 = g.axis == 0 && g.ia.estride == 1 && ((uintptr_t)g.in & 7) == 0 &&
                             (g.ia.off & 1) == 0 && (g.ia.bstride & 1) == 0 && (g.ia.vstride & 1) == 0;
+        constexpr int SP = WIDE ? STG_PITCH_W : STG_PITCH;   // axis-0 staging pitch
+        auto stg_buf = [&](int i) { return WIDE ? 0 : (i & 1); };
         auto prefetch = [&](int i) {
             if (i < nlocal) {
-                const uint32_t dst = stg0 + (uint32_t)((i & 1) * STG_FLOATS * 4);
+                const uint32_t dst = stg0 + (uint32_t)(stg_buf(i) * STG_FLOATS * 4);
                 const long long* ib = ibase + (i & 1) * TV;
                 if (g.axis == 0) {
                     // warp w: rows (TV/NPW) w ..., lanes along the row
@@ -307,7 +343,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                         const long long base = ib[r];
                         if (base < 0) continue;
                         const float* src = g.in + base;
-                        const uint32_t drow = dst + (uint32_t)(r * STG_PITCH * 4);
+                        const uint32_t drow = dst + (uint32_t)(r * SP * 4);
                         if (pairs8) {
                             for (int m2 = lane; 2 * m2 < N; m2 += 32) cp_async4<8>(drow + 8u * m2, src + 2 * m2);
                         } else {
@@ -332,40 +368,60 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             cp_commit();
         };
         bases(0);
-        bases(1);
+        if (!WIDE) bases(1);
         producer_sync();
         prefetch(0);
-        prefetch(1);
+        if (!WIDE) prefetch(1);
         const int vl = t & 15, kq = t >> 4;
         for (int i = 0; i < nlocal && !failed; ++i) {
             const int b = i % NB, u = i / NB;
-            const long long v0 = (long long)(blockIdx.x + (long long)i * gridDim.x) * TV;
+            const long long v0 = (long long)(grp + (long long)i * ngrp) * TV;
             const bool ok_free = u < 1 || mbar_wait(afree0 + 8 * b, (u - 1) & 1);
             if (role_any<1>(!ok_free)) { failed = true; break; }
-            cp_wait1();          // the group of tile i has landed (tile i+1 may be in flight)
+            if (WIDE) cp_wait0();   // the group of tile i has landed (one staging buffer)
+            else cp_wait1();        // the group of tile i has landed (tile i+1 may be in flight)
             producer_sync();
-            const float* raw = stg + (i & 1) * STG_FLOATS;
+            const float* raw = stg + stg_buf(i) * STG_FLOATS;
             const bool okv = v0 + vl < g.nvec;
             auto X = [&](int m) -> float {
-                return g.axis == 0 ? raw[vl * STG_PITCH + m] : raw[m * TV + vl];
+                return g.axis == 0 ? raw[vl * SP + m] : raw[m * TV + vl];
             };
-            // pair sums / differences: vector vl, pair group kg = kq (8 pairs)
+            // normal: pair sums sv / differences dv of vector vl, pairs 8 kq .. 8 kq + 7;
+            // wide: the values of half hh (sums or differences), pairs 16 kq .. 16 kq + 15
+            // in sv (first 8) and dv (last 8)
             float sv[8], dv[8];
             float psum_s = 0.f, psum_d = 0.f, lmax = 0.f;
+            if constexpr (!WIDE) {
 #pragma unroll
-            for (int tt = 0; tt < 8; ++tt) {
-                const int k = 8 * kq + tt;  // pair index, m = k + 1 (DCT)
-                float a = 0.f, c = 0.f;
-                if (okv && k < P) {
-                    a = X(dct ? k + 1 : k);
-                    c = X(dct ? N - 2 - k : N - 1 - k);
+                for (int tt = 0; tt < 8; ++tt) {
+                    const int k = 8 * kq + tt;  // pair index, m = k + 1 (DCT)
+                    float a = 0.f, c = 0.f;
+                    if (okv && k < P) {
+                        a = X(dct ? k + 1 : k);
+                        c = X(dct ? N - 2 - k : N - 1 - k);
+                    }
+                    const float s = a + c, d = a - c;
+                    sv[tt] = s;
+                    dv[tt] = d;
+                    psum_s += s;
+                    psum_d += ((k + 1) & 1) ? -d : d;   // (-1)^m d_m, m = k + 1
+                    lmax = fmaxf(lmax, fmaxf(fabsf(s), fabsf(d)));
                 }
-                const float s = a + c, d = a - c;
-                sv[tt] = s;
-                dv[tt] = d;
-                psum_s += s;
-                psum_d += ((k + 1) & 1) ? -d : d;   // (-1)^m d_m, m = k + 1
-                lmax = fmaxf(lmax, fmaxf(fabsf(s), fabsf(d)));
+            } else {
+#pragma unroll
+                for (int tt = 0; tt < 16; ++tt) {
+                    const int k = 16 * kq + tt;
+                    float a = 0.f, c = 0.f;
+                    if (okv && k < P) {
+                        a = X(dct ? k + 1 : k);
+                        c = X(dct ? N - 2 - k : N - 1 - k);
+                    }
+                    const float w = hh == 0 ? a + c : a - c;
+                    if (tt < 8) sv[tt] = w;
+                    else dv[tt - 8] = w;
+                    psum_s += (hh == 0 || !((k + 1) & 1)) ? w : -w;   // sum s_m, or sum (-1)^m d_m
+                    lmax = fmaxf(lmax, fabsf(w));
+                }
             }
             // lanes l and l ^ 16 hold the same vector (pair groups kq, kq ^ 1)
             psum_s += __shfl_xor_sync(0xffffffffu, psum_s, 16);
@@ -378,16 +434,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             }
             if (dct && kq == 0) {
                 const float x0 = okv ? X(0) : 0.f, xn = okv ? X(N - 1) : 0.f;
-                e0[b * TV + vl] = x0 + xn;
+                // wide: e0 holds the end term of this role's half
+                e0[b * TV + vl] = (WIDE && hh == 1) ? x0 - xn : x0 + xn;
                 e1[b * TV + vl] = x0 - xn;
             }
             if (t < TV) {
                 const long long v = v0 + t;
                 obase[b * TV + t] = v < g.nvec ? vaddr(g.oa, v) : -1;
             }
-            bases(i + 2);
-            producer_sync();     // raw buffer b consumed, partials and bases of tile i+2 ready
-            prefetch(i + 2);
+            bases(i + (WIDE ? 1 : 2));
+            producer_sync();     // raw buffer consumed, partials and bases of the next prefetch ready
+            prefetch(i + (WIDE ? 1 : 2));
             // every thread forms the scale of its own vector from the 8 warp
             // partials (threads 0..TV-1 also publish it for the epilogue)
             int ex = 0;
@@ -411,6 +468,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                     vexp[vv] = ex;
                     vdown[vv] = ldexpf(g.norm, -ex);
                     if (dct) {
+                        // wide: sp0 is X_0 (half 0) or X_{N-1} (half 1) of this role
                         sp0[vv] = (e0[vv] + 2.f * ss) * g.norm;
                         sp1[vv] = (e1[vv] + 2.f * sd) * g.norm;
                         e0[vv] *= g.norm;
@@ -420,7 +478,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             }
             const float up = ldexpf(1.f, ex);
             unsigned char* db = sdat + b * 4 * DAT_BYTES;
-            {
+            if constexpr (!WIDE) {
                 uint32_t hs[4], ls[4], hd[4], ld[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
@@ -439,6 +497,26 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                 *(uint4*)(db + 1 * DAT_BYTES + o) = make_uint4(ls[0], ls[1], ls[2], ls[3]);
                 *(uint4*)(db + 2 * DAT_BYTES + o) = make_uint4(hd[0], hd[1], hd[2], hd[3]);
                 *(uint4*)(db + 3 * DAT_BYTES + o) = make_uint4(ld[0], ld[1], ld[2], ld[3]);
+            } else {
+                // K-major, 256 pairs: [hi 8 KB | lo 8 KB]; pairs 16 kq .. +7 from sv, +8 .. +15 from dv
+                uint32_t h0[4], l0[4], h1[4], l1[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    __half a0, a1, b0, b1;
+                    split_h(sv[2 * q] * up, a0, b0);
+                    split_h(sv[2 * q + 1] * up, a1, b1);
+                    h0[q] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
+                    l0[q] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
+                    split_h(dv[2 * q] * up, a0, b0);
+                    split_h(dv[2 * q + 1] * up, a1, b1);
+                    h1[q] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
+                    l1[q] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
+                }
+                const uint32_t o0 = dat_off_w(vl, 16 * kq), o1 = dat_off_w(vl, 16 * kq + 8);
+                *(uint4*)(db + o0) = make_uint4(h0[0], h0[1], h0[2], h0[3]);
+                *(uint4*)(db + 2 * DAT_BYTES + o0) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
+                *(uint4*)(db + o1) = make_uint4(h1[0], h1[1], h1[2], h1[3]);
+                *(uint4*)(db + 2 * DAT_BYTES + o1) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_arrive(full0 + 8 * b);
@@ -457,20 +535,43 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             if (!__all_sync(0xffffffffu, ok)) { failed = true; break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (lane == 0) {
+                if constexpr (!WIDE) {
 #pragma unroll 1
-                for (int h = 0; h < 2; ++h) {
-                    const uint32_t acc = tbase + (uint32_t)(b * 2 * TV + h * TV);
-                    const uint32_t mh = mat0 + (uint32_t)(2 * h) * MAT_BYTES, ml = mh + MAT_BYTES;
-                    const uint32_t dh = dat0 + (uint32_t)(b * 4 + 2 * h) * DAT_BYTES, dl = dh + DAT_BYTES;
+                    for (int h = 0; h < 2; ++h) {
+                        // hi x hi in chunks of KC_STEPS K-steps (columns (2h + chunk) TV),
+                        // the correction products at (4 + h) TV
+                        const uint32_t accb = tbase + (uint32_t)(b * ACC_COLS + 2 * h * TV);
+                        const uint32_t acc2 = tbase + (uint32_t)(b * ACC_COLS + (4 + h) * TV);
+                        const uint32_t mh = mat0 + (uint32_t)(2 * h) * MAT_BYTES, ml = mh + MAT_BYTES;
+                        const uint32_t dh = dat0 + (uint32_t)(b * 4 + 2 * h) * DAT_BYTES, dl = dh + DAT_BYTES;
 #pragma unroll 1
-                    for (int ks = 0; ks < PP / 16; ++ks) {
-                        const uint64_t a_hi = sdesc(mh + 256u * ks, 128u, 2048u);
-                        const uint64_t a_lo = sdesc(ml + 256u * ks, 128u, 2048u);
-                        const uint64_t b_hi = sdesc(dh + 256u * ks, 128u, 2048u);
-                        const uint64_t b_lo = sdesc(dl + 256u * ks, 128u, 2048u);
-                        mma_f16(acc, a_hi, b_hi, idesc, ks > 0 ? 1u : 0u);
-                        mma_f16(acc, a_hi, b_lo, idesc, 1u);
-                        mma_f16(acc, a_lo, b_hi, idesc, 1u);
+                        for (int ks = 0; ks < PP / 16; ++ks) {
+                            const uint64_t a_hi = sdesc(mh + 256u * ks, 128u, 2048u);
+                            const uint64_t a_lo = sdesc(ml + 256u * ks, 128u, 2048u);
+                            const uint64_t b_hi = sdesc(dh + 256u * ks, 128u, 2048u);
+                            const uint64_t b_lo = sdesc(dl + 256u * ks, 128u, 2048u);
+                            mma_f16(accb + (uint32_t)((ks / KC_STEPS) * TV), a_hi, b_hi, idesc,
+                                    (ks % KC_STEPS) > 0 ? 1u : 0u);
+                            mma_f16(acc2, a_hi, b_lo, idesc, ks > 0 ? 1u : 0u);
+                            mma_f16(acc2, a_lo, b_hi, idesc, 1u);
+                        }
+                    }
+                } else {
+                    // this role's 128 x 256 slice [hi 64 KB | lo 64 KB] against 256 pairs;
+                    // hi x hi in one accumulator, the two correction products in a second
+                    const uint32_t accb = tbase + (uint32_t)(b * ACC_COLS), acc2 = accb + 4 * TV;
+                    const uint32_t mh = mat0, ml = mat0 + 2 * MAT_BYTES;
+                    const uint32_t dh = dat0 + (uint32_t)(b * 4) * DAT_BYTES, dl = dh + 2 * DAT_BYTES;
+#pragma unroll 1
+                    for (int ks = 0; ks < PW_K / 16; ++ks) {
+                        const uint64_t a_hi = sdesc(mh + 256u * ks, 128u, 4096u);
+                        const uint64_t a_lo = sdesc(ml + 256u * ks, 128u, 4096u);
+                        const uint64_t b_hi = sdesc(dh + 256u * ks, 128u, 4096u);
+                        const uint64_t b_lo = sdesc(dl + 256u * ks, 128u, 4096u);
+                        mma_f16(accb + (uint32_t)((ks / KC_STEPS) * TV), a_hi, b_hi, idesc,
+                                (ks % KC_STEPS) > 0 ? 1u : 0u);
+                        mma_f16(acc2, a_hi, b_lo, idesc, ks > 0 ? 1u : 0u);
+                        mma_f16(acc2, a_lo, b_hi, idesc, 1u);
                     }
                 }
                 mma_commit(mmad0 + 8 * b);
@@ -498,54 +599,111 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             const bool ok = mbar_wait(full0 + 8 * b, u & 1) && mbar_wait(mmad0 + 8 * b, u & 1);
             if (role_any<2>(!ok)) { failed = true; break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            float va[8], vb[8];
-            tmem_ld8(tbase + lanebits + (uint32_t)(b * 2 * TV + 8 * ch), va);
-            tmem_ld8(tbase + lanebits + (uint32_t)(b * 2 * TV + TV + 8 * ch), vb);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            float* S = (float*)(sdat + b * 4 * DAT_BYTES);
-            if (j < P) {
-                const int ia = (dct ? 2 * j + 2 : 2 * j) - koff, ib = 2 * j + 1 - koff;
+            if constexpr (!WIDE) {
+                float va[8], va1[8], vb[8], vb1[8], ca[8], cb[8];
+                const uint32_t tb0 = tbase + lanebits + (uint32_t)(b * ACC_COLS + 8 * ch);
+                tmem_ld8(tb0, va);
+                tmem_ld8(tb0 + TV, va1);
+                tmem_ld8(tb0 + 2 * TV, vb);
+                tmem_ld8(tb0 + 3 * TV, vb1);
+                tmem_ld8(tb0 + 4 * TV, ca);
+                tmem_ld8(tb0 + 5 * TV, cb);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                float* S = (float*)(sdat + b * 4 * DAT_BYTES);
+                if (j < P) {
+                    const int ia = (dct ? 2 * j + 2 : 2 * j) - koff, ib = 2 * j + 1 - koff;
+    #pragma unroll
+                    for (int cc = 0; cc < 8; ++cc) {
+                        const int c = 8 * ch + cc;
+                        const float down = vdown[b * TV + c];
+                        float av = ((va[cc] + va1[cc]) + ca[cc]) * down, bv = ((vb[cc] + vb1[cc]) + cb[cc]) * down;
+                        if (dct) { av += e0[b * TV + c]; bv += e1[b * TV + c]; }
+                        if (g.axis == 0) {
+                            S[c * (2 * PP) + ia] = av;
+                            S[c * (2 * PP) + ib] = bv;
+                        } else {
+                            S[ia * TV + (c ^ ((ia >> 1) & 15))] = av;
+                            S[ib * TV + (c ^ ((ib >> 1) & 15))] = bv;
+                        }
+                    }
+                }
+                epilogue_sync();
+                if (g.axis == 0) {
+                    for (int c = e; c < TV; c += NEW) {
+                        const long long ob = obase[b * TV + c];
+                        if (ob < 0) continue;
+                        const float* sr = S + c * (2 * PP);
+                        float* op = outp + ob + (long long)(lane + koff) * g.oa.estride;
+                        const long long ostep = 32 * g.oa.estride;
+                        for (int k = lane; k < nk; k += 32, op += ostep) *op = sr[k];
+                    }
+                } else {
+                    const int c = lane & 15;
+                    const long long ob = obase[b * TV + c];
+                    if (ob >= 0) {
+                        const int k0 = 2 * e + (lane >> 4);
+                        float* op = outp + ob + (long long)(k0 + koff) * g.oa.estride;
+                        const long long ostep = 2 * NEW * g.oa.estride;
+                        for (int k = k0; k < nk; k += 2 * NEW, op += ostep) *op = S[k * TV + (c ^ ((k >> 1) & 15))];
+                    }
+                }
+                if (dct && e == 0 && lane < TV) {
+                    const long long ob = obase[b * TV + lane];
+                    if (ob >= 0) {
+                        outp[ob] = sp0[b * TV + lane];
+                        outp[ob + (long long)(N - 1) * g.oa.estride] = sp1[b * TV + lane];
+                    }
+                }
+            } else {
+                // one accumulator: modes 128 mb + j of half hh, output element 2 (128 mb + j) + par
+                float v0[8], v1[8], v2[8], v3[8], vc[8];
+                const uint32_t tb0 = tbase + lanebits + (uint32_t)(b * ACC_COLS + 8 * ch);
+                tmem_ld8(tb0, v0);
+                tmem_ld8(tb0 + TV, v1);
+                tmem_ld8(tb0 + 2 * TV, v2);
+                tmem_ld8(tb0 + 3 * TV, v3);
+                tmem_ld8(tb0 + 4 * TV, vc);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                float* S = (float*)(sdat + b * 4 * DAT_BYTES);
+                const int par = dct ? (hh == 0 ? 1 : 0) : (hh == 0 ? 0 : 1);
+                const int jg = 128 * mb + j;
 #pragma unroll
                 for (int cc = 0; cc < 8; ++cc) {
                     const int c = 8 * ch + cc;
-                    const float down = vdown[b * TV + c];
-                    float av = va[cc] * down, bv = vb[cc] * down;
-                    if (dct) { av += e0[b * TV + c]; bv += e1[b * TV + c]; }
-                    if (g.axis == 0) {
-                        S[c * (2 * PP) + ia] = av;
-                        S[c * (2 * PP) + ib] = bv;
-                    } else {
-                        S[ia * TV + (c ^ ((ia >> 1) & 15))] = av;
-                        S[ib * TV + (c ^ ((ib >> 1) & 15))] = bv;
+                    float av = (((v0[cc] + v1[cc]) + (v2[cc] + v3[cc])) + vc[cc]) * vdown[b * TV + c];
+                    if (dct) av += e0[b * TV + c];
+                    if (g.axis == 0) S[c * 128 + j] = av;
+                    else S[j * TV + (c ^ ((j >> 1) & 15))] = av;
+                }
+                epilogue_sync();
+                if (g.axis == 0) {
+                    for (int c = e; c < TV; c += NEW) {
+                        const long long ob = obase[b * TV + c];
+                        if (ob < 0) continue;
+                        const float* sr = S + c * 128;
+                        for (int jl = lane; jl < 128; jl += 32) {
+                            const int jj2 = 128 * mb + jl;
+                            if (jj2 < P) outp[ob + (long long)(2 * jj2 + par + koff) * g.oa.estride] = sr[jl];
+                        }
+                    }
+                } else {
+                    const int c = lane & 15;
+                    const long long ob = obase[b * TV + c];
+                    if (ob >= 0) {
+                        for (int jl = 2 * e + (lane >> 4); jl < 128; jl += 2 * NEW) {
+                            const int jj2 = 128 * mb + jl;
+                            if (jj2 < P)
+                                outp[ob + (long long)(2 * jj2 + par + koff) * g.oa.estride] =
+                                    S[jl * TV + (c ^ ((jl >> 1) & 15))];
+                        }
                     }
                 }
-            }
-            epilogue_sync();
-            if (g.axis == 0) {
-                for (int c = e; c < TV; c += NEW) {
-                    const long long ob = obase[b * TV + c];
-                    if (ob < 0) continue;
-                    const float* sr = S + c * (2 * PP);
-                    float* op = outp + ob + (long long)(lane + koff) * g.oa.estride;
-                    const long long ostep = 32 * g.oa.estride;
-                    for (int k = lane; k < nk; k += 32, op += ostep) *op = sr[k];
+                // X_0 (half 0) or X_{N-1} (half 1), written by the first mode block
+                if (dct && mb == 0 && e == 0 && lane < TV) {
+                    const long long ob = obase[b * TV + lane];
+                    if (ob >= 0) outp[ob + (hh == 0 ? 0LL : (long long)(N - 1) * g.oa.estride)] = sp0[b * TV + lane];
                 }
-            } else {
-                const int c = lane & 15;
-                const long long ob = obase[b * TV + c];
-                if (ob >= 0) {
-                    const int k0 = 2 * e + (lane >> 4);
-                    float* op = outp + ob + (long long)(k0 + koff) * g.oa.estride;
-                    const long long ostep = 2 * NEW * g.oa.estride;
-                    for (int k = k0; k < nk; k += 2 * NEW, op += ostep) *op = S[k * TV + (c ^ ((k >> 1) & 15))];
-                }
-            }
-            if (dct && e == 0 && lane < TV) {
-                const long long ob = obase[b * TV + lane];
-                if (ob >= 0) {
-                    outp[ob] = sp0[b * TV + lane];
-                    outp[ob + (long long)(N - 1) * g.oa.estride] = sp1[b * TV + lane];
-                }
+                (void)jg;
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             mbar_arrive(afree0 + 8 * b);
@@ -555,7 +713,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     __syncthreads();
     if (warp == NPW + NEW) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tbase));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "n"(TMEM_COLS));
     }
 }
 

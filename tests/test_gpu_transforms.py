@@ -1,9 +1,11 @@
 """DCT-I / DST-I transforms of the CUDA path against SciPy (FP64).
 
 FP32 storage on grids with even N and (N-2)/2 <= 128 runs the tcgen05
-tensor-core contractions (FP16 hi/lo split operands, FP32 accumulation);
+tensor-core contractions (up to 256 pairs, with NFGS_TC_WIDE set, the
+four-role kernel) (FP16 hi/lo split operands, FP32 accumulation);
 their error against the FP64 transform must stay at FP32 level: relative
-L2 error <= 2e-6 (forward) and <= 2e-6 (inverse) per volume.  FP64 storage
+L2 error <= 2e-6 (forward) and <= 2e-6 (inverse) per volume (measured
+3.6e-7 to 6.3e-7 since the hi x hi products accumulate in 64-pair chunks).  FP64 storage
 runs the SIMT contractions and must agree to 1e-12.
 """
 
@@ -17,9 +19,20 @@ pytestmark = pytest.mark.gpu
 
 
 def _solver(nx, ny, nz, dtype):
+    import os
+
     from nfgs_b200 import NFGSSolverGPU
 
-    return NFGSSolverGPU(nx, ny, nz, 1.0, 1.0, 1.0, device="cuda:0", dtype=dtype, pad_calculation_domain=False)
+    # more than 128 pairs: the four-role tensor-core kernel, enabled on request
+    wide = (nx - 2) // 2 > 128 or (ny - 2) // 2 > 128
+    old = os.environ.get("NFGS_TC_WIDE")
+    if wide:
+        os.environ["NFGS_TC_WIDE"] = "1"
+    try:
+        return NFGSSolverGPU(nx, ny, nz, 1.0, 1.0, 1.0, device="cuda:0", dtype=dtype, pad_calculation_domain=False)
+    finally:
+        if wide and old is None:
+            os.environ.pop("NFGS_TC_WIDE", None)
 
 
 def _apply(s, chain, inverse, x):
@@ -40,7 +53,9 @@ def _ref(chain, inverse, x):
     return g(g(x, type=t, axis=-1), type=t, axis=-2)
 
 
-@pytest.mark.parametrize("shape", [(18, 18, 5), (66, 34, 4), (130, 258, 3), (258, 258, 5), (194, 258, 3), (66, 66, 65), (258, 258, 129)])
+@pytest.mark.parametrize("shape", [(18, 18, 5), (66, 34, 4), (130, 258, 3), (258, 258, 5), (194, 258, 3), (66, 66, 65),
+                                   (258, 258, 129), (514, 514, 3), (514, 258, 4), (258, 386, 3), (514, 514, 65),
+                                   (258, 386, 65)])
 @pytest.mark.parametrize("dtype,tol", [("float32", 2e-6), ("float64", 1e-12)])
 def test_transforms_match_scipy(shape, dtype, tol):
     nx, ny, nz = shape
