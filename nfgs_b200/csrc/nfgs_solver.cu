@@ -468,11 +468,6 @@ static int tc_setup(Handle* h) {
     if (!h->f32 || (nx % 2) || (ny % 2)) return NFGS_OK;
     const int px = (nx - 2) / 2, py = (ny - 2) / 2;
     if (px < 1 || py < 1 || px > tc::PW_K || py > tc::PW_K) return NFGS_OK;
-    // Above 128 pairs the four-role kernel is 3.4x faster per transform, but an
-    // FP32 solve of a 514^2 x 257 quadrupole through it stalls at a higher
-    // sigma_J than through the SIMT contractions (0.36-0.42 vs 0.32-0.38), so
-    // it is used only on request.
-    if ((px > tc::PP || py > tc::PP) && getenv("NFGS_TC_WIDE") == nullptr) return NFGS_OK;
     if (getenv("NFGS_DISABLE_TC") != nullptr) return NFGS_OK;
     int dev = 0, nsm = 0;
     CK(cudaGetDevice(&dev));

@@ -16,10 +16,10 @@
 // column) and split into FP16 hi + lo; the matrix (|entries| <= 2) is split
 // likewise; three products hi*hi + hi*lo + lo*hi per K step give ~2^-21
 // relative error per product against the vector's maximum.  The tensor
-// core's internal accumulation does not round to nearest, so long running
-// sums drift: the hi*hi products accumulate in chunks of 64 pairs and the
+// core's internal accumulation truncates, which biases long running sums
+// toward zero: the hi*hi products accumulate in chunks of 32 pairs and the
 // correction products apart, each in its own TMEM accumulator, and the
-// epilogue adds them in FP32.
+// epilogue adds them in FP32 (round to nearest).
 //
 // One persistent CTA per SM, warp-specialised and pipelined (NB = 3 tiles
 // between operand build and epilogue):
@@ -64,13 +64,16 @@ constexpr long long WAIT_LIMIT = 1LL << 22;   // mbarrier polls before giving up
 // of 16 rows of up to 514 elements.
 constexpr int PW_K = 256;                     // K extent of the wide layout
 // TMEM accumulators per operand buffer (columns of TV = 16): the hi x hi
-// products accumulate in chunks of KC_STEPS K-steps (64 pairs), one
+// products accumulate in chunks of KC_STEPS K-steps (32 pairs), one
 // accumulator each, and the correction products in their own; the
-// epilogue adds them in FP32.  Normal: 2 halves x (2 chunks + 1); wide:
-// 4 chunks + 1.
-constexpr int KC_STEPS = 4;
-constexpr int ACC_COLS = 6 * TV;              // columns per buffer (96)
-constexpr int TMEM_COLS = 512;                // allocation (NB * ACC_COLS = 288 used)
+// epilogue adds them in FP32.  Normal: 2 halves x (4 chunks + 1); wide:
+// 8 chunks + 1.
+constexpr int KC_STEPS = 2;
+constexpr int NCH_N = PP / 16 / KC_STEPS;     // hi x hi chunks per half, normal (4)
+constexpr int NCH_W = 256 / 16 / KC_STEPS;    // hi x hi chunks, wide (8)
+constexpr int ACC_COLS = 2 * (NCH_N + 1) * TV;  // columns per buffer (160)
+static_assert(NCH_W + 1 <= 2 * (NCH_N + 1), "wide accumulators fit a buffer's columns");
+constexpr int TMEM_COLS = 512;                // allocation (NB * ACC_COLS = 480 used)
 static_assert(NB * ACC_COLS <= TMEM_COLS, "accumulators fit the TMEM allocation");
 constexpr int STG_PITCH_W = 2 * PW_K + 10;    // wide axis-0 staging pitch (fits the staging area once)
 static_assert(TV * STG_PITCH_W <= 2 * TV * STG_PITCH, "wide staging fits");
@@ -182,6 +185,30 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
         : "r"(taddr));
 #pragma unroll
     for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+
+// sum over NCH chunk accumulators (8 columns each at col, col + TV, ...)
+// and the correction accumulator after them, in FP32 round-to-nearest
+template <int NCH>
+__device__ __forceinline__ void acc_sum(uint32_t col, float (&v)[8]) {
+    float t[8], u[8];
+    tmem_ld8(col, v);
+    tmem_ld8(col + TV, t);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] += t[q];
+#pragma unroll
+    for (int c = 2; c < NCH; c += 2) {
+        tmem_ld8(col + c * TV, t);
+        tmem_ld8(col + (c + 1) * TV, u);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] += t[q] + u[q];
+    }
+    tmem_ld8(col + NCH * TV, t);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] += t[q];
 }
 
 template <int B>
@@ -538,10 +565,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                 if constexpr (!WIDE) {
 #pragma unroll 1
                     for (int h = 0; h < 2; ++h) {
-                        // hi x hi in chunks of KC_STEPS K-steps (columns (2h + chunk) TV),
-                        // the correction products at (4 + h) TV
-                        const uint32_t accb = tbase + (uint32_t)(b * ACC_COLS + 2 * h * TV);
-                        const uint32_t acc2 = tbase + (uint32_t)(b * ACC_COLS + (4 + h) * TV);
+                        // hi x hi in chunks of KC_STEPS K-steps (columns (h (NCH_N + 1) + chunk) TV),
+                        // the correction products after them
+                        const uint32_t accb = tbase + (uint32_t)(b * ACC_COLS + h * (NCH_N + 1) * TV);
+                        const uint32_t acc2 = accb + NCH_N * TV;
                         const uint32_t mh = mat0 + (uint32_t)(2 * h) * MAT_BYTES, ml = mh + MAT_BYTES;
                         const uint32_t dh = dat0 + (uint32_t)(b * 4 + 2 * h) * DAT_BYTES, dl = dh + DAT_BYTES;
 #pragma unroll 1
@@ -559,7 +586,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                 } else {
                     // this role's 128 x 256 slice [hi 64 KB | lo 64 KB] against 256 pairs;
                     // hi x hi in one accumulator, the two correction products in a second
-                    const uint32_t accb = tbase + (uint32_t)(b * ACC_COLS), acc2 = accb + 4 * TV;
+                    const uint32_t accb = tbase + (uint32_t)(b * ACC_COLS), acc2 = accb + NCH_W * TV;
                     const uint32_t mh = mat0, ml = mat0 + 2 * MAT_BYTES;
                     const uint32_t dh = dat0 + (uint32_t)(b * 4) * DAT_BYTES, dl = dh + 2 * DAT_BYTES;
 #pragma unroll 1
@@ -600,15 +627,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             if (role_any<2>(!ok)) { failed = true; break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if constexpr (!WIDE) {
-                float va[8], va1[8], vb[8], vb1[8], ca[8], cb[8];
+                // each half: the sum of its chunk accumulators, then its corrections
+                float va[8], vb[8];
                 const uint32_t tb0 = tbase + lanebits + (uint32_t)(b * ACC_COLS + 8 * ch);
-                tmem_ld8(tb0, va);
-                tmem_ld8(tb0 + TV, va1);
-                tmem_ld8(tb0 + 2 * TV, vb);
-                tmem_ld8(tb0 + 3 * TV, vb1);
-                tmem_ld8(tb0 + 4 * TV, ca);
-                tmem_ld8(tb0 + 5 * TV, cb);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                acc_sum<NCH_N>(tb0, va);
+                acc_sum<NCH_N>(tb0 + (NCH_N + 1) * TV, vb);
                 float* S = (float*)(sdat + b * 4 * DAT_BYTES);
                 if (j < P) {
                     const int ia = (dct ? 2 * j + 2 : 2 * j) - koff, ib = 2 * j + 1 - koff;
@@ -616,7 +639,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                     for (int cc = 0; cc < 8; ++cc) {
                         const int c = 8 * ch + cc;
                         const float down = vdown[b * TV + c];
-                        float av = ((va[cc] + va1[cc]) + ca[cc]) * down, bv = ((vb[cc] + vb1[cc]) + cb[cc]) * down;
+                        float av = va[cc] * down, bv = vb[cc] * down;
                         if (dct) { av += e0[b * TV + c]; bv += e1[b * TV + c]; }
                         if (g.axis == 0) {
                             S[c * (2 * PP) + ia] = av;
@@ -656,21 +679,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                 }
             } else {
                 // one accumulator: modes 128 mb + j of half hh, output element 2 (128 mb + j) + par
-                float v0[8], v1[8], v2[8], v3[8], vc[8];
-                const uint32_t tb0 = tbase + lanebits + (uint32_t)(b * ACC_COLS + 8 * ch);
-                tmem_ld8(tb0, v0);
-                tmem_ld8(tb0 + TV, v1);
-                tmem_ld8(tb0 + 2 * TV, v2);
-                tmem_ld8(tb0 + 3 * TV, v3);
-                tmem_ld8(tb0 + 4 * TV, vc);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                float va[8];
+                acc_sum<NCH_W>(tbase + lanebits + (uint32_t)(b * ACC_COLS + 8 * ch), va);
                 float* S = (float*)(sdat + b * 4 * DAT_BYTES);
                 const int par = dct ? (hh == 0 ? 1 : 0) : (hh == 0 ? 0 : 1);
                 const int jg = 128 * mb + j;
 #pragma unroll
                 for (int cc = 0; cc < 8; ++cc) {
                     const int c = 8 * ch + cc;
-                    float av = (((v0[cc] + v1[cc]) + (v2[cc] + v3[cc])) + vc[cc]) * vdown[b * TV + c];
+                    float av = va[cc] * vdown[b * TV + c];
                     if (dct) av += e0[b * TV + c];
                     if (g.axis == 0) S[c * 128 + j] = av;
                     else S[j * TV + (c ^ ((j >> 1) & 15))] = av;

@@ -6,8 +6,9 @@ observed box), fields compared on the device.
 
     python -m nfgs_b200.large_solve --fp64 --report large.json
 
-NFGS_TC_WIDE=1 in the environment runs the transforms (256 pairs per axis)
-on the four-role tensor-core kernel instead of the SIMT contractions.
+The transforms (256 pairs per axis) run on the four-role tensor-core
+kernel; NFGS_DISABLE_TC=1 in the environment runs them on the SIMT
+contractions instead.
 """
 
 from __future__ import annotations
@@ -59,7 +60,7 @@ def main(argv=None):
     args = ap.parse_args(argv)
 
     out = {"grid": [args.n, args.n, args.nz], "seed": args.seed,
-           "tc_wide": os.environ.get("NFGS_TC_WIDE") is not None}
+           "transforms": "simt" if os.environ.get("NFGS_DISABLE_TC") else "tcgen05"}
     s = _solver(args.n, args.nz, args.seed, "float32")
     out["calc_grid"] = [s.Nx, s.Ny, s.Nz]
     cells = s.Nx * s.Ny * s.Nz

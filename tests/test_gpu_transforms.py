@@ -1,11 +1,11 @@
 """DCT-I / DST-I transforms of the CUDA path against SciPy (FP64).
 
-FP32 storage on grids with even N and (N-2)/2 <= 128 runs the tcgen05
-tensor-core contractions (up to 256 pairs, with NFGS_TC_WIDE set, the
-four-role kernel) (FP16 hi/lo split operands, FP32 accumulation);
+FP32 storage on grids with even N and (N-2)/2 <= 256 runs the tcgen05
+tensor-core contractions (above 128 pairs the four-role kernel; FP16 hi/lo
+split operands, FP32 accumulation in 32-pair chunks);
 their error against the FP64 transform must stay at FP32 level: relative
 L2 error <= 2e-6 (forward) and <= 2e-6 (inverse) per volume (measured
-3.6e-7 to 6.3e-7 since the hi x hi products accumulate in 64-pair chunks).  FP64 storage
+1.5e-7 to 6e-7).  FP64 storage
 runs the SIMT contractions and must agree to 1e-12.
 """
 
@@ -19,20 +19,9 @@ pytestmark = pytest.mark.gpu
 
 
 def _solver(nx, ny, nz, dtype):
-    import os
-
     from nfgs_b200 import NFGSSolverGPU
 
-    # more than 128 pairs: the four-role tensor-core kernel, enabled on request
-    wide = (nx - 2) // 2 > 128 or (ny - 2) // 2 > 128
-    old = os.environ.get("NFGS_TC_WIDE")
-    if wide:
-        os.environ["NFGS_TC_WIDE"] = "1"
-    try:
-        return NFGSSolverGPU(nx, ny, nz, 1.0, 1.0, 1.0, device="cuda:0", dtype=dtype, pad_calculation_domain=False)
-    finally:
-        if wide and old is None:
-            os.environ.pop("NFGS_TC_WIDE", None)
+    return NFGSSolverGPU(nx, ny, nz, 1.0, 1.0, 1.0, device="cuda:0", dtype=dtype, pad_calculation_domain=False)
 
 
 def _apply(s, chain, inverse, x):
