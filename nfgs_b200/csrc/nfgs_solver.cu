@@ -2667,6 +2667,26 @@ struct NfgsScanObj {
     int device = 0;
 };
 
+// (Re)build the scan graph: `iters` chained copies of each handle's
+// iteration graph, the handles' chains independent of one another.
+static int scan_build(NfgsScanObj* sc) {
+    if (sc->exec) { cudaGraphExecDestroy(sc->exec); sc->exec = nullptr; }
+    if (sc->graph) { cudaGraphDestroy(sc->graph); sc->graph = nullptr; }
+    if (cudaGraphCreate(&sc->graph, 0) != cudaSuccess) return fail(NFGS_ECUDA, "scan: graph create");
+    for (Handle* h : sc->hs) {
+        cudaGraphNode_t prev = nullptr;
+        for (int k = 0; k < sc->iters; ++k) {
+            cudaGraphNode_t nd;
+            if (cudaGraphAddChildGraphNode(&nd, sc->graph, prev ? &prev : nullptr, prev ? 1 : 0, h->graph) !=
+                cudaSuccess)
+                return fail(NFGS_ECUDA, "scan: add child graph");
+            prev = nd;
+        }
+    }
+    if (cudaGraphInstantiate(&sc->exec, sc->graph, 0) != cudaSuccess) return fail(NFGS_ECUDA, "scan: instantiate");
+    return NFGS_OK;
+}
+
 int nfgs_scan_create(void* const* handles, int32_t n, int32_t iters, void** scan_out) {
     g_err.clear();
     if (!handles || n <= 0 || iters <= 0 || !scan_out) return fail(NFGS_EINVAL, "scan: bad arguments");
@@ -2683,7 +2703,6 @@ int nfgs_scan_create(void* const* handles, int32_t n, int32_t iters, void** scan
         delete sc;
         return code;
     };
-    if (cudaGraphCreate(&sc->graph, 0) != cudaSuccess) return bail(fail(NFGS_ECUDA, "scan: graph create"));
     for (int i = 0; i < n; ++i) {
         Handle* h = (Handle*)handles[i];
         if (!h || h->geom.device != sc->device) return bail(fail(NFGS_EINVAL, "scan: handles must share a device"));
@@ -2694,17 +2713,12 @@ int nfgs_scan_create(void* const* handles, int32_t n, int32_t iters, void** scan
         // the begin work (gs_cfcf start) ran on the handle's stream
         if (cudaStreamSynchronize(h->s) != cudaSuccess) return bail(fail(NFGS_ECUDA, "scan: sync"));
         h->advanced = 1;
-        cudaGraphNode_t prev = nullptr;
-        for (int k = 0; k < iters; ++k) {
-            cudaGraphNode_t nd;
-            if (cudaGraphAddChildGraphNode(&nd, sc->graph, prev ? &prev : nullptr, prev ? 1 : 0, h->graph) !=
-                cudaSuccess)
-                return bail(fail(NFGS_ECUDA, "scan: add child graph"));
-            prev = nd;
-        }
         sc->hs.push_back(h);
     }
-    if (cudaGraphInstantiate(&sc->exec, sc->graph, 0) != cudaSuccess) return bail(fail(NFGS_ECUDA, "scan: instantiate"));
+    {
+        const int r = scan_build(sc);
+        if (r != NFGS_OK) return bail(r);
+    }
     if (cudaStreamCreateWithFlags(&sc->s, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(NFGS_ECUDA, "scan: stream"));
     *scan_out = sc;
@@ -2723,6 +2737,15 @@ int nfgs_scan_launch(void* scan, int32_t* n_active_out) {
         CK(cudaMemcpy(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost));
         h->launches += sc->iters * h->graph_kernels;
         active += h->ctl_h->stopped ? 0 : 1;
+    }
+    // once half the solves of the graph have stopped, rebuild it from the
+    // others: stopped solves' kernels would still be launched (and return)
+    if (active > 0 && 2 * active <= (int)sc->hs.size()) {
+        std::vector<Handle*> keep;
+        for (Handle* h : sc->hs)
+            if (!h->ctl_h->stopped) keep.push_back(h);
+        sc->hs.swap(keep);
+        TRY(scan_build(sc));
     }
     if (n_active_out) *n_active_out = active;
     return NFGS_OK;
