@@ -1480,8 +1480,10 @@ static int autotune_stencil(Handle* h, int polarity) {
         if (e[0] == '0') return NFGS_OK;
     const int nz = h->g.nz;
     const auto key = std::make_tuple(h->g.nx, h->g.ny, nz, (int)h->f32);
+    // the lock is held through the tuning: handles of one shape begun on
+    // several threads wait for the first one's choice and all use it
+    std::lock_guard<std::mutex> lk(g_tune_mu);
     {
-        std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune_nseg.find(key);
         if (it != g_tune_nseg.end()) {
             const int per = (nz + it->second - 1) / it->second;
@@ -1517,7 +1519,6 @@ static int autotune_stencil(Handle* h, int polarity) {
     cudaEventDestroy(b);
     h->fs_grid.z = best;
     h->fs_nb = (int)(h->fs_grid.x * h->fs_grid.y * best);
-    std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune_nseg[key] = (int)best;
     return NFGS_OK;
 }

@@ -6,8 +6,10 @@ begun on its own handle (gs_cfcf start, per-iteration CUDA graph captured),
 and one CUDA graph holding `iters` iterations of every solve -- independent
 chains, so solves of different sizes fill the GPU together -- is launched
 until every solve has met its stop rule.  Solves that stopped skip their work
-on the device; the results are those of the same solves run one by one.
-The fused stencil's z-segment count is autotuned per grid shape.
+on the device, and the graph is rebuilt from the running solves whenever
+half have stopped; the results are those of the same solves run one by one.
+The solvers are set up by a thread pool (the first of each grid shape alone,
+so that the fused stencil's per-shape z-segment tuning runs on a quiet GPU).
 
     python -m nfgs_b200.scan --boundaries 33 --report scan.json
 """
@@ -57,16 +59,39 @@ def _solver(case):
     return s
 
 
-def run_scan(cases, iters: int = 8, max_iter: int = 3000, stop=STOP):
-    """All cases in one batched run; returns (histories, timings)."""
+def run_scan(cases, iters: int = 8, max_iter: int = 3000, stop=STOP, workers: int = 8):
+    """All cases in one batched run; returns (histories, timings).  The
+    solvers are set up (created, boundary, gs_cfcf start) by `workers`
+    threads: each handle has its own stream and the library's shared state
+    is locked, and the set-up is mostly host work and synchronous copies."""
     import torch
+    from concurrent.futures import ThreadPoolExecutor
+
+    def begin(c):
+        s = _solver(c)
+        return s, s._iterate_begin(max_iter=max_iter, verbose=False, use_graph=True, **stop)
 
     t0 = time.perf_counter()
-    solvers, ctxs = [], []
-    for c in cases:
-        s = _solver(c)
-        ctxs.append(s._iterate_begin(max_iter=max_iter, verbose=False, use_graph=True, **stop))
-        solvers.append(s)
+    # the first solve of each grid shape alone (its stencil tuning runs on a
+    # quiet GPU), then the rest concurrently
+    firsts, seen = [], set()
+    for q, c in enumerate(cases):
+        if (c["n"], c["nz"]) not in seen:
+            seen.add((c["n"], c["nz"]))
+            firsts.append(q)
+    pairs = [None] * len(cases)
+    for q in firsts:
+        pairs[q] = begin(cases[q])
+    rest = [q for q in range(len(cases)) if pairs[q] is None]
+    if workers > 1:
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            for q, pr in zip(rest, ex.map(lambda q: begin(cases[q]), rest)):
+                pairs[q] = pr
+    else:
+        for q in rest:
+            pairs[q] = begin(cases[q])
+    solvers = [p[0] for p in pairs]
+    ctxs = [p[1] for p in pairs]
     lib = L.lib()
     arr = (C.c_void_p * len(solvers))(*[s._h.value if isinstance(s._h, C.c_void_p) else s._h for s in solvers])
     scan = C.c_void_p()
