@@ -515,13 +515,25 @@ static int tc_launch(Handle* h, int which, int inverse, const float* in, tc::Add
     a.skip = skip;
     a.err = h->tc_err;
     const int ntiles = (nvec + tc::TV - 1) / tc::TV;
+    // programmatic stream serialisation: the kernel waits (griddepcontrol)
+    // for its predecessor before reading its outputs, so its prologue (TMEM,
+    // barriers, the constant matrix copy) may overlap the predecessor's end
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.blockDim = dim3(tc::NTHREADS);
+    cfg.dynamicSmemBytes = tc::SMEM_TOTAL;
+    cfg.stream = h->s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     if (h->tc_wide[which]) {
         // four roles per tile group: one CTA per SM in groups of four
-        const int grid = 4 * std::min(ntiles, h->tc_nsm / 4);
-        tc::k_tc_transform<true><<<grid, tc::NTHREADS, tc::SMEM_TOTAL, h->s>>>(a);
+        cfg.gridDim = dim3((unsigned)(4 * std::min(ntiles, h->tc_nsm / 4)));
+        CK(cudaLaunchKernelEx(&cfg, tc::k_tc_transform<true>, a));
     } else {
-        const int grid = std::min(ntiles, h->tc_nsm);
-        tc::k_tc_transform<false><<<grid, tc::NTHREADS, tc::SMEM_TOTAL, h->s>>>(a);
+        cfg.gridDim = dim3((unsigned)std::min(ntiles, h->tc_nsm));
+        CK(cudaLaunchKernelEx(&cfg, tc::k_tc_transform<false>, a));
     }
     CK(cudaGetLastError());
     h->launches++;

@@ -272,7 +272,6 @@ __device__ __forceinline__ void split_h(float x, __half& hi, __half& lo) {
 template <bool WIDE>
 __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    if (g.skip != nullptr && *g.skip) return;
     unsigned char* smat = smem;
     unsigned char* sdat = smem + SMEM_MAT;
     float* stg = (float*)(smem + SMEM_MAT + SMEM_DAT);   // [2][STG_FLOATS]
@@ -300,7 +299,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     const int role = WIDE ? (int)(blockIdx.x & 3) : 0;
     const int hh = role >> 1, mb = role & 1;    // wide: matrix half and 128-mode block
     const int ntiles = (g.nvec + TV - 1) / TV;
-    const int nlocal = grp < ntiles ? (ntiles - 1 - grp) / ngrp + 1 : 0;
     const uint32_t full0 = smem_u32(bars), mmad0 = smem_u32(bars + NB), afree0 = smem_u32(bars + 2 * NB);
     if (tid == 0) {
         for (int b = 0; b < NB; ++b) {
@@ -323,21 +321,32 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     const bool dct = g.kind == 0;
     bool failed = false;
 
-    float* outp = g.out;
-    if (g.out_table != nullptr) outp = (float*)((char*)g.out_table[*g.out_sel]);
-
-    // The matrix operands (128 KB) are copied in by the MMA and epilogue
-    // warps, which need them first at the first MMA; the producers start on
-    // the first tiles meanwhile.
-    auto load_matrices = [&]() {
+    // The matrix operands (128 KB, constant) are copied in by the MMA and
+    // epilogue warps, which need them first at the first MMA; the copy starts
+    // before the wait for the previous kernel (programmatic launch: this
+    // prologue may overlap its end), and the producers start on the first
+    // tiles meanwhile.
+    if (warp >= NPW) {
         const uint32_t d0 = smem_u32(smat);
         const uint4* src = g.mat + (size_t)role * (SMEM_MAT / 16);
         for (int q = tid - NPROD; q < SMEM_MAT / 16; q += NEPI + 32) cp_async4<16>(d0 + 16u * q, src + q);
         cp_commit();
+    }
+    auto load_matrices = [&]() {
         cp_wait0();
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("bar.sync 3, %0;" ::"n"(NEPI + 32) : "memory");
     };
+    // let the next kernel start its prologue; then wait for the previous
+    // kernel, whose outputs (input vectors, skip flag, output selection) all
+    // reads below depend on
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const bool skipped = g.skip != nullptr && *g.skip;
+    const int nlocal = (!skipped && grp < ntiles) ? (ntiles - 1 - grp) / ngrp + 1 : 0;
+
+    float* outp = g.out;
+    if (g.out_table != nullptr && !skipped) outp = (float*)((char*)g.out_table[*g.out_sel]);
 
     if (warp < NPW) {
         // ================= producers
