@@ -324,7 +324,7 @@ static int from_storage(Handle* h, const void* src, double* dst, long long n) {
 // ---------------------------------------------------------------------------
 // Host-built tables
 // ---------------------------------------------------------------------------
-static std::vector<double> dct_matrix(int n, bool inverse) {
+static std::vector<double> dct_matrix_build(int n, bool inverse) {
     std::vector<double> m((size_t)n * n);
     const double s = inverse ? 1.0 / (2.0 * (n - 1)) : 1.0;
     for (int k = 0; k < n; ++k)
@@ -337,7 +337,7 @@ static std::vector<double> dct_matrix(int n, bool inverse) {
     return m;
 }
 
-static std::vector<double> dst_matrix(int n, bool inverse) {
+static std::vector<double> dst_matrix_build(int n, bool inverse) {
     std::vector<double> m((size_t)n * n);
     const double s = inverse ? 1.0 / (2.0 * (n + 1)) : 1.0;
     for (int k = 0; k < n; ++k)
@@ -372,7 +372,7 @@ static int upload_t(Handle* h, void** dp, const std::vector<double>& v) {
 // Operand image of one transform: four fp16 matrices [half A hi | half A lo |
 // half B hi | half B lo], each 128 modes x 128 pairs in the no-swizzle
 // K-major UMMA layout (j/8)*2048 + (k/8)*128 + (j%8)*16 + (k%8)*2 bytes.
-static std::vector<uint16_t> tc_image(int kind, int n, int P) {
+static std::vector<uint16_t> tc_image_build(int kind, int n, int P) {
     std::vector<uint16_t> img(4 * 128 * 128, 0);
     const int period = kind == 0 ? n - 1 : n + 1;  // DCT: N-1, DST: n+1
     for (int h = 0; h < 2; ++h)
@@ -400,7 +400,7 @@ static std::vector<uint16_t> tc_image(int kind, int n, int P) {
 // Wide image (128 < P <= 256): four roles r = 2 h + mb, each the 128 x 256
 // slice (modes 128 mb .. +127 of half h, all pairs) in K-major core-matrix
 // layout (8-row groups 4096 B apart), [hi 64 KB | lo 64 KB] per role.
-static std::vector<uint16_t> tc_image_wide(int kind, int n, int P) {
+static std::vector<uint16_t> tc_image_wide_build(int kind, int n, int P) {
     const size_t per = (size_t)128 * tc::PW_K;   // halves per hi (or lo) slice
     std::vector<uint16_t> img(4 * 2 * per, 0);
     const int period = kind == 0 ? n - 1 : n + 1;
@@ -427,6 +427,38 @@ static std::vector<uint16_t> tc_image_wide(int kind, int n, int P) {
             }
     }
     return img;
+}
+
+// The transform matrices depend only on their length and kind: they are
+// built once per process (a solver created after the first of its size
+// skips the cosine tables) and copied out of this cache.
+static std::mutex g_mat_mu;
+static std::map<std::tuple<int, int, int>, std::vector<double>> g_mat_cache;
+static std::map<std::tuple<int, int, int, int>, std::vector<uint16_t>> g_img_cache;
+
+static std::vector<double> dct_matrix(int n, bool inverse) {
+    std::lock_guard<std::mutex> lk(g_mat_mu);
+    auto& v = g_mat_cache[std::make_tuple(0, n, (int)inverse)];
+    if (v.empty()) v = dct_matrix_build(n, inverse);
+    return v;
+}
+static std::vector<double> dst_matrix(int n, bool inverse) {
+    std::lock_guard<std::mutex> lk(g_mat_mu);
+    auto& v = g_mat_cache[std::make_tuple(1, n, (int)inverse)];
+    if (v.empty()) v = dst_matrix_build(n, inverse);
+    return v;
+}
+static std::vector<uint16_t> tc_image(int kind, int n, int P) {
+    std::lock_guard<std::mutex> lk(g_mat_mu);
+    auto& v = g_img_cache[std::make_tuple(0, kind, n, P)];
+    if (v.empty()) v = tc_image_build(kind, n, P);
+    return v;
+}
+static std::vector<uint16_t> tc_image_wide(int kind, int n, int P) {
+    std::lock_guard<std::mutex> lk(g_mat_mu);
+    auto& v = g_img_cache[std::make_tuple(1, kind, n, P)];
+    if (v.empty()) v = tc_image_wide_build(kind, n, P);
+    return v;
 }
 
 // Fused stencil plan: 32 x 8 column tiles and z segments of about 16
