@@ -312,6 +312,25 @@ int nfgs_scan_destroy(void* scan);
 int nfgs_iterate_start_state(void* handle, void** phi_out, void** az_out);
 int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int32_t mode, double* out3);
 
+/* soft_cfcf start: replaces the gs_cfcf start prepared by nfgs_iterate_begin
+ * (call it between nfgs_iterate_begin and the first nfgs_iterate_advance,
+ * NFGS_ESTATE otherwise).  Replaces NFGSSolverGPU._soft_cfcf_initial_state
+ * (nfgs_solver.py:6427-6484), which compute_initial_conditions /
+ * iterate(init_mode="soft_cfcf") call (nfgs_solver.py:6613-6628,
+ * 6937-6955): per horizontal mode, the z profile minimising
+ * |D_z L_k Phi|^2 + (k^2 + epsilon)|L_k Phi|^2 (Phi) and
+ * |L_k A_z|^2 + epsilon(|D_z A_z|^2 + k^2|A_z|^2) (A_z), L_k = D_zz - k^2,
+ * with the bottom data and the transparent top Robin row exact, solved by a
+ * banded Cholesky of the normal equations (normal_ridge * max(1, max diag)
+ * added to the diagonal).  epsilon, normal_ridge >= 0 (NFGS_EINVAL), the
+ * reference's soft_cfcf_epsilon (default 1e-4 / min(dx, dy, dz)^2) and
+ * soft_cfcf_normal_ridge.  Nz >= 5 and Nx, Ny >= 3 (NFGS_EINVAL).  A
+ * non-finite solve is NFGS_ESTATE (the reference's RuntimeError).
+ * out4 = {curl-current energy, current energy, objective = curl-current +
+ * epsilon * current (the modal quadrature, nfgs_solver.py:6486-6540),
+ * sigma_J of the start}. */
+int nfgs_iterate_soft_cfcf_start(void* handle, double epsilon, double normal_ridge, double* out4);
+
 /* ------------------------------------------------------------------------
  * Evaluation metrics of a solution on a region of interest, in one FP64-
  * accumulating pass on the GPU.  Replaces the NumPy metrics the reference

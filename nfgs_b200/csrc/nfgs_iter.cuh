@@ -538,7 +538,7 @@ __global__ void k_zero_mode(Geo g, DevCtl* ctl, const double* s00) {
 template <typename T>
 __global__ void k_finalize(Geo g, StateTab st, const DevCtl* ctl, int use_ctl_mu, double mu_fixed,
                            const int* cand_sel, const int* cur_sel, const T* __restrict__ phi_above,
-                           const T* __restrict__ dphi_target, double proj_w, int do_relax) {
+                           const T* __restrict__ dphi_target, double proj_w, int do_relax, int zero_az_top) {
     if (ctl != nullptr && ctl->stopped) return;
     const long long P = g.P;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -570,4 +570,7 @@ __global__ void k_finalize(Geo g, StateTab st, const DevCtl* ctl, int use_ctl_mu
             if (k < g.nz - 1) az[q] = m1 * az[q] + m0 * azo[q];
         }
     }
+    // Az_new[-1] = 0 (nfgs_solver.py:6792): a buffer that held a start state
+    // with a non-zero top plane (soft_cfcf) is cleared when it is reused
+    if (zero_az_top && g.nz > 1) az[(long long)(g.nz - 1) * P + idx] = T(0);
 }

@@ -11,6 +11,7 @@
 #include "nfgs_tc.cuh"
 #include "nfgs_stencil.cuh"
 #include "nfgs_metrics.cuh"
+#include "nfgs_soft.cuh"
 #include <cuda_fp16.h>
 
 #include <cmath>
@@ -187,6 +188,12 @@ static int alloc(Handle* h, T** p, size_t bytes) {
     h->owned.push_back({q, bytes});
     *p = (T*)q;
     return NFGS_OK;
+}
+
+// Return one owned allocation to the pool (stream-ordered).
+static void release(Handle* h, void* p) {
+    for (auto it = h->owned.begin(); it != h->owned.end(); ++it)
+        if (it->p == p) { cudaFreeAsync(it->p, h->s); h->owned.erase(it); return; }
 }
 
 // 32 MB pinned host chunks for device-to-host staging, shared by every
@@ -614,11 +621,14 @@ static int forward_transforms(Handle* h, const DevCtl* ctl) {
 // planes 1..nz-1; Dirichlet-chain planes 1..nz-2 into the interior of
 // az[*cand_sel].
 template <typename T>
-static int inverse_transforms(Handle* h, const DevCtl* ctl, const int* cand_sel) {
+static int inverse_transforms(Handle* h, const DevCtl* ctl, const int* cand_sel, int az_top = 0) {
     const Geo& g = h->g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const long long P = g.P, PI = h->PI;
     const int nxi = nx - 2, nyi = ny - 2;
+    // A_z planes 1..nz-2 (the iteration's top plane is zero); the soft_cfcf
+    // start also transforms its Robin top plane
+    const int naz = az_top ? nz - 1 : nz - 2;
     const int* skip = ctl ? &ctl->stopped : nullptr;
     void* const* ptab = (void* const*)h->st_dev->phi;
     void* const* atab = (void* const*)h->st_dev->az;
@@ -628,7 +638,7 @@ static int inverse_transforms(Handle* h, const DevCtl* ctl, const int* cand_sel)
         TRY(tc_launch(h, 1, 1, sb, cols(P, nx, P, nx), ta, nullptr, nullptr, cols(P, nx, P, nx), (int)nc, skip));
         TRY(tc_launch(h, 0, 1, ta, rows(P, nr, nx), nullptr, ptab, cand_sel, rows(P, nr, nx), (int)nr, skip));
         if (nz > 2) {
-            const long long nci = (long long)(nz - 2) * nxi, nri = (long long)(nz - 2) * nyi;
+            const long long nci = (long long)naz * nxi, nri = (long long)naz * nyi;
             TRY(tc_launch(h, 3, 1, sj, cols(PI, nxi, PI, nxi), tb, nullptr, nullptr, cols(PI, nxi, PI, nxi), (int)nci,
                           skip));
             TRY(tc_launch(h, 2, 1, tb, rows(PI, nri, nxi), nullptr, atab, cand_sel,
@@ -646,9 +656,9 @@ static int inverse_transforms(Handle* h, const DevCtl* ctl, const int* cand_sel)
     if (nz > 2) {
         const char* sjp = (const char*)h->sj + (size_t)PI * h->esz;
         char* tbp = (char*)h->tmpB + (size_t)PI * h->esz;
-        TRY(apply_y<T>(h, h->idsty_t, sjp, nxi, PI, tbp, nxi, PI, nyi, nyi, nxi, nz - 2, ctl));
+        TRY(apply_y<T>(h, h->idsty_t, sjp, nxi, PI, tbp, nxi, PI, nyi, nyi, nxi, naz, ctl));
         TRY(apply_x<T>(h, h->idstx_t, tbp, nxi, PI, (void*)(intptr_t)((P + nx + 1) * h->esz), nx, P, nyi, nxi, nxi,
-                       nz - 2, atab, cand_sel, ctl));
+                       naz, atab, cand_sel, ctl));
     }
     return NFGS_OK;
 }
@@ -1487,7 +1497,7 @@ static int enqueue_iteration(Handle* h) {
         const long long P = h->g.P;
         k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(
             h->g, h->st, c, 1, 1.0, &c->cand, &c->cur, (const T*)h->phiab_t, (const T*)h->dphi_t,
-            h->prm.projection_weight, 1);
+            h->prm.projection_weight, 1, 1);
         CK(cudaGetLastError());
         h->launches++;
     }
@@ -1611,7 +1621,7 @@ static int iterate_begin_t(Handle* h, const NfgsStop* stop) {
         const long long P = h->g.P;
         k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(
             h->g, h->st, nullptr, 0, 1.0, &h->consts[0], &h->consts[0], (const T*)h->phiab_t, (const T*)h->dphi_t,
-            h->prm.projection_weight, 0);
+            h->prm.projection_weight, 0, 1);
         CK(cudaGetLastError());
         h->launches++;
     }
@@ -1653,13 +1663,24 @@ static int start_state(Handle* h, void** phi, void** az) {
 // supplied sigma_J is lower, 2 replaces it unconditionally.  Buffer 2 is free
 // right after iterate_begin (current = best = 0, candidate = 1).
 template <typename T>
+static int adopt_buffer2(Handle* h, int mode, double* out);
+
+template <typename T>
 static int restart_from_t(Handle* h, const void* phi, const void* az, int mode, double* out) {
     if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
     if (h->advanced) return fail(NFGS_ESTATE, "the iteration has already advanced");
     const size_t vb = (size_t)h->g.V * h->esz;
-    if (!h->dsmall) TRY(alloc(h, &h->dsmall, 8 * sizeof(double)));
     CK(cudaMemcpyAsync(h->st.phi[2], phi, vb, cudaMemcpyDeviceToDevice, h->s));
     CK(cudaMemcpyAsync(h->st.az[2], az, vb, cudaMemcpyDeviceToDevice, h->s));
+    return adopt_buffer2<T>(h, mode, out);
+}
+
+// Evaluate the state in buffer 2 and, per `mode`, make it the start (the
+// tail of restart_from_t, shared with the soft_cfcf start).
+template <typename T>
+static int adopt_buffer2(Handle* h, int mode, double* out) {
+    const size_t vb = (size_t)h->g.V * h->esz;
+    if (!h->dsmall) TRY(alloc(h, &h->dsmall, 8 * sizeof(double)));
     TRY(run_stencil<T>(h, &h->consts[2], nullptr, 1, h->stop.polarity_mask));
     sum_partials(h);
     k_scal_out<<<1, 1, 0, h->s>>>(h->g, h->scal, h->dsmall);
@@ -1689,6 +1710,93 @@ static int restart_from_t(Handle* h, const void* phi, const void* az, int mode, 
     out[0] = sc[0];
     out[1] = s_gs;
     out[2] = accept ? 1.0 : 0.0;
+    return NFGS_OK;
+}
+
+// soft_cfcf start (nfgs_solver.py:6427-6484): after iterate_begin, the
+// modal profiles of the Phi (DCT-I) and A_z (interior DST-I) modes go into
+// the modal buffers, the inverse transforms (A_z with its Robin top plane)
+// build the state in buffer 2, the bottom Phi plane is restored, and the
+// state replaces the gs_cfcf start.  out[0..2]: curl-current energy, current
+// energy and objective of the modal quadrature (nfgs_solver.py:6486-6540),
+// out[3]: sigma_J of the start.
+template <typename T>
+static int soft_cfcf_start_t(Handle* h, double eps, double ridge, double* out) {
+    if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
+    if (h->advanced) return fail(NFGS_ESTATE, "the iteration has already advanced");
+    const Geo& g = h->g;
+    if (g.nz < 5) return fail(NFGS_EINVAL, "soft_cfcf requires Nz >= 5");
+    if (g.nx < 3 || g.ny < 3) return fail(NFGS_EINVAL, "soft_cfcf requires Nx, Ny >= 3");
+    if (!(eps >= 0.0) || !std::isfinite(eps)) return fail(NFGS_EINVAL, "soft_cfcf_epsilon must be non-negative");
+    if (!(ridge >= 0.0) || !std::isfinite(ridge))
+        return fail(NFGS_EINVAL, "soft_cfcf_normal_ridge must be non-negative");
+    const long long P = g.P, PI = h->PI;
+    const long long n = g.nz - 2;
+    // modes per launch: band + vector scratch of at most 256 MB
+    const long long per_mode = n * (soft::BS + 1) * 8;
+    const long long CH = std::max(1LL, std::min(P, (256LL << 20) / per_mode));
+    double *band = nullptr, *vec = nullptr, *en = nullptr, *sums = nullptr;
+    int* err = nullptr;
+    auto cleanup = [&]() {
+        if (band) release(h, band);
+        if (vec) release(h, vec);
+        if (en) release(h, en);
+        if (sums) release(h, sums);
+        if (err) release(h, err);
+    };
+    int rc = NFGS_OK;
+    do {
+        if ((rc = alloc(h, &band, (size_t)(n * soft::BS * CH) * 8)) != NFGS_OK) break;
+        if ((rc = alloc(h, &vec, (size_t)(n * CH) * 8)) != NFGS_OK) break;
+        if ((rc = alloc(h, &en, (size_t)(2 * (P + PI)) * 8)) != NFGS_OK) break;
+        if ((rc = alloc(h, &sums, 4 * 8)) != NFGS_OK) break;
+        if ((rc = alloc(h, &err, sizeof(int))) != NFGS_OK) break;
+    } while (0);
+    if (rc != NFGS_OK) { cleanup(); return rc; }
+    cudaError_t ce = cudaMemsetAsync(err, 0, sizeof(int), h->s);
+    for (int kind = 0; kind < 2 && ce == cudaSuccess; ++kind) {
+        const long long M = kind == 0 ? P : PI;
+        const double* kk = kind == 0 ? h->kN : h->lamD;
+        const double* bot = kind == 0 ? h->phi_bot_hat : h->az_bot_hat;
+        T* hat = (T*)(kind == 0 ? h->sb : h->sj);
+        double* enk = kind == 0 ? en : en + 2 * P;
+        for (long long m0 = 0; m0 < M && ce == cudaSuccess; m0 += CH) {
+            const long long cnt = std::min(CH, M - m0);
+            soft::k_soft_profile<T><<<(unsigned)((cnt + 127) / 128), 128, 0, h->s>>>(
+                g, kind, m0, cnt, M, kk, bot, eps, ridge, CH, band, vec, hat, enk, err);
+            ce = cudaGetLastError();
+            h->launches++;
+        }
+        if (ce == cudaSuccess) {
+            soft::k_soft_sum<<<1, 256, 0, h->s>>>(enk, M, sums + 2 * kind);
+            ce = cudaGetLastError();
+            h->launches++;
+        }
+    }
+    int herr = 0;
+    double hs[4] = {0, 0, 0, 0};
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, h->s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(hs, sums, sizeof hs, cudaMemcpyDeviceToHost, h->s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->s);
+    cleanup();
+    CK(ce);
+    if (herr == soft::ERR_NONFINITE) return fail(NFGS_ESTATE, "soft_cfcf modal normal solve produced non-finite values");
+    if (herr != 0) return fail(NFGS_EUNSUPPORTED, "soft_cfcf modal rows wider than the kernel's band");
+    // state in buffer 2: Phi planes 1..nz-1, A_z interior planes 1..nz-1
+    // (walls and the bottom plane as every state holds them), Phi bottom
+    TRY(inverse_transforms<T>(h, nullptr, &h->consts[2], 1));
+    k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(g, h->st, nullptr, 0, 1.0, &h->consts[2],
+                                                                &h->consts[2], (const T*)h->phiab_t,
+                                                                (const T*)h->dphi_t, 0.0, 0, 0);
+    CK(cudaGetLastError());
+    h->launches++;
+    const double fac = g.dx * g.dy * g.dz / (4.0 * (double)(g.nx - 1) * (double)(g.ny - 1));
+    out[0] = fac * (hs[0] + hs[2]);
+    out[1] = fac * (hs[1] + hs[3]);
+    out[2] = out[0] + eps * out[1];
+    double ad[3];
+    TRY(adopt_buffer2<T>(h, 2, ad));
+    out[3] = ad[0];
     return NFGS_OK;
 }
 
@@ -2085,7 +2193,7 @@ static int step_t(Handle* h, double mu, int polarity) {
     const long long P = h->g.P;
     k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(h->g, h->st, nullptr, 0, mu, &h->consts[cand],
                                                                 &h->consts[cur], (const T*)h->phiab_t,
-                                                                (const T*)h->dphi_t, h->prm.projection_weight, 1);
+                                                                (const T*)h->dphi_t, h->prm.projection_weight, 1, 1);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->s));
     h->cur_host = cand;
@@ -2257,7 +2365,7 @@ static int time_phases_t(Handle* h, int n_iters, double* ms_out) {
         CK(cudaEventRecord(ev[4], h->s));
         k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(h->g, h->st, nullptr, 0, 1.0, &h->consts[cand],
                                                                     &h->consts[cur], (const T*)h->phiab_t,
-                                                                    (const T*)h->dphi_t, h->prm.projection_weight, 1);
+                                                                    (const T*)h->dphi_t, h->prm.projection_weight, 1, 1);
         CK(cudaGetLastError());
         CK(cudaEventRecord(ev[5], h->s));
         CK(cudaEventSynchronize(ev[5]));
@@ -2698,6 +2806,15 @@ int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int
     if (!h || !phi || !az || !out3) return fail(NFGS_EINVAL, "null argument");
     if (mode < 0 || mode > 2) return fail(NFGS_EINVAL, "mode must be 0, 1 or 2");
     return h->f32 ? restart_from_t<float>(h, phi, az, mode, out3) : restart_from_t<double>(h, phi, az, mode, out3);
+}
+
+int nfgs_iterate_soft_cfcf_start(void* handle, double epsilon, double normal_ridge, double* out4) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (h) cudaSetDevice(h->geom.device);
+    if (!h || !out4) return fail(NFGS_EINVAL, "null argument");
+    return h->f32 ? soft_cfcf_start_t<float>(h, epsilon, normal_ridge, out4)
+                  : soft_cfcf_start_t<double>(h, epsilon, normal_ridge, out4);
 }
 
 // ---------------------------------------------------------------------------

@@ -3,13 +3,13 @@
 Mirrors the public API of the reference ``nfgs_solver.NFGSSolverGPU``
 (nfgs_solver.py:3905-7196 in spaceprod/NFGS): the constructor with its
 policy keywords, ``set_bottom_vector_boundary`` / ``set_bottom_boundary``,
-``iterate`` (gs_cfcf start, sigma_best stop, optional adaptive mu) and
+``iterate`` (gs_cfcf or soft_cfcf start, sigma_best stop, optional adaptive mu) and
 ``fields_to_numpy``.  All numerical work runs in libnfgs_b200.so on the
 GPU; this module only validates options, sizes the grid, places the
 observed maps and assembles the ``history`` dictionary.
 
 Options that select the reference's ablation branches (coupled k=0 modes,
-cfcf / soft_cfcf starts, two-stage poloidal update, collocated current,
+the cfcf start, two-stage poloidal update, collocated current,
 fixed-point stop mode with per-iteration diagnostics) raise
 ``NotImplementedError``.
 """
@@ -298,6 +298,13 @@ class NFGSSolverGPU:
         self.poloidal_update_mode = pum
         self.record_iteration_diagnostics = record
         self.buffer_thickness = 0 if buffer_thickness is None else int(buffer_thickness)
+        # nfgs_solver.py:4299-4305 (the batch size is recorded only: the
+        # device solves every mode in one pass)
+        grid_scale = min(self.dx, self.dy, self.dz)
+        self.soft_cfcf_epsilon = 1.0e-4 / (grid_scale * grid_scale) if soft_eps is None else float(soft_eps)
+        self.soft_cfcf_mode_batch_size = soft_bs
+        self.soft_cfcf_normal_ridge = soft_ridge
+        self._init_diagnostics = None
         self.fov_slice_yx = None
         self._observed_shape_zyx = None
         self._bottom_current_grid_mode = None
@@ -585,8 +592,12 @@ class NFGSSolverGPU:
             raise ValueError("fixed-point tolerances must be positive")
         if int(fixed_point_patience) < 1:
             raise ValueError("fixed_point_patience must be >= 1")
-        if mode not in ("gs_cfcf", "learned"):
-            raise NotImplementedError(f"init_mode={init_mode!r}: only the gs_cfcf start is built for B200")
+        if mode not in ("gs_cfcf", "soft_cfcf", "learned"):
+            raise NotImplementedError(f"init_mode={init_mode!r}: the gs_cfcf and soft_cfcf starts are built for B200")
+        if mode == "soft_cfcf" and self.Nz < 5:
+            raise ValueError("soft_cfcf requires Nz >= 5")
+        if mode == "soft_cfcf" and (self.Nx < 3 or self.Ny < 3):
+            raise ValueError("soft_cfcf requires Nx, Ny >= 3")
         if polarity_mask not in _POLARITY:
             raise ValueError("polarity_mask must be 'positive', 'negative', or 'both'")
         if self.gaussian_separation_diagnostics is None:
@@ -605,6 +616,11 @@ class NFGSSolverGPU:
             use_graph=int(bool(use_graph)))
         lib = self._lib
         L.check(lib.nfgs_iterate_begin(self._h, L.C.byref(stop)))
+        self._init_diagnostics = {"init_mode": "gs_cfcf", "mfr_count": 0,
+                                  "gaussian_separation": self.gaussian_separation_diagnostics,
+                                  "coupled_k0": self._k0_diagnostics}
+        if mode == "soft_cfcf":
+            self._init_diagnostics = self._soft_cfcf_start()
         self.learned_start_info = None
         if mode == "learned":
             from . import learned as _learned
@@ -617,10 +633,25 @@ class NFGSSolverGPU:
             am_text = f"{am:.3e}" if am is not None else "off"
             print(f"Initial  sigma={sc[0]:.4e}  divB={sc[1]:.4e}  E={sc[2]:.4e} "
                   f"(mu0={mu}, adaptive={adaptive_mu}, alpha_max={am_text}, toroidal_bc=True)")
-        return dict(lib=lib, verbose=verbose, per_step_callback=per_step_callback, step_by_step=step_by_step,
+        return dict(lib=lib, mode=mode, verbose=verbose, per_step_callback=per_step_callback, step_by_step=step_by_step,
                     check_every=check_every, max_iter=max_iter, stop_mode=stop_mode, update_tol=update_tol,
                     observable_tol=observable_tol, fixed_point_pde_tol=fixed_point_pde_tol,
                     fixed_point_patience=fixed_point_patience, eps=eps, use_imp=use_imp)
+
+    def _soft_cfcf_start(self):
+        """soft_cfcf start on the device (nfgs_solver.py:6427-6484), after
+        nfgs_iterate_begin: replaces the gs_cfcf start; returns the init
+        diagnostics with the modal energies (nfgs_solver.py:6473-6483)."""
+        out = np.zeros(4)
+        L.check(self._lib.nfgs_iterate_soft_cfcf_start(self._h, float(self.soft_cfcf_epsilon),
+                                                       float(self.soft_cfcf_normal_ridge), L.dptr(out)))
+        return {"init_mode": "soft_cfcf", "mfr_count": 0, "soft_cfcf_epsilon": self.soft_cfcf_epsilon,
+                "soft_cfcf_mode_batch_size": self.soft_cfcf_mode_batch_size,
+                "soft_cfcf_normal_ridge": self.soft_cfcf_normal_ridge,
+                "soft_cfcf": {"curl_current_energy": float(out[0]), "current_energy": float(out[1]),
+                              "objective": float(out[2])},
+                "gaussian_separation": self.gaussian_separation_diagnostics,
+                "coupled_k0": self._k0_diagnostics}
 
     def _iterate_loop(self, ctx):
         lib, per_step_callback, check_every = ctx["lib"], ctx["per_step_callback"], ctx["check_every"]
@@ -662,7 +693,9 @@ class NFGSSolverGPU:
         code = lib.nfgs_iterate_end(self._h, L.C.byref(res), L.dptr(hist), hist.shape[0])
         n = int(res.n_hist)
         hist = hist[:n]
-        zr = [0.0] + [float(v) for v in hist[:, 7]]
+        # the gs_cfcf start's zero-source solve records a 0.0 ratio first; the
+        # soft_cfcf start runs no source solve (nfgs_solver.py:5457-5476)
+        zr = ([] if ctx.get("mode") == "soft_cfcf" else [0.0]) + [float(v) for v in hist[:, 7]]
         if code == L.NFGS_EPOLICY:
             # the failing source of the next step is the last recorded ratio
             self._source_zero_mode_history = zr
@@ -710,9 +743,7 @@ class NFGSSolverGPU:
             "auto_rbsl_improvement_grace": 0,
             "last_sigma_improvement": None if math.isnan(res.last_sigma_improvement)
             else float(res.last_sigma_improvement),
-            "init_diagnostics": {"init_mode": "gs_cfcf", "mfr_count": 0,
-                                 "gaussian_separation": self.gaussian_separation_diagnostics,
-                                 "coupled_k0": self._k0_diagnostics},
+            "init_diagnostics": dict(self._init_diagnostics),
             "source_partition_mode": self.source_partition_mode,
             "bottom_current_grid_mode": self._bottom_current_grid_mode,
             "vertical_current_operator": self.vertical_current_operator,

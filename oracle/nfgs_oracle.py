@@ -311,7 +311,7 @@ class OracleNFGS:
     """FP64 restatement of ``NFGSSolverGPU`` (nfgs_solver.py:3905-7196).
 
     Supported: gaussian_separated partition, staggered_face current,
-    direct poloidal update, gs_cfcf start, sigma_best stop (with optional
+    direct poloidal update, gs_cfcf and soft_cfcf starts, sigma_best stop (with optional
     adaptive_mu rollback), mixed bottom Robin weight rho in [0, 1] or the
     bottom-divergence projection, frozen/omitted/external/user horizontal
     zero modes.
@@ -330,7 +330,7 @@ class OracleNFGS:
                  weak_field_floor_b2=1e-20, gaussian_horizontal_operator="spectral",
                  bottom_parallel_current_mode="observed_full",
                  user_supplied_open_bz=None, user_supplied_horizontal_field=None,
-                 external_potential_field=None):
+                 external_potential_field=None, soft_cfcf_epsilon=None, soft_cfcf_normal_ridge=0.0):
         ix, iy, iz = int(Nx), int(Ny), int(Nz)
         mode = str(calculation_domain_mode).lower().replace("-", "_")
         # nfgs_solver.py:771-819
@@ -384,6 +384,11 @@ class OracleNFGS:
         self.user_open_bz = user_supplied_open_bz
         self.user_h = user_supplied_horizontal_field
         self.external = external_potential_field
+        # nfgs_solver.py:4299-4305
+        gs = min(self.dx, self.dy, self.dz)
+        self.soft_cfcf_epsilon = 1.0e-4 / (gs * gs) if soft_cfcf_epsilon is None else float(soft_cfcf_epsilon)
+        self.soft_cfcf_normal_ridge = float(soft_cfcf_normal_ridge)
+        self.soft_cfcf_diagnostics = None
         self.source_zero_mode_history: list[float] = []
         self.last_source_zero_mode_by_height: list[float] = []
         self.projection_history: list[dict] = []
@@ -1045,13 +1050,52 @@ class OracleNFGS:
             alpha = np.clip(alpha, -am, am)
         return self.faces_to_centres(alpha[None] * Bf)
 
-    def compute_initial_conditions(self):
-        """gs_cfcf start (nfgs_solver.py:6613-6645)."""
+    def compute_initial_conditions(self, init_mode="gs_cfcf"):
+        """gs_cfcf start (nfgs_solver.py:6613-6645); soft_cfcf dispatches to
+        soft_cfcf_initial_state."""
+        mode = str(init_mode).lower().replace("-", "_")
+        if mode in ("soft_cfcf", "yi_soft"):
+            return self.soft_cfcf_initial_state()
+        if mode != "gs_cfcf":
+            raise NotImplementedError("the oracle restates the gs_cfcf and soft_cfcf starts")
         zeros = np.zeros((self.Nz, self.Ny, self.Nx))
         phi = self.solve_phi_c(zeros, self.Phi_above_bottom)
         phi = self.apply_projection(phi)
         bcz = lap_xy(phi, self.dx, self.dy)
         az = self.solve_az(zeros)
+        B, J, Bc = self.reconstruct(phi, az, bcz)
+        return B, J, phi, az, Bc
+
+    def soft_cfcf_initial_state(self):
+        """soft_cfcf start (nfgs_solver.py:6427-6484): per horizontal mode the
+        z profile minimising the modal curl(J) functional with the bottom and
+        transparent-top rows exact; Phi_c and A_z from the inverse transforms,
+        bottom planes restored, A_z walls zero."""
+        from . import soft_cfcf_oracle as SO
+
+        if self.Nz < 5:
+            raise ValueError("soft_cfcf requires Nz >= 5")
+        if self.Nx < 3 or self.Ny < 3:
+            raise ValueError("soft_cfcf requires Nx, Ny >= 3")
+        nz, ny, nx = self.Nz, self.Ny, self.Nx
+        eps, ridge = self.soft_cfcf_epsilon, self.soft_cfcf_normal_ridge
+        k_phi = np.sqrt(np.maximum(-self.lam_neumann(), 0.0))
+        pb = dct2(self.Phi_above_bottom)
+        pb[0, 0] = 0.0
+        phi_hat = SO.modal_profiles(k_phi, pb, "phi", nz, self.dz, eps, ridge).reshape(nz, ny, nx)
+        phi = idct2(phi_hat)
+        phi[0] = self.Phi_above_bottom
+        k_az = np.sqrt(np.maximum(-self.lam_dirichlet(), 0.0))
+        ab = dst2(self.Az_bottom[1:-1, 1:-1])
+        az_hat = SO.modal_profiles(k_az, ab, "az", nz, self.dz, eps, ridge).reshape(nz, ny - 2, nx - 2)
+        az = np.zeros((nz, ny, nx))
+        az[:, 1:-1, 1:-1] = idst2(az_hat)
+        az[0] = self.Az_bottom
+        self._az_walls_zero(az)
+        en = SO.modal_energies(phi_hat, k_phi, az_hat, k_az, nx, ny, self.dx, self.dy, self.dz)
+        en["objective"] = en["curl_current_energy"] + eps * en["current_energy"]
+        self.soft_cfcf_diagnostics = en
+        bcz = lap_xy(phi, self.dx, self.dy)
         B, J, Bc = self.reconstruct(phi, az, bcz)
         return B, J, phi, az, Bc
 
@@ -1100,11 +1144,11 @@ class OracleNFGS:
                 mu_min=0.02, mu_max=1.0, mu_backoff=0.5, mu_growth=1.1, growth_streak=5,
                 divergence_factor=2.0, max_rollbacks=12, stop_mode="sigma_best", **_ignored):
         """Stable driver (nfgs_solver.py:3522-3850) with the NFGS wrapper (6937-7009)."""
-        if str(init_mode).lower().replace("-", "_") != "gs_cfcf":
-            raise NotImplementedError("the oracle restates the gs_cfcf start only")
+        if str(init_mode).lower().replace("-", "_") not in ("gs_cfcf", "soft_cfcf", "yi_soft"):
+            raise NotImplementedError("the oracle restates the gs_cfcf and soft_cfcf starts")
         if stop_mode != "sigma_best":
             raise ValueError("stop_mode='fixed_point' requires record_iteration_diagnostics=True")
-        B, J, phi, az, Bc = self.compute_initial_conditions()
+        B, J, phi, az, Bc = self.compute_initial_conditions(init_mode)
         sigma0, divb0, e0 = self.compute_sigma(B, J), self.compute_divB(B), self.compute_energy(B)
         hist = {k: [] for k in ("sigma", "divB", "energy", "mu", "rollback", "sigma_relative_change",
                                 "energy_relative_change", "fixed_point_criteria_met")}
