@@ -200,7 +200,7 @@ __device__ Aff row_at(const Mode& m, double eps, int r, double* w, int* err) {
 // DCT endpoint weights applied for Phi (nfgs_solver.py:6486-6540).
 // Scratch: band[(i*BS + d)*CH + t], vec[i*CH + t] for the chunk's thread t.
 template <typename T>
-__global__ void __launch_bounds__(128) k_soft_profile(Geo g, int kind, long long m0, long long cnt, long long M,
+__global__ void __launch_bounds__(128, 4) k_soft_profile(Geo g, int kind, long long m0, long long cnt, long long M,
                                                       const double* __restrict__ kk, const double* __restrict__ bot,
                                                       double eps, double ridge, long long CH,
                                                       double* __restrict__ band, double* __restrict__ vec,

@@ -1732,9 +1732,10 @@ static int soft_cfcf_start_t(Handle* h, double eps, double ridge, double* out) {
         return fail(NFGS_EINVAL, "soft_cfcf_normal_ridge must be non-negative");
     const long long P = g.P, PI = h->PI;
     const long long n = g.nz - 2;
-    // modes per launch: band + vector scratch of at most 256 MB
+    // modes per launch: band + vector scratch of at most 1 GB (about 90k
+    // modes at 257 heights, more than the ~76k threads the SMs hold at once)
     const long long per_mode = n * (soft::BS + 1) * 8;
-    const long long CH = std::max(1LL, std::min(P, (256LL << 20) / per_mode));
+    const long long CH = std::max(1LL, std::min(P, (1LL << 30) / per_mode));
     double *band = nullptr, *vec = nullptr, *en = nullptr, *sums = nullptr;
     int* err = nullptr;
     auto cleanup = [&]() {

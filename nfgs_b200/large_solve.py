@@ -8,7 +8,9 @@ observed box), fields compared on the device.
 
 The transforms (256 pairs per axis) run on the four-role tensor-core
 kernel; NFGS_DISABLE_TC=1 in the environment runs them on the SIMT
-contractions instead.
+contractions instead.  --soft also solves from the soft_cfcf start and
+times both starts (iterate_begin with the start's evaluation, CUDA-synchronised
+wall time, best of three).
 """
 
 from __future__ import annotations
@@ -34,14 +36,29 @@ def _solver(n, nz, seed, dtype):
     return s
 
 
-def _solve(s, max_iter):
+def _solve(s, max_iter, init_mode="gs_cfcf"):
     import torch
 
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    h = s.iterate(max_iter=max_iter, verbose=False, **STOP)
+    h = s.iterate(max_iter=max_iter, verbose=False, init_mode=init_mode, **STOP)
     torch.cuda.synchronize()
     return h, time.perf_counter() - t0
+
+
+def _start_seconds(s, init_mode, reps=3):
+    """Best wall time of a begun-and-ended iteration (the start state, its
+    sigma_J, divB and energy), synchronised."""
+    import torch
+
+    best = float("inf")
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.iterate(max_iter=0, verbose=False, init_mode=init_mode, **STOP)
+        torch.cuda.synchronize()
+        best = min(best, time.perf_counter() - t0)
+    return best
 
 
 def main(argv=None):
@@ -56,6 +73,7 @@ def main(argv=None):
     ap.add_argument("--max-iter", type=int, default=3000)
     ap.add_argument("--phase-iters", type=int, default=5)
     ap.add_argument("--fp64", action="store_true", help="also solve in FP64 and score the FP32 result against it")
+    ap.add_argument("--soft", action="store_true", help="also solve from the soft_cfcf start and time both starts")
     ap.add_argument("--report", default=None)
     args = ap.parse_args(argv)
 
@@ -73,7 +91,14 @@ def main(argv=None):
     out["gcell_iter_per_s"] = cells / (ph.sum() * 1e-3) / 1e9
     h, t = _solve(s, args.max_iter)
     out["fp32"] = {"iterations": len(h["sigma"]), "best_iter": h["best_iter"], "best_sigma": h["best_sigma"],
-                   "stop_reason": h["stop_reason"], "seconds": t}
+                   "stop_reason": h["stop_reason"], "seconds": t, "initial_sigma": h["initial_sigma"]}
+    if args.soft:
+        out["start_seconds"] = {m: _start_seconds(s, m) for m in ("gs_cfcf", "soft_cfcf")}
+        hs, ts = _solve(s, args.max_iter, "soft_cfcf")
+        out["fp32_soft_cfcf"] = {"iterations": len(hs["sigma"]), "best_iter": hs["best_iter"],
+                                 "best_sigma": hs["best_sigma"], "stop_reason": hs["stop_reason"], "seconds": ts,
+                                 "initial_sigma": hs["initial_sigma"],
+                                 "soft_cfcf": hs["init_diagnostics"]["soft_cfcf"]}
     if args.fp64:
         s64 = _solver(args.n, args.nz, args.seed, "float64")
         h64, t64 = _solve(s64, args.max_iter)
