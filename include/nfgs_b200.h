@@ -368,6 +368,47 @@ int nfgs_field_metrics(const void* ref, const void* sol, const void* cur, int32_
                        int32_t nx, const double* spacing3, const int32_t* roi6, double* out, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Field-line tracing and squashing-factor (Q) maps on a seed plane.
+ * Replace the FastQSL tracer and Q step that the reference drives through
+ * CuPy for its topology maps: compute_y0_qmap / compute_bottom_qmap
+ * (nfgs/_backend/util/fastqsl_plane.py:203-506), which launch TraceAllBline
+ * (third_party/FastQSL/fastqslpy/cu/TraceBlineAdaptive.cu:429) over the seeds
+ * and then QCalcPlane.  Written from the published definition of Q (Titov,
+ * Hornig & Demoulin 2002; Titov 2007), not from that source.
+ *
+ * nfgs_trace_field_lines: b = device (3, nz, ny, nx) volume of dtype (NFGS_F32
+ * or NFGS_F64), at least 2 nodes per axis.  Positions are grid-index units
+ * (x in [0, nx-1], y in [0, ny-1], z in [0, nz-1]), B trilinear between
+ * nodes.  Each of the n seeds (device (n, 3) xyz of dtype; clamped into the
+ * box) is traced along +B and along -B with classical RK4 steps of length
+ * `step` along the unit field direction, until the step that leaves the box
+ * (cut where its chord meets the first face, the end snapped onto that face)
+ * or max_steps steps.  normal3 = unit normal n0 of the seed plane.
+ * Outputs (device, dtype unless stated):
+ *   ends   (2, n, 3)  forward then backward end points;
+ *   flags  (2, n)     int32: face reached 1..6 = x=0, x=nx-1, y=0, y=ny-1,
+ *                     z=0, z=nz-1; 0 max_steps reached; -1 zero field met;
+ *   bn     (3, n)     B.n0 at the seed, |B.n| at the forward and backward
+ *                     ends (n the face normal; NaN without a face);
+ *   length (2, n)     path length of each half, grid units.
+ * stream: a cudaStream_t (NULL for the legacy default stream) on the current
+ * device; the call returns when the outputs are complete.
+ *
+ * nfgs_qmap_plane: the n = nu * nv seeds of the trace formed a regular grid
+ * of unit spacing on the plane (seed iu + nu * iv, iu along the unit in-plane
+ * axis u, iv along v).  q (nv, nu) of dtype: with a = dr/du, b = dr/dv of the
+ * forward (+) and backward (-) end points by central differences,
+ *   Q = [|a+|^2 |b-|^2 + |b+|^2 |a-|^2 - 2 (a+.b+)(a-.b-)] |Bn+ Bn-| / Bn0^2;
+ * NaN on the plane's border and where the five lines of a direction (the
+ * seed and its four neighbours) do not all end on one face.
+ * ------------------------------------------------------------------------ */
+int nfgs_trace_field_lines(const void* b, int32_t dtype, int32_t nz, int32_t ny, int32_t nx, const void* seeds,
+                           int64_t n, const double* normal3, double step, int32_t max_steps, void* ends,
+                           int32_t* flags, void* bn, void* length, void* stream);
+int nfgs_qmap_plane(int32_t dtype, int32_t nu, int32_t nv, const void* ends, const int32_t* flags, const void* bn,
+                    void* q, void* stream);
+
+/* ------------------------------------------------------------------------
  * Learned warm start: operator kernels of a 3-D neural operator on a
  * truncated cosine basis.  No reference counterpart (the reference starts
  * every solve from the zero-source state, nfgs_solver.py:6613-6645).

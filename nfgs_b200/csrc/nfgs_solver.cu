@@ -12,6 +12,7 @@
 #include "nfgs_stencil.cuh"
 #include "nfgs_metrics.cuh"
 #include "nfgs_soft.cuh"
+#include "nfgs_trace.cuh"
 #include <cuda_fp16.h>
 
 #include <cmath>
@@ -2708,6 +2709,32 @@ static int gaussian_above_noalloc_impl(Handle* h, double* out, cudaStream_t st) 
 // ===========================================================================
 // C ABI
 // ===========================================================================
+namespace {
+
+template <typename T>
+static int trace_lines_t(const void* b, int32_t nz, int32_t ny, int32_t nx, const void* seeds, int64_t n,
+                         const double* nrm, double step, int32_t max_steps, void* ends, int32_t* flags, void* bn,
+                         void* len, cudaStream_t s) {
+    const long long V = (long long)nz * ny * nx;
+    T* pk = nullptr;
+    CK(cudaMallocAsync((void**)&pk, (size_t)V * 4 * sizeof(T), s));
+    trace::k_pack<T><<<(unsigned)((V + 255) / 256), 256, 0, s>>>((const T*)b, V, pk);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && n > 0) {
+        const trace::Box bx{nx, ny, nz};
+        trace::k_trace<T><<<(unsigned)((2 * n + 127) / 128), 128, 0, s>>>(
+            pk, bx, (const T*)seeds, n, (T)nrm[0], (T)nrm[1], (T)nrm[2], (T)step, max_steps, (T*)ends, flags,
+            (T*)bn, (T*)len);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(pk, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(NFGS_ECUDA, std::string("trace: ") + cudaGetErrorString(e));
+    return NFGS_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* nfgs_last_error(void) { return g_err.c_str(); }
@@ -3033,6 +3060,42 @@ int nfgs_field_metrics(const void* ref, const void* sol, const void* cur, int32_
     a.dx = spacing3[0]; a.dy = spacing3[1]; a.dz = spacing3[2];
     cudaStream_t s = (cudaStream_t)stream;
     return dtype == NFGS_F32 ? field_metrics_t<float>(a, s, out) : field_metrics_t<double>(a, s, out);
+}
+
+int nfgs_trace_field_lines(const void* b, int32_t dtype, int32_t nz, int32_t ny, int32_t nx, const void* seeds,
+                           int64_t n, const double* normal3, double step, int32_t max_steps, void* ends,
+                           int32_t* flags, void* bn, void* length, void* stream) {
+    g_err.clear();
+    if (!b || !normal3 || (n > 0 && (!seeds || !ends || !flags || !bn || !length)))
+        return fail(NFGS_EINVAL, "null argument");
+    if (dtype != NFGS_F32 && dtype != NFGS_F64) return fail(NFGS_EINVAL, "dtype must be F32 or F64");
+    if (nz < 2 || ny < 2 || nx < 2) return fail(NFGS_EINVAL, "the field needs at least 2 nodes per axis");
+    if (n < 0 || 2 * n > (int64_t)INT32_MAX * 128) return fail(NFGS_EINVAL, "bad seed count");
+    if (!(step > 0.0) || !std::isfinite(step)) return fail(NFGS_EINVAL, "step must be positive");
+    if (max_steps < 1) return fail(NFGS_EINVAL, "max_steps must be positive");
+    cudaStream_t s = (cudaStream_t)stream;
+    return dtype == NFGS_F32
+               ? trace_lines_t<float>(b, nz, ny, nx, seeds, n, normal3, step, max_steps, ends, flags, bn, length, s)
+               : trace_lines_t<double>(b, nz, ny, nx, seeds, n, normal3, step, max_steps, ends, flags, bn, length,
+                                       s);
+}
+
+int nfgs_qmap_plane(int32_t dtype, int32_t nu, int32_t nv, const void* ends, const int32_t* flags, const void* bn,
+                    void* q, void* stream) {
+    g_err.clear();
+    if (!ends || !flags || !bn || !q) return fail(NFGS_EINVAL, "null argument");
+    if (dtype != NFGS_F32 && dtype != NFGS_F64) return fail(NFGS_EINVAL, "dtype must be F32 or F64");
+    if (nu < 1 || nv < 1 || nv > 65535) return fail(NFGS_EINVAL, "bad seed plane size");
+    cudaStream_t s = (cudaStream_t)stream;
+    const dim3 grid((unsigned)((nu + 127) / 128), (unsigned)nv);
+    if (dtype == NFGS_F32)
+        trace::k_qmap<float><<<grid, 128, 0, s>>>(nu, nv, (const float*)ends, flags, (const float*)bn, (float*)q);
+    else
+        trace::k_qmap<double><<<grid, 128, 0, s>>>(nu, nv, (const double*)ends, flags, (const double*)bn, (double*)q);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(NFGS_ECUDA, std::string("qmap: ") + cudaGetErrorString(e));
+    return NFGS_OK;
 }
 
 int nfgs_get_scalars_state(void* handle, int32_t which, double* phi, double* az, double* scalars3) {

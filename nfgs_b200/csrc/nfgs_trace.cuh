@@ -1,0 +1,215 @@
+// Field-line tracing and the squashing factor Q on a seed plane.
+//
+// Positions are in grid-index units (x in [0, nx-1], y in [0, ny-1],
+// z in [0, nz-1]); B is sampled on the nodes of a (3, nz, ny, nx) volume and
+// interpolated trilinearly.  A line follows the unit field direction with
+// classical fourth-order Runge-Kutta steps of fixed length; the step that
+// leaves the box is cut where its chord meets the first face, and the end
+// point is snapped onto that face.  Q (Titov, Hornig & Demoulin 2002;
+// Titov 2007) is ||D||^2 / |det D| for the footpoint map D; for seeds on a
+// plane with in-plane unit axes u, v, the derivatives a = dr/du, b = dr/dv of
+// the two end points give ||D||^2 |det D|^-1 =
+//   [|a+|^2 |b-|^2 + |b+|^2 |a-|^2 - 2 (a+.b+)(a-.b-)] |Bn+ Bn-| / Bn0^2,
+// using flux conservation |det(dr/d(u,v))| = |Bn0 / Bn|.
+//
+// One thread per (seed, direction): the threads of a warp trace neighbouring
+// seeds, whose lines stay close, so the corner loads of the interpolation
+// hit the same L1/L2 lines.  The field is repacked as 4 values per node
+// (one 16-byte load in FP32, two in FP64).
+#pragma once
+#include "nfgs_common.cuh"
+
+namespace trace {
+
+template <typename T>
+__device__ __forceinline__ void load3(const T* __restrict__ p, T& x, T& y, T& z);
+
+template <>
+__device__ __forceinline__ void load3<float>(const float* __restrict__ p, float& x, float& y, float& z) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    x = v.x; y = v.y; z = v.z;
+}
+
+template <>
+__device__ __forceinline__ void load3<double>(const double* __restrict__ p, double& x, double& y, double& z) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+    x = a.x; y = a.y; z = __ldg(p + 2);
+}
+
+// (3, nz, ny, nx) component-major -> 4 values per node
+template <typename T>
+__global__ void k_pack(const T* __restrict__ b, long long V, T* __restrict__ pk) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= V) return;
+    pk[4 * c] = b[c];
+    pk[4 * c + 1] = b[V + c];
+    pk[4 * c + 2] = b[2 * V + c];
+    pk[4 * c + 3] = T(0);
+}
+
+struct Box {
+    int nx, ny, nz;
+};
+
+// trilinear interpolation at a position clamped into the box
+template <typename T>
+__device__ __forceinline__ void interp(const T* __restrict__ pk, Box bx, T x, T y, T z, T& ox, T& oy, T& oz) {
+    x = fmin(fmax(x, T(0)), T(bx.nx - 1));
+    y = fmin(fmax(y, T(0)), T(bx.ny - 1));
+    z = fmin(fmax(z, T(0)), T(bx.nz - 1));
+    const int i = min((int)floor(x), bx.nx - 2);
+    const int j = min((int)floor(y), bx.ny - 2);
+    const int k = min((int)floor(z), bx.nz - 2);
+    const T fx = x - T(i), fy = y - T(j), fz = z - T(k);
+    const long long sx = 4, sy = 4LL * bx.nx, sz = 4LL * bx.nx * bx.ny;
+    const T* p = pk + k * sz + j * sy + i * sx;
+    T c[8][3];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        load3<T>(p + ((q >> 2) & 1) * sz + ((q >> 1) & 1) * sy + (q & 1) * sx, c[q][0], c[q][1], c[q][2]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const T x00 = c[0][d] + fx * (c[1][d] - c[0][d]);
+        const T x10 = c[2][d] + fx * (c[3][d] - c[2][d]);
+        const T x01 = c[4][d] + fx * (c[5][d] - c[4][d]);
+        const T x11 = c[6][d] + fx * (c[7][d] - c[6][d]);
+        const T y0 = x00 + fy * (x10 - x00);
+        const T y1 = x01 + fy * (x11 - x01);
+        const T v = y0 + fz * (y1 - y0);
+        if (d == 0) ox = v; else if (d == 1) oy = v; else oz = v;
+    }
+}
+
+// unit direction s B / |B|; false where |B| = 0
+template <typename T>
+__device__ __forceinline__ bool direction(const T* __restrict__ pk, Box bx, T s, const T (&p)[3], T (&d)[3]) {
+    T b0, b1, b2;
+    interp<T>(pk, bx, p[0], p[1], p[2], b0, b1, b2);
+    const T m = sqrt(b0 * b0 + b1 * b1 + b2 * b2);
+    if (!(m > T(0))) return false;
+    const T f = s / m;
+    d[0] = b0 * f; d[1] = b1 * f; d[2] = b2 * f;
+    return true;
+}
+
+// Trace seed `si` along +B (dir 0) or -B (dir 1).  ends (2, n, 3), flags
+// (2, n), bn (3, n): B.n0 at the seed, |B.n| at the forward and backward
+// ends; len (2, n) per direction.
+template <typename T>
+__global__ void __launch_bounds__(128) k_trace(const T* __restrict__ pk, Box bx, const T* __restrict__ seeds,
+                                               long long n, T n0x, T n0y, T n0z, T h, int max_steps,
+                                               T* __restrict__ ends, int* __restrict__ flags, T* __restrict__ bn,
+                                               T* __restrict__ len) {
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= 2 * n) return;
+    const int dir = tid >= n ? 1 : 0;
+    const long long si = tid - (long long)dir * n;
+    const T s = dir == 0 ? T(1) : T(-1);
+    const T hi[3] = {T(bx.nx - 1), T(bx.ny - 1), T(bx.nz - 1)};
+    // seeds are clamped into the box, so every chord that leaves it starts inside
+    T p[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) p[d] = fmin(fmax(seeds[3 * si + d], T(0)), hi[d]);
+    if (dir == 0) {
+        T b0, b1, b2;
+        interp<T>(pk, bx, p[0], p[1], p[2], b0, b1, b2);
+        bn[si] = b0 * n0x + b1 * n0y + b2 * n0z;
+    }
+    const T h2 = h * T(0.5), h6 = h / T(6);
+    T length = T(0);
+    int flag = 0;
+    for (int it = 0; it < max_steps; ++it) {
+        T k1[3], k2[3], k3[3], k4[3], q[3];
+        if (!direction<T>(pk, bx, s, p, k1)) { flag = -1; break; }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) q[d] = p[d] + h2 * k1[d];
+        if (!direction<T>(pk, bx, s, q, k2)) { flag = -1; break; }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) q[d] = p[d] + h2 * k2[d];
+        if (!direction<T>(pk, bx, s, q, k3)) { flag = -1; break; }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) q[d] = p[d] + h * k3[d];
+        if (!direction<T>(pk, bx, s, q, k4)) { flag = -1; break; }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) q[d] = p[d] + h6 * (k1[d] + T(2) * k2[d] + T(2) * k3[d] + k4[d]);
+        bool inside = true;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) inside = inside && q[d] >= T(0) && q[d] <= hi[d];
+        if (inside) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) p[d] = q[d];
+            length += h;
+            continue;
+        }
+        // the chord p -> q meets the first face at fraction t
+        T t = T(2);
+        int face = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (q[d] < T(0)) {
+                const T td = (T(0) - p[d]) / (q[d] - p[d]);
+                if (td < t) { t = td; face = 2 * d + 1; }
+            } else if (q[d] > hi[d]) {
+                const T td = (hi[d] - p[d]) / (q[d] - p[d]);
+                if (td < t) { t = td; face = 2 * d + 2; }
+            }
+        }
+        if (face == 0) break;  // unreachable with p inside: kept as a guard on the face index
+#pragma unroll
+        for (int d = 0; d < 3; ++d) p[d] = p[d] + t * (q[d] - p[d]);
+        const int fd = (face - 1) >> 1;
+        p[fd] = (face & 1) ? T(0) : hi[fd];
+        length += t * h;
+        flag = face;
+        break;
+    }
+    ends[3 * tid] = p[0];
+    ends[3 * tid + 1] = p[1];
+    ends[3 * tid + 2] = p[2];
+    flags[tid] = flag;
+    len[tid] = length;
+    T e;
+    if (flag > 0) {
+        T b[3];
+        interp<T>(pk, bx, p[0], p[1], p[2], b[0], b[1], b[2]);
+        e = fabs(b[(flag - 1) >> 1]);
+    } else {
+        e = T(NAN);
+    }
+    bn[n * (1 + dir) + si] = e;
+}
+
+// Q on a regular nv x nu seed plane (seed iu + nu iv, unit spacing)
+template <typename T>
+__global__ void k_qmap(int nu, int nv, const T* __restrict__ ends, const int* __restrict__ flags,
+                       const T* __restrict__ bn, T* __restrict__ q) {
+    const int iu = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iv = blockIdx.y;
+    if (iu >= nu || iv >= nv) return;
+    const long long n = (long long)nu * nv;
+    const long long c = (long long)iv * nu + iu;
+    if (iu == 0 || iv == 0 || iu == nu - 1 || iv == nv - 1) { q[c] = T(NAN); return; }
+    const long long nb[4] = {c + 1, c - 1, c + nu, c - nu};
+    T a[2][3], b[2][3];
+    for (int dir = 0; dir < 2; ++dir) {
+        const int* f = flags + dir * n;
+        const int fc = f[c];
+        bool ok = fc > 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) ok = ok && f[nb[r]] == fc;
+        if (!ok) { q[c] = T(NAN); return; }
+        const T* e = ends + 3 * dir * n;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            a[dir][d] = (e[3 * nb[0] + d] - e[3 * nb[1] + d]) * T(0.5);
+            b[dir][d] = (e[3 * nb[2] + d] - e[3 * nb[3] + d]) * T(0.5);
+        }
+    }
+    auto dot = [](const T (&x)[3], const T (&y)[3]) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
+    const T br = dot(a[0], a[0]) * dot(b[1], b[1]) + dot(b[0], b[0]) * dot(a[1], a[1]) -
+                 T(2) * dot(a[0], b[0]) * dot(a[1], b[1]);
+    const T b0 = bn[c];
+    q[c] = br * fabs(bn[n + c] * bn[2 * n + c]) / (b0 * b0);
+}
+
+}  // namespace trace

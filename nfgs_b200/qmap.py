@@ -1,0 +1,255 @@
+"""Field-line tracing and squashing-factor (Q) maps on the GPU.
+
+Drop-in for the reference's topology-map helpers
+``compute_y0_qmap`` / ``compute_bottom_qmap``
+(nfgs/_backend/util/fastqsl_plane.py:203-506), which trace every seed of a
+plane with FastQSL through CuPy and evaluate Q with its QCalcPlane.  Here the
+library's own tracer (``nfgs_trace_field_lines``: trilinear B, fixed-step
+RK4, ends snapped onto the face the line leaves through) and Q kernel
+(``nfgs_qmap_plane``: Q = ||D||^2/|det D| of the footpoint map from central
+differences over the seed plane) run on device tensors; nothing of the field
+goes through the host when it is passed as a CUDA tensor, e.g. from
+``NFGSSolverGPU.fields_to_torch()``.
+
+Differences from the reference helpers, by design:
+* one fixed RK4 step (``step_len``, default 1/8 cell) instead of FastQSL's
+  adaptive RKF45; ``tol``, ``block_x`` and ``trace_chunk_seeds`` are accepted
+  and recorded only (the library launches every seed at once);
+* flags are the face codes of ``nfgs_trace_field_lines`` (1..6 for
+  x=0, x=nx-1, y=0, y=ny-1, z=0, z=nz-1; 0 unfinished; -1 zero field);
+* ``include_twist=True`` raises NotImplementedError.
+
+    python -m nfgs_b200.qmap --n 256 --nz 128 --report qmap.json
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import time
+
+import numpy as np
+
+from . import _lib as L
+
+Y0_PLANE_COORDINATE_CONTRACT = "physical_midplane_fractional_index_v2"
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def physical_midplane_grid_index(n_nodes: int) -> float:
+    """Grid coordinate of the physical midpoint of a node axis
+    (fastqsl_plane.py:49-54)."""
+    n = int(n_nodes)
+    if n < 1:
+        raise ValueError(f"n_nodes must be positive, got {n_nodes}")
+    return 0.5 * float(n - 1)
+
+
+def _volume(bx, by, bz, dtype):
+    """(3, nz, ny, nx) contiguous CUDA tensor of dtype from three arrays or tensors."""
+    torch = _torch()
+    comps = []
+    for a in (bx, by, bz):
+        t = a if isinstance(a, torch.Tensor) else torch.as_tensor(np.asarray(a))
+        comps.append(t.to(device="cuda", dtype=dtype))
+    if comps[0].ndim != 3 or comps[0].shape != comps[1].shape or comps[0].shape != comps[2].shape:
+        raise ValueError("bx, by, and bz must have the same (nz,ny,nx) shape")
+    return torch.stack(comps).contiguous()
+
+
+def spectral_gaussian_lowpass(b, sigma_cells: float):
+    """Isotropic Gaussian low-pass of each component in Fourier space, sigma in
+    cells (fastqsl_plane.py:82-101), on the device; b (3, nz, ny, nx)."""
+    torch = _torch()
+    sigma = float(sigma_cells)
+    if sigma <= 0.0:
+        return b
+    if not bool(torch.isfinite(b).all()):
+        raise ValueError("field must be finite for spectral filtering")
+    shape = b.shape[1:]
+    k2 = None
+    for ax, n in enumerate(shape):
+        f = torch.fft.fftfreq(n, dtype=torch.float64, device=b.device) ** 2
+        view = [1, 1, 1]
+        view[ax] = n
+        f = f.view(view)
+        k2 = f if k2 is None else k2 + f
+    transfer = torch.exp(-0.5 * ((2.0 * math.pi * sigma) ** 2) * k2)
+    out = torch.fft.ifftn(torch.fft.fftn(b.double(), dim=(1, 2, 3)) * transfer, dim=(1, 2, 3)).real
+    return out.to(torch.float32).to(b.dtype).contiguous()
+
+
+def trace_field_lines(b, seeds, *, normal=(0.0, 0.0, 1.0), step_len: float = 1.0 / 8.0, max_steps=None):
+    """Trace seeds (n, 3 xyz grid units) through b (3, nz, ny, nx CUDA
+    tensor, float32 or float64) along +B and -B.  Returns device tensors:
+    ends (2, n, 3), flags (2, n) int32, bn (3, n), length (2, n)."""
+    torch = _torch()
+    if b.dtype not in (torch.float32, torch.float64) or b.device.type != "cuda" or b.ndim != 4 or b.shape[0] != 3:
+        raise ValueError("b must be a (3, nz, ny, nx) float32/float64 CUDA tensor")
+    b = b.contiguous()
+    _, nz, ny, nx = (int(v) for v in b.shape)
+    seeds = seeds.to(device=b.device, dtype=b.dtype).reshape(-1, 3).contiguous()
+    n = int(seeds.shape[0])
+    if max_steps is None:
+        max_steps = int(math.ceil(4.0 * (nx + ny + nz) / float(step_len)))
+    ends = torch.empty((2, n, 3), dtype=b.dtype, device=b.device)
+    flags = torch.empty((2, n), dtype=torch.int32, device=b.device)
+    bn = torch.empty((3, n), dtype=b.dtype, device=b.device)
+    length = torch.empty((2, n), dtype=b.dtype, device=b.device)
+    nrm = np.asarray(normal, dtype=np.float64)
+    code = L.NFGS_F32 if b.dtype == torch.float32 else L.NFGS_F64
+    stream = torch.cuda.current_stream(b.device)
+    L.check(L.lib().nfgs_trace_field_lines(
+        C.c_void_p(b.data_ptr()), code, nz, ny, nx, C.c_void_p(seeds.data_ptr()), n, L.dptr(nrm),
+        float(step_len), int(max_steps), C.c_void_p(ends.data_ptr()), C.c_void_p(flags.data_ptr()),
+        C.c_void_p(bn.data_ptr()), C.c_void_p(length.data_ptr()), C.c_void_p(stream.cuda_stream)))
+    return {"ends": ends, "flags": flags, "bn": bn, "length": length, "max_steps": max_steps}
+
+
+def q_on_plane(tr, nu: int, nv: int):
+    """Q (nv, nu) on the device from a trace of an nv x nu unit-spacing seed grid."""
+    torch = _torch()
+    q = torch.empty((nv, nu), dtype=tr["ends"].dtype, device=tr["ends"].device)
+    code = L.NFGS_F32 if q.dtype == torch.float32 else L.NFGS_F64
+    stream = torch.cuda.current_stream(q.device)
+    L.check(L.lib().nfgs_qmap_plane(code, int(nu), int(nv), C.c_void_p(tr["ends"].data_ptr()),
+                                    C.c_void_p(tr["flags"].data_ptr()), C.c_void_p(tr["bn"].data_ptr()),
+                                    C.c_void_p(q.data_ptr()), C.c_void_p(stream.cuda_stream)))
+    return q
+
+
+def _bundle(tr, q, plane_shape, meta):
+    nv, nu = plane_shape
+    ends = tr["ends"].float().cpu().numpy()
+    flags = tr["flags"].cpu().numpy()
+    length = (tr["length"][0] + tr["length"][1]).float().cpu().numpy()
+    return {
+        "q": q.float().cpu().numpy(),
+        "flag_start": flags[1].reshape(nv, nu).astype(np.int32),
+        "flag_end": flags[0].reshape(nv, nu).astype(np.int32),
+        "start_xyz": ends[1].reshape(nv, nu, 3).astype(np.float32),
+        "end_xyz": ends[0].reshape(nv, nu, 3).astype(np.float32),
+        "line_len": length.reshape(nv, nu).astype(np.float32),
+        "metadata": meta,
+    }
+
+
+def compute_y0_qmap(bx, by, bz, *, fastqsl_root=None, y_index=None, step_len: float = 1.0 / 8.0, tol: float = 0.1,
+                    block_x: int = 128, trace_chunk_seeds: int = 8192, b_smooth_sigma_cells: float = 0.0,
+                    include_twist: bool = False, dtype: str = "float32", max_steps=None):
+    """Q on the x-z plane at y = y_index (default the physical midplane),
+    shape (nz, nx), seeds at every x-z node (fastqsl_plane.py:203-383)."""
+    torch = _torch()
+    if include_twist:
+        raise NotImplementedError("include_twist: the twist line integral is not built for B200")
+    dt = torch.float64 if str(dtype) in ("float64", "torch.float64") else torch.float32
+    b = spectral_gaussian_lowpass(_volume(bx, by, bz, dt), b_smooth_sigma_cells)
+    _, nz, ny, nx = (int(v) for v in b.shape)
+    iy = physical_midplane_grid_index(ny) if y_index is None else float(y_index)
+    if not 0.0 <= iy <= float(ny - 1):
+        raise ValueError(f"y_index={iy} is outside [0,{ny - 1}]")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    z, x = torch.meshgrid(torch.arange(nz, dtype=dt, device=b.device), torch.arange(nx, dtype=dt, device=b.device),
+                          indexing="ij")
+    seeds = torch.stack([x.reshape(-1), torch.full_like(x.reshape(-1), iy), z.reshape(-1)], dim=1)
+    tr = trace_field_lines(b, seeds, normal=(0.0, 1.0, 0.0), step_len=step_len, max_steps=max_steps)
+    q = q_on_plane(tr, nx, nz)
+    torch.cuda.synchronize()
+    meta = {"algorithm": "B200 RK4 tracer + footpoint-map Q on y=0", "shape_zyx": [nz, ny, nx],
+            "plane_y_index": iy, "plane_coordinate_contract": Y0_PLANE_COORDINATE_CONTRACT,
+            "plane_is_fractional": bool(not float(iy).is_integer()), "plane_shape_zx": [nz, nx],
+            "step_len_grid": float(step_len), "tolerance": float(tol), "max_steps": tr["max_steps"],
+            "block": [int(block_x), 1, 1], "trace_chunk_seeds": int(trace_chunk_seeds), "trace_n_chunks": 1,
+            "downsample": 1, "qmap_b_smooth_sigma_cells": float(b_smooth_sigma_cells),
+            "elapsed_s": time.perf_counter() - t0, "twist_included": False,
+            "dtype": "float64" if dt == torch.float64 else "float32"}
+    return _bundle(tr, q, (nz, nx), meta)
+
+
+def compute_bottom_qmap(bx, by, bz, *, fastqsl_root=None, z_index=None, step_len: float = 1.0 / 8.0,
+                        tol: float = 0.1, block_x: int = 128, trace_chunk_seeds: int = 8192,
+                        b_smooth_sigma_cells: float = 0.0, dtype: str = "float32", max_steps=None):
+    """Q on the bottom x-y plane, shape (ny, nx); seeds half a cell above the
+    bottom face by default (z = 0.5), normal +z (fastqsl_plane.py:385-506)."""
+    torch = _torch()
+    dt = torch.float64 if str(dtype) in ("float64", "torch.float64") else torch.float32
+    b = spectral_gaussian_lowpass(_volume(bx, by, bz, dt), b_smooth_sigma_cells)
+    _, nz, ny, nx = (int(v) for v in b.shape)
+    iz = 0.5 if z_index is None else float(z_index)
+    if not 0.0 <= iz <= float(nz - 1):
+        raise ValueError(f"z_index={iz} is outside [0,{nz - 1}]")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    y, x = torch.meshgrid(torch.arange(ny, dtype=dt, device=b.device), torch.arange(nx, dtype=dt, device=b.device),
+                          indexing="ij")
+    seeds = torch.stack([x.reshape(-1), y.reshape(-1), torch.full_like(x.reshape(-1), iz)], dim=1)
+    tr = trace_field_lines(b, seeds, normal=(0.0, 0.0, 1.0), step_len=step_len, max_steps=max_steps)
+    q = q_on_plane(tr, nx, ny)
+    torch.cuda.synchronize()
+    meta = {"algorithm": "B200 RK4 tracer + footpoint-map Q on the bottom plane", "shape_zyx": [nz, ny, nx],
+            "plane_z_index": iz, "plane_shape_yx": [ny, nx], "step_len_grid": float(step_len),
+            "tolerance": float(tol), "max_steps": tr["max_steps"], "block": [int(block_x), 1, 1],
+            "trace_chunk_seeds": int(trace_chunk_seeds), "trace_n_chunks": 1, "downsample": 1,
+            "qmap_b_smooth_sigma_cells": float(b_smooth_sigma_cells), "elapsed_s": time.perf_counter() - t0,
+            "dtype": "float64" if dt == torch.float64 else "float32"}
+    return _bundle(tr, q, (ny, nx), meta)
+
+
+def main(argv=None):
+    """Time the y=0 and bottom Q maps of a solved TD-type rope (--field solve)
+    or of the analytic TD field itself (--field td)."""
+    import torch
+
+    from .scan import KW, STOP
+    from .solver import NFGSSolverGPU
+    from .synthetic import td_bottom, td_volume
+
+    ap = argparse.ArgumentParser(description="Q maps of a TD-type flux rope")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--nz", type=int, default=128)
+    ap.add_argument("--field", choices=["solve", "td"], default="solve")
+    ap.add_argument("--iters", type=int, default=400)
+    ap.add_argument("--report", default=None)
+    args = ap.parse_args(argv)
+    if args.field == "solve":
+        h = 16.0 / (args.n - 1)
+        bx, by, bz = td_bottom(args.n, args.n, seed=1, extent=8.0)
+        s = NFGSSolverGPU(args.n, args.n, args.nz, h, h, h, bottom_divergence_robin_weight=0.5, **KW)
+        s.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+        hist = s.iterate(max_iter=args.iters, verbose=False, **STOP)
+        f = s.fields_to_torch()
+        out = {"field": "NFGS solution", "grid_zyx": [int(v) for v in f.shape[1:]], "best_sigma": hist["best_sigma"]}
+    else:
+        f = torch.as_tensor(td_volume(args.n, args.n, args.nz, seed=1, extent=8.0), dtype=torch.float32,
+                            device="cuda")
+        out = {"field": "analytic TD (td_volume seed 1)", "grid_zyx": [int(v) for v in f.shape[1:]]}
+    for name, fn in (("y0", compute_y0_qmap), ("bottom", compute_bottom_qmap)):
+        fn(f[0], f[1], f[2])  # warm-up
+        r = fn(f[0], f[1], f[2])
+        lens = r["line_len"]
+        qv = r["q"][np.isfinite(r["q"])]
+        seeds = r["q"].size
+        out[name] = {"seeds": seeds, "seconds": r["metadata"]["elapsed_s"],
+                     "lines_per_s": 2 * seeds / r["metadata"]["elapsed_s"],
+                     "mean_line_len": float(np.mean(lens)),
+                     "rk4_steps_per_s": float(np.sum(lens)) / r["metadata"]["step_len_grid"] / r["metadata"]["elapsed_s"],
+                     "q_valid": int(qv.size), "q_median": float(np.median(qv)) if qv.size else None,
+                     "log10_q_p99": float(np.log10(np.percentile(qv, 99))) if qv.size else None}
+    torch.cuda.synchronize()
+    print(json.dumps(out), flush=True)
+    if args.report:
+        with open(args.report, "w") as fh:
+            json.dump(out, fh, indent=1)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
