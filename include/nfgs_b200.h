@@ -408,6 +408,23 @@ int nfgs_trace_field_lines(const void* b, int32_t dtype, int32_t nz, int32_t ny,
 int nfgs_qmap_plane(int32_t dtype, int32_t nu, int32_t nv, const void* ends, const int32_t* flags, const void* bn,
                     void* q, void* stream);
 
+/* nfgs_trace_qperp: Q_perp of Titov (2007) at each seed, which needs no seed
+ * plane and stays defined where B lies in the plane of the seeds (where the
+ * plane form above divides by Bn0 = 0).  Per seed, five lines are traced both
+ * ways: through the seed and through seed +- delta e1, seed +- delta e2, with
+ * e1, e2 unit vectors perpendicular to B at the seed (e1 = unit(b x a), a the
+ * coordinate axis least aligned with b = B/|B|; e2 = b x e1).  With
+ * a = dr/dp, b = dr/dq of the end points by central differences over
+ * +-delta,
+ *   Q = [|a+|^2 |b-|^2 + |b+|^2 |a-|^2 - 2 (a+.b+)(a-.b-)] |Bn+ Bn-| / |B0|^2;
+ * NaN unless all five lines of each direction end on one face, or where
+ * B0 = 0.  Outputs as nfgs_trace_field_lines for the central line (ends
+ * (2, n, 3), flags (2, n), length (2, n)) except bn (3, n) = |B0|, |Bn+|,
+ * |Bn-|; q (n).  delta > 0 in grid units. */
+int nfgs_trace_qperp(const void* b, int32_t dtype, int32_t nz, int32_t ny, int32_t nx, const void* seeds, int64_t n,
+                     double delta, double step, int32_t max_steps, void* ends, int32_t* flags, void* bn, void* length,
+                     void* q, void* stream);
+
 /* ------------------------------------------------------------------------
  * Learned warm start: operator kernels of a 3-D neural operator on a
  * truncated cosine basis.  No reference counterpart (the reference starts

@@ -2735,6 +2735,50 @@ static int trace_lines_t(const void* b, int32_t nz, int32_t ny, int32_t nx, cons
 
 }  // namespace
 
+namespace {
+
+template <typename T>
+static int trace_qperp_t(const void* b, int32_t nz, int32_t ny, int32_t nx, const void* seeds, int64_t n,
+                         double delta, double step, int32_t max_steps, void* ends, int32_t* flags, void* bn,
+                         void* len, void* q, cudaStream_t s) {
+    const long long V = (long long)nz * ny * nx;
+    T *pk = nullptr, *e5 = nullptr;
+    int* f5 = nullptr;
+    CK(cudaMallocAsync((void**)&pk, (size_t)V * 4 * sizeof(T), s));
+    cudaError_t e = cudaMallocAsync((void**)&e5, (size_t)std::max<int64_t>(n, 1) * 30 * sizeof(T), s);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&f5, (size_t)std::max<int64_t>(n, 1) * 10 * sizeof(int), s);
+    if (e == cudaSuccess) {
+        trace::k_pack<T><<<(unsigned)((V + 255) / 256), 256, 0, s>>>((const T*)b, V, pk);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && n > 0) {
+        const trace::Box bx{nx, ny, nz};
+        trace::k_trace_perp<T><<<(unsigned)((10 * n + 127) / 128), 128, 0, s>>>(
+            pk, bx, (const T*)seeds, n, (T)delta, (T)step, max_steps, e5, f5, (T*)bn, (T*)len);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            trace::k_qperp<T><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(n, (T)delta, e5, f5, (const T*)bn, (T*)q);
+            e = cudaGetLastError();
+        }
+        // the central line of each direction
+        for (int d = 0; d < 2 && e == cudaSuccess; ++d) {
+            e = cudaMemcpyAsync((T*)ends + (size_t)3 * d * n, e5 + (size_t)3 * (d * 5) * n, (size_t)3 * n * sizeof(T),
+                                cudaMemcpyDeviceToDevice, s);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(flags + (size_t)d * n, f5 + (size_t)(d * 5) * n, (size_t)n * sizeof(int),
+                                    cudaMemcpyDeviceToDevice, s);
+        }
+    }
+    if (f5) cudaFreeAsync(f5, s);
+    if (e5) cudaFreeAsync(e5, s);
+    cudaFreeAsync(pk, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(NFGS_ECUDA, std::string("trace: ") + cudaGetErrorString(e));
+    return NFGS_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* nfgs_last_error(void) { return g_err.c_str(); }
@@ -3078,6 +3122,24 @@ int nfgs_trace_field_lines(const void* b, int32_t dtype, int32_t nz, int32_t ny,
                ? trace_lines_t<float>(b, nz, ny, nx, seeds, n, normal3, step, max_steps, ends, flags, bn, length, s)
                : trace_lines_t<double>(b, nz, ny, nx, seeds, n, normal3, step, max_steps, ends, flags, bn, length,
                                        s);
+}
+
+int nfgs_trace_qperp(const void* b, int32_t dtype, int32_t nz, int32_t ny, int32_t nx, const void* seeds, int64_t n,
+                     double delta, double step, int32_t max_steps, void* ends, int32_t* flags, void* bn, void* length,
+                     void* q, void* stream) {
+    g_err.clear();
+    if (!b || (n > 0 && (!seeds || !ends || !flags || !bn || !length || !q))) return fail(NFGS_EINVAL, "null argument");
+    if (dtype != NFGS_F32 && dtype != NFGS_F64) return fail(NFGS_EINVAL, "dtype must be F32 or F64");
+    if (nz < 2 || ny < 2 || nx < 2) return fail(NFGS_EINVAL, "the field needs at least 2 nodes per axis");
+    if (n < 0 || 10 * n > (int64_t)INT32_MAX * 128) return fail(NFGS_EINVAL, "bad seed count");
+    if (!(step > 0.0) || !std::isfinite(step)) return fail(NFGS_EINVAL, "step must be positive");
+    if (!(delta > 0.0) || !std::isfinite(delta)) return fail(NFGS_EINVAL, "delta must be positive");
+    if (max_steps < 1) return fail(NFGS_EINVAL, "max_steps must be positive");
+    cudaStream_t s = (cudaStream_t)stream;
+    return dtype == NFGS_F32 ? trace_qperp_t<float>(b, nz, ny, nx, seeds, n, delta, step, max_steps, ends, flags, bn,
+                                                    length, q, s)
+                             : trace_qperp_t<double>(b, nz, ny, nx, seeds, n, delta, step, max_steps, ends, flags,
+                                                     bn, length, q, s);
 }
 
 int nfgs_qmap_plane(int32_t dtype, int32_t nu, int32_t nv, const void* ends, const int32_t* flags, const void* bn,

@@ -92,44 +92,25 @@ __device__ __forceinline__ bool direction(const T* __restrict__ pk, Box bx, T s,
     return true;
 }
 
-// Trace seed `si` along +B (dir 0) or -B (dir 1).  ends (2, n, 3), flags
-// (2, n), bn (3, n): B.n0 at the seed, |B.n| at the forward and backward
-// ends; len (2, n) per direction.
+// Trace one line from p (inside the box) along s B: p becomes the end point;
+// returns the face code (1..6), 0 after max_steps, -1 at a zero field.
 template <typename T>
-__global__ void __launch_bounds__(128) k_trace(const T* __restrict__ pk, Box bx, const T* __restrict__ seeds,
-                                               long long n, T n0x, T n0y, T n0z, T h, int max_steps,
-                                               T* __restrict__ ends, int* __restrict__ flags, T* __restrict__ bn,
-                                               T* __restrict__ len) {
-    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= 2 * n) return;
-    const int dir = tid >= n ? 1 : 0;
-    const long long si = tid - (long long)dir * n;
-    const T s = dir == 0 ? T(1) : T(-1);
-    const T hi[3] = {T(bx.nx - 1), T(bx.ny - 1), T(bx.nz - 1)};
-    // seeds are clamped into the box, so every chord that leaves it starts inside
-    T p[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) p[d] = fmin(fmax(seeds[3 * si + d], T(0)), hi[d]);
-    if (dir == 0) {
-        T b0, b1, b2;
-        interp<T>(pk, bx, p[0], p[1], p[2], b0, b1, b2);
-        bn[si] = b0 * n0x + b1 * n0y + b2 * n0z;
-    }
+__device__ int trace_line(const T* __restrict__ pk, Box bx, const T (&hi)[3], T (&p)[3], T s, T h, int max_steps,
+                          T& length) {
     const T h2 = h * T(0.5), h6 = h / T(6);
-    T length = T(0);
-    int flag = 0;
+    length = T(0);
     for (int it = 0; it < max_steps; ++it) {
         T k1[3], k2[3], k3[3], k4[3], q[3];
-        if (!direction<T>(pk, bx, s, p, k1)) { flag = -1; break; }
+        if (!direction<T>(pk, bx, s, p, k1)) return -1;
 #pragma unroll
         for (int d = 0; d < 3; ++d) q[d] = p[d] + h2 * k1[d];
-        if (!direction<T>(pk, bx, s, q, k2)) { flag = -1; break; }
+        if (!direction<T>(pk, bx, s, q, k2)) return -1;
 #pragma unroll
         for (int d = 0; d < 3; ++d) q[d] = p[d] + h2 * k2[d];
-        if (!direction<T>(pk, bx, s, q, k3)) { flag = -1; break; }
+        if (!direction<T>(pk, bx, s, q, k3)) return -1;
 #pragma unroll
         for (int d = 0; d < 3; ++d) q[d] = p[d] + h * k3[d];
-        if (!direction<T>(pk, bx, s, q, k4)) { flag = -1; break; }
+        if (!direction<T>(pk, bx, s, q, k4)) return -1;
 #pragma unroll
         for (int d = 0; d < 3; ++d) q[d] = p[d] + h6 * (k1[d] + T(2) * k2[d] + T(2) * k3[d] + k4[d]);
         bool inside = true;
@@ -154,29 +135,150 @@ __global__ void __launch_bounds__(128) k_trace(const T* __restrict__ pk, Box bx,
                 if (td < t) { t = td; face = 2 * d + 2; }
             }
         }
-        if (face == 0) break;  // unreachable with p inside: kept as a guard on the face index
+        if (face == 0) return 0;  // a non-finite step: no face (p stays inside)
 #pragma unroll
         for (int d = 0; d < 3; ++d) p[d] = p[d] + t * (q[d] - p[d]);
         const int fd = (face - 1) >> 1;
         p[fd] = (face & 1) ? T(0) : hi[fd];
         length += t * h;
-        flag = face;
-        break;
+        return face;
     }
+    return 0;
+}
+
+// |B.n| at an end on face `flag` (NaN without a face)
+template <typename T>
+__device__ __forceinline__ T end_bn(const T* __restrict__ pk, Box bx, const T (&p)[3], int flag) {
+    if (flag <= 0) return T(NAN);
+    T b[3];
+    interp<T>(pk, bx, p[0], p[1], p[2], b[0], b[1], b[2]);
+    return fabs(b[(flag - 1) >> 1]);
+}
+
+// Trace seed `si` along +B (dir 0) or -B (dir 1).  ends (2, n, 3), flags
+// (2, n), bn (3, n): B.n0 at the seed, |B.n| at the forward and backward
+// ends; len (2, n) per direction.
+template <typename T>
+__global__ void __launch_bounds__(128) k_trace(const T* __restrict__ pk, Box bx, const T* __restrict__ seeds,
+                                               long long n, T n0x, T n0y, T n0z, T h, int max_steps,
+                                               T* __restrict__ ends, int* __restrict__ flags, T* __restrict__ bn,
+                                               T* __restrict__ len) {
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= 2 * n) return;
+    const int dir = tid >= n ? 1 : 0;
+    const long long si = tid - (long long)dir * n;
+    const T hi[3] = {T(bx.nx - 1), T(bx.ny - 1), T(bx.nz - 1)};
+    // seeds are clamped into the box, so every chord that leaves it starts inside
+    T p[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) p[d] = fmin(fmax(seeds[3 * si + d], T(0)), hi[d]);
+    if (dir == 0) {
+        T b0, b1, b2;
+        interp<T>(pk, bx, p[0], p[1], p[2], b0, b1, b2);
+        bn[si] = b0 * n0x + b1 * n0y + b2 * n0z;
+    }
+    T length;
+    const int flag = trace_line<T>(pk, bx, hi, p, dir == 0 ? T(1) : T(-1), h, max_steps, length);
     ends[3 * tid] = p[0];
     ends[3 * tid + 1] = p[1];
     ends[3 * tid + 2] = p[2];
     flags[tid] = flag;
     len[tid] = length;
-    T e;
-    if (flag > 0) {
-        T b[3];
-        interp<T>(pk, bx, p[0], p[1], p[2], b[0], b[1], b[2]);
-        e = fabs(b[(flag - 1) >> 1]);
-    } else {
-        e = T(NAN);
+    bn[n * (1 + dir) + si] = end_bn<T>(pk, bx, p, flag);
+}
+
+// Perpendicular frame at a seed: b = B0/|B0|, e1 = unit(b x a) with a the
+// coordinate axis least aligned with b, e2 = b x e1.  False where |B0| = 0.
+template <typename T>
+__device__ __forceinline__ bool perp_frame(const T (&B)[3], T& bm, T (&e1)[3], T (&e2)[3]) {
+    bm = sqrt(B[0] * B[0] + B[1] * B[1] + B[2] * B[2]);
+    if (!(bm > T(0))) return false;
+    const T b[3] = {B[0] / bm, B[1] / bm, B[2] / bm};
+    int ax = 0;
+    if (fabs(b[1]) < fabs(b[ax])) ax = 1;
+    if (fabs(b[2]) < fabs(b[ax])) ax = 2;
+    T c[3];  // b x a
+    if (ax == 0) { c[0] = T(0); c[1] = b[2]; c[2] = -b[1]; }
+    else if (ax == 1) { c[0] = -b[2]; c[1] = T(0); c[2] = b[0]; }
+    else { c[0] = b[1]; c[1] = -b[0]; c[2] = T(0); }
+    const T cm = sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) e1[d] = c[d] / cm;
+    e2[0] = b[1] * e1[2] - b[2] * e1[1];
+    e2[1] = b[2] * e1[0] - b[0] * e1[2];
+    e2[2] = b[0] * e1[1] - b[1] * e1[0];
+    return true;
+}
+
+// Q_perp lines: per seed, the line through the seed and four through
+// seed +- delta e1, seed +- delta e2 (clamped into the box), each traced both
+// ways.  Thread tid = (dir * 5 + a) * n + si.  ends (2, 5, n, 3), flags
+// (2, 5, n); bn (3, n): |B0|, |Bn+|, |Bn-| of the central line; len (2, n)
+// of the central line.
+template <typename T>
+__global__ void __launch_bounds__(128) k_trace_perp(const T* __restrict__ pk, Box bx, const T* __restrict__ seeds,
+                                                    long long n, T delta, T h, int max_steps, T* __restrict__ ends,
+                                                    int* __restrict__ flags, T* __restrict__ bn,
+                                                    T* __restrict__ len) {
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= 10 * n) return;
+    const long long si = tid % n;
+    const int da = (int)(tid / n);
+    const int dir = da / 5, a = da % 5;
+    const T hi[3] = {T(bx.nx - 1), T(bx.ny - 1), T(bx.nz - 1)};
+    T p[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) p[d] = fmin(fmax(seeds[3 * si + d], T(0)), hi[d]);
+    T B0[3], bm, e1[3], e2[3];
+    interp<T>(pk, bx, p[0], p[1], p[2], B0[0], B0[1], B0[2]);
+    const bool ok = perp_frame<T>(B0, bm, e1, e2);
+    if (a == 0 && dir == 0) bn[si] = ok ? bm : T(0);
+    if (ok && a > 0) {
+        const T sg = (a & 1) ? T(1) : T(-1);
+        const T* e = a <= 2 ? e1 : e2;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) p[d] = fmin(fmax(p[d] + sg * delta * e[d], T(0)), hi[d]);
     }
-    bn[n * (1 + dir) + si] = e;
+    T length = T(0);
+    const int flag = ok ? trace_line<T>(pk, bx, hi, p, dir == 0 ? T(1) : T(-1), h, max_steps, length) : -1;
+    ends[3 * tid] = p[0];
+    ends[3 * tid + 1] = p[1];
+    ends[3 * tid + 2] = p[2];
+    flags[tid] = flag;
+    if (a == 0) {
+        len[dir * n + si] = length;
+        bn[n * (1 + dir) + si] = end_bn<T>(pk, bx, p, flag);
+    }
+}
+
+// Q_perp = [|a+|^2 |b-|^2 + |b+|^2 |a-|^2 - 2 (a+.b+)(a-.b-)] |Bn+ Bn-| / |B0|^2
+// with a = dr/dp, b = dr/dq by central differences over +-delta along e1, e2
+// (Titov 2007); NaN unless the five lines of each direction end on one face.
+template <typename T>
+__global__ void k_qperp(long long n, T delta, const T* __restrict__ ends, const int* __restrict__ flags,
+                        const T* __restrict__ bn, T* __restrict__ q) {
+    const long long si = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (si >= n) return;
+    T a[2][3], b[2][3];
+    const T inv = T(1) / (T(2) * delta);
+    for (int dir = 0; dir < 2; ++dir) {
+        const int f0 = flags[(dir * 5) * n + si];
+        bool ok = f0 > 0;
+#pragma unroll
+        for (int r = 1; r < 5; ++r) ok = ok && flags[(dir * 5 + r) * n + si] == f0;
+        if (!ok) { q[si] = T(NAN); return; }
+        const T* e = ends + 3 * (dir * 5) * n;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            a[dir][d] = (e[3 * (1 * n + si) + d] - e[3 * (2 * n + si) + d]) * inv;
+            b[dir][d] = (e[3 * (3 * n + si) + d] - e[3 * (4 * n + si) + d]) * inv;
+        }
+    }
+    auto dot = [](const T (&x)[3], const T (&y)[3]) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
+    const T br = dot(a[0], a[0]) * dot(b[1], b[1]) + dot(b[0], b[0]) * dot(a[1], a[1]) -
+                 T(2) * dot(a[0], b[0]) * dot(a[1], b[1]);
+    const T b0 = bn[si];
+    q[si] = b0 > T(0) ? br * fabs(bn[n + si] * bn[2 * n + si]) / (b0 * b0) : T(NAN);
 }
 
 // Q on a regular nv x nu seed plane (seed iu + nu iv, unit spacing)

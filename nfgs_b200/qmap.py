@@ -11,6 +11,12 @@ differences over the seed plane) run on device tensors; nothing of the field
 goes through the host when it is passed as a CUDA tensor, e.g. from
 ``NFGSSolverGPU.fields_to_torch()``.
 
+Q comes by default from Titov's (2007) Q_perp: each seed gets four more
+lines offset by +-delta perpendicular to B (``nfgs_trace_qperp``), so Q is
+defined also where B lies in the seed plane (By = 0 on the y = 0 midplane of
+a symmetric rope, where the seed-grid form divides by Bn0 = 0);
+``q_method="plane"`` selects the seed-grid central differences instead.
+
 Differences from the reference helpers, by design:
 * one fixed RK4 step (``step_len``, default 1/8 cell) instead of FastQSL's
   adaptive RKF45; ``tol``, ``block_x`` and ``trace_chunk_seeds`` are accepted
@@ -113,6 +119,53 @@ def trace_field_lines(b, seeds, *, normal=(0.0, 0.0, 1.0), step_len: float = 1.0
     return {"ends": ends, "flags": flags, "bn": bn, "length": length, "max_steps": max_steps}
 
 
+def trace_qperp(b, seeds, *, delta: float = 0.25, step_len: float = 1.0 / 8.0, max_steps=None):
+    """Q_perp (Titov 2007) at each seed: five lines per seed (the seed and
+    +-delta along two unit vectors perpendicular to B), traced both ways.
+    Returns device tensors q (n,), ends (2, n, 3), flags (2, n) int32,
+    bn (3, n) = |B0|, |Bn+|, |Bn-|, length (2, n) of the central line."""
+    torch = _torch()
+    if b.dtype not in (torch.float32, torch.float64) or b.device.type != "cuda" or b.ndim != 4 or b.shape[0] != 3:
+        raise ValueError("b must be a (3, nz, ny, nx) float32/float64 CUDA tensor")
+    b = b.contiguous()
+    _, nz, ny, nx = (int(v) for v in b.shape)
+    seeds = seeds.to(device=b.device, dtype=b.dtype).reshape(-1, 3).contiguous()
+    n = int(seeds.shape[0])
+    if max_steps is None:
+        max_steps = int(math.ceil(4.0 * (nx + ny + nz) / float(step_len)))
+    out = {"q": torch.empty((n,), dtype=b.dtype, device=b.device),
+           "ends": torch.empty((2, n, 3), dtype=b.dtype, device=b.device),
+           "flags": torch.empty((2, n), dtype=torch.int32, device=b.device),
+           "bn": torch.empty((3, n), dtype=b.dtype, device=b.device),
+           "length": torch.empty((2, n), dtype=b.dtype, device=b.device)}
+    code = L.NFGS_F32 if b.dtype == torch.float32 else L.NFGS_F64
+    stream = torch.cuda.current_stream(b.device)
+    L.check(L.lib().nfgs_trace_qperp(
+        C.c_void_p(b.data_ptr()), code, nz, ny, nx, C.c_void_p(seeds.data_ptr()), n, float(delta), float(step_len),
+        int(max_steps), C.c_void_p(out["ends"].data_ptr()), C.c_void_p(out["flags"].data_ptr()),
+        C.c_void_p(out["bn"].data_ptr()), C.c_void_p(out["length"].data_ptr()), C.c_void_p(out["q"].data_ptr()),
+        C.c_void_p(stream.cuda_stream)))
+    out["max_steps"] = max_steps
+    return out
+
+
+def _plane_q(b, seeds, nu, nv, normal, q_method, step_len, max_steps, delta):
+    """Trace the nv x nu seed grid and evaluate Q by the chosen method; the
+    plane's border is NaN either way (the reference keeps only the interior)."""
+    if q_method == "perp":
+        tr = trace_qperp(b, seeds, delta=delta, step_len=step_len, max_steps=max_steps)
+        q = tr["q"].reshape(nv, nu).clone()
+        q[0, :] = float("nan")
+        q[-1, :] = float("nan")
+        q[:, 0] = float("nan")
+        q[:, -1] = float("nan")
+        return tr, q
+    if q_method == "plane":
+        tr = trace_field_lines(b, seeds, normal=normal, step_len=step_len, max_steps=max_steps)
+        return tr, q_on_plane(tr, nu, nv)
+    raise ValueError("q_method must be 'perp' or 'plane'")
+
+
 def q_on_plane(tr, nu: int, nv: int):
     """Q (nv, nu) on the device from a trace of an nv x nu unit-spacing seed grid."""
     torch = _torch()
@@ -143,9 +196,13 @@ def _bundle(tr, q, plane_shape, meta):
 
 def compute_y0_qmap(bx, by, bz, *, fastqsl_root=None, y_index=None, step_len: float = 1.0 / 8.0, tol: float = 0.1,
                     block_x: int = 128, trace_chunk_seeds: int = 8192, b_smooth_sigma_cells: float = 0.0,
-                    include_twist: bool = False, dtype: str = "float32", max_steps=None):
+                    include_twist: bool = False, dtype: str = "float32", max_steps=None, q_method: str = "perp",
+                    delta: float = 0.25):
     """Q on the x-z plane at y = y_index (default the physical midplane),
-    shape (nz, nx), seeds at every x-z node (fastqsl_plane.py:203-383)."""
+    shape (nz, nx), seeds at every x-z node (fastqsl_plane.py:203-383).
+    q_method "perp" (default): Q_perp from lines offset perpendicular to B by
+    +-delta, defined where B lies in the plane (By = 0 on the midplane of a
+    symmetric field); "plane": central differences over the seed grid."""
     torch = _torch()
     if include_twist:
         raise NotImplementedError("include_twist: the twist line integral is not built for B200")
@@ -160,10 +217,10 @@ def compute_y0_qmap(bx, by, bz, *, fastqsl_root=None, y_index=None, step_len: fl
     z, x = torch.meshgrid(torch.arange(nz, dtype=dt, device=b.device), torch.arange(nx, dtype=dt, device=b.device),
                           indexing="ij")
     seeds = torch.stack([x.reshape(-1), torch.full_like(x.reshape(-1), iy), z.reshape(-1)], dim=1)
-    tr = trace_field_lines(b, seeds, normal=(0.0, 1.0, 0.0), step_len=step_len, max_steps=max_steps)
-    q = q_on_plane(tr, nx, nz)
+    tr, q = _plane_q(b, seeds, nx, nz, (0.0, 1.0, 0.0), q_method, step_len, max_steps, delta)
     torch.cuda.synchronize()
-    meta = {"algorithm": "B200 RK4 tracer + footpoint-map Q on y=0", "shape_zyx": [nz, ny, nx],
+    meta = {"algorithm": f"B200 RK4 tracer + Q ({q_method}) on y=0", "q_method": q_method, "delta": float(delta),
+            "shape_zyx": [nz, ny, nx],
             "plane_y_index": iy, "plane_coordinate_contract": Y0_PLANE_COORDINATE_CONTRACT,
             "plane_is_fractional": bool(not float(iy).is_integer()), "plane_shape_zx": [nz, nx],
             "step_len_grid": float(step_len), "tolerance": float(tol), "max_steps": tr["max_steps"],
@@ -176,7 +233,8 @@ def compute_y0_qmap(bx, by, bz, *, fastqsl_root=None, y_index=None, step_len: fl
 
 def compute_bottom_qmap(bx, by, bz, *, fastqsl_root=None, z_index=None, step_len: float = 1.0 / 8.0,
                         tol: float = 0.1, block_x: int = 128, trace_chunk_seeds: int = 8192,
-                        b_smooth_sigma_cells: float = 0.0, dtype: str = "float32", max_steps=None):
+                        b_smooth_sigma_cells: float = 0.0, dtype: str = "float32", max_steps=None,
+                        q_method: str = "perp", delta: float = 0.25):
     """Q on the bottom x-y plane, shape (ny, nx); seeds half a cell above the
     bottom face by default (z = 0.5), normal +z (fastqsl_plane.py:385-506)."""
     torch = _torch()
@@ -191,10 +249,10 @@ def compute_bottom_qmap(bx, by, bz, *, fastqsl_root=None, z_index=None, step_len
     y, x = torch.meshgrid(torch.arange(ny, dtype=dt, device=b.device), torch.arange(nx, dtype=dt, device=b.device),
                           indexing="ij")
     seeds = torch.stack([x.reshape(-1), y.reshape(-1), torch.full_like(x.reshape(-1), iz)], dim=1)
-    tr = trace_field_lines(b, seeds, normal=(0.0, 0.0, 1.0), step_len=step_len, max_steps=max_steps)
-    q = q_on_plane(tr, nx, ny)
+    tr, q = _plane_q(b, seeds, nx, ny, (0.0, 0.0, 1.0), q_method, step_len, max_steps, delta)
     torch.cuda.synchronize()
-    meta = {"algorithm": "B200 RK4 tracer + footpoint-map Q on the bottom plane", "shape_zyx": [nz, ny, nx],
+    meta = {"algorithm": f"B200 RK4 tracer + Q ({q_method}) on the bottom plane", "q_method": q_method,
+            "delta": float(delta), "shape_zyx": [nz, ny, nx],
             "plane_z_index": iz, "plane_shape_yx": [ny, nx], "step_len_grid": float(step_len),
             "tolerance": float(tol), "max_steps": tr["max_steps"], "block": [int(block_x), 1, 1],
             "trace_chunk_seeds": int(trace_chunk_seeds), "trace_n_chunks": 1, "downsample": 1,
@@ -238,9 +296,11 @@ def main(argv=None):
         qv = r["q"][np.isfinite(r["q"])]
         seeds = r["q"].size
         out[name] = {"seeds": seeds, "seconds": r["metadata"]["elapsed_s"],
-                     "lines_per_s": 2 * seeds / r["metadata"]["elapsed_s"],
+                     "lines_per_s": (10 if r["metadata"]["q_method"] == "perp" else 2) * seeds
+                     / r["metadata"]["elapsed_s"],
                      "mean_line_len": float(np.mean(lens)),
-                     "rk4_steps_per_s": float(np.sum(lens)) / r["metadata"]["step_len_grid"] / r["metadata"]["elapsed_s"],
+                     "central_rk4_steps_per_s": float(np.sum(lens)) / r["metadata"]["step_len_grid"]
+                     / r["metadata"]["elapsed_s"],
                      "q_valid": int(qv.size), "q_median": float(np.median(qv)) if qv.size else None,
                      "log10_q_p99": float(np.log10(np.percentile(qv, 99))) if qv.size else None}
     torch.cuda.synchronize()

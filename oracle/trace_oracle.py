@@ -172,3 +172,55 @@ def dipole_field(nx, ny, nz, depth=6.0, tilt=0.4):
     rr = np.sqrt((r * r).sum(axis=0))
     mr = (m[:, None, None, None] * r).sum(axis=0)
     return (3.0 * mr * r / rr ** 5 - m[:, None, None, None] / rr ** 3) * depth ** 3
+
+
+def perp_frame(B):
+    """Unit vectors e1, e2 perpendicular to B (m, 3): e1 = unit(b x a) with a
+    the coordinate axis least aligned with b, e2 = b x e1; |B| (m,)."""
+    bm = np.sqrt((B * B).sum(axis=1))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        b = B / bm[:, None]
+    ax = np.argmin(np.abs(b), axis=1)  # first minimum: x before y before z
+    a = np.eye(3)[ax]
+    c = np.cross(b, a)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        e1 = c / np.sqrt((c * c).sum(axis=1))[:, None]
+    e2 = np.cross(b, e1)
+    return bm, e1, e2
+
+
+def qperp(b, seeds, delta, step, max_steps):
+    """Q_perp (Titov 2007) at each seed from five lines traced both ways (the
+    seed and seed +- delta e1, +- delta e2); returns q (n,) and the central
+    line's (ends, flags, bn = (|B0|, |Bn+|, |Bn-|), length)."""
+    b = np.asarray(b, dtype=np.float64)
+    pk = np.ascontiguousarray(np.moveaxis(b, 0, -1))
+    nz, ny, nx, _ = pk.shape
+    hi = np.array([nx - 1.0, ny - 1.0, nz - 1.0])
+    s0 = np.clip(np.asarray(seeds, dtype=np.float64).reshape(-1, 3), 0.0, hi)
+    n = s0.shape[0]
+    bm, e1, e2 = perp_frame(interp(pk, s0))
+    ok = bm > 0
+    e1[~ok] = 0.0
+    e2[~ok] = 0.0
+    aux = [s0, s0 + delta * e1, s0 - delta * e1, s0 + delta * e2, s0 - delta * e2]
+    allseeds = np.clip(np.concatenate(aux), 0.0, hi)
+    ends, flags, bnx, length = trace(b, allseeds, (0.0, 0.0, 1.0), step, max_steps)
+    E = ends.reshape(2, 5, n, 3)
+    F = flags.reshape(2, 5, n)
+    F[:, :, ~ok] = -1
+    good = np.ones(n, dtype=bool)
+    for d in range(2):
+        good &= (F[d, 0] > 0) & np.all(F[d] == F[d, 0][None], axis=0)
+    a = [(E[d, 1] - E[d, 2]) / (2.0 * delta) for d in range(2)]
+    bb = [(E[d, 3] - E[d, 4]) / (2.0 * delta) for d in range(2)]
+
+    def dot(u, v):
+        return (u * v).sum(axis=-1)
+
+    br = dot(a[0], a[0]) * dot(bb[1], bb[1]) + dot(bb[0], bb[0]) * dot(a[1], a[1]) - 2.0 * dot(a[0], bb[0]) * dot(a[1], bb[1])
+    bne = bnx[1:].reshape(2, 5, n)[:, 0]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        q = np.where(good & ok, br * np.abs(bne[0] * bne[1]) / (bm * bm), np.nan)
+    bn = np.stack([np.where(ok, bm, 0.0), bne[0], bne[1]])
+    return q, E[:, 0], F[:, 0], bn, length.reshape(2, 5, n)[:, 0]

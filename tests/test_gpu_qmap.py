@@ -151,3 +151,60 @@ def test_reference_helpers_contract():
     ref = np.fft.ifftn(np.fft.fftn(b[0].astype(np.float64)) * np.exp(-0.5 * (2 * np.pi * sig) ** 2 * k2)).real
     got = Q.spectral_gaussian_lowpass(torch.as_tensor(b, device="cuda"), sig)[0].cpu().numpy()
     np.testing.assert_allclose(got, ref.astype(np.float32), rtol=1e-5, atol=1e-6 * np.abs(ref).max())
+
+
+def gpu_qperp(b, seeds, dtype, delta=0.25, max_steps=2000):
+    import torch
+
+    from nfgs_b200.qmap import trace_qperp
+
+    bt = torch.as_tensor(b, dtype=dtype, device="cuda")
+    st = torch.as_tensor(seeds, dtype=dtype, device="cuda")
+    return host(trace_qperp(bt, st, delta=delta, step_len=0.125, max_steps=max_steps))
+
+
+@pytest.mark.parametrize("dtype_name", ["float64", "float32"])
+def test_qperp_known_answer_on_the_plane_containing_b(dtype_name):
+    import torch
+
+    from oracle import trace_oracle as T
+
+    nx, ny, nz, L = 41, 41, 21, 20.0
+    z, x = np.meshgrid(np.arange(nz, dtype=float), np.arange(nx, dtype=float), indexing="ij")
+    seeds = np.stack([x.ravel(), np.full(x.size, 20.0), z.ravel()], axis=1)
+    r = gpu_qperp(T.hyperbolic_field(nx, ny, nz, L), seeds, getattr(torch, dtype_name))
+    q = r["q"].reshape(nz, nx)
+    np.testing.assert_allclose(q[3:18, 14:27], 2.0 * np.cosh(2.0), rtol=2e-4 if dtype_name == "float64" else 5e-3)
+
+
+def test_qperp_fp64_matches_oracle():
+    import torch
+
+    from oracle import trace_oracle as T
+
+    nx, ny, nz = 48, 40, 24
+    b = T.dipole_field(nx, ny, nz)
+    seeds = plane_seeds(nx, ny, 0.5)
+    r = gpu_qperp(b, seeds, torch.float64, max_steps=4000)
+    q, ends, flags, bn, length = T.qperp(b, seeds, 0.25, 0.125, 4000)
+    np.testing.assert_array_equal(r["flags"], flags)
+    np.testing.assert_allclose(r["ends"], ends, atol=1e-9)
+    np.testing.assert_allclose(r["length"], length, rtol=1e-11, atol=1e-9)
+    np.testing.assert_allclose(r["bn"], bn, rtol=1e-11, atol=1e-14, equal_nan=True)
+    assert np.array_equal(np.isnan(r["q"]), np.isnan(q))
+    fin = np.isfinite(q)
+    assert fin.sum() > 0.5 * q.size
+    np.testing.assert_allclose(r["q"][fin], q[fin], rtol=1e-6)
+
+
+def test_y0_helper_defaults_to_qperp():
+    from nfgs_b200 import qmap as Q
+    from oracle import trace_oracle as T
+
+    nx, ny, nz, L = 41, 41, 21, 20.0
+    b = T.hyperbolic_field(nx, ny, nz, L).astype(np.float32)
+    r = Q.compute_y0_qmap(b[0], b[1], b[2])  # y index 20: the plane containing B
+    assert r["metadata"]["q_method"] == "perp"
+    np.testing.assert_allclose(r["q"][3:18, 14:27], 2.0 * np.cosh(2.0), rtol=5e-3)
+    rp = Q.compute_y0_qmap(b[0], b[1], b[2], q_method="plane")
+    assert not np.isfinite(rp["q"]).any()

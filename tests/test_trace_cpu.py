@@ -75,3 +75,39 @@ def test_exits_and_flags():
     # max steps: a short budget leaves the line unfinished
     _, f2, _, l2 = T.trace(b, np.array([[5.0, 2.0, 1.5]]), (1, 0, 0), 0.125, 4)
     assert f2[0, 0] == 0 and l2[0, 0] == 0.5
+
+
+def test_qperp_where_the_seed_plane_contains_b():
+    """On the y = yc plane of the hyperbolic field By = 0: the seed-grid form
+    has no finite value (it divides by Bn0 = 0), Q_perp gives 2 cosh(2H/L)."""
+    nx, ny, nz, L = 41, 41, 21, 20.0
+    b = T.hyperbolic_field(nx, ny, nz, L)
+    z, x = np.meshgrid(np.arange(nz, dtype=float), np.arange(nx, dtype=float), indexing="ij")
+    seeds = np.stack([x.ravel(), np.full(x.size, 20.0), z.ravel()], axis=1)
+    q, ends, flags, bn, length = T.qperp(b, seeds, 0.25, 0.125, 2000)
+    q = q.reshape(nz, nx)
+    np.testing.assert_allclose(q[3:18, 14:27], 2.0 * np.cosh(2.0), rtol=2e-4)
+    e, f, bnp, _ = T.trace(b, seeds, (0, 1, 0), 0.125, 2000)
+    assert not np.isfinite(T.qmap(nx, nz, e, f, bnp)).any()
+    # the central line is the plain trace
+    np.testing.assert_array_equal(flags, f)
+    np.testing.assert_allclose(ends, e, atol=0)
+    np.testing.assert_allclose(bn[0], np.sqrt((T.interp(np.moveaxis(b, 0, -1), seeds) ** 2).sum(axis=1)))
+
+
+def test_qperp_frame_and_uniform_field():
+    B = np.array([[0.0, 0.0, 2.0], [1.0, 1.0, 1.0], [0.3, -2.0, 0.1]])
+    bm, e1, e2 = T.perp_frame(B)
+    b = B / bm[:, None]
+    for v in (e1, e2):
+        np.testing.assert_allclose((v * b).sum(axis=1), 0.0, atol=1e-15)
+        np.testing.assert_allclose((v * v).sum(axis=1), 1.0, rtol=1e-15)
+    np.testing.assert_allclose((e1 * e2).sum(axis=1), 0.0, atol=1e-15)
+    bu = np.zeros((3, 9, 10, 11))
+    bu[2] = 1.0
+    bu[0] = 0.3
+    bu[1] = -0.2
+    x, y = np.meshgrid(np.arange(3.0, 8.0), np.arange(3.0, 7.0), indexing="xy")
+    seeds = np.stack([x.ravel(), y.ravel(), np.full(x.size, 4.0)], axis=1)
+    q, *_ = T.qperp(bu, seeds, 0.25, 0.125, 1000)
+    np.testing.assert_allclose(q, 2.0, rtol=1e-10)
