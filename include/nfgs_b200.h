@@ -390,7 +390,13 @@ int nfgs_field_metrics(const void* ref, const void* sol, const void* cur, int32_
  *                     z=0, z=nz-1; 0 max_steps reached; -1 zero field met;
  *   bn     (3, n)     B.n0 at the seed, |B.n| at the forward and backward
  *                     ends (n the face normal; NaN without a face);
- *   length (2, n)     path length of each half, grid units.
+ *   length (2, n)     path length of each half, grid units;
+ *   twist  (2, n)     NULL, or the twist of each half: the integral of
+ *                     J.B / (4 pi |B|^2) ds along it (J = curl B by
+ *                     second-order differences in grid units, one-sided at
+ *                     the walls; at least 3 nodes per axis), with the RK4
+ *                     stages of the line (as the reference's include_twist,
+ *                     fastqsl_plane.py:287-305).
  * stream: a cudaStream_t (NULL for the legacy default stream) on the current
  * device; the call returns when the outputs are complete.
  *
@@ -404,7 +410,7 @@ int nfgs_field_metrics(const void* ref, const void* sol, const void* cur, int32_
  * ------------------------------------------------------------------------ */
 int nfgs_trace_field_lines(const void* b, int32_t dtype, int32_t nz, int32_t ny, int32_t nx, const void* seeds,
                            int64_t n, const double* normal3, double step, int32_t max_steps, void* ends,
-                           int32_t* flags, void* bn, void* length, void* stream);
+                           int32_t* flags, void* bn, void* length, void* twist, void* stream);
 int nfgs_qmap_plane(int32_t dtype, int32_t nu, int32_t nv, const void* ends, const int32_t* flags, const void* bn,
                     void* q, void* stream);
 
@@ -419,11 +425,11 @@ int nfgs_qmap_plane(int32_t dtype, int32_t nu, int32_t nv, const void* ends, con
  *   Q = [|a+|^2 |b-|^2 + |b+|^2 |a-|^2 - 2 (a+.b+)(a-.b-)] |Bn+ Bn-| / |B0|^2;
  * NaN unless all five lines of each direction end on one face, or where
  * B0 = 0.  Outputs as nfgs_trace_field_lines for the central line (ends
- * (2, n, 3), flags (2, n), length (2, n)) except bn (3, n) = |B0|, |Bn+|,
- * |Bn-|; q (n).  delta > 0 in grid units. */
+ * (2, n, 3), flags (2, n), length (2, n), twist (2, n) or NULL) except
+ * bn (3, n) = |B0|, |Bn+|, |Bn-|; q (n).  delta > 0 in grid units. */
 int nfgs_trace_qperp(const void* b, int32_t dtype, int32_t nz, int32_t ny, int32_t nx, const void* seeds, int64_t n,
                      double delta, double step, int32_t max_steps, void* ends, int32_t* flags, void* bn, void* length,
-                     void* q, void* stream);
+                     void* q, void* twist, void* stream);
 
 /* ------------------------------------------------------------------------
  * Learned warm start: operator kernels of a 3-D neural operator on a

@@ -120,10 +120,10 @@ SIGNATURES = {
     "nfgs_iterate_restart_from": (C.c_int, [_P, _P, _P, C.c_int32, _DP]),
     "nfgs_iterate_soft_cfcf_start": (C.c_int, [_P, C.c_double, C.c_double, _DP]),
     "nfgs_trace_field_lines": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int64, _DP,
-                                         C.c_double, C.c_int32, _P, _P, _P, _P, _P]),
+                                         C.c_double, C.c_int32, _P, _P, _P, _P, _P, _P]),
     "nfgs_qmap_plane": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P, _P]),
     "nfgs_trace_qperp": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int64, C.c_double,
-                                   C.c_double, C.c_int32, _P, _P, _P, _P, _P, _P]),
+                                   C.c_double, C.c_int32, _P, _P, _P, _P, _P, _P, _P]),
     # learned warm start operator kernels (device pointers)
     "nfgs_nn_last_error": (C.c_char_p, []),
     "nfgs_nn_pointwise": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, C.c_int64, C.c_int32, _P]),

@@ -2711,50 +2711,60 @@ static int gaussian_above_noalloc_impl(Handle* h, double* out, cudaStream_t st) 
 // ===========================================================================
 namespace {
 
+// B (and with a twist output J = curl B in grid units) packed per node
+template <typename T>
+static cudaError_t pack_field(const void* b, int nx, int ny, int nz, bool tw, T** pk, cudaStream_t s) {
+    const long long V = (long long)nz * ny * nx;
+    cudaError_t e = cudaMallocAsync((void**)pk, (size_t)V * (tw ? 8 : 4) * sizeof(T), s);
+    if (e != cudaSuccess) return e;
+    if (tw) trace::k_pack<T, true><<<(unsigned)((V + 255) / 256), 256, 0, s>>>((const T*)b, nx, ny, nz, *pk);
+    else trace::k_pack<T, false><<<(unsigned)((V + 255) / 256), 256, 0, s>>>((const T*)b, nx, ny, nz, *pk);
+    return cudaGetLastError();
+}
+
 template <typename T>
 static int trace_lines_t(const void* b, int32_t nz, int32_t ny, int32_t nx, const void* seeds, int64_t n,
                          const double* nrm, double step, int32_t max_steps, void* ends, int32_t* flags, void* bn,
-                         void* len, cudaStream_t s) {
-    const long long V = (long long)nz * ny * nx;
+                         void* len, void* tw, cudaStream_t s) {
     T* pk = nullptr;
-    CK(cudaMallocAsync((void**)&pk, (size_t)V * 4 * sizeof(T), s));
-    trace::k_pack<T><<<(unsigned)((V + 255) / 256), 256, 0, s>>>((const T*)b, V, pk);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = pack_field<T>(b, nx, ny, nz, tw != nullptr, &pk, s);
     if (e == cudaSuccess && n > 0) {
-        const trace::Box bx{nx, ny, nz};
-        trace::k_trace<T><<<(unsigned)((2 * n + 127) / 128), 128, 0, s>>>(
-            pk, bx, (const T*)seeds, n, (T)nrm[0], (T)nrm[1], (T)nrm[2], (T)step, max_steps, (T*)ends, flags,
-            (T*)bn, (T*)len);
+        const trace::Box bx{nx, ny, nz, tw ? 8 : 4};
+        const unsigned grid = (unsigned)((2 * n + 127) / 128);
+        if (tw)
+            trace::k_trace<T, true><<<grid, 128, 0, s>>>(pk, bx, (const T*)seeds, n, (T)nrm[0], (T)nrm[1],
+                                                         (T)nrm[2], (T)step, max_steps, (T*)ends, flags, (T*)bn,
+                                                         (T*)len, (T*)tw);
+        else
+            trace::k_trace<T, false><<<grid, 128, 0, s>>>(pk, bx, (const T*)seeds, n, (T)nrm[0], (T)nrm[1],
+                                                          (T)nrm[2], (T)step, max_steps, (T*)ends, flags, (T*)bn,
+                                                          (T*)len, nullptr);
         e = cudaGetLastError();
     }
-    cudaFreeAsync(pk, s);
+    if (pk) cudaFreeAsync(pk, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(NFGS_ECUDA, std::string("trace: ") + cudaGetErrorString(e));
     return NFGS_OK;
 }
 
-}  // namespace
-
-namespace {
-
 template <typename T>
 static int trace_qperp_t(const void* b, int32_t nz, int32_t ny, int32_t nx, const void* seeds, int64_t n,
                          double delta, double step, int32_t max_steps, void* ends, int32_t* flags, void* bn,
-                         void* len, void* q, cudaStream_t s) {
-    const long long V = (long long)nz * ny * nx;
+                         void* len, void* q, void* tw, cudaStream_t s) {
     T *pk = nullptr, *e5 = nullptr;
     int* f5 = nullptr;
-    CK(cudaMallocAsync((void**)&pk, (size_t)V * 4 * sizeof(T), s));
-    cudaError_t e = cudaMallocAsync((void**)&e5, (size_t)std::max<int64_t>(n, 1) * 30 * sizeof(T), s);
+    cudaError_t e = pack_field<T>(b, nx, ny, nz, tw != nullptr, &pk, s);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&e5, (size_t)std::max<int64_t>(n, 1) * 30 * sizeof(T), s);
     if (e == cudaSuccess) e = cudaMallocAsync((void**)&f5, (size_t)std::max<int64_t>(n, 1) * 10 * sizeof(int), s);
-    if (e == cudaSuccess) {
-        trace::k_pack<T><<<(unsigned)((V + 255) / 256), 256, 0, s>>>((const T*)b, V, pk);
-        e = cudaGetLastError();
-    }
     if (e == cudaSuccess && n > 0) {
-        const trace::Box bx{nx, ny, nz};
-        trace::k_trace_perp<T><<<(unsigned)((10 * n + 127) / 128), 128, 0, s>>>(
-            pk, bx, (const T*)seeds, n, (T)delta, (T)step, max_steps, e5, f5, (T*)bn, (T*)len);
+        const trace::Box bx{nx, ny, nz, tw ? 8 : 4};
+        const unsigned grid = (unsigned)((10 * n + 127) / 128);
+        if (tw)
+            trace::k_trace_perp<T, true><<<grid, 128, 0, s>>>(pk, bx, (const T*)seeds, n, (T)delta, (T)step,
+                                                              max_steps, e5, f5, (T*)bn, (T*)len, (T*)tw);
+        else
+            trace::k_trace_perp<T, false><<<grid, 128, 0, s>>>(pk, bx, (const T*)seeds, n, (T)delta, (T)step,
+                                                               max_steps, e5, f5, (T*)bn, (T*)len, nullptr);
         e = cudaGetLastError();
         if (e == cudaSuccess) {
             trace::k_qperp<T><<<(unsigned)((n + 127) / 128), 128, 0, s>>>(n, (T)delta, e5, f5, (const T*)bn, (T*)q);
@@ -2771,7 +2781,7 @@ static int trace_qperp_t(const void* b, int32_t nz, int32_t ny, int32_t nx, cons
     }
     if (f5) cudaFreeAsync(f5, s);
     if (e5) cudaFreeAsync(e5, s);
-    cudaFreeAsync(pk, s);
+    if (pk) cudaFreeAsync(pk, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(NFGS_ECUDA, std::string("trace: ") + cudaGetErrorString(e));
     return NFGS_OK;
@@ -3108,7 +3118,7 @@ int nfgs_field_metrics(const void* ref, const void* sol, const void* cur, int32_
 
 int nfgs_trace_field_lines(const void* b, int32_t dtype, int32_t nz, int32_t ny, int32_t nx, const void* seeds,
                            int64_t n, const double* normal3, double step, int32_t max_steps, void* ends,
-                           int32_t* flags, void* bn, void* length, void* stream) {
+                           int32_t* flags, void* bn, void* length, void* twist, void* stream) {
     g_err.clear();
     if (!b || !normal3 || (n > 0 && (!seeds || !ends || !flags || !bn || !length)))
         return fail(NFGS_EINVAL, "null argument");
@@ -3117,16 +3127,17 @@ int nfgs_trace_field_lines(const void* b, int32_t dtype, int32_t nz, int32_t ny,
     if (n < 0 || 2 * n > (int64_t)INT32_MAX * 128) return fail(NFGS_EINVAL, "bad seed count");
     if (!(step > 0.0) || !std::isfinite(step)) return fail(NFGS_EINVAL, "step must be positive");
     if (max_steps < 1) return fail(NFGS_EINVAL, "max_steps must be positive");
+    if (twist && (nz < 3 || ny < 3 || nx < 3)) return fail(NFGS_EINVAL, "the twist needs at least 3 nodes per axis");
     cudaStream_t s = (cudaStream_t)stream;
-    return dtype == NFGS_F32
-               ? trace_lines_t<float>(b, nz, ny, nx, seeds, n, normal3, step, max_steps, ends, flags, bn, length, s)
-               : trace_lines_t<double>(b, nz, ny, nx, seeds, n, normal3, step, max_steps, ends, flags, bn, length,
-                                       s);
+    return dtype == NFGS_F32 ? trace_lines_t<float>(b, nz, ny, nx, seeds, n, normal3, step, max_steps, ends, flags,
+                                                    bn, length, twist, s)
+                             : trace_lines_t<double>(b, nz, ny, nx, seeds, n, normal3, step, max_steps, ends, flags,
+                                                     bn, length, twist, s);
 }
 
 int nfgs_trace_qperp(const void* b, int32_t dtype, int32_t nz, int32_t ny, int32_t nx, const void* seeds, int64_t n,
                      double delta, double step, int32_t max_steps, void* ends, int32_t* flags, void* bn, void* length,
-                     void* q, void* stream) {
+                     void* q, void* twist, void* stream) {
     g_err.clear();
     if (!b || (n > 0 && (!seeds || !ends || !flags || !bn || !length || !q))) return fail(NFGS_EINVAL, "null argument");
     if (dtype != NFGS_F32 && dtype != NFGS_F64) return fail(NFGS_EINVAL, "dtype must be F32 or F64");
@@ -3135,11 +3146,12 @@ int nfgs_trace_qperp(const void* b, int32_t dtype, int32_t nz, int32_t ny, int32
     if (!(step > 0.0) || !std::isfinite(step)) return fail(NFGS_EINVAL, "step must be positive");
     if (!(delta > 0.0) || !std::isfinite(delta)) return fail(NFGS_EINVAL, "delta must be positive");
     if (max_steps < 1) return fail(NFGS_EINVAL, "max_steps must be positive");
+    if (twist && (nz < 3 || ny < 3 || nx < 3)) return fail(NFGS_EINVAL, "the twist needs at least 3 nodes per axis");
     cudaStream_t s = (cudaStream_t)stream;
     return dtype == NFGS_F32 ? trace_qperp_t<float>(b, nz, ny, nx, seeds, n, delta, step, max_steps, ends, flags, bn,
-                                                    length, q, s)
+                                                    length, q, twist, s)
                              : trace_qperp_t<double>(b, nz, ny, nx, seeds, n, delta, step, max_steps, ends, flags,
-                                                     bn, length, q, s);
+                                                     bn, length, q, twist, s);
 }
 
 int nfgs_qmap_plane(int32_t dtype, int32_t nu, int32_t nv, const void* ends, const int32_t* flags, const void* bn,

@@ -36,24 +36,52 @@ __device__ __forceinline__ void load3<double>(const double* __restrict__ p, doub
     x = a.x; y = a.y; z = __ldg(p + 2);
 }
 
-// (3, nz, ny, nx) component-major -> 4 values per node
-template <typename T>
-__global__ void k_pack(const T* __restrict__ b, long long V, T* __restrict__ pk) {
+// second-order derivative in grid units along a line of n samples (the
+// centred difference inside, three-point one-sided ends; n >= 3)
+template <typename T, typename F>
+__device__ __forceinline__ T grad1(F f, int i, int n) {
+    if (i == 0) return (T(-3) * f(0) + T(4) * f(1) - f(2)) * T(0.5);
+    if (i == n - 1) return (T(3) * f(n - 1) - T(4) * f(n - 2) + f(n - 3)) * T(0.5);
+    return (f(i + 1) - f(i - 1)) * T(0.5);
+}
+
+// (3, nz, ny, nx) component-major -> (Bx, By, Bz, 0) per node, followed with
+// TW by (Jx, Jy, Jz, 0), J = curl B in grid units
+template <typename T, bool TW>
+__global__ void k_pack(const T* __restrict__ b, int nx, int ny, int nz, T* __restrict__ pk) {
+    const long long V = (long long)nx * ny * nz;
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= V) return;
-    pk[4 * c] = b[c];
-    pk[4 * c + 1] = b[V + c];
-    pk[4 * c + 2] = b[2 * V + c];
-    pk[4 * c + 3] = T(0);
+    constexpr int S = TW ? 8 : 4;
+    pk[S * c] = b[c];
+    pk[S * c + 1] = b[V + c];
+    pk[S * c + 2] = b[2 * V + c];
+    pk[S * c + 3] = T(0);
+    if constexpr (TW) {
+        const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+        const long long P = (long long)nx * ny;
+        auto ax = [&](int comp) { return [=](int q) { return b[comp * V + c + (q - i)]; }; };
+        auto ay = [&](int comp) { return [=](int q) { return b[comp * V + c + (long long)(q - j) * nx]; }; };
+        auto az = [&](int comp) { return [=](int q) { return b[comp * V + c + (long long)(q - k) * P]; }; };
+        const T dbz_dy = grad1<T>(ay(2), j, ny), dby_dz = grad1<T>(az(1), k, nz);
+        const T dbx_dz = grad1<T>(az(0), k, nz), dbz_dx = grad1<T>(ax(2), i, nx);
+        const T dby_dx = grad1<T>(ax(1), i, nx), dbx_dy = grad1<T>(ay(0), j, ny);
+        pk[S * c + 4] = dbz_dy - dby_dz;
+        pk[S * c + 5] = dbx_dz - dbz_dx;
+        pk[S * c + 6] = dby_dx - dbx_dy;
+        pk[S * c + 7] = T(0);
+    }
 }
 
 struct Box {
     int nx, ny, nz;
+    int st;  // values per node in the packed field: 4 (B) or 8 (B, J)
 };
 
 // trilinear interpolation at a position clamped into the box
 template <typename T>
-__device__ __forceinline__ void interp(const T* __restrict__ pk, Box bx, T x, T y, T z, T& ox, T& oy, T& oz) {
+__device__ __forceinline__ void interp(const T* __restrict__ pk, Box bx, T x, T y, T z, T& ox, T& oy, T& oz,
+                                       int off = 0) {
     x = fmin(fmax(x, T(0)), T(bx.nx - 1));
     y = fmin(fmax(y, T(0)), T(bx.ny - 1));
     z = fmin(fmax(z, T(0)), T(bx.nz - 1));
@@ -61,8 +89,8 @@ __device__ __forceinline__ void interp(const T* __restrict__ pk, Box bx, T x, T 
     const int j = min((int)floor(y), bx.ny - 2);
     const int k = min((int)floor(z), bx.nz - 2);
     const T fx = x - T(i), fy = y - T(j), fz = z - T(k);
-    const long long sx = 4, sy = 4LL * bx.nx, sz = 4LL * bx.nx * bx.ny;
-    const T* p = pk + k * sz + j * sy + i * sx;
+    const long long sx = bx.st, sy = (long long)bx.st * bx.nx, sz = (long long)bx.st * bx.nx * bx.ny;
+    const T* p = pk + k * sz + j * sy + i * sx + off;
     T c[8][3];
 #pragma unroll
     for (int q = 0; q < 8; ++q)
@@ -92,27 +120,50 @@ __device__ __forceinline__ bool direction(const T* __restrict__ pk, Box bx, T s,
     return true;
 }
 
+// unit direction and, with TW, the twist integrand J.B / (4 pi |B|^2)
+template <typename T, bool TW>
+__device__ __forceinline__ bool dir_tw(const T* __restrict__ pk, Box bx, T s, const T (&p)[3], T (&d)[3], T& f) {
+    T b0, b1, b2;
+    interp<T>(pk, bx, p[0], p[1], p[2], b0, b1, b2);
+    const T m2 = b0 * b0 + b1 * b1 + b2 * b2;
+    const T m = sqrt(m2);
+    if (!(m > T(0))) return false;
+    const T g = s / m;
+    d[0] = b0 * g; d[1] = b1 * g; d[2] = b2 * g;
+    if constexpr (TW) {
+        T j0, j1, j2;
+        interp<T>(pk, bx, p[0], p[1], p[2], j0, j1, j2, 4);
+        f = (j0 * b0 + j1 * b1 + j2 * b2) / (T(4.0 * 3.14159265358979323846) * m2);
+    }
+    return true;
+}
+
 // Trace one line from p (inside the box) along s B: p becomes the end point;
-// returns the face code (1..6), 0 after max_steps, -1 at a zero field.
-template <typename T>
+// returns the face code (1..6), 0 after max_steps, -1 at a zero field.  With
+// TW, twist integrates J.B / (4 pi |B|^2) ds with the same RK4 stages (the
+// cut last step contributes its fraction t).
+template <typename T, bool TW = false>
 __device__ int trace_line(const T* __restrict__ pk, Box bx, const T (&hi)[3], T (&p)[3], T s, T h, int max_steps,
-                          T& length) {
+                          T& length, T& twist) {
     const T h2 = h * T(0.5), h6 = h / T(6);
     length = T(0);
+    twist = T(0);
     for (int it = 0; it < max_steps; ++it) {
         T k1[3], k2[3], k3[3], k4[3], q[3];
-        if (!direction<T>(pk, bx, s, p, k1)) return -1;
+        T f1 = T(0), f2 = T(0), f3 = T(0), f4 = T(0);
+        if (!dir_tw<T, TW>(pk, bx, s, p, k1, f1)) return -1;
 #pragma unroll
         for (int d = 0; d < 3; ++d) q[d] = p[d] + h2 * k1[d];
-        if (!direction<T>(pk, bx, s, q, k2)) return -1;
+        if (!dir_tw<T, TW>(pk, bx, s, q, k2, f2)) return -1;
 #pragma unroll
         for (int d = 0; d < 3; ++d) q[d] = p[d] + h2 * k2[d];
-        if (!direction<T>(pk, bx, s, q, k3)) return -1;
+        if (!dir_tw<T, TW>(pk, bx, s, q, k3, f3)) return -1;
 #pragma unroll
         for (int d = 0; d < 3; ++d) q[d] = p[d] + h * k3[d];
-        if (!direction<T>(pk, bx, s, q, k4)) return -1;
+        if (!dir_tw<T, TW>(pk, bx, s, q, k4, f4)) return -1;
 #pragma unroll
         for (int d = 0; d < 3; ++d) q[d] = p[d] + h6 * (k1[d] + T(2) * k2[d] + T(2) * k3[d] + k4[d]);
+        const T dtw = TW ? h6 * (f1 + T(2) * f2 + T(2) * f3 + f4) : T(0);
         bool inside = true;
 #pragma unroll
         for (int d = 0; d < 3; ++d) inside = inside && q[d] >= T(0) && q[d] <= hi[d];
@@ -120,6 +171,7 @@ __device__ int trace_line(const T* __restrict__ pk, Box bx, const T (&hi)[3], T 
 #pragma unroll
             for (int d = 0; d < 3; ++d) p[d] = q[d];
             length += h;
+            if (TW) twist += dtw;
             continue;
         }
         // the chord p -> q meets the first face at fraction t
@@ -141,6 +193,7 @@ __device__ int trace_line(const T* __restrict__ pk, Box bx, const T (&hi)[3], T 
         const int fd = (face - 1) >> 1;
         p[fd] = (face & 1) ? T(0) : hi[fd];
         length += t * h;
+        if (TW) twist += t * dtw;
         return face;
     }
     return 0;
@@ -158,11 +211,11 @@ __device__ __forceinline__ T end_bn(const T* __restrict__ pk, Box bx, const T (&
 // Trace seed `si` along +B (dir 0) or -B (dir 1).  ends (2, n, 3), flags
 // (2, n), bn (3, n): B.n0 at the seed, |B.n| at the forward and backward
 // ends; len (2, n) per direction.
-template <typename T>
+template <typename T, bool TW>
 __global__ void __launch_bounds__(128) k_trace(const T* __restrict__ pk, Box bx, const T* __restrict__ seeds,
                                                long long n, T n0x, T n0y, T n0z, T h, int max_steps,
                                                T* __restrict__ ends, int* __restrict__ flags, T* __restrict__ bn,
-                                               T* __restrict__ len) {
+                                               T* __restrict__ len, T* __restrict__ tw) {
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= 2 * n) return;
     const int dir = tid >= n ? 1 : 0;
@@ -177,13 +230,14 @@ __global__ void __launch_bounds__(128) k_trace(const T* __restrict__ pk, Box bx,
         interp<T>(pk, bx, p[0], p[1], p[2], b0, b1, b2);
         bn[si] = b0 * n0x + b1 * n0y + b2 * n0z;
     }
-    T length;
-    const int flag = trace_line<T>(pk, bx, hi, p, dir == 0 ? T(1) : T(-1), h, max_steps, length);
+    T length, twist;
+    const int flag = trace_line<T, TW>(pk, bx, hi, p, dir == 0 ? T(1) : T(-1), h, max_steps, length, twist);
     ends[3 * tid] = p[0];
     ends[3 * tid + 1] = p[1];
     ends[3 * tid + 2] = p[2];
     flags[tid] = flag;
     len[tid] = length;
+    if (TW) tw[tid] = twist;
     bn[n * (1 + dir) + si] = end_bn<T>(pk, bx, p, flag);
 }
 
@@ -215,11 +269,11 @@ __device__ __forceinline__ bool perp_frame(const T (&B)[3], T& bm, T (&e1)[3], T
 // ways.  Thread tid = (dir * 5 + a) * n + si.  ends (2, 5, n, 3), flags
 // (2, 5, n); bn (3, n): |B0|, |Bn+|, |Bn-| of the central line; len (2, n)
 // of the central line.
-template <typename T>
+template <typename T, bool TW>
 __global__ void __launch_bounds__(128) k_trace_perp(const T* __restrict__ pk, Box bx, const T* __restrict__ seeds,
                                                     long long n, T delta, T h, int max_steps, T* __restrict__ ends,
                                                     int* __restrict__ flags, T* __restrict__ bn,
-                                                    T* __restrict__ len) {
+                                                    T* __restrict__ len, T* __restrict__ tw) {
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= 10 * n) return;
     const long long si = tid % n;
@@ -239,14 +293,16 @@ __global__ void __launch_bounds__(128) k_trace_perp(const T* __restrict__ pk, Bo
 #pragma unroll
         for (int d = 0; d < 3; ++d) p[d] = fmin(fmax(p[d] + sg * delta * e[d], T(0)), hi[d]);
     }
-    T length = T(0);
-    const int flag = ok ? trace_line<T>(pk, bx, hi, p, dir == 0 ? T(1) : T(-1), h, max_steps, length) : -1;
+    T length = T(0), twist = T(0);
+    const int flag =
+        ok ? trace_line<T, TW>(pk, bx, hi, p, dir == 0 ? T(1) : T(-1), h, max_steps, length, twist) : -1;
     ends[3 * tid] = p[0];
     ends[3 * tid + 1] = p[1];
     ends[3 * tid + 2] = p[2];
     flags[tid] = flag;
     if (a == 0) {
         len[dir * n + si] = length;
+        if (TW) tw[dir * n + si] = twist;
         bn[n * (1 + dir) + si] = end_bn<T>(pk, bx, p, flag);
     }
 }

@@ -23,7 +23,9 @@ Differences from the reference helpers, by design:
   and recorded only (the library launches every seed at once);
 * flags are the face codes of ``nfgs_trace_field_lines`` (1..6 for
   x=0, x=nx-1, y=0, y=ny-1, z=0, z=nz-1; 0 unfinished; -1 zero field);
-* ``include_twist=True`` raises NotImplementedError.
+* ``include_twist=True`` integrates J.B / (4 pi |B|^2) along both halves of
+  the central line with the RK4 stages of the trace (J = curl B by
+  second-order differences in grid units, as fastqsl_plane.py:287-305).
 
     python -m nfgs_b200.qmap --n 256 --nz 128 --report qmap.json
 """
@@ -92,10 +94,12 @@ def spectral_gaussian_lowpass(b, sigma_cells: float):
     return out.to(torch.float32).to(b.dtype).contiguous()
 
 
-def trace_field_lines(b, seeds, *, normal=(0.0, 0.0, 1.0), step_len: float = 1.0 / 8.0, max_steps=None):
+def trace_field_lines(b, seeds, *, normal=(0.0, 0.0, 1.0), step_len: float = 1.0 / 8.0, max_steps=None,
+                      twist: bool = False):
     """Trace seeds (n, 3 xyz grid units) through b (3, nz, ny, nx CUDA
     tensor, float32 or float64) along +B and -B.  Returns device tensors:
-    ends (2, n, 3), flags (2, n) int32, bn (3, n), length (2, n)."""
+    ends (2, n, 3), flags (2, n) int32, bn (3, n), length (2, n), and with
+    twist=True the twist of each half (2, n)."""
     torch = _torch()
     if b.dtype not in (torch.float32, torch.float64) or b.device.type != "cuda" or b.ndim != 4 or b.shape[0] != 3:
         raise ValueError("b must be a (3, nz, ny, nx) float32/float64 CUDA tensor")
@@ -109,21 +113,28 @@ def trace_field_lines(b, seeds, *, normal=(0.0, 0.0, 1.0), step_len: float = 1.0
     flags = torch.empty((2, n), dtype=torch.int32, device=b.device)
     bn = torch.empty((3, n), dtype=b.dtype, device=b.device)
     length = torch.empty((2, n), dtype=b.dtype, device=b.device)
+    tw = torch.empty((2, n), dtype=b.dtype, device=b.device) if twist else None
     nrm = np.asarray(normal, dtype=np.float64)
     code = L.NFGS_F32 if b.dtype == torch.float32 else L.NFGS_F64
     stream = torch.cuda.current_stream(b.device)
     L.check(L.lib().nfgs_trace_field_lines(
         C.c_void_p(b.data_ptr()), code, nz, ny, nx, C.c_void_p(seeds.data_ptr()), n, L.dptr(nrm),
         float(step_len), int(max_steps), C.c_void_p(ends.data_ptr()), C.c_void_p(flags.data_ptr()),
-        C.c_void_p(bn.data_ptr()), C.c_void_p(length.data_ptr()), C.c_void_p(stream.cuda_stream)))
-    return {"ends": ends, "flags": flags, "bn": bn, "length": length, "max_steps": max_steps}
+        C.c_void_p(bn.data_ptr()), C.c_void_p(length.data_ptr()), C.c_void_p(tw.data_ptr() if twist else None),
+        C.c_void_p(stream.cuda_stream)))
+    out = {"ends": ends, "flags": flags, "bn": bn, "length": length, "max_steps": max_steps}
+    if twist:
+        out["twist"] = tw
+    return out
 
 
-def trace_qperp(b, seeds, *, delta: float = 0.25, step_len: float = 1.0 / 8.0, max_steps=None):
+def trace_qperp(b, seeds, *, delta: float = 0.25, step_len: float = 1.0 / 8.0, max_steps=None,
+                twist: bool = False):
     """Q_perp (Titov 2007) at each seed: five lines per seed (the seed and
     +-delta along two unit vectors perpendicular to B), traced both ways.
     Returns device tensors q (n,), ends (2, n, 3), flags (2, n) int32,
-    bn (3, n) = |B0|, |Bn+|, |Bn-|, length (2, n) of the central line."""
+    bn (3, n) = |B0|, |Bn+|, |Bn-|, length (2, n) of the central line, and
+    with twist=True its twist per half (2, n)."""
     torch = _torch()
     if b.dtype not in (torch.float32, torch.float64) or b.device.type != "cuda" or b.ndim != 4 or b.shape[0] != 3:
         raise ValueError("b must be a (3, nz, ny, nx) float32/float64 CUDA tensor")
@@ -138,22 +149,24 @@ def trace_qperp(b, seeds, *, delta: float = 0.25, step_len: float = 1.0 / 8.0, m
            "flags": torch.empty((2, n), dtype=torch.int32, device=b.device),
            "bn": torch.empty((3, n), dtype=b.dtype, device=b.device),
            "length": torch.empty((2, n), dtype=b.dtype, device=b.device)}
+    if twist:
+        out["twist"] = torch.empty((2, n), dtype=b.dtype, device=b.device)
     code = L.NFGS_F32 if b.dtype == torch.float32 else L.NFGS_F64
     stream = torch.cuda.current_stream(b.device)
     L.check(L.lib().nfgs_trace_qperp(
         C.c_void_p(b.data_ptr()), code, nz, ny, nx, C.c_void_p(seeds.data_ptr()), n, float(delta), float(step_len),
         int(max_steps), C.c_void_p(out["ends"].data_ptr()), C.c_void_p(out["flags"].data_ptr()),
         C.c_void_p(out["bn"].data_ptr()), C.c_void_p(out["length"].data_ptr()), C.c_void_p(out["q"].data_ptr()),
-        C.c_void_p(stream.cuda_stream)))
+        C.c_void_p(out["twist"].data_ptr() if twist else None), C.c_void_p(stream.cuda_stream)))
     out["max_steps"] = max_steps
     return out
 
 
-def _plane_q(b, seeds, nu, nv, normal, q_method, step_len, max_steps, delta):
+def _plane_q(b, seeds, nu, nv, normal, q_method, step_len, max_steps, delta, twist=False):
     """Trace the nv x nu seed grid and evaluate Q by the chosen method; the
     plane's border is NaN either way (the reference keeps only the interior)."""
     if q_method == "perp":
-        tr = trace_qperp(b, seeds, delta=delta, step_len=step_len, max_steps=max_steps)
+        tr = trace_qperp(b, seeds, delta=delta, step_len=step_len, max_steps=max_steps, twist=twist)
         q = tr["q"].reshape(nv, nu).clone()
         q[0, :] = float("nan")
         q[-1, :] = float("nan")
@@ -161,7 +174,7 @@ def _plane_q(b, seeds, nu, nv, normal, q_method, step_len, max_steps, delta):
         q[:, -1] = float("nan")
         return tr, q
     if q_method == "plane":
-        tr = trace_field_lines(b, seeds, normal=normal, step_len=step_len, max_steps=max_steps)
+        tr = trace_field_lines(b, seeds, normal=normal, step_len=step_len, max_steps=max_steps, twist=twist)
         return tr, q_on_plane(tr, nu, nv)
     raise ValueError("q_method must be 'perp' or 'plane'")
 
@@ -183,7 +196,10 @@ def _bundle(tr, q, plane_shape, meta):
     ends = tr["ends"].float().cpu().numpy()
     flags = tr["flags"].cpu().numpy()
     length = (tr["length"][0] + tr["length"][1]).float().cpu().numpy()
-    return {
+    extra = {}
+    if "twist" in tr:
+        extra["twist"] = (tr["twist"][0] + tr["twist"][1]).double().cpu().numpy().reshape(nv, nu)
+    return {**extra,
         "q": q.float().cpu().numpy(),
         "flag_start": flags[1].reshape(nv, nu).astype(np.int32),
         "flag_end": flags[0].reshape(nv, nu).astype(np.int32),
@@ -204,8 +220,6 @@ def compute_y0_qmap(bx, by, bz, *, fastqsl_root=None, y_index=None, step_len: fl
     +-delta, defined where B lies in the plane (By = 0 on the midplane of a
     symmetric field); "plane": central differences over the seed grid."""
     torch = _torch()
-    if include_twist:
-        raise NotImplementedError("include_twist: the twist line integral is not built for B200")
     dt = torch.float64 if str(dtype) in ("float64", "torch.float64") else torch.float32
     b = spectral_gaussian_lowpass(_volume(bx, by, bz, dt), b_smooth_sigma_cells)
     _, nz, ny, nx = (int(v) for v in b.shape)
@@ -217,7 +231,8 @@ def compute_y0_qmap(bx, by, bz, *, fastqsl_root=None, y_index=None, step_len: fl
     z, x = torch.meshgrid(torch.arange(nz, dtype=dt, device=b.device), torch.arange(nx, dtype=dt, device=b.device),
                           indexing="ij")
     seeds = torch.stack([x.reshape(-1), torch.full_like(x.reshape(-1), iy), z.reshape(-1)], dim=1)
-    tr, q = _plane_q(b, seeds, nx, nz, (0.0, 1.0, 0.0), q_method, step_len, max_steps, delta)
+    tr, q = _plane_q(b, seeds, nx, nz, (0.0, 1.0, 0.0), q_method, step_len, max_steps, delta,
+                     twist=bool(include_twist))
     torch.cuda.synchronize()
     meta = {"algorithm": f"B200 RK4 tracer + Q ({q_method}) on y=0", "q_method": q_method, "delta": float(delta),
             "shape_zyx": [nz, ny, nx],
@@ -226,7 +241,7 @@ def compute_y0_qmap(bx, by, bz, *, fastqsl_root=None, y_index=None, step_len: fl
             "step_len_grid": float(step_len), "tolerance": float(tol), "max_steps": tr["max_steps"],
             "block": [int(block_x), 1, 1], "trace_chunk_seeds": int(trace_chunk_seeds), "trace_n_chunks": 1,
             "downsample": 1, "qmap_b_smooth_sigma_cells": float(b_smooth_sigma_cells),
-            "elapsed_s": time.perf_counter() - t0, "twist_included": False,
+            "elapsed_s": time.perf_counter() - t0, "twist_included": bool(include_twist),
             "dtype": "float64" if dt == torch.float64 else "float32"}
     return _bundle(tr, q, (nz, nx), meta)
 

@@ -52,12 +52,23 @@ def interp(pk, pts):
     return y0 + fz * (y1 - y0)
 
 
-def trace(b, seeds, normal, step, max_steps):
+def curl_grid(b):
+    """J = curl B in grid units with second-order differences (centred inside,
+    three-point one-sided at the walls), b (3, nz, ny, nx); the reference's
+    include_twist current (fastqsl_plane.py:287-305)."""
+    g = [[np.gradient(b[c], axis=a, edge_order=2) for a in range(3)] for c in range(3)]  # g[c][axis z,y,x]
+    return np.stack([g[2][1] - g[1][0], g[0][0] - g[2][2], g[1][2] - g[0][1]])
+
+
+def trace(b, seeds, normal, step, max_steps, twist=False):
     """Trace every seed along +B and -B.  b (3, nz, ny, nx); seeds (n, 3).
     Returns ends (2, n, 3), flags (2, n), bn (3, n), length (2, n) with the
-    layout and codes of nfgs_trace_field_lines."""
+    layout and codes of nfgs_trace_field_lines; with twist=True also the
+    twist of each half (2, n): J.B / (4 pi |B|^2) integrated with the RK4
+    stages of the line (a cut last step contributes its fraction)."""
     b = np.asarray(b, dtype=np.float64)
     pk = np.ascontiguousarray(np.moveaxis(b, 0, -1))
+    pj = np.ascontiguousarray(np.moveaxis(curl_grid(b), 0, -1)) if twist else None
     nz, ny, nx, _ = pk.shape
     hi = np.array([nx - 1.0, ny - 1.0, nz - 1.0])
     seeds = np.clip(np.asarray(seeds, dtype=np.float64).reshape(-1, 3), 0.0, hi)
@@ -69,31 +80,36 @@ def trace(b, seeds, normal, step, max_steps):
     sgn = np.concatenate([np.ones(n), -np.ones(n)])[:, None]
     flags = np.zeros(2 * n, dtype=np.int32)
     length = np.zeros(2 * n)
+    tw = np.zeros(2 * n)
     act = np.arange(2 * n)
 
     def direction(q, s):
         v = interp(pk, q)
-        m = np.sqrt((v * v).sum(axis=1))
+        m2 = (v * v).sum(axis=1)
+        m = np.sqrt(m2)
         ok = m > 0
         with np.errstate(invalid="ignore", divide="ignore"):
             d = v * (s / m[:, None])
+            f = (interp(pj, q) * v).sum(axis=1) / (4.0 * np.pi * m2) if twist else np.zeros(len(q))
         d[~ok] = 0.0  # the line stops there; keep later stages finite
-        return d, ok
+        return d, ok, f
 
     for _ in range(max_steps):
         if act.size == 0:
             break
         pa, s = p[act], sgn[act]
-        k1, o1 = direction(pa, s)
-        k2, o2 = direction(pa + 0.5 * step * k1, s)
-        k3, o3 = direction(pa + 0.5 * step * k2, s)
-        k4, o4 = direction(pa + step * k3, s)
+        k1, o1, f1 = direction(pa, s)
+        k2, o2, f2 = direction(pa + 0.5 * step * k1, s)
+        k3, o3, f3 = direction(pa + 0.5 * step * k2, s)
+        k4, o4, f4 = direction(pa + step * k3, s)
         ok = o1 & o2 & o3 & o4
         flags[act[~ok]] = -1
         q = pa + (step / 6.0) * (k1 + 2.0 * k2 + 2.0 * k3 + k4)
+        dtw = (step / 6.0) * (f1 + 2.0 * f2 + 2.0 * f3 + f4)
         inside = np.all((q >= 0.0) & (q <= hi), axis=1) & ok
         p[act[inside]] = q[inside]
         length[act[inside]] += step
+        tw[act[inside]] += dtw[inside]
         out = ok & ~inside
         if out.any():
             po, qo, ids = pa[out], q[out], act[out]
@@ -112,6 +128,7 @@ def trace(b, seeds, normal, step, max_steps):
             e[np.arange(ids.size), fd] = np.where(face % 2 == 1, 0.0, hi[fd])
             p[ids] = e
             length[ids] += t * step
+            tw[ids] += t * dtw[out]
             flags[ids] = face
         act = act[inside]
     ends = p.reshape(2, n, 3)
@@ -122,6 +139,8 @@ def trace(b, seeds, normal, step, max_steps):
         if okf.any():
             bv = interp(pk, ends[d][okf])
             bn[1 + d, okf] = np.abs(bv[np.arange(bv.shape[0]), (f[okf] - 1) // 2])
+    if twist:
+        return ends, flags, bn, length.reshape(2, n), tw.reshape(2, n)
     return ends, flags, bn, length.reshape(2, n)
 
 

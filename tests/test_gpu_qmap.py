@@ -141,8 +141,6 @@ def test_reference_helpers_contract():
     assert rb["q"].shape == (28, 33) and np.isfinite(rb["q"]).sum() > 100
     with pytest.raises(ValueError, match="outside"):
         Q.compute_y0_qmap(b[0], b[1], b[2], y_index=40.0)
-    with pytest.raises(NotImplementedError):
-        Q.compute_y0_qmap(b[0], b[1], b[2], include_twist=True)
     # spectral pre-smoothing (fastqsl_plane.py:82-101) restated in NumPy
     sig = 0.75
     freqs = [np.fft.fftfreq(n) for n in b.shape[1:]]
@@ -208,3 +206,46 @@ def test_y0_helper_defaults_to_qperp():
     np.testing.assert_allclose(r["q"][3:18, 14:27], 2.0 * np.cosh(2.0), rtol=5e-3)
     rp = Q.compute_y0_qmap(b[0], b[1], b[2], q_method="plane")
     assert not np.isfinite(rp["q"]).any()
+
+
+@pytest.mark.parametrize("dtype_name", ["float64", "float32"])
+def test_twist_known_answer_and_oracle(dtype_name):
+    """B = (0, sin ax, cos ax): twist = sin(a) L / (4 pi) per half; FP64 also
+    equals the oracle on the dipole field."""
+    import torch
+
+    from nfgs_b200.qmap import trace_field_lines, trace_qperp
+    from oracle import trace_oracle as T
+
+    dt = getattr(torch, dtype_name)
+    nx, ny, nz, al = 12, 20, 20, 0.3
+    z, y, x = np.meshgrid(np.arange(nz, dtype=float), np.arange(ny, dtype=float), np.arange(nx, dtype=float),
+                          indexing="ij")
+    b = np.stack([np.zeros_like(x), np.sin(al * x), np.cos(al * x)])
+    seeds = np.array([[xx, 10.0, zz] for xx in range(2, 10) for zz in (4.0, 9.5)])
+    bt = torch.as_tensor(b, dtype=dt, device="cuda")
+    st = torch.as_tensor(seeds, dtype=dt, device="cuda")
+    tr = host(trace_field_lines(bt, st, normal=(0, 1, 0), max_steps=2000, twist=True))
+    tol = 1e-12 if dtype_name == "float64" else 2e-5
+    np.testing.assert_allclose(tr["twist"], np.sin(al) * tr["length"] / (4 * np.pi), rtol=tol, atol=1e-7)
+    qp = host(trace_qperp(bt, st, max_steps=2000, twist=True))
+    np.testing.assert_allclose(qp["twist"], tr["twist"], rtol=tol, atol=1e-7)
+    if dtype_name == "float64":
+        bd = T.dipole_field(30, 26, 16)
+        sd = plane_seeds(30, 26, 0.5)
+        g = host(trace_field_lines(torch.as_tensor(bd, device="cuda"), torch.as_tensor(sd, device="cuda"),
+                                   max_steps=4000, twist=True))
+        _, f, _, _, two = T.trace(bd, sd, (0, 0, 1), 0.125, 4000, twist=True)
+        np.testing.assert_array_equal(g["flags"], f)
+        np.testing.assert_allclose(g["twist"], two, rtol=1e-9, atol=1e-12)
+
+
+def test_y0_helper_twist_bundle():
+    from nfgs_b200 import qmap as Q
+    from oracle import trace_oracle as T
+
+    b = T.dipole_field(33, 28, 17).astype(np.float32)
+    r = Q.compute_y0_qmap(b[0], b[1], b[2], include_twist=True)
+    assert r["twist"].shape == (17, 33) and r["twist"].dtype == np.float64
+    assert r["metadata"]["twist_included"]
+    assert np.isfinite(r["twist"]).all()

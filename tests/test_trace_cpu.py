@@ -111,3 +111,17 @@ def test_qperp_frame_and_uniform_field():
     seeds = np.stack([x.ravel(), y.ravel(), np.full(x.size, 4.0)], axis=1)
     q, *_ = T.qperp(bu, seeds, 0.25, 0.125, 1000)
     np.testing.assert_allclose(q, 2.0, rtol=1e-10)
+
+
+def test_twist_of_a_linear_force_free_field():
+    """B = (0, sin ax, cos ax) has J = a B; with grid differences J.B = sin(a)
+    at interior x, so each line's twist is sin(a) L / (4 pi)."""
+    nx, ny, nz, al = 12, 20, 20, 0.3
+    z, y, x = np.meshgrid(np.arange(nz, dtype=float), np.arange(ny, dtype=float), np.arange(nx, dtype=float),
+                          indexing="ij")
+    b = np.stack([np.zeros_like(x), np.sin(al * x), np.cos(al * x)])
+    seeds = np.array([[xx, 10.0, zz] for xx in range(2, 10) for zz in (4.0, 9.5)])
+    ends, flags, bn, length, tw = T.trace(b, seeds, (0, 1, 0), 0.125, 2000, twist=True)
+    assert (flags > 0).all()
+    np.testing.assert_allclose(tw, np.sin(al) * length / (4 * np.pi), rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(T.curl_grid(b)[2][:, :, 1:-1], np.sin(al) * b[2][:, :, 1:-1], rtol=1e-12, atol=1e-15)
