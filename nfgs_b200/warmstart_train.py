@@ -171,8 +171,14 @@ def train(ds, cfg: LN.Config, epochs: int, lr: float = 1e-3, batch: int = 4, val
 def evaluate(model, seeds, n: int = 256, nz: int = 128, eps=(1e-4, 1e-3), max_iter: int = 3000, log=print):
     torch = _torch()
     solver = NFGSSolverGPU(n, n, nz, 1.0, 1.0, 1.0, **SOLVER_KW)
-    # bases and scratch of this grid are built once, outside the timed runs
+    # bases and scratch of this grid are built once, outside the timed runs,
+    # and the learned start runs once untimed (its one-time set-up, as the
+    # plain path's graph capture and stencil tuning happen in the sigma* run)
     model.forward(torch.zeros((model.cfg.cin, solver.Nz, solver.Ny, solver.Nx), device="cuda"))
+    if seeds:
+        bx, by, bz = sunspot_magnetogram(n, seeds[0])
+        solver.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+        solver.iterate(max_iter=2, verbose=False, init_mode="learned", warm_start=model, **STOP)
     torch.cuda.synchronize()
     rows = []
     for sd in seeds:
