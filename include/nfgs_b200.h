@@ -305,7 +305,11 @@ int nfgs_scan_destroy(void* scan);
  * nfgs_iterate_restart_from: phi, az are device arrays of the same shape and
  * type, complete when called (the library reads them on its own stream).
  * mode 0: only evaluate their sigma_J; 1: make them the start when their
- * sigma_J is lower than the gs_cfcf start's; 2: make them the start.
+ * sigma_J is lower than the gs_cfcf start's; 2: make them the start;
+ * 3: evaluate like 0 but leave the start's sources to be restored by the
+ * next call of another mode or by the first nfgs_iterate_advance (several
+ * candidates in a row then cost one restore); 4: only that restore (phi and
+ * az may be NULL; out3[0] NaN).
  * out3 = {sigma of the supplied state, sigma of the gs_cfcf start, 1 if it
  * became the start}.  Must come before the first nfgs_iterate_advance
  * (NFGS_ESTATE otherwise). */
@@ -460,6 +464,10 @@ int nfgs_nn_reduce3(const float* in, float* out, int32_t C, int32_t nz, int32_t 
 int nfgs_nn_expand3(const float* in, float* out, int32_t C, int32_t nz, int32_t ny, int32_t nx, const float* Mz,
                     const float* My, const float* Mx, int32_t kz, int32_t ky, int32_t kx, int32_t accumulate,
                     float* t1, float* t2, void* stream);
+/* out (C, mz, my, mx) = trilinear resampling of in (C, nz, ny, nx) between node grids spanning the same box
+ * (target node z' at source coordinate z' (nz-1)/(mz-1), likewise y, x). */
+int nfgs_nn_resample_linear(const float* in, float* out, int32_t C, int32_t nz, int32_t ny, int32_t nx, int32_t mz,
+                            int32_t my, int32_t mx, void* stream);
 /* yh[o,k] = sum_i W[(k*ci + i)*co + o] xh[i,k] */
 int nfgs_nn_modemix(const float* xh, const float* W, float* yh, int32_t ci, int32_t co, int32_t nm, void* stream);
 /* gxh = W^T gyh per mode; gW += xh gyh^T per mode */

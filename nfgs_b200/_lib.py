@@ -135,6 +135,8 @@ SIGNATURES = {
                                   C.c_int32, C.c_int32, _P, _P, _P]),
     "nfgs_nn_expand3": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, C.c_int32,
                                   C.c_int32, C.c_int32, C.c_int32, _P, _P, _P]),
+    "nfgs_nn_resample_linear": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                          C.c_int32, _P]),
     "nfgs_nn_modemix": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, C.c_int32, _P]),
     "nfgs_nn_modemix_bwd": (C.c_int, [_P, _P, _P, _P, _P, C.c_int32, C.c_int32, C.c_int32, _P]),
     "nfgs_nn_mse": (C.c_int, [_P, _P, _P, _P, C.c_int64, C.c_double, _P, _P, _P]),

@@ -371,6 +371,37 @@ int nfgs_nn_gelu_bwd(const float* x, const float* gy, float* gx, int64_t n, int3
     return NFGS_OK;
 }
 
+// Trilinear resampling between node grids spanning the same box: target node
+// (z', y', x') sits at source coordinates z' (nz-1)/(mz-1), ... (a single
+// node maps to coordinate 0).
+__global__ void k_resample_linear(const float* __restrict__ in, float* __restrict__ out, int C, int nz, int ny,
+                                  int nx, int mz, int my, int mx) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long tot = (long long)C * mz * my * mx;
+    if (t >= tot) return;
+    const int xo = (int)(t % mx), yo = (int)((t / mx) % my), zo = (int)((t / ((long long)mx * my)) % mz);
+    const int c = (int)(t / ((long long)mx * my * mz));
+    auto axis = [](int o, int m, int n, int& i0, int& i1, float& w) {
+        const float f = m > 1 ? (float)o * (float)(n - 1) / (float)(m - 1) : 0.f;
+        i0 = min(max((int)floorf(f), 0), max(n - 2, 0));
+        i1 = min(i0 + 1, n - 1);
+        w = fminf(fmaxf(f - (float)i0, 0.f), 1.f);
+    };
+    int x0, x1, y0, y1, z0, z1;
+    float wx, wy, wz;
+    axis(xo, mx, nx, x0, x1, wx);
+    axis(yo, my, ny, y0, y1, wy);
+    axis(zo, mz, nz, z0, z1, wz);
+    const float* b = in + (long long)c * nz * ny * nx;
+    auto at = [&](int z, int y, int x) { return b[((long long)z * ny + y) * nx + x]; };
+    const float c00 = at(z0, y0, x0) + wx * (at(z0, y0, x1) - at(z0, y0, x0));
+    const float c01 = at(z0, y1, x0) + wx * (at(z0, y1, x1) - at(z0, y1, x0));
+    const float c10 = at(z1, y0, x0) + wx * (at(z1, y0, x1) - at(z1, y0, x0));
+    const float c11 = at(z1, y1, x0) + wx * (at(z1, y1, x1) - at(z1, y1, x0));
+    const float d0 = c00 + wy * (c01 - c00), d1 = c10 + wy * (c11 - c10);
+    out[t] = d0 + wz * (d1 - d0);
+}
+
 // in (C, nz, ny, nx) -> out (C, kz, ky, kx); t1 (C*nz*ny*kx), t2 (C*nz*ky*kx) scratch
 int nfgs_nn_reduce3(const float* in, float* out, int32_t C, int32_t nz, int32_t ny, int32_t nx, const float* Mz,
                     const float* My, const float* Mx, int32_t kz, int32_t ky, int32_t kx, float* t1, float* t2,
@@ -414,6 +445,16 @@ int nfgs_nn_expand3(const float* in, float* out, int32_t C, int32_t nz, int32_t 
     NNCK(cudaGetLastError());
     const long long rows = (long long)C * nz * ny;
     k_expand_x<<<nblk(rows * nx, 256), 256, 0, s>>>(t2, Mx, out, rows, nx, kx, accumulate);
+    NNCK(cudaGetLastError());
+    return NFGS_OK;
+}
+
+int nfgs_nn_resample_linear(const float* in, float* out, int32_t C, int32_t nz, int32_t ny, int32_t nx, int32_t mz,
+                            int32_t my, int32_t mx, void* stream) {
+    if (!in || !out || C <= 0 || nz <= 0 || ny <= 0 || nx <= 0 || mz <= 0 || my <= 0 || mx <= 0)
+        return nn_fail(NFGS_EINVAL, "resample_linear: bad arguments");
+    const long long tot = (long long)C * mz * my * mx;
+    k_resample_linear<<<nblk(tot, 256), 256, 0, (cudaStream_t)stream>>>(in, out, C, nz, ny, nx, mz, my, mx);
     NNCK(cudaGetLastError());
     return NFGS_OK;
 }

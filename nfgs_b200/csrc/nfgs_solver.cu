@@ -146,6 +146,7 @@ struct Handle {
     int fs_tuned = 0;          // the fused-stencil segment count has been tuned
     long long pface_len = 0;   // doubles in pface
     int advanced = 0;          // the current iteration has taken a step
+    int stale_start = 0;       // restart mode 3 left the candidate's sources in place of the start's
     cudaEvent_t pin_ev[2] = {nullptr, nullptr};
 };
 
@@ -1666,11 +1667,34 @@ static int start_state(Handle* h, void** phi, void** az) {
 template <typename T>
 static int adopt_buffer2(Handle* h, int mode, double* out);
 
+// Sources and sums of the start state (buffer 0) again, and buffer 2 a copy
+// of it: the modal solves never write some boundary entries of a candidate
+// buffer, so nothing of a rejected state may outlive the restart calls.
+template <typename T>
+static int restore_start(Handle* h) {
+    const size_t vb = (size_t)h->g.V * h->esz;
+    TRY(run_stencil<T>(h, &h->consts[0], nullptr, 1, h->stop.polarity_mask));
+    sum_partials(h);
+    CK(cudaMemcpyAsync(h->st.phi[2], h->st.phi[0], vb, cudaMemcpyDeviceToDevice, h->s));
+    CK(cudaMemcpyAsync(h->st.az[2], h->st.az[0], vb, cudaMemcpyDeviceToDevice, h->s));
+    h->stale_start = 0;
+    return NFGS_OK;
+}
+
 template <typename T>
 static int restart_from_t(Handle* h, const void* phi, const void* az, int mode, double* out) {
     if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
     if (h->advanced) return fail(NFGS_ESTATE, "the iteration has already advanced");
     const size_t vb = (size_t)h->g.V * h->esz;
+    if (mode == 4) {
+        if (h->stale_start) TRY(restore_start<T>(h));
+        CK(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->s));
+        CK(cudaStreamSynchronize(h->s));
+        out[0] = std::nan("");
+        out[1] = h->ctl_h->sigma0;
+        out[2] = 0.0;
+        return NFGS_OK;
+    }
     CK(cudaMemcpyAsync(h->st.phi[2], phi, vb, cudaMemcpyDeviceToDevice, h->s));
     CK(cudaMemcpyAsync(h->st.az[2], az, vb, cudaMemcpyDeviceToDevice, h->s));
     return adopt_buffer2<T>(h, mode, out);
@@ -1698,14 +1722,13 @@ static int adopt_buffer2(Handle* h, int mode, double* out) {
         CK(cudaMemcpyAsync(h->st.az[0], h->st.az[2], vb, cudaMemcpyDeviceToDevice, h->s));
         k_ctl_init<<<1, 1, 0, h->s>>>(h->g, h->ctl, h->scal, h->hist);
         CK(cudaGetLastError());
+        h->stale_start = 0;
+    } else if (mode == 3) {
+        // evaluation only: the start's sources are restored by the next
+        // restart call of another mode or before the first advance
+        h->stale_start = 1;
     } else {
-        // restore the sources of the gs_cfcf start, and overwrite the rejected
-        // state: the modal solves never write some boundary entries of a
-        // candidate buffer, so nothing of it may outlive this call
-        TRY(run_stencil<T>(h, &h->consts[0], nullptr, 1, h->stop.polarity_mask));
-        sum_partials(h);
-        CK(cudaMemcpyAsync(h->st.phi[2], h->st.phi[0], vb, cudaMemcpyDeviceToDevice, h->s));
-        CK(cudaMemcpyAsync(h->st.az[2], h->st.az[0], vb, cudaMemcpyDeviceToDevice, h->s));
+        TRY(restore_start<T>(h));
     }
     CK(cudaStreamSynchronize(h->s));
     out[0] = sc[0];
@@ -1834,6 +1857,7 @@ static int ensure_graph_t(Handle* h) {
 template <typename T>
 static int iterate_advance_t(Handle* h, int max_steps, int32_t* stop_reason, int32_t* n_done) {
     if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
+    if (h->stale_start) TRY(restore_start<T>(h));
     h->advanced = 1;
     CK(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(DevCtl), cudaMemcpyDeviceToHost, h->s));
     CK(cudaStreamSynchronize(h->s));
@@ -2885,8 +2909,8 @@ int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int
     g_err.clear();
     Handle* h = (Handle*)handle;
     if (h) cudaSetDevice(h->geom.device);
-    if (!h || !phi || !az || !out3) return fail(NFGS_EINVAL, "null argument");
-    if (mode < 0 || mode > 2) return fail(NFGS_EINVAL, "mode must be 0, 1 or 2");
+    if (!h || !out3 || (mode != 4 && (!phi || !az))) return fail(NFGS_EINVAL, "null argument");
+    if (mode < 0 || mode > 4) return fail(NFGS_EINVAL, "mode must be 0 to 4");
     return h->f32 ? restart_from_t<float>(h, phi, az, mode, out3) : restart_from_t<double>(h, phi, az, mode, out3);
 }
 

@@ -78,6 +78,10 @@ class Config:
     # the output is band-limited to these cosine modes per axis (z, y, x),
     # capped by the grid; (0, 0, 0) leaves it unfiltered
     out_modes: tuple = (24, 24, 24)
+    # (nz, ny, nx) of the calculation grids the network was trained on; the
+    # learned start evaluates it there (features resampled, output brought
+    # back by cosine synthesis); () evaluates it on the solver's grid
+    train_shape: tuple = ()
 
     def param_shapes(self) -> list[tuple[str, tuple]]:
         w, nm = self.width, int(np.prod(self.modes))
@@ -203,7 +207,7 @@ class NeuralOperator:
     def load(cls, path: str | Path, device="cuda") -> "NeuralOperator":
         d = np.load(path, allow_pickle=False)
         c = json.loads(str(d["config"]))
-        for key in ("modes", "in_scale", "out_scale", "out_modes"):
+        for key in ("modes", "in_scale", "out_scale", "out_modes", "train_shape"):
             if key in c:
                 c[key] = tuple(c[key])
         cfg = Config(**c)
@@ -446,8 +450,44 @@ def band_limit(model: NeuralOperator, field, modes):
     return out
 
 
+def resample_linear(model: NeuralOperator, field, shape):
+    """Trilinear resampling of a (C, nz, ny, nx) device field onto a node grid
+    of `shape` spanning the same box (nfgs_nn_resample_linear)."""
+    torch = _torch()
+    C_, nz, ny, nx = field.shape
+    dst = tuple(int(v) for v in shape)
+    f = field.float().contiguous()
+    out = torch.empty((C_,) + dst, device=field.device)
+    _ck(model.lib.nfgs_nn_resample_linear(_p(f), _p(out), C_, nz, ny, nx, dst[0], dst[1], dst[2], model._stream()))
+    return out
+
+
+def resample_modes(model: NeuralOperator, field, shape, modes):
+    """A field band-limited to `modes` cosine modes per axis (x <= 32) moved
+    to a node grid of `shape` spanning the same box: analysis on the source
+    grid (nfgs_nn_reduce3), synthesis on the target (nfgs_nn_expand3); exact
+    for band-limited fields."""
+    torch = _torch()
+    C_, nz, ny, nx = field.shape
+    src, dst = (nz, ny, nx), tuple(int(v) for v in shape)
+    k = tuple(max(1, min(int(m), a, b)) for m, a, b in zip(modes, src, dst))
+    A = [torch.from_numpy(cosine_bases(n, kk)[0]).to(field.device) for n, kk in zip(src, k)]
+    S = [torch.from_numpy(cosine_bases(n, kk)[1]).to(field.device) for n, kk in zip(dst, k)]
+    f = field.float().contiguous()
+    coef = torch.empty(C_ * k[0] * k[1] * k[2], device=field.device)
+    big = torch.empty(C_ * max(nz * ny * k[2], dst[0] * dst[1] * k[2]), device=field.device)
+    small = torch.empty(C_ * max(nz * k[1] * k[2], dst[0] * k[1] * k[2]), device=field.device)
+    out = torch.empty((C_,) + dst, device=field.device)
+    st = model._stream()
+    _ck(model.lib.nfgs_nn_reduce3(_p(f), _p(coef), C_, nz, ny, nx, _p(A[0]), _p(A[1]), _p(A[2]), k[0], k[1], k[2],
+                                  _p(big), _p(small), st))
+    _ck(model.lib.nfgs_nn_expand3(_p(coef), _p(out), C_, dst[0], dst[1], dst[2], _p(S[0]), _p(S[1]), _p(S[2]),
+                                  k[0], k[1], k[2], 0, _p(small), _p(big), st))
+    return out
+
+
 def learned_start(solver, model, fallback: bool = True, scales_tried=(1.0, 0.6, 0.35, 0.2),
-                  filters_tried=None) -> dict:
+                  filters_tried=None, eval_shape="train") -> dict:
     """After nfgs_iterate_begin: hand a predicted start to the solver.
 
     model: a NeuralOperator, or a callable (solver, phi, az) -> (phi, az)
@@ -456,7 +496,11 @@ def learned_start(solver, model, fallback: bool = True, scales_tried=(1.0, 0.6, 
     and the one with the lowest sigma_J is kept when it beats the gs_cfcf
     start (fallback) -- the plain iteration then runs unchanged.  Each band
     limit of filters_tried (default model.start_filters) is tried with every
-    scale."""
+    scale.  eval_shape (nz, ny, nx): evaluate the network on that grid from
+    trilinearly resampled features, and bring its band-limited output back by
+    cosine synthesis; "train" (default): the network's training grid
+    (cfg.train_shape, or the solver grid when that is not recorded); None:
+    the solver grid."""
     torch = _torch()
     phi, az = start_state_views(solver)
     lib = solver._lib
@@ -477,8 +521,16 @@ def learned_start(solver, model, fallback: bool = True, scales_tried=(1.0, 0.6, 
 
     x = features(solver, phi, az, model.cfg.in_scale)
     bs, ls = scales(solver)
+    if isinstance(eval_shape, str):
+        eval_shape = tuple(model.cfg.train_shape) or None
     with torch.no_grad():
-        y = model.forward(x)
+        if eval_shape is not None and tuple(eval_shape) != tuple(x.shape[1:]):
+            if not all(0 < k <= 32 for k in model.cfg.out_modes[2:]) or not all(k > 0 for k in model.cfg.out_modes):
+                raise ValueError("eval_shape needs a network with band-limited output (out_modes, x <= 32)")
+            yc = model.forward(resample_linear(model, x, eval_shape))
+            y = resample_modes(model, yc, x.shape[1:], model.cfg.out_modes)
+        else:
+            y = model.forward(x)
         m = masks(solver.Nz, solver.Ny, solver.Nx, x.device)
         osc = torch.tensor(model.cfg.out_scale, device=x.device, dtype=torch.float32).view(2, 1, 1, 1)
         corr = ((y * m) * osc * (bs * ls)).double()
@@ -489,12 +541,14 @@ def learned_start(solver, model, fallback: bool = True, scales_tried=(1.0, 0.6, 
         for lam in scales_tried:
             cp = (phi.double() + lam * cf[0]).to(phi.dtype).contiguous()
             ca = (az.double() + lam * cf[1]).to(az.dtype).contiguous()
-            s_new, s_gs, _ = evaluate(cp, ca, 0)
+            s_new, s_gs, _ = evaluate(cp, ca, 3)  # the start's sources are restored once, below
             tried.append((flt, lam, s_new))
             if np.isfinite(s_new) and (best is None or s_new < best[1]):
                 best = (lam, s_new, cp, ca, flt)
     accepted = False
     if best is not None and (not fallback or best[1] < s_gs):
         _, _, accepted = evaluate(best[2], best[3], 2)
+    else:
+        L.check(lib.nfgs_iterate_restart_from(solver._h, None, None, 4, L.dptr(out)))
     return {"sigma_learned": best[1] if best else float("nan"), "sigma_gs_cfcf": s_gs, "accepted": accepted,
             "scale": best[0] if best else None, "filter": best[4] if best else None, "tried": tried}

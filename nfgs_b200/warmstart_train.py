@@ -251,7 +251,10 @@ def main(argv=None):
                       log=lambda m: print(m, flush=True))
         report["generation_s"] = time.perf_counter() - t0
         report["generation_mean_iterations"] = float(np.mean(ds["iters"]))
-        cfg = LN.Config()
+        from .grid import calculation_grid
+
+        cg = calculation_grid(args.n, args.n, args.nz)
+        cfg = LN.Config(train_shape=(cg["nz"], cg["ny"], cg["nx"]))
         print(f"training ({sum(int(np.prod(s)) for _, s in cfg.param_shapes())} parameters)", flush=True)
         model, tr = train(ds, cfg, args.epochs, args.lr, args.batch, log=lambda m: print(m, flush=True))
         report["training"] = tr

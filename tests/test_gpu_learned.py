@@ -236,3 +236,72 @@ def test_learned_start_accepts_better_state_and_falls_back():
                     init_mode="learned", warm_start=noisy)
     assert not h3["learned_start"]["accepted"]
     assert h3["sigma"] == plain["sigma"]
+
+
+def test_resampling_between_grids():
+    """Trilinear resampling reproduces a linear field exactly; cosine
+    resampling of a band-limited field equals its synthesis on the target."""
+    from nfgs_b200 import learned as LN
+
+    cfg = LN.Config(cin=2, width=8, layers=1, modes=(3, 3, 3), hidden=8, cout=2, out_modes=(4, 5, 6))
+    model = LN.NeuralOperator(cfg)
+    src, dst = (9, 14, 17), (5, 8, 10)
+    z, y, x = np.meshgrid(*(np.linspace(0, 1, n) for n in src), indexing="ij")
+    lin = np.stack([1 + 2 * x - 3 * y + 0.5 * z, x * 0 + 4.0]).astype(np.float32)
+    out = LN.resample_linear(model, torch.from_numpy(lin).cuda(), dst).cpu().numpy()
+    z2, y2, x2 = np.meshgrid(*(np.linspace(0, 1, n) for n in dst), indexing="ij")
+    np.testing.assert_allclose(out[0], 1 + 2 * x2 - 3 * y2 + 0.5 * z2, atol=2e-6)
+    np.testing.assert_allclose(out[1], 4.0, atol=1e-6)
+    rng = np.random.default_rng(2)
+    k = (4, 5, 6)
+    coef = rng.normal(size=(2,) + k)
+
+    def synth(shape):
+        Sz, Sy, Sx = (LN.cosine_bases(n, kk)[1] for n, kk in zip(shape, k))
+        return np.einsum("cabd,ai,bj,dk->cijk", coef, Sz, Sy, Sx)
+
+    f = torch.from_numpy(synth(src).astype(np.float32)).cuda()
+    g = LN.resample_modes(model, f, dst, k).cpu().numpy()
+    ref = synth(dst)
+    np.testing.assert_allclose(g, ref, atol=2e-5 * np.abs(ref).max())
+
+
+def test_restart_evaluate_only_modes_restore_the_start():
+    """Mode 3 evaluates candidates without restoring the start's sources;
+    mode 4, or the first advance, restores them: the run then equals the plain
+    one bit for bit."""
+    import ctypes as C
+
+    from nfgs_b200 import NFGSSolverGPU
+    from nfgs_b200 import _lib as L
+    from nfgs_b200.learned import start_state_views
+    from nfgs_b200.synthetic import sunspot_magnetogram
+
+    bx, by, bz = sunspot_magnetogram(40, seed=12)
+    kw = dict(dtype="float32", bottom_divergence_robin_weight=0.5, d0_zero_mode_policy="project",
+              source_zero_mode_policy="project")
+    stop = dict(max_iter=60, tol=1e-5, patience=40, sigma_improvement_tol=1e-5, verbose=False)
+
+    def make():
+        s = NFGSSolverGPU(40, 40, 20, 1.0, 1.0, 1.0, **kw)
+        s.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+        return s
+
+    plain = make().iterate(**stop)
+    for final_mode in (4, None):
+        s = make()
+        ctx = s._iterate_begin(**stop)
+        phi, az = start_state_views(s)
+        out = np.zeros(3)
+        for scale in (1.5, 0.5):
+            cp, ca = (phi * scale).contiguous(), (az * scale).contiguous()
+            torch.cuda.synchronize()
+            L.check(s._lib.nfgs_iterate_restart_from(s._h, C.c_void_p(cp.data_ptr()), C.c_void_p(ca.data_ptr()),
+                                                     3, L.dptr(out)))
+            assert np.isfinite(out[0]) and out[2] == 0.0
+        if final_mode == 4:
+            L.check(s._lib.nfgs_iterate_restart_from(s._h, None, None, 4, L.dptr(out)))
+            assert np.isnan(out[0])
+        s._iterate_loop(ctx)
+        h = s._iterate_finish(ctx)
+        assert h["sigma"] == plain["sigma"]
