@@ -542,6 +542,22 @@ class NFGSSolverGPU:
     # ------------------------------------------------------------------
     # Iteration (nfgs_solver.py:6937-7009 -> 3522-3850)
     # ------------------------------------------------------------------
+    def compute_initial_conditions(self, *, init_mode="gs_cfcf", **_unused):
+        """The start state of `init_mode` (gs_cfcf, nfgs_solver.py:6613-6645;
+        soft_cfcf, 6427-6484) as host arrays (B, J, Phi_c, A_z, B_c) on the
+        calculation grid, B_c = B - B_background.  It is built on the device
+        as iterate() builds it; until the next iterate(), fields_to_numpy()
+        returns this state."""
+        mode = str(init_mode).lower().replace("-", "_")
+        if mode == "learned":
+            raise ValueError("NFGS supports init_mode='gs_cfcf', 'cfcf', or 'soft_cfcf'")
+        ctx = self._iterate_begin(max_iter=0, verbose=False, init_mode=init_mode)
+        self._iterate_finish(ctx)  # no step: the start is the current and the selected state
+        B, J = self._state_fields(which=1)
+        phi, az, _ = self._get_state(1)
+        dt = self._np_dtype
+        return B, J, phi.astype(dt), az.astype(dt), (B - self.B_background).astype(dt)
+
     def iterate(self, max_iter=200, tol=1e-5, mu=1.0, patience=1, verbose=True, polarity_mask="both", *,
                 init_mode="gs_cfcf", sigma_improvement_tol: Optional[float] = 1e-5,
                 per_step_callback: Optional[Callable] = None, adaptive_mu: bool = False, mu_min: float = 0.02,

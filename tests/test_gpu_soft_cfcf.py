@@ -153,3 +153,24 @@ def test_start_is_replaced_only_before_advance():
     assert t.Nz == 4
     with pytest.raises(ValueError, match="Nz >= 5"):
         t.iterate(init_mode="soft_cfcf", max_iter=2, verbose=False)
+
+
+@pytest.mark.parametrize("mode", ["gs_cfcf", "soft_cfcf"])
+def test_compute_initial_conditions(mode):
+    """NFGSSolverGPU.compute_initial_conditions returns the reference's start
+    state (B, J, Phi_c, A_z, B_c) for both built start modes (FP64)."""
+    if mode == "soft_cfcf":
+        meta, data = load("small_eps_ridge")
+    else:
+        gold = Path(__file__).resolve().parent / "golden"
+        meta = json.loads((gold / "small_rho03_buffer.json").read_text())
+        data = dict(np.load(gold / "small_rho03_buffer.npz"))
+    s = solver(meta, data, "float64")
+    B, J, phi, az, bc = s.compute_initial_conditions(init_mode=mode)
+    assert B.shape == (3, s.Nz, s.Ny, s.Nx) and phi.shape == (s.Nz, s.Ny, s.Nx)
+    assert rel(phi, data["init_phi"]) < 1e-10
+    assert rel(az, data["init_az"]) < 1e-10
+    if "init_B" in data:
+        assert rel(B, data["init_B"]) < 1e-10
+        assert rel(J, data["init_J"]) < 1e-9
+    np.testing.assert_allclose(bc, B - s.B_background, rtol=0, atol=1e-12)
