@@ -105,9 +105,49 @@ __global__ void __launch_bounds__(256) gemm_strided_kernel(GemmArgs g) {
     }
 }
 
+// Small problems (a few planes: the boundary set-up's 2-D transforms) would
+// occupy a few dozen 64 x 64 tiles; 16 x 16 tiles with one output per thread
+// spread them over the SMs.
+template <typename T>
+__global__ void __launch_bounds__(256) gemm_small_kernel(GemmArgs g) {
+    if (g.ctl != nullptr && g.ctl->stopped) return;
+    __shared__ T As[16][17];
+    __shared__ T Bs[16][17];
+    const int b = blockIdx.z;
+    const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
+    const int r = blockIdx.y * 16 + tr, c = blockIdx.x * 16 + tc;
+    const T* A = (const T*)g.A + (long long)b * g.a_bs;
+    const T* Bm = (const T*)g.B + (long long)b * g.b_bs;
+    T acc = T(0);
+    for (int k0 = 0; k0 < g.K; k0 += 16) {
+        // A tile rows r0.., columns k0..: thread (tr, tc) loads A(r0 + tr, k0 + tc)
+        const int ar = blockIdx.y * 16 + tr, ak = k0 + tc;
+        As[tr][tc] = (ar < g.M && ak < g.K) ? A[(long long)ar * g.a_rs + (long long)ak * g.a_cs] : T(0);
+        const int bk = k0 + tr, bc = blockIdx.x * 16 + tc;
+        Bs[tr][tc] = (bk < g.K && bc < g.N) ? Bm[(long long)bk * g.b_rs + (long long)bc * g.b_cs] : T(0);
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) acc = fma(As[tr][kk], Bs[kk][tc], acc);
+        __syncthreads();
+    }
+    if (r >= g.M || c >= g.N) return;
+    char* cbase;
+    if (g.c_table != nullptr) cbase = (char*)g.c_table[*g.c_sel] + (long long)(intptr_t)g.C;
+    else cbase = (char*)g.C;
+    T* C = (T*)cbase + (long long)b * g.c_bs;
+    C[(long long)r * g.c_rs + (long long)c * g.c_cs] = acc;
+}
+
 template <typename T>
 static inline cudaError_t launch_gemm(const GemmArgs& g, cudaStream_t s) {
     if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return cudaSuccess;
+    const long long big_tiles =
+        (long long)((g.N + GEMM_BN - 1) / GEMM_BN) * ((g.M + GEMM_BM - 1) / GEMM_BM) * g.batch;
+    if (big_tiles < 148 && g.batch <= 65535) {
+        dim3 grid((g.N + 15) / 16, (g.M + 15) / 16, g.batch);
+        gemm_small_kernel<T><<<grid, 256, 0, s>>>(g);
+        return cudaGetLastError();
+    }
     dim3 grid((g.N + GEMM_BN - 1) / GEMM_BN, (g.M + GEMM_BM - 1) / GEMM_BM, g.batch);
     gemm_strided_kernel<T><<<grid, 256, 0, s>>>(g);
     return cudaGetLastError();

@@ -127,6 +127,56 @@ __global__ void k_reduce4(const double* __restrict__ a, long long n, double* out
     }
 }
 
+// Two-stage form for long arrays: block b reduces the chunk
+// [b*chunk, (b+1)*chunk) in a fixed order into part[4b..4b+3]; then one block
+// combines the partials in a fixed order.
+__global__ void k_reduce4_part(const double* __restrict__ a, long long n, long long chunk, double* part) {
+    __shared__ double sh[3 * 32];
+    __shared__ double smax[32];
+    const long long q0 = (long long)blockIdx.x * chunk, q1 = min(n, q0 + chunk);
+    double v[3] = {0, 0, 0};
+    double mx = 0.0;
+    for (long long q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+        double x = a[q];
+        v[0] += x;
+        v[1] += x * x;
+        v[2] += fabs(x);
+        mx = fmax(mx, fabs(x));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = mx;
+    block_reduce<3>(v, sh);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) m = fmax(m, smax[w]);
+        part[4 * blockIdx.x] = v[0]; part[4 * blockIdx.x + 1] = v[1];
+        part[4 * blockIdx.x + 2] = v[2]; part[4 * blockIdx.x + 3] = m;
+    }
+}
+
+__global__ void k_reduce4_final(const double* __restrict__ part, int nb, double* out) {
+    __shared__ double sh[3 * 32];
+    __shared__ double smax[32];
+    double v[3] = {0, 0, 0};
+    double mx = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        v[0] += part[4 * b];
+        v[1] += part[4 * b + 1];
+        v[2] += part[4 * b + 2];
+        mx = fmax(mx, part[4 * b + 3]);
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = mx;
+    block_reduce<3>(v, sh);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) m = fmax(m, smax[w]);
+        out[0] = v[0]; out[1] = v[1]; out[2] = v[2]; out[3] = m;
+    }
+}
+
 // 2-D derivative of a (ny, nx) map, one-sided ends
 // (nfgs_solver.py:1429-1469): axis 0 -> d/dx, 1 -> d/dy.
 __device__ __forceinline__ double d2d(const double* a, int nx, int ny, int j, int i, int axis, double h) {

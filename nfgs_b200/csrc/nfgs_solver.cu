@@ -293,8 +293,25 @@ static std::vector<double> d2h(Handle* h, const double* p, size_t n) {
 
 // reductions of n FP64 values: sum, sum of squares, sum |x|, max |x|
 static int reduce4(Handle* h, const double* a, long long n, double out[4]) {
-    k_reduce4<<<1, 1024, 0, h->s>>>(a, n, h->scal);
-    h->launches++;
+    if (n > (1LL << 18)) {
+        // volumes: 512 fixed chunks, then their fixed-order combination
+        constexpr int NBP = 512;
+        const long long chunk = (n + NBP - 1) / NBP;
+        double* part = nullptr;
+        CK(cudaMallocAsync((void**)&part, NBP * 4 * sizeof(double), h->s));
+        k_reduce4_part<<<NBP, 256, 0, h->s>>>(a, n, chunk, part);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            k_reduce4_final<<<1, 512, 0, h->s>>>(part, NBP, h->scal);
+            e = cudaGetLastError();
+        }
+        cudaFreeAsync(part, h->s);
+        CK(e);
+        h->launches += 2;
+    } else {
+        k_reduce4<<<1, 1024, 0, h->s>>>(a, n, h->scal);
+        h->launches++;
+    }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, h->scal, 4 * sizeof(double), cudaMemcpyDeviceToHost, h->s));
     CK(cudaStreamSynchronize(h->s));
