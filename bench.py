@@ -26,6 +26,7 @@ import math
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 from pathlib import Path
@@ -79,7 +80,8 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{index}.csv"
+        # the raw samples (the JSON line carries their summary); NFGS_CLOCKS_DIR keeps them
+        self.path = Path(os.environ.get("NFGS_CLOCKS_DIR", tempfile.gettempdir())) / f"nfgs_clocks_{index}.csv"
 
     def start(self):
         try:
