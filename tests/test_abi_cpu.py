@@ -113,6 +113,12 @@ def test_option_validation_before_device():
         NFGSSolverGPU(16, 16, 8, 1, 1, 1, alpha_clip_scale=1.0, alpha_limit_factor=2.0)
     with pytest.raises(TypeError):
         NFGSSolverGPU(16, 16, 8, 1, 1, 1, not_an_option=1)
+    with pytest.raises(ValueError, match="soft_cfcf_epsilon"):
+        NFGSSolverGPU(16, 16, 8, 1, 1, 1, soft_cfcf_epsilon=-1.0)
+    with pytest.raises(ValueError, match="soft_cfcf_normal_ridge"):
+        NFGSSolverGPU(16, 16, 8, 1, 1, 1, soft_cfcf_normal_ridge=-1e-3)
+    with pytest.raises(ValueError, match="soft_cfcf_mode_batch_size"):
+        NFGSSolverGPU(16, 16, 8, 1, 1, 1, soft_cfcf_mode_batch_size=0)
 
 
 def test_oracle_transforms_are_the_dense_matrices():
