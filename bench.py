@@ -134,8 +134,12 @@ def dist_setup():
         import torch.distributed as dist
         from datetime import timedelta
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        # one replica per GPU over NCCL; gloo where no GPU is visible (the
+        # host-side logic of the replicas, tested on CPU)
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
 
@@ -143,19 +147,23 @@ def dist_setup():
 def barrier_sync(pg, local):
     import torch
 
-    if torch.cuda.is_available():
+    cuda = torch.cuda.is_available()
+    if cuda:
         torch.cuda.synchronize(local)
     if pg is not None:
         pg.barrier()
-        torch.cuda.synchronize(local)
+        if cuda:
+            torch.cuda.synchronize(local)
 
 
 def max_over_ranks(pg, value: float, local: int) -> float:
+    """The slowest replica's time: every rank gets the maximum."""
     if pg is None:
         return value
     import torch
 
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dev = f"cuda:{local}" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
