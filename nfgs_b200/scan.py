@@ -12,6 +12,10 @@ The solvers are set up by a thread pool (the first of each grid shape alone,
 so that the fused stencil's per-shape z-segment tuning runs on a quiet GPU).
 
     python -m nfgs_b200.scan --boundaries 33 --report scan.json
+
+Under torchrun (one process per GPU) the solves are dealt round-robin to the
+ranks, each rank runs its share as one batched scan, and rank 0 reports the
+gathered results (replicas: no data crosses GPUs).
 """
 
 from __future__ import annotations
@@ -19,6 +23,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import os
 import time
 
 import numpy as np
@@ -131,6 +136,36 @@ def run_serial(cases, max_iter: int = 3000, stop=STOP):
     return hists, dict(serial_iterate_s=t_iter)
 
 
+def shard_cases(cases, rank: int, world: int):
+    """Indices of the cases of one replica: round-robin over the list, which
+    mixes the grid sizes of every boundary across the ranks."""
+    return list(range(rank, len(cases), world))
+
+
+def distributed_scan(cases, pg, rank: int, world: int, runner=None, **kw):
+    """Under torchrun: each rank runs its share of the solves as one batched
+    scan on its GPU (the solves are independent; no data crosses ranks), then
+    the per-solve results and timings are gathered to every rank.  Returns
+    (results in case order, timing); timing's scan_s is the slowest rank's."""
+    runner = run_scan if runner is None else runner
+    mine = shard_cases(cases, rank, world)
+    hists, timing = runner([cases[i] for i in mine], **kw)
+    slim = [dict(best_sigma=h["best_sigma"], best_iter=h["best_iter"], iterations=len(h["sigma"]),
+                 stop_reason=h["stop_reason"], sigma=list(h["sigma"])) for h in hists]
+    parts = [None] * world
+    pg.all_gather_object(parts, (mine, slim, timing))
+    results = [None] * len(cases)
+    for idx, res, _t in parts:
+        for i, r in zip(idx, res):
+            results[i] = r
+    cells = sum(t["cell_iterations"] for _, _, t in parts)
+    scan_s = max(t["scan_s"] for _, _, t in parts)
+    timing = dict(setup_s=max(t["setup_s"] for _, _, t in parts), scan_s=scan_s, ranks=world,
+                  cell_iterations=cells, gcell_iter_per_s=cells / scan_s / 1e9,
+                  per_rank=[t for _, _, t in parts])
+    return results, timing
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--boundaries", type=int, default=33)
@@ -140,6 +175,30 @@ def main(argv=None):
     ap.add_argument("--report", default=None)
     args = ap.parse_args(argv)
     cases = td_scan_cases(args.boundaries)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        # replicas: one GPU per rank, each with its share of the solves
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        rank, local = int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        try:
+            results, timing = distributed_scan(cases, dist, rank, world, iters=args.iters, max_iter=args.max_iter)
+        finally:
+            dist.destroy_process_group()
+        if rank == 0:
+            out = dict(solves=len(cases), timing=timing,
+                       results=[dict(boundary=c["boundary"], n=c["n"], nz=c["nz"], rho=c["rho"],
+                                     **{k: r[k] for k in ("best_sigma", "best_iter", "iterations", "stop_reason")})
+                                for c, r in zip(cases, results)])
+            print(json.dumps({k: v for k, v in out.items() if k != "results"}), flush=True)
+            if args.report:
+                with open(args.report, "w") as f:
+                    json.dump(out, f, indent=1)
+        return 0
     hists, timing = run_scan(cases, args.iters, args.max_iter)
     out = dict(solves=len(cases), timing=timing,
                results=[dict(boundary=c["boundary"], n=c["n"], nz=c["nz"], rho=c["rho"],
