@@ -1,0 +1,61 @@
+"""Properties at the benchmark size (256 x 256 x 128 input, calculation grid
+258 x 258 x 129), where the oracle would take minutes per iteration:
+
+* repeatability: two FP32 solves of the same boundary give bit-identical
+  histories (fixed-order reductions, no atomics in the sums);
+* precision: the FP32 production path (tcgen05 transforms, fused stencil)
+  follows the FP64 path (FP64 contractions, same kernels otherwise) on a
+  well-conditioned sunspot boundary to the FP32 bar over 20 iterations;
+* the soft_cfcf start at this size: FP32 and FP64 starts agree, and the
+  iteration from it is finite and improves sigma_J.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+KW = dict(bottom_divergence_robin_weight=0.5, horizontal_zero_mode_policy="frozen_linear_harmonic",
+          d0_zero_mode_policy="project", source_zero_mode_policy="project", vertical_current_operator="staggered_face")
+
+
+def solver(dtype):
+    from nfgs_b200 import NFGSSolverGPU
+    from nfgs_b200.synthetic import sunspot_magnetogram
+
+    bx, by, bz = sunspot_magnetogram(256, seed=77)
+    s = NFGSSolverGPU(256, 256, 128, 1.0, 1.0, 1.0, dtype=dtype, **KW)
+    s.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+    assert (s.Nx, s.Ny, s.Nz) == (258, 258, 129)
+    return s
+
+
+STOP = dict(max_iter=20, tol=1e-30, patience=0, sigma_improvement_tol=None, verbose=False)
+
+
+def test_fp32_repeatable_bitwise():
+    a = solver("float32").iterate(**STOP)
+    b = solver("float32").iterate(**STOP)
+    assert a["sigma"] == b["sigma"] and a["energy"] == b["energy"] and a["divB"] == b["divB"]
+
+
+def test_fp32_follows_fp64():
+    h32 = solver("float32").iterate(**STOP)
+    h64 = solver("float64").iterate(**STOP)
+    assert len(h32["sigma"]) == len(h64["sigma"]) == 20
+    np.testing.assert_allclose(h32["sigma"], h64["sigma"], rtol=2e-3)
+    np.testing.assert_allclose(h32["energy"], h64["energy"], rtol=5e-4)  # measured 1.1e-4
+    assert h32["initial_sigma"] == pytest.approx(h64["initial_sigma"], rel=5e-4)  # measured 6.4e-5
+
+
+def test_soft_cfcf_start_full_size():
+    d = {}
+    for dt in ("float32", "float64"):
+        h = solver(dt).iterate(init_mode="soft_cfcf", **dict(STOP, max_iter=10))
+        d[dt] = h
+        assert np.isfinite(h["sigma"]).all()
+        assert min(h["sigma"]) < h["initial_sigma"]
+    assert d["float32"]["initial_sigma"] == pytest.approx(d["float64"]["initial_sigma"], rel=5e-4)
+    e32, e64 = (d[k]["init_diagnostics"]["soft_cfcf"] for k in ("float32", "float64"))
+    for key in ("curl_current_energy", "current_energy", "objective"):
+        assert e32[key] == pytest.approx(e64[key], rel=5e-4), key
