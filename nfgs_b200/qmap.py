@@ -20,7 +20,8 @@ a symmetric rope, where the seed-grid form divides by Bn0 = 0);
 Differences from the reference helpers, by design:
 * one fixed RK4 step (``step_len``, default 1/8 cell) instead of FastQSL's
   adaptive RKF45; ``tol``, ``block_x`` and ``trace_chunk_seeds`` are accepted
-  and recorded only (the library launches every seed at once);
+  and recorded only (the library launches every seed at once), and
+  ``fastqsl_root`` is accepted and ignored;
 * flags are the face codes of ``nfgs_trace_field_lines`` (1..6 for
   x=0, x=nx-1, y=0, y=ny-1, z=0, z=nz-1; 0 unfinished; -1 zero field);
 * ``include_twist=True`` integrates J.B / (4 pi |B|^2) along both halves of
