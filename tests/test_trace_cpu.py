@@ -125,3 +125,23 @@ def test_twist_of_a_linear_force_free_field():
     assert (flags > 0).all()
     np.testing.assert_allclose(tw, np.sin(al) * length / (4 * np.pi), rtol=1e-12, atol=1e-14)
     np.testing.assert_allclose(T.curl_grid(b)[2][:, :, 1:-1], np.sin(al) * b[2][:, :, 1:-1], rtol=1e-12, atol=1e-15)
+
+
+def test_qmap_host_helpers():
+    """Host-side rules of nfgs_b200.qmap that need no GPU: the physical
+    midplane index (fastqsl_plane.py:49-54) and the input checks made before
+    any library call."""
+    import pytest
+    import torch
+
+    from nfgs_b200 import qmap as Q
+
+    assert Q.physical_midplane_grid_index(256) == 127.5
+    assert Q.physical_midplane_grid_index(1) == 0.0
+    with pytest.raises(ValueError):
+        Q.physical_midplane_grid_index(0)
+    cpu = torch.zeros((3, 4, 4, 4))
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        Q.trace_field_lines(cpu, torch.zeros((1, 3)))
+    with pytest.raises(ValueError, match="CUDA tensor"):
+        Q.trace_qperp(cpu, torch.zeros((1, 3)))
