@@ -1,9 +1,10 @@
 #!/usr/bin/env python3
 """Benchmark of the NFGS reconstruction hot path on B200.
 
-Workload (one GPU): a seeded Titov-Demoulin-type flux rope on a 256x256x128
-grid (calculation grid 258x258x129), rho = 0.5, FP32 storage, gs_cfcf
-start.  One *step* is one NFGSSolverGPU.iterate() call of ITERS NFPT
+Workload (one GPU): the Titov-Demoulin flux rope of the reference's own
+generator model (R=3, a=1, d=1.5, L=2; q and I0 from seed 1) on a
+256x256x128 grid (calculation grid 258x258x129), rho = 0.5, FP32 storage,
+gs_cfcf start.  One *step* is one NFGSSolverGPU.iterate() call of ITERS NFPT
 iterations with the stop rule disabled, on a boundary that is already
 resident on the device.  The metric is Gcell-iter/s on the calculation
 grid (cells x iterations / device seconds, CUDA events on the solver's
@@ -12,10 +13,14 @@ stream, max over ranks).
   python bench.py [--gpus N --steps K --warmup W]            # B200 path
   python bench.py --impl reference [--steps K --warmup W]    # CPU reference arm
 
-The reference arm times the CPU restatement of the reference algorithm
-(the oracle: NumPy/SciPy FP64) on the host cores for the same workload and
-metric, one NFPT iteration per step.  Under torchrun (N > 1) every rank
-solves its own replica (the path does not shard); rank 0 prints the line.
+The reference arm runs the reference's own solver (nfgs_solver.NFGSSolverGPU
+as installed in baseline/_ref by baseline/install_reference.sh) on the host
+cores in FP32, one NFPT iteration (with its sigma_J / divB / energy) per
+step; where that install is absent it times the CPU restatement of the
+algorithm (the oracle, FP64) and says so.  The B200 line also carries the
+reference's PyTorch CUDA path on the same GPU (``reference_torch_cuda``).
+Under torchrun (N > 1) every rank solves its own replica (the path does
+not shard); rank 0 prints the line.
 """
 
 from __future__ import annotations
@@ -36,7 +41,9 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "Gcell-iter/s (NFGS NFPT iterations, calc grid 258x258x129, TD-type flux rope 256x256x128)"
+METRIC = "Gcell-iter/s (NFGS NFPT iterations, calc grid 258x258x129, TD99 flux rope 256x256x128)"
+WORKLOAD = ("td99 flux rope (reference generator model, seed 1) 256x256x128 -> calc 258x258x129, rho=0.5, "
+            "FP32, gs_cfcf start, NFPT iterations with sigma_J / divB / energy every iteration")
 NX, NY, NZ = 256, 256, 128
 EXTENT = 8.0
 RHO = 0.5
@@ -46,7 +53,8 @@ RHO = 0.5
 ALG_BYTES_PER_CELL_ITER = 76.0
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
 # the dominant kernels on this workload, from one ncu capture each
-KERNEL_TRAFFIC = {"stencil": 172.354304e6 + 50.836480e6}
+KERNEL_TRAFFIC = {"stencil": 172.43e6 + 54.71e6}
+REF_DIR = ROOT / "baseline" / "_ref"
 
 
 def load_peaks():
@@ -168,8 +176,68 @@ def max_over_ranks(pg, value: float, local: int) -> float:
     return float(t.item())
 
 
-def cpu_reference_rate(iters: int = 2, threads: int | None = None) -> dict:
-    """Oracle (CPU restatement of the reference) Gcell-iter/s on this workload."""
+def reference_module():
+    """The reference's own solver module as installed in baseline/_ref, or None."""
+    if not (REF_DIR / "nfgs_solver.py").exists():
+        return None
+    if str(REF_DIR) not in sys.path:
+        sys.path.insert(0, str(REF_DIR))
+    import nfgs_solver
+
+    return nfgs_solver
+
+
+def _ref_cpu_solver(mod):
+    import torch
+
+    torch.set_num_threads(os.cpu_count() or 1)
+    bx, by, bz = boundary()
+    dx, dy, dz = spacing()
+    s = mod.NFGSSolverGPU(NX, NY, NZ, dx, dy, dz, device="cpu", dtype=torch.float32, calculation_domain_mode="mudpack",
+                          record_iteration_diagnostics=False, **solver_kwargs())
+    s.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+    return s
+
+
+def _ref_step(s, st):
+    """One NFPT iteration of the reference with the diagnostics its iterate
+    takes every iteration (nfgs_solver.py:3656-3679)."""
+    st = s.iteration_step(*st, mu=1.0)
+    s.compute_sigma(st[0], st[1])
+    s.compute_divB(st[0])
+    s.compute_energy(st[0])
+    return st
+
+
+def cpu_reference_rate(max_iters: int = 10, budget_s: float = 25.0) -> dict:
+    """Reference CPU Gcell-iter/s on this workload: the reference's own FP32
+    code on all host threads (one warm-up iteration, then up to max_iters
+    timed iterations within budget_s, at least 3); the FP64 oracle port when
+    the reference install is absent."""
+    mod = reference_module()
+    if mod is None:
+        return cpu_port_rate(iters=2)
+    import torch
+
+    s = _ref_cpu_solver(mod)
+    with torch.inference_mode():
+        st = s.compute_initial_conditions(init_mode="gs_cfcf")
+        st = _ref_step(s, st)
+        n, t0 = 0, time.perf_counter()
+        while n < max_iters and (n < 3 or time.perf_counter() - t0 < budget_s):
+            st = _ref_step(s, st)
+            n += 1
+        dt = time.perf_counter() - t0
+    cells = s.Nx * s.Ny * s.Nz
+    return {"value": cells * n / dt / 1e9, "unit": "Gcell-iter/s", "cores": torch.get_num_threads(),
+            "kind": "reference",
+            "sample": f"{n} NFPT iterations (iteration_step + sigma_J/divB/energy) of the reference nfgs_solver "
+                      f"(torch CPU, FP32) on the same {s.Nx}x{s.Ny}x{s.Nz} workload after its gs_cfcf start and one "
+                      f"warm-up iteration; {dt:.1f} s on {torch.get_num_threads()} threads"}
+
+
+def cpu_port_rate(iters: int = 2) -> dict:
+    """Oracle (CPU restatement of the reference, FP64) Gcell-iter/s on this workload."""
     from oracle.nfgs_oracle import OracleNFGS
 
     bx, by, bz = boundary()
@@ -189,13 +257,47 @@ def cpu_reference_rate(iters: int = 2, threads: int | None = None) -> dict:
     return {"value": cells * iters / dt / 1e9, "unit": "Gcell-iter/s", "cores": os.cpu_count(), "kind": "port",
             "sample": f"{iters} NFPT iterations (+ sigma/divB/energy) of the FP64 NumPy/SciPy oracle on the "
                       f"same {o.Nx}x{o.Ny}x{o.Nz} workload after its gs_cfcf start; {dt:.1f} s; transforms on "
-                      f"{os.cpu_count()} threads, element-wise work on one"}
+                      f"{os.cpu_count()} threads, element-wise work on one (reference install absent)"}
 
 
 def run_reference(args):
-    world, rank, local, pg = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0, None
+    world, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    mod = reference_module()
+    if mod is None:
+        return run_reference_port(args, world)
+    import torch
+
+    s = _ref_cpu_solver(mod)
+    cells = s.Nx * s.Ny * s.Nz
+    with torch.inference_mode():
+        st = s.compute_initial_conditions(init_mode="gs_cfcf")
+        for _ in range(args.warmup):
+            st = _ref_step(s, st)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            st = _ref_step(s, st)
+        dt = time.perf_counter() - t0
+    value = cells * args.steps / dt / 1e9
+    threads = torch.get_num_threads()
+    line = {
+        "metric": METRIC, "value": value, "unit": "Gcell-iter/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (TD99 flux rope of the reference generator model, seed 1)",
+        "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "calc_grid": [s.Nx, s.Ny, s.Nz], "iters_per_step": 1},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "Gcell-iter/s", "cores": threads, "kind": "reference",
+                         "sample": f"{args.steps} timed NFPT iterations (iteration_step + sigma_J/divB/energy) of the "
+                                   f"reference nfgs_solver, torch CPU FP32 on {threads} threads, after its gs_cfcf "
+                                   f"start and {args.warmup} warm-up iterations"},
+        "e2e": {"value": value, "unit": "Gcell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_port(args, world):
     from oracle.nfgs_oracle import OracleNFGS
 
     bx, by, bz = boundary()
@@ -219,17 +321,62 @@ def run_reference(args):
     line = {
         "metric": METRIC, "value": value, "unit": "Gcell-iter/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded TD-type flux rope)",
-        "config": {"workload": "td_flux_rope 256x256x128 -> calc 258x258x129, rho=0.5, one NFPT iteration per step",
-                   "grid": [NX, NY, NZ], "calc_grid": [o.Nx, o.Ny, o.Nz]},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (TD99 flux rope of the reference generator model, seed 1)",
+        "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "calc_grid": [o.Nx, o.Ny, o.Nz], "iters_per_step": 1},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "Gcell-iter/s", "cores": os.cpu_count(), "kind": "port",
                          "sample": f"{args.steps} timed NFPT iterations of the FP64 NumPy/SciPy restatement of the "
-                                   f"reference algorithm; transforms on {os.cpu_count()} threads"},
+                                   f"reference algorithm (reference install absent); transforms on {os.cpu_count()} "
+                                   f"threads"},
         "e2e": {"value": value, "unit": "Gcell-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def reference_torch_cuda(dev: str, iters: int, mine: dict) -> dict | None:
+    """The reference's PyTorch CUDA path on the same GPU, same boundary and
+    FP32 production kwargs (examples/reconstruct_npz.py:31-40 plus the
+    projection policies): Gcell-iter/s of iterate() with the stop rule off
+    (init included, as in this bench's own steps), and its time to the
+    production sigma_J stop, beside this build's figures."""
+    mod = reference_module()
+    if mod is None:
+        return {"unavailable": "reference install (baseline/_ref) absent"}
+    import torch
+
+    bx, by, bz = boundary()
+    dx, dy, dz = spacing()
+    s = mod.NFGSSolverGPU(NX, NY, NZ, dx, dy, dz, device=dev, dtype=torch.float32, calculation_domain_mode="mudpack",
+                          record_iteration_diagnostics=False, **solver_kwargs())
+    s.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0, ijzbcor=3)
+    cells = s.Nx * s.Ny * s.Nz
+    off = dict(tol=1e-30, mu=1.0, patience=0, sigma_improvement_tol=None, verbose=False, init_mode="gs_cfcf")
+    with torch.inference_mode():
+        s.iterate(max_iter=2, **off)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        s.iterate(max_iter=iters, **off)
+        torch.cuda.synchronize(dev)
+        dt = time.perf_counter() - t0
+        t1 = time.perf_counter()
+        h = s.iterate(max_iter=3000, tol=1e-5, mu=1.0, patience=40, sigma_improvement_tol=1e-5, verbose=False,
+                      init_mode="gs_cfcf", stop_mode="sigma_best")
+        torch.cuda.synchronize(dev)
+        dstop = time.perf_counter() - t1
+    rate = cells * iters / dt / 1e9
+    out = {"value": rate, "unit": "Gcell-iter/s", "iters": iters, "seconds": dt,
+           "plain_over_reference": mine["value"] / rate,
+           "time_to_sigma_stop": {"seconds": dstop, "iterations": len(h["sigma"]), "best_iter": h["best_iter"],
+                                  "best_sigma": h["best_sigma"], "stop_reason": h["stop_reason"]},
+           "note": "reference nfgs_solver.NFGSSolverGPU on the same B200, torch CUDA FP32, wall time with "
+                   "torch.cuda.synchronize brackets; iterate() of the stop-rule-off workload includes its gs_cfcf "
+                   "start like this bench's steps"}
+    if mine.get("stop"):
+        out["time_to_sigma_stop"]["plain_over_reference"] = dstop / mine["stop"]["seconds"]
+    del s
+    torch.cuda.empty_cache()
+    return out
 
 
 def learned_vs_plain(seeds=(1_000_000, 1_000_001, 1_000_002), eps=1e-3):
@@ -339,17 +486,20 @@ def run_b200(args):
     lvp = None
     if world == 1 and args.learned:
         lvp = learned_vs_plain()
+    ref_cuda = None
+    if rank == 0 and world == 1 and args.ref_cuda:
+        ref_cuda = reference_torch_cuda(dev, args.ref_cuda_iters, {"value": value, "stop": t_stop})
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_reference_rate(iters=args.cpu_iters)
+        cpu = cpu_reference_rate(max_iters=args.cpu_iters)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Gcell-iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded TD-type flux rope, seed 1)",
-            "config": {"workload": f"td_flux_rope 256x256x128 -> calc {s.Nx}x{s.Ny}x{s.Nz}, rho=0.5, fp32 storage, "
-                                   f"gs_cfcf + {args.iters} NFPT iterations per step, stop rule off",
-                       "grid": [NX, NY, NZ], "calc_grid": [s.Nx, s.Ny, s.Nz], "iters_per_step": args.iters,
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (TD99 flux rope of the reference generator model, seed 1)",
+            "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "calc_grid": [s.Nx, s.Ny, s.Nz],
+                       "iters_per_step": args.iters, "stop_rule": "off (one iterate() call of iters_per_step)",
                        "parallelism": f"replicas x{world}",
                        "l2": "working set > L2: each iteration streams phi, A_z and the 103 MB background"},
             "e2e": {"value": e2e_value, "unit": "Gcell-iter/s", "h2d_bytes_per_step": 3 * NX * NY * 8,
@@ -360,6 +510,7 @@ def run_b200(args):
             "clocks": ck,
             "time_to_sigma_stop": t_stop,
             "learned_vs_plain": lvp,
+            "reference_torch_cuda": ref_cuda,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -398,7 +549,10 @@ def main():
     ap.add_argument("--iters", type=int, default=100)
     ap.add_argument("--check-every", type=int, default=50)
     ap.add_argument("--phase-iters", type=int, default=10)
-    ap.add_argument("--cpu-iters", type=int, default=2)
+    ap.add_argument("--cpu-iters", type=int, default=10)
+    ap.add_argument("--ref-cuda-iters", type=int, default=20)
+    ap.add_argument("--no-ref-cuda", dest="ref_cuda", action="store_false",
+                    help="skip the reference PyTorch CUDA leg")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-stop-run", dest="stop_run", action="store_false")
     ap.add_argument("--no-learned", dest="learned", action="store_false",

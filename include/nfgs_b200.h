@@ -229,9 +229,13 @@ int nfgs_gaussian_above(void* handle, double* out);
  * default stream) without synchronising; scratch comes from one static
  * 16 MiB device array that this library reserves on every GPU it loads on,
  * so the calculation plane may hold at most 419,430 cells (NFGS_EINVAL
- * beyond that).  The first call on a device looks the array up, and should
- * come before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race. */
+ * beyond that).  Every call looks the array's device address up on the
+ * handle's device (so a device reset leaves no stale address behind); the
+ * first call on a device also loads the module, and should come before any
+ * stream capture.  The call is ordered after the work already queued on the
+ * handle's own stream, and a later nfgs_set_boundary or nfgs_destroy of the
+ * handle waits for it to finish.  The caller's current device is restored on
+ * return.  All calls share the array: calls that overlap on the GPU race. */
 int nfgs_gaussian_above_noalloc(void* handle, double* out_dev, void* stream);
 
 /* Fixed 2-D products of the boundary set-up (FP64, calc grid, (ny, nx)):

@@ -63,6 +63,10 @@ struct Handle {
     size_t esz = 4;
     cudaStream_t s = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // ordering of nfgs_gaussian_above_noalloc (caller's stream) against the
+    // handle's stream: ev_na_in marks the handle's work it must follow,
+    // ev_na_out the end of its last call (set_boundary and destroy wait on it)
+    cudaEvent_t ev_na_in = nullptr, ev_na_out = nullptr;
     std::vector<Buf> owned;
     int launches = 0;
 
@@ -229,6 +233,8 @@ static void free_all(Handle* h) {
         if (h->pin_ev[q]) cudaEventDestroy(h->pin_ev[q]);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->ev_na_in) cudaEventDestroy(h->ev_na_in);
+    if (h->ev_na_out) cudaEventDestroy(h->ev_na_out);
     if (h->s) cudaStreamDestroy(h->s);
 }
 
@@ -2501,6 +2507,8 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
     CKC(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
     CKC(cudaEventCreate(&h->ev0));
     CKC(cudaEventCreate(&h->ev1));
+    CKC(cudaEventCreateWithFlags(&h->ev_na_in, cudaEventDisableTiming));
+    CKC(cudaEventCreateWithFlags(&h->ev_na_out, cudaEventDisableTiming));
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const long long P = g.P, V = g.V, PI = h->PI;
     // transforms
@@ -2656,23 +2664,16 @@ namespace {
 constexpr long long kNoAllocScratchDoubles = 1LL << 21;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
 
-constexpr int kMaxDevices = 128;
-static std::mutex g_noalloc_mu;
-static double* g_noalloc_ptr[kMaxDevices] = {};
-
-// Device address of the scratch array for `dev`, looked up once per device
-// with that device current (the array's name is only a host-side stand-in).
-static int noalloc_scratch(int dev, double** out) {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (dev < 0 || dev >= kMaxDevices) return fail(NFGS_EINVAL, "device ordinal out of range");
-    if (g_noalloc_ptr[dev] == nullptr) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || p == nullptr)
-            return fail(NFGS_ECUDA, std::string("cudaGetSymbolAddress(scratch) failed: ") + cudaGetErrorString(e));
-        g_noalloc_ptr[dev] = (double*)p;
-    }
-    *out = g_noalloc_ptr[dev];
+// Device address of the scratch array on the current device.  The array's
+// name is only a host-side stand-in; the address is looked up on every call
+// (cheap once the module is loaded), so a device or primary-context reset
+// between calls leaves no stale pointer behind.
+static int noalloc_scratch(double** out) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+        return fail(NFGS_ECUDA, std::string("cudaGetSymbolAddress(scratch) failed: ") + cudaGetErrorString(e));
+    *out = (double*)p;
     return NFGS_OK;
 }
 
@@ -2713,7 +2714,11 @@ static int gaussian_above_noalloc_impl(Handle* h, double* out, cudaStream_t st) 
     }
     if (!h->boundary_set) return fail(NFGS_ESTATE, "NFGS Gaussian separation is not configured");
     double* w = nullptr;
-    TRY(noalloc_scratch(h->geom.device, &w));
+    TRY(noalloc_scratch(&w));
+    // follow the handle's own queued work (boundary set-up writes the planes
+    // read here)
+    CK(cudaEventRecord(h->ev_na_in, h->s));
+    CK(cudaStreamWaitEvent(st, h->ev_na_in, 0));
     double *t1 = w, *t2 = w + P, *gx = w + 2 * P, *gy = w + 3 * P, *dph = w + 4 * P;
     double *kN = h->kN, *pah = h->phi_above_hat, *alx = h->alx, *aly = h->aly, *bza = h->bz_above;
     const double dx = g.dx, dy = g.dy;
@@ -2742,6 +2747,8 @@ static int gaussian_above_noalloc_impl(Handle* h, double* out, cudaStream_t st) 
         out[P + q] = -gy[q];
         out[2 * P + q] = bza[q];
     }));
+    // a later nfgs_set_boundary / nfgs_destroy waits for this call to finish
+    CK(cudaEventRecord(h->ev_na_out, st));
     return NFGS_OK;
 }
 
@@ -2861,6 +2868,10 @@ int nfgs_create(const NfgsGeom* geom, const NfgsParams* params, void** handle_ou
 int nfgs_destroy(void* handle) {
     if (!handle) return NFGS_OK;
     Handle* h = (Handle*)handle;
+    cudaSetDevice(h->geom.device);
+    // a pending nfgs_gaussian_above_noalloc on another stream reads this
+    // handle's buffers
+    if (h->s && h->ev_na_out) cudaStreamWaitEvent(h->s, h->ev_na_out, 0);
     if (h->s) cudaStreamSynchronize(h->s);
     free_all(h);
     delete h;
@@ -2880,6 +2891,9 @@ int nfgs_set_boundary(void* handle, const double* bx, const double* by, const do
         opts->src_x0 + opts->copy_nx > opts->nx_obs)
         return fail(NFGS_EINVAL, "inconsistent boundary placement");
     if (opts->nzo < 1 || opts->nzo > h->g.nz) return fail(NFGS_EINVAL, "observed height out of range");
+    // the boundary planes are rewritten on h->s: a pending
+    // nfgs_gaussian_above_noalloc on another stream must finish reading first
+    if (h->ev_na_out) CK(cudaStreamWaitEvent(h->s, h->ev_na_out, 0));
     h->fov_y0 = opts->fov_y0;
     h->fov_x0 = opts->fov_x0;
     h->nyo = opts->copy_ny;
@@ -3241,8 +3255,14 @@ int nfgs_gaussian_above_noalloc(void* handle, double* out_dev, void* stream) {
     g_err.clear();
     Handle* h = (Handle*)handle;
     if (!h || !out_dev) return fail(NFGS_EINVAL, "null argument");
-    if (cudaSetDevice(h->geom.device) != cudaSuccess) return fail(NFGS_ECUDA, "cudaSetDevice failed");
-    return gaussian_above_noalloc_impl(h, out_dev, (cudaStream_t)stream);
+    // the caller's current device is restored on return
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) return fail(NFGS_ECUDA, "cudaGetDevice failed");
+    if (prev != h->geom.device && cudaSetDevice(h->geom.device) != cudaSuccess)
+        return fail(NFGS_ECUDA, "cudaSetDevice failed");
+    const int rc = gaussian_above_noalloc_impl(h, out_dev, (cudaStream_t)stream);
+    if (prev != h->geom.device) cudaSetDevice(prev);
+    return rc;
 }
 
 int nfgs_get_plane(void* handle, int32_t which, double* out) {

@@ -1,15 +1,16 @@
 """Seeded synthetic boundaries for benchmarks and tests.
 
-* ``td_bottom``: a Titov-Demoulin-type flux rope (Titov & Demoulin 1999,
-  A&A 351, 707): a ring current of major radius R and minor radius a whose
-  centre lies at depth d, two magnetic charges +-q at (+-L, 0, -d) on the
-  ring's symmetry axis, and a line current I0 along that axis giving the
-  toroidal field.  The ring's vector potential is the standard circular
-  loop potential with complete elliptic integrals outside the tube and its
-  first-order continuation in k inside the tube; B = curl A is taken with
-  centred differences.  The ring current I takes the equilibrium value of
-  the published model.  Only the z = 0 plane is returned; ``td_volume``
-  returns the 3-D field for metric checks.
+* ``td_bottom`` / ``td_volume``: the Titov-Demoulin flux rope (Titov &
+  Demoulin 1999, A&A 351, 707) as the reference generates it
+  (``generate_td_model``, nfgs/_backend/td.py:370-581): two magnetic
+  charges +-q at (+-L, 0, -d); a ring current of major radius R and minor
+  radius a centred at depth d whose vector potential is the circular-loop
+  potential with complete elliptic integrals outside the tube and its
+  first-order continuation in k inside, differentiated exactly (chain rule
+  in k); a line current I0 along the ring's symmetry axis whose toroidal
+  field is the model's sqrt(1/R^2 + 2 chi (1 - rho^2/a^2) I^2/(a^2 I0^2)) +
+  1/r - 1/R profile; the ring current I at the model's equilibrium value.
+  Only the z = 0 plane is returned by ``td_bottom``.
 * ``sunspot_magnetogram``: 2-6 Gaussian spots with random twist, net flux
   balanced to zero.
 * ``quadrupole_magnetogram``: four Gaussian poles with random shear.
@@ -20,90 +21,108 @@ All units are the model's own; grids are (ny, nx) maps in zyx order.
 from __future__ import annotations
 
 import numpy as np
-from scipy import special
 
 __all__ = ["td_params", "td_bottom", "td_volume", "sunspot_magnetogram", "quadrupole_magnetogram",
            "bipolar_boundary"]
 
 
-def td_params(seed: int, R=3.0, a=1.0, d=1.5, L=2.0, q=None, twist=None) -> dict:
-    """Seeded TD parameters: q in [0.5, 2], I0 = -sign * I_eq * U(0.8, 1.2)."""
+MU0_TD = 4.0 * np.pi * 1e-1  # the reference generator's permeability (td.py:385)
+
+
+def td_params(seed: int, R=3.0, a=1.0, d=1.5, L=2.0, q=None, twist=None, l_i=0.5) -> dict:
+    """Seeded TD parameters: q ~ U(0.5, 2); I0 = -f I_eq with f ~ U(0.8, 1.2).
+
+    I_eq is the equilibrium ring current of the model (td.py:401-403); the
+    minus sign is the reference generator's internal I0 convention, opposite
+    to the published table (nfgs/_backend/scripts/run_analytic_validation.py:670)."""
     rng = np.random.default_rng(seed)
     q = float(rng.uniform(0.5, 2.0)) if q is None else float(q)
-    l_i = 0.5
-    I_eq = 8.0 * np.pi * q * L * R * (R * R + L * L) ** -1.5 / (np.log(8.0 * R / a) - 1.5 + l_i / 2.0)
+    I_eq = td_ring_current(q, R, a, L, l_i)
     f = float(rng.uniform(0.8, 1.2)) if twist is None else float(twist)
-    return {"R": R, "a": a, "d": d, "L": L, "q": q, "I": I_eq, "I0": -f * I_eq}
+    return {"R": R, "a": a, "d": d, "L": L, "q": q, "I": I_eq, "I0": -f * I_eq, "l_i": l_i}
 
 
-def _ring_potential(x, y, z, R, a, d, I):
-    """theta-component of the ring-current vector potential (mu = 1)."""
-    rp = np.sqrt(y * y + (z + d) ** 2)
-    rp = np.maximum(rp, 1e-12)
-    rho = np.sqrt(x * x + (rp - R) ** 2)
-
-    def A_of_k(k):
-        m = np.clip(k * k, 0.0, 1.0 - 1e-15)
-        K = special.ellipk(m)
-        E = special.ellipe(m)
-        return ((2.0 - m) * K - 2.0 * E) / np.maximum(k, 1e-15)
-
-    k = 2.0 * np.sqrt(rp * R / ((rp + R) ** 2 + x * x))
-    outside = (I / (2.0 * np.pi)) * np.sqrt(R / rp) * A_of_k(k)
-    # inside the tube: first-order continuation from the tube surface
-    ka = 2.0 * np.sqrt(rp * R / (4.0 * rp * R + a * a))
-    h = 1e-6
-    dA = (A_of_k(ka + h) - A_of_k(ka - h)) / (2.0 * h)
-    inside = (I / (2.0 * np.pi)) * np.sqrt(R / rp) * (A_of_k(ka) + dA * (k - ka))
-    return np.where(rho < a, inside, outside), rp
+def td_ring_current(q, R, a, L, l_i=0.5, mu0=MU0_TD):
+    """Equilibrium ring current of the TD model (td.py:401-403)."""
+    return (8.0 * np.pi * q * L * R * (R * R + L * L) ** -1.5 / mu0) / (np.log(8.0 * R / a) - 1.5 + l_i / 2.0)
 
 
-def _td_B(x, y, z, p, h=1e-4):
-    R, a, d, L, q, I, I0 = p["R"], p["a"], p["d"], p["L"], p["q"], p["I"], p["I0"]
-    # charges
-    B = np.zeros((3,) + x.shape)
+def _loop_kernel(k, K, E, eps):
+    """A(k) = ((2 - k^2) K - 2 E) / k of the circular-loop potential and its
+    first k-derivative, with the reference's guards near k = 0 and k = 1."""
+    k2 = k * k
+    omk2 = np.maximum(1.0 - k2, eps)
+    A = ((2.0 - k2) * K - 2.0 * E) / np.where(k == 0.0, 1e-30, k)
+    dA = ((2.0 - k2) * E - 2.0 * omk2 * K) / (np.maximum(k2, eps) * omk2)
+    dA = np.where(k2 < max(eps, 1e-30), 0.0, dA)
+    return A, dA, omk2
+
+
+def td99_field(x, y, z, *, R, a, d, L, q, I0, l_i=0.5, mu0=MU0_TD, p_bt=1.0, k_eps=1e-12):
+    """(Bx, By, Bz) of the TD model at points x, y, z (any equal shapes)."""
+    from scipy import special as sp
+
+    x, y, z = (np.asarray(v, dtype=np.float64) for v in (x, y, z))
+    I = td_ring_current(q, R, a, L, l_i, mu0)
+    zd = z + d
+    r = np.sqrt(y * y + zd * zd)
+    rho = np.sqrt(x * x + (r - R) ** 2)
+    inside = (a - rho > 0).astype(np.float64)
+    rs = np.where(r == 0.0, 1e-30, r)
+    # magnetic charges
+    bx = np.zeros_like(x)
+    by = np.zeros_like(x)
+    bz = np.zeros_like(x)
     for sgn, xc in ((1.0, L), (-1.0, -L)):
-        rx, ry, rz = x - xc, y, z + d
-        r3 = np.maximum((rx * rx + ry * ry + rz * rz) ** 1.5, 1e-12)
-        B[0] += sgn * q * rx / r3
-        B[1] += sgn * q * ry / r3
-        B[2] += sgn * q * rz / r3
-
-    # ring current: A = A_theta theta_hat, theta_hat = (0, -(z+d)/rp, y/rp)
-    def A_vec(xx, yy, zz):
-        At, rp = _ring_potential(xx, yy, zz, R, a, d, I)
-        return np.zeros_like(At), -At * (zz + d) / rp, At * yy / rp
-
-    def dA(axis):
-        e = [0.0, 0.0, 0.0]
-        e[axis] = h
-        ap = A_vec(x + e[0], y + e[1], z + e[2])
-        am = A_vec(x - e[0], y - e[1], z - e[2])
-        return [(ap[c] - am[c]) / (2 * h) for c in range(3)]
-
-    dx_, dy_, dz_ = dA(0), dA(1), dA(2)
-    B[0] += dy_[2] - dz_[1]
-    B[1] += dz_[0] - dx_[2]
-    B[2] += dx_[1] - dy_[0]
-    # line current along the symmetry axis: B = I0 / (2 pi rp) theta_hat,
-    # confined by a smooth cut-off to the flux-rope neighbourhood
-    rp = np.maximum(np.sqrt(y * y + (z + d) ** 2), 1e-12)
-    rho = np.sqrt(x * x + (rp - R) ** 2)
-    inside = np.exp(-(rho / a) ** 4)
-    bt = I0 / (2.0 * np.pi * rp) * (R / a) * inside
-    B[1] += -bt * (z + d) / rp
-    B[2] += bt * y / rp
-    return B
+        rx = x - xc
+        r3 = (rx * rx + y * y + zd * zd) ** 1.5
+        bx += sgn * q * rx / r3
+        by += sgn * q * y / r3
+        bz += sgn * q * zd / r3
+    # toroidal field of the axial line current, along theta = (0, -(z+d), y)/r
+    prof = np.maximum(0.0, 1.0 - rho * rho / (a * a)) * float(p_bt)
+    root = np.sqrt(np.maximum(1.0 / (R * R) + 2.0 * inside / (a * a) * (I * I / (I0 * I0)) * prof, 0.0))
+    bt = (mu0 * I0 / (2.0 * np.pi)) * (root + 1.0 / r - 1.0 / R)
+    by += -bt * zd / r
+    bz += bt * y / r
+    # poloidal field of the ring current from its exact potential derivatives
+    s2 = (r + R) ** 2 + x * x
+    k = 2.0 * np.sqrt(r * R) / np.sqrt(s2)
+    ka = 2.0 * np.sqrt(r * R) / np.sqrt(4.0 * r * R + a * a)
+    if k_eps > 0.0:
+        k = np.clip(k, 0.0, 1.0 - k_eps)
+        ka = np.clip(ka, 0.0, 1.0 - k_eps)
+    dk_dx = -x * k / s2
+    dk_dr = k * (R * R + x * x - r * r) / (2.0 * rs * s2)
+    dka_dr = ka * a * a / (2.0 * rs * (a * a + 4.0 * R * r))
+    A_k, dA_k, _ = _loop_kernel(k, sp.ellipk(k * k), sp.ellipe(k * k), k_eps)
+    Ka, Ea = sp.ellipk(ka * ka), sp.ellipe(ka * ka)
+    A_a, dA_a, omka2 = _loop_kernel(ka, Ka, Ea, k_eps)
+    ka2 = ka * ka
+    kas = np.where(ka == 0.0, 1e-30, ka)
+    d2A_a = ((7.0 * ka2 - 4.0 - ka2 * ka2) * (Ea / omka2) + (4.0 - 5.0 * ka2) * Ka) / (kas ** 3 * omka2)
+    d2A_a = np.where(ka2 < max(k_eps, 1e-30), 0.0, d2A_a)
+    pre = (mu0 * I / (2.0 * np.pi)) * np.sqrt(R / rs)
+    A_out = pre * A_k
+    A_in = pre * (A_a + dA_a * (k - ka))
+    dAdx = np.where(inside > 0, pre * dA_a * dk_dx, pre * dA_k * dk_dx)
+    dAdr = np.where(inside > 0, pre * (dA_a * dk_dr + d2A_a * dka_dr * (k - ka)) - A_in * 0.5 / rs,
+                    pre * dA_k * dk_dr - A_out * 0.5 / rs)
+    A_I = np.where(inside > 0, A_in, A_out)
+    bperp = -dAdx
+    bx += dAdr + A_I / rs
+    by += bperp * (y / rs)
+    bz += bperp * (zd / rs)
+    return bx, by, bz
 
 
 def td_bottom(nx: int, ny: int, seed: int = 0, extent: float = 8.0, **kw):
-    """Bottom maps (Bx, By, Bz), each (ny, nx), of a TD-type rope on [-extent, extent]^2."""
+    """Bottom maps (Bx, By, Bz), each (ny, nx), of the TD rope on [-extent, extent]^2."""
     p = td_params(seed, **kw)
     xs = np.linspace(-extent, extent, nx)
     ys = np.linspace(-extent, extent, ny)
     y, x = np.meshgrid(ys, xs, indexing="ij")
-    B = _td_B(x, y, np.zeros_like(x), p)
-    return B[0], B[1], B[2]
+    return td99_field(x, y, np.zeros_like(x), **{k: p[k] for k in ("R", "a", "d", "L", "q", "I0", "l_i")})
 
 
 def td_volume(nx: int, ny: int, nz: int, seed: int = 0, extent: float = 8.0, **kw):
@@ -113,7 +132,7 @@ def td_volume(nx: int, ny: int, nz: int, seed: int = 0, extent: float = 8.0, **k
     ys = np.linspace(-extent, extent, ny)
     zs = np.linspace(0.0, extent, nz)
     z, y, x = np.meshgrid(zs, ys, xs, indexing="ij")
-    return _td_B(x, y, z, p)
+    return np.stack(td99_field(x, y, z, **{k: p[k] for k in ("R", "a", "d", "L", "q", "I0", "l_i")}))
 
 
 def sunspot_magnetogram(n: int, seed: int, ny: int | None = None):

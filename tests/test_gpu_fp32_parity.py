@@ -1,0 +1,212 @@
+"""The production dtype (FP32) against FP64 at the configurations of record.
+
+Fixtures (tests/golden/fp32/, written by tests/golden/make_fp32_golden.py
+from the reference solver itself, FP64 and FP32 on the CPU):
+
+* ``lowlou64_rho05`` -- config 1: Low-Lou n=1, m=1, l=0.3, Phi=pi/4 on a
+  64^3 lattice, dx=dy=dz=1, rho=0.5, gs_cfcf, max_iter 500, production stop
+  rule; compared to the analytic interior as well;
+* ``td99_96_rho05`` -- config 2 reduced to a size the CPU reference
+  finishes: the reference TD generator with R=3, a=1, d=1.5, L=2 (q and I0
+  of seed 1) on [-8, 8]^2 at 96x96x48, rho=0.5, max_iter 3000.
+
+What is asserted, through the C ABI on the GPU:
+
+1. the FP64 build equals the reference's FP64 run (stop reason, best and
+   final iteration, sigma / energy / divB histories, final fields, div-B
+   fraction, and for config 1 the metrics against the analytic field);
+2. FP32 against FP64 (this build's FP64 run, pinned by 1): the gs_cfcf start
+   Phi_c and A_z within 1e-5 relative L2, the stated FP32 bar, or twice the
+   reference's own FP32-vs-FP64 deviation where that is larger; the start's
+   and first step's B and J within twice the reference's own deviation (or
+   1e-5); the final cropped fields after the sigma stop within three times
+   the reference's own deviation;
+3. the solution metrics of the FP32 result against the FP64 result --
+   C_vec, C_CS, E'_n, E'_m, epsilon (energy ratio), sigma_J (ROI) and the
+   div-B fraction -- within three times the reference's own FP32 figures
+   (each tolerance is written beside its assertion with the reference's
+   number);
+4. config 1: the FP32 result's metrics against the analytic interior
+   within 2e-3 (C_vec, C_CS) / 5e-3 (E'_n, E'_m, epsilon, sigma_J) of the
+   reference FP32 result's.
+
+The TD rope is ill-conditioned in FP32 for any implementation: the
+reference's own FP32 start is 2.1e-5 from FP64 in Phi_c, its first step
+1.3e-3 in B, its final field 8.2e-3 in B (best iteration 20 vs 19).
+"""
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLD = Path(__file__).resolve().parent / "golden" / "fp32"
+CASES = ["lowlou64_rho05", "td99_96_rho05"]
+B_KEYS, J_KEYS = ("Bx", "By", "Bz"), ("Jx", "Jy", "Jz")
+
+
+def load(name):
+    return json.loads((GOLD / f"{name}.json").read_text()), dict(np.load(GOLD / f"{name}.npz"))
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+_CACHE = {}
+
+
+def solve(name, dtype):
+    """Start state, first step and the full solve of one case, cached per module."""
+    key = (name, dtype)
+    if key in _CACHE:
+        return _CACHE[key]
+    from nfgs_b200 import NFGSSolverGPU
+
+    meta, data = load(name)
+    nx, ny, nz = meta["shape"]
+    dx, dy, dz = meta["spacing"]
+
+    def make():
+        s = NFGSSolverGPU(nx, ny, nz, dx, dy, dz, device="cuda", dtype=dtype, **meta["ctor"])
+        s.set_bottom_vector_boundary(data["bx_in"], data["by_in"], data["bz_in"], zero_net_current=False,
+                                     smooth_passes=0, ijzbcor=3)
+        return s
+
+    s = make()
+    B0, J0, phi0, az0, _ = s.compute_initial_conditions(init_mode="gs_cfcf")
+    s._step(1.0)
+    B1, J1 = s._state_fields(1)
+    s = make()
+    st = meta["stop"]
+    h = s.iterate(max_iter=meta["max_iter"], tol=st["tol"], mu=st["mu"], patience=st["patience"],
+                  sigma_improvement_tol=st["sigma_improvement_tol"], stop_mode=st["stop_mode"], verbose=False)
+    f = {k: v.astype(np.float64) for k, v in s.fields_to_numpy().items()}
+    out = dict(B0=B0.astype(np.float64), J0=J0.astype(np.float64), phi0=phi0.astype(np.float64),
+               az0=az0.astype(np.float64), B1=B1.astype(np.float64), J1=J1.astype(np.float64), h=h, f=f,
+               spacing=(dx, dy, dz))
+    _CACHE[key] = out
+    return out
+
+
+def metrics(ref, sol, cur, spacing):
+    from oracle.metrics_oracle import field_metrics
+
+    b = np.stack([sol[k] for k in B_KEYS])
+    r = None if ref is None else np.stack([ref[k] for k in B_KEYS])
+    j = None if cur is None else np.stack([cur[k] for k in J_KEYS])
+    nz, ny, nx = b.shape[1:]
+    return field_metrics(r, b, j, spacing, (0, nz, 0, ny, 0, nx))
+
+
+def divb_fraction(f, spacing):
+    """The reference's compute_divB (nfgs_solver.py:2689-2693) of cropped fields."""
+    from oracle.metrics_oracle import divergence
+
+    b = np.stack([f[k] for k in B_KEYS])
+    div = divergence(b, spacing)
+    bm = np.sqrt(np.sum(b * b, axis=0))
+    return float(np.abs(div).mean() / (6.0 * bm.mean() / min(spacing) + 1e-12))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_equals_reference_run(name):
+    meta, data = load(name)
+    r = solve(name, "float64")
+    h, ref = r["h"], meta["fp64"]
+    assert h["stop_reason"] == ref["stop_reason"]
+    assert h["best_iter"] == ref["best_iter"]
+    assert h["final_iter"] == ref["final_iter"]
+    np.testing.assert_allclose(h["sigma"], data["hist_sigma_fp64"], rtol=1e-7)
+    np.testing.assert_allclose(h["energy"], data["hist_energy_fp64"], rtol=1e-8)
+    np.testing.assert_allclose(h["divB"], data["hist_divB_fp64"], rtol=1e-6)
+    np.testing.assert_allclose([h["initial_sigma"], h["initial_divB"], h["initial_energy"]], ref["init_scalars"],
+                               rtol=1e-8)
+    assert abs(h["best_sigma"] - ref["best_sigma"]) <= 1e-8 * ref["best_sigma"]
+    for k in B_KEYS + J_KEYS:
+        assert rel(r["f"][k][::4, ::4, ::4], data["final64_" + k + "_s4"]) < 1e-6, k
+        assert abs(np.linalg.norm(r["f"][k]) / data["final64_" + k + "_norm"][0] - 1) < 1e-8, k
+    assert divb_fraction(r["f"], r["spacing"]) == pytest.approx(ref["divB_fraction_final"], rel=1e-7)
+    if "fp64_vs_analytic" in meta:
+        an = analytic(meta, data, r["f"]["Bx"].shape[0])
+        m = metrics(an, r["f"], r["f"], r["spacing"])
+        for k in ("C_vec", "C_CS", "Eprime_n", "Eprime_m", "epsilon", "sigma_J"):
+            assert m[k] == pytest.approx(meta["fp64_vs_analytic"][k], rel=1e-7, abs=1e-10), k
+
+
+def analytic(meta, data, nzo):
+    from oracle.lowlou_oracle import lowlou_field, zyx_components
+
+    an = meta["analytic"]
+    f = lowlou_field(data["lowlou_breaks"], data["lowlou_coeffs"], float(data["lowlou_a2"][0]), n=an["n"],
+                     l=an["l"], psi=an["psi"], resolution=tuple(an["resolution"]), bounds=tuple(an["bounds"]))
+    return {k: v[:nzo] for k, v in zip(B_KEYS, zyx_components(f))}
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp32_start_and_first_step(name):
+    meta, _ = load(name)
+    dev = meta["fp32_vs_fp64_deviation"]
+    a, b = solve(name, "float32"), solve(name, "float64")
+    bar = 1e-5
+    # start state scalars: 1e-5 (lowlou: reference 9.9e-7 / 6.6e-7; TD: 2.1e-5 / 1.4e-6)
+    assert rel(a["phi0"], b["phi0"]) <= max(bar, 2 * dev["init_phi"])
+    assert rel(a["az0"], b["az0"]) <= max(bar, 2 * dev["init_az"])
+    # start fields (lowlou: reference B 2.8e-5, J 1.2e-4; TD: 1.1e-4, 7.5e-4)
+    assert rel(a["B0"], b["B0"]) <= max(bar, 2 * dev["init_B"])
+    assert rel(a["J0"], b["J0"]) <= max(bar, 2 * dev["init_J"])
+    # first NFPT step (lowlou: reference B 8.2e-5, J 2.6e-4; TD: 1.3e-3, 2.3e-3)
+    assert rel(a["B1"], b["B1"]) <= max(bar, 2 * dev["step1_B"])
+    assert rel(a["J1"], b["J1"]) <= max(bar, 2 * dev["step1_J"])
+    # start sigma_J and energy
+    assert a["h"]["initial_sigma"] == pytest.approx(b["h"]["initial_sigma"], rel=1e-4)
+    assert a["h"]["initial_energy"] == pytest.approx(b["h"]["initial_energy"], rel=1e-5)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp32_final_fields_and_metrics(name):
+    meta, _ = load(name)
+    dev, mref = meta["fp32_vs_fp64_deviation"], meta["fp32_vs_fp64_metrics"]
+    a, b = solve(name, "float32"), solve(name, "float64")
+    fa, fb = a["f"], b["f"]
+    # final cropped fields after the sigma stop (lowlou: reference B 1.4e-4, J 3.0e-4; TD: 8.2e-3, 1.8e-2)
+    assert rel(np.stack([fa[k] for k in B_KEYS]), np.stack([fb[k] for k in B_KEYS])) <= 3 * dev["final_B"]
+    assert rel(np.stack([fa[k] for k in J_KEYS]), np.stack([fb[k] for k in J_KEYS])) <= 3 * dev["final_J"]
+    m = metrics(fb, fa, fa, a["spacing"])
+    ms = metrics(fb, fb, fb, a["spacing"])
+    # C_vec: reference 1 - 9.0e-9 (lowlou), 1 - 3.2e-5 (TD)
+    assert 1 - m["C_vec"] <= max(3 * (1 - mref["C_vec"]), 1e-7)
+    # C_CS: reference 1 - 2.3e-7 / 1 - 1.0e-4
+    assert 1 - m["C_CS"] <= max(3 * (1 - mref["C_CS"]), 1e-6)
+    # E'_n: reference 1 - 2.8e-4 / 1 - 8.0e-3;  E'_m: 1 - 6.3e-4 / 1 - 1.1e-2
+    assert 1 - m["Eprime_n"] <= 3 * (1 - mref["Eprime_n"])
+    assert 1 - m["Eprime_m"] <= 3 * (1 - mref["Eprime_m"])
+    # energy ratio: reference 1 + 4.3e-5 / 1 + 3.0e-3
+    assert abs(m["epsilon"] - 1) <= 3 * abs(mref["epsilon"] - 1)
+    # sigma_J on the ROI relative to FP64's: reference's own relative gap
+    ref_gap = abs(mref["sigma_J"] - meta["fp64_sigma_J_roi"]) / meta["fp64_sigma_J_roi"]
+    assert abs(m["sigma_J"] - ms["sigma_J"]) / ms["sigma_J"] <= max(3 * ref_gap, 1e-4)
+    # best sigma_J of the solve (the stop criterion's value)
+    ref_best_gap = abs(meta["fp32"]["best_sigma"] - meta["fp64"]["best_sigma"]) / meta["fp64"]["best_sigma"]
+    assert abs(a["h"]["best_sigma"] - b["h"]["best_sigma"]) / b["h"]["best_sigma"] <= max(3 * ref_best_gap, 1e-4)
+    # div-B fraction: reference 2.343e-4 vs 2.357e-4 (lowlou), 1.378e-4 vs 1.433e-4 (TD)
+    ref_div_gap = abs(meta["fp32"]["divB_fraction_final"] / meta["fp64"]["divB_fraction_final"] - 1)
+    assert abs(divb_fraction(fa, a["spacing"]) / divb_fraction(fb, a["spacing"]) - 1) <= max(3 * ref_div_gap, 1e-3)
+
+
+def test_fp32_config1_against_analytic():
+    """Config 1: the FP32 result against the analytic Low-Lou interior, beside
+    the reference FP32 result (C_vec 0.98084, E'_n 0.5978, sigma_J 0.1861)."""
+    meta, data = load("lowlou64_rho05")
+    a = solve("lowlou64_rho05", "float32")
+    an = analytic(meta, data, a["f"]["Bx"].shape[0])
+    m = metrics(an, a["f"], a["f"], a["spacing"])
+    ref = meta["fp32_vs_analytic"]
+    for k, tol in (("C_vec", 2e-3), ("C_CS", 2e-3), ("Eprime_n", 5e-3), ("Eprime_m", 5e-3), ("epsilon", 5e-3),
+                   ("sigma_J", 5e-3)):
+        assert abs(m[k] - ref[k]) <= tol * max(abs(ref[k]), 1.0), (k, m[k], ref[k])

@@ -113,3 +113,49 @@ def test_iterate_history_and_fields(name):
     for k, v in h["source_diagnostics"].items():
         if k in sd:
             assert abs(v - sd[k]) <= 1e-6 * abs(sd[k]) + 1e-10, k
+
+
+@pytest.mark.parametrize("name", ["lowlou64_rho05", "td99_96_rho05"])
+def test_oracle_reproduces_reference_runs_of_record(name):
+    """The oracle against the reference's FP64 runs of config 1 (Low-Lou 64^3)
+    and the reduced config 2 (TD generator, 96x96x48): stop reason, best
+    iteration, sigma history, final fields (every 4th cell, stored as FP32),
+    div-B fraction, and config 1's metrics against the analytic interior."""
+    import json
+
+    from oracle.metrics_oracle import divergence, field_metrics
+    from oracle.nfgs_oracle import OracleNFGS
+
+    gold = Path(__file__).resolve().parent / "golden" / "fp32"
+    meta = json.loads((gold / f"{name}.json").read_text())
+    data = dict(np.load(gold / f"{name}.npz"))
+    nx, ny, nz = meta["shape"]
+    sp = tuple(meta["spacing"])
+    o = OracleNFGS(nx, ny, nz, *sp, **{k: v for k, v in meta["ctor"].items() if k != "vertical_current_operator"})
+    o.set_bottom_vector_boundary(data["bx_in"], data["by_in"], data["bz_in"], zero_net_current=False,
+                                 smooth_passes=0, ijzbcor=3)
+    st = meta["stop"]
+    h = o.iterate(max_iter=meta["max_iter"], tol=st["tol"], mu=1.0, patience=st["patience"],
+                  sigma_improvement_tol=st["sigma_improvement_tol"])
+    assert h["stop_reason"] == meta["fp64"]["stop_reason"]
+    assert h["best_iter"] == meta["fp64"]["best_iter"]
+    np.testing.assert_allclose(h["sigma"], data["hist_sigma_fp64"], rtol=1e-9)
+    f = o.fields_to_numpy()
+    for k in ("Bx", "By", "Bz", "Jx", "Jy", "Jz"):
+        w = data["final64_" + k + "_s4"].astype(np.float64)
+        assert np.linalg.norm(f[k][::4, ::4, ::4] - w) / np.linalg.norm(w) < 1e-7, k
+    b = np.stack([f[k] for k in ("Bx", "By", "Bz")])
+    bm = np.sqrt(np.sum(b * b, axis=0))
+    divb = float(np.abs(divergence(b, sp)).mean() / (6.0 * bm.mean() / min(sp) + 1e-12))
+    assert divb == pytest.approx(meta["fp64"]["divB_fraction_final"], rel=1e-9)
+    if "fp64_vs_analytic" in meta:
+        from oracle.lowlou_oracle import lowlou_field, zyx_components
+
+        an = meta["analytic"]
+        fa = lowlou_field(data["lowlou_breaks"], data["lowlou_coeffs"], float(data["lowlou_a2"][0]), n=an["n"],
+                          l=an["l"], psi=an["psi"], resolution=tuple(an["resolution"]), bounds=tuple(an["bounds"]))
+        ref = np.stack(zyx_components(fa))[:, :b.shape[1]]
+        j = np.stack([f[k] for k in ("Jx", "Jy", "Jz")])
+        m = field_metrics(ref, b, j, sp, (0, b.shape[1], 0, b.shape[2], 0, b.shape[3]))
+        for k in ("C_vec", "C_CS", "Eprime_n", "Eprime_m", "epsilon", "sigma_J"):
+            assert m[k] == pytest.approx(meta["fp64_vs_analytic"][k], rel=1e-9), k

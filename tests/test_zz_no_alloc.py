@@ -51,6 +51,41 @@ def test_noalloc_matches_allocating_entry_point_on_repeated_calls():
         assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-11
 
 
+def test_noalloc_on_a_side_stream_and_fp32_spectral_handle():
+    """The call on a caller-owned side stream, read only after that stream is
+    synchronised, and an FP32 handle with the default (spectral) Gaussian
+    operator, against the allocating entry point; the handle is then given a
+    new boundary (which waits for the call) and called again."""
+    import torch
+
+    from nfgs_b200 import _lib as L
+    from nfgs_b200.synthetic import bipolar_boundary
+
+    lib = L.lib()
+    s = _solver(34, 38, 14, 7, "float32")
+    want = s.gaussian_above_bottom_field()
+    side = torch.cuda.Stream()
+    for _ in range(2):
+        buf = torch.full((3 * s.Ny * s.Nx,), float("nan"), dtype=torch.float64, device="cuda:0")
+        torch.cuda.current_stream().synchronize()
+        assert _call(lib, s, buf, side.cuda_stream) == 0, lib.nfgs_last_error()
+        side.synchronize()
+        got = buf.cpu().numpy().reshape(3, s.Ny, s.Nx)
+        assert np.isfinite(got).all()
+        assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-11
+    bx, by, bz = bipolar_boundary(38, 34, 11)
+    buf = torch.full((3 * s.Ny * s.Nx,), float("nan"), dtype=torch.float64, device="cuda:0")
+    assert _call(lib, s, buf, side.cuda_stream) == 0, lib.nfgs_last_error()
+    s.set_bottom_vector_boundary(bx, by, bz, zero_net_current=False, smooth_passes=0)
+    side.synchronize()
+    want2 = s.gaussian_above_bottom_field()
+    buf2 = torch.full((3 * s.Ny * s.Nx,), float("nan"), dtype=torch.float64, device="cuda:0")
+    assert _call(lib, s, buf2, side.cuda_stream) == 0, lib.nfgs_last_error()
+    side.synchronize()
+    got2 = buf2.cpu().numpy().reshape(3, s.Ny, s.Nx)
+    assert np.linalg.norm(got2 - want2) / np.linalg.norm(want2) < 1e-11
+
+
 def test_noalloc_rejects_planes_beyond_the_static_limit():
     import torch
 
