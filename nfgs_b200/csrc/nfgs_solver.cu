@@ -10,6 +10,7 @@
 #include "nfgs_setup.cuh"
 #include "nfgs_tc.cuh"
 #include "nfgs_stencil.cuh"
+#include "nfgs_stencil2.cuh"
 #include "nfgs_metrics.cuh"
 #include "nfgs_soft.cuh"
 #include "nfgs_trace.cuh"
@@ -112,6 +113,7 @@ struct Handle {
     dim3 sgrid, sblock;
     // fused stencil plan (source-producing passes)
     bool fs_on = false;
+    bool fs_v2 = false;        // warp-row stencil (fs2::k_stencil2) instead of fs::k_stencil
     dim3 fs_grid;
     int fs_nb = 0;
     // partial-sum layout of the last stencil pass
@@ -500,17 +502,31 @@ static std::vector<uint16_t> tc_image_wide(int kind, int n, int P) {
 static int fs_setup(Handle* h) {
     const int nx = h->g.nx, ny = h->g.ny, nz = h->g.nz;
     if (nz < 3 || nx < 3 || ny < 3 || getenv("NFGS_DISABLE_FUSED_STENCIL") != nullptr) return NFGS_OK;
-    const size_t smem = h->f32 ? fs::smem_bytes<float>() : fs::smem_bytes<double>();
+    // NFGS_STENCIL_V1=1 keeps the entry-list stencil (fs::k_stencil)
+    const bool v2 = getenv("NFGS_STENCIL_V1") == nullptr;
     int per_sm = 0;
-    if (h->f32) {
-        CK(cudaFuncSetAttribute(fs::k_stencil<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs::k_stencil<float>, fs::NT, smem));
+    if (v2) {
+        const size_t smem = h->f32 ? fs2::smem_bytes<float>() : fs2::smem_bytes<double>();
+        if (h->f32) {
+            CK(cudaFuncSetAttribute(fs2::k_stencil2<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs2::k_stencil2<float>, fs2::NT, smem));
+        } else {
+            CK(cudaFuncSetAttribute(fs2::k_stencil2<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs2::k_stencil2<double>, fs2::NT, smem));
+        }
     } else {
-        CK(cudaFuncSetAttribute(fs::k_stencil<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs::k_stencil<double>, fs::NT, smem));
+        const size_t smem = h->f32 ? fs::smem_bytes<float>() : fs::smem_bytes<double>();
+        if (h->f32) {
+            CK(cudaFuncSetAttribute(fs::k_stencil<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs::k_stencil<float>, fs::NT, smem));
+        } else {
+            CK(cudaFuncSetAttribute(fs::k_stencil<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs::k_stencil<double>, fs::NT, smem));
+        }
     }
     if (per_sm < 1) return NFGS_OK;
-    const int gx = fs::ntiles(nx, fs::TX), gy = fs::ntiles(ny, fs::TY);
+    const int gx = v2 ? fs2::tiles(nx, fs2::W) : fs::ntiles(nx, fs::TX);
+    const int gy = v2 ? fs2::tiles(ny, fs2::H) : fs::ntiles(ny, fs::TY);
     const long long tiles = (long long)gx * gy;
     int best = std::max(1, std::min(16, nz / 16));
     if (const char* e = getenv("NFGS_STENCIL_NSEG")) {
@@ -524,6 +540,7 @@ static int fs_setup(Handle* h) {
     h->fs_grid = dim3((unsigned)gx, (unsigned)gy, (unsigned)best);
     h->fs_nb = (int)(tiles * best);
     h->fs_on = true;
+    h->fs_v2 = v2;
     return NFGS_OK;
 }
 
@@ -721,7 +738,8 @@ static int run_fused(Handle* h, const int* sel, const int* skip, int polarity) {
     a.nseg = (int)h->fs_grid.z;
     a.gx = (int)h->fs_grid.x;
     a.gy = (int)h->fs_grid.y;
-    fs::k_stencil<T><<<h->fs_grid, fs::NT, fs::smem_bytes<T>(), h->s>>>(a);
+    if (h->fs_v2) fs2::k_stencil2<T><<<h->fs_grid, fs2::NT, fs2::smem_bytes<T>(), h->s>>>(a);
+    else fs::k_stencil<T><<<h->fs_grid, fs::NT, fs::smem_bytes<T>(), h->s>>>(a);
     CK(cudaGetLastError());
     h->launches++;
     h->sum_pf = h->pface;
