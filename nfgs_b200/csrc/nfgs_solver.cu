@@ -114,6 +114,7 @@ struct Handle {
     // fused stencil plan (source-producing passes)
     bool fs_on = false;
     bool fs_v2 = false;        // warp-row stencil (fs2::k_stencil2) instead of fs::k_stencil
+    int fs_cw = 1;             // its staging chunk: 2 FP32 elements (8 bytes) on even-width grids
     dim3 fs_grid;
     int fs_nb = 0;
     // partial-sum layout of the last stencil pass
@@ -507,12 +508,16 @@ static int fs_setup(Handle* h) {
     int per_sm = 0;
     if (v2) {
         const size_t smem = h->f32 ? fs2::smem_bytes<float>() : fs2::smem_bytes<double>();
-        if (h->f32) {
-            CK(cudaFuncSetAttribute(fs2::k_stencil2<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs2::k_stencil2<float>, fs2::NT, smem));
+        h->fs_cw = (h->f32 && nx % 2 == 0) ? 2 : 1;
+        if (h->f32 && h->fs_cw == 2) {
+            CK(cudaFuncSetAttribute(fs2::k_stencil2<float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs2::k_stencil2<float, 2>, fs2::NT, smem));
+        } else if (h->f32) {
+            CK(cudaFuncSetAttribute(fs2::k_stencil2<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs2::k_stencil2<float, 1>, fs2::NT, smem));
         } else {
-            CK(cudaFuncSetAttribute(fs2::k_stencil2<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs2::k_stencil2<double>, fs2::NT, smem));
+            CK(cudaFuncSetAttribute(fs2::k_stencil2<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fs2::k_stencil2<double, 1>, fs2::NT, smem));
         }
     } else {
         const size_t smem = h->f32 ? fs::smem_bytes<float>() : fs::smem_bytes<double>();
@@ -738,7 +743,10 @@ static int run_fused(Handle* h, const int* sel, const int* skip, int polarity) {
     a.nseg = (int)h->fs_grid.z;
     a.gx = (int)h->fs_grid.x;
     a.gy = (int)h->fs_grid.y;
-    if (h->fs_v2) fs2::k_stencil2<T><<<h->fs_grid, fs2::NT, fs2::smem_bytes<T>(), h->s>>>(a);
+    if (sizeof(T) == 4 && h->fs_v2 && h->fs_cw == 2)
+        fs2::k_stencil2<T, sizeof(T) == 4 ? 2 : 1><<<h->fs_grid, fs2::NT, fs2::smem_bytes<T>(), h->s>>>(a);
+    else if (h->fs_v2)
+        fs2::k_stencil2<T, 1><<<h->fs_grid, fs2::NT, fs2::smem_bytes<T>(), h->s>>>(a);
     else fs::k_stencil<T><<<h->fs_grid, fs::NT, fs::smem_bytes<T>(), h->s>>>(a);
     CK(cudaGetLastError());
     h->launches++;

