@@ -339,6 +339,23 @@ int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int
  * sigma_J of the start}. */
 int nfgs_iterate_soft_cfcf_start(void* handle, double epsilon, double normal_ridge, double* out4);
 
+/* The cfcf start: between nfgs_iterate_begin and the first advance, the
+ * gs_cfcf start is replaced by the Stable-NFPT curl-free-current state
+ * projected into the NFGS scalars.  Replaces
+ * NFGSSolverGPU._build_stable_cfcf_initial_state (nfgs_solver.py:6080-6147),
+ * which compute_initial_conditions / iterate(init_mode="cfcf") call
+ * (nfgs_solver.py:6613-6628, 6937-6955).  A_z is the zero-source Dirichlet
+ * extension of the stable solver's T = Poisson2D(-Jz), its Jz the legacy
+ * helper-grid current (nfgs_solver.py:2331-2351, 3394-3398, 1498-1567);
+ * Phi_c solves lap_xy Phi_c = B_z - B_background,z on planes 1..nz-1, B_z
+ * the potential field's harmonic extension of Bz_obs with a Neumann top
+ * (nfgs_solver.py:1611-1627) with the BC1 wall and top copies when
+ * lateral_bc1 != 0 (the lateral_wall "paper_bc1" / "BC1" / "paper";
+ * nfgs_solver.py:2138-2164).  mean_bcz_out (nz doubles, may be NULL): the
+ * mean B_c,z per height (stable_cfcf_mean_bcz_by_height).  out2 = {sigma_J
+ * of the start, 1 if A_z differs from the gs_cfcf start's}. */
+int nfgs_iterate_cfcf_start(void* handle, int32_t lateral_bc1, double* mean_bcz_out, double* out2);
+
 /* ------------------------------------------------------------------------
  * Evaluation metrics of a solution on a region of interest, in one FP64-
  * accumulating pass on the GPU.  Replaces the NumPy metrics the reference

@@ -119,6 +119,7 @@ SIGNATURES = {
     "nfgs_iterate_start_state": (C.c_int, [_P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "nfgs_iterate_restart_from": (C.c_int, [_P, _P, _P, C.c_int32, _DP]),
     "nfgs_iterate_soft_cfcf_start": (C.c_int, [_P, C.c_double, C.c_double, _DP]),
+    "nfgs_iterate_cfcf_start": (C.c_int, [_P, C.c_int32, _DP, _DP]),
     "nfgs_trace_field_lines": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int64, _DP,
                                          C.c_double, C.c_int32, _P, _P, _P, _P, _P, _P]),
     "nfgs_qmap_plane": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P, _P]),

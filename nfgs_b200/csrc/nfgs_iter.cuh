@@ -538,7 +538,8 @@ __global__ void k_zero_mode(Geo g, DevCtl* ctl, const double* s00) {
 template <typename T>
 __global__ void k_finalize(Geo g, StateTab st, const DevCtl* ctl, int use_ctl_mu, double mu_fixed,
                            const int* cand_sel, const int* cur_sel, const T* __restrict__ phi_above,
-                           const T* __restrict__ dphi_target, double proj_w, int do_relax, int zero_az_top) {
+                           const T* __restrict__ dphi_target, double proj_w, int do_relax, int zero_az_top,
+                           const T* __restrict__ az_bottom) {
     if (ctl != nullptr && ctl->stopped) return;
     const long long P = g.P;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -562,6 +563,9 @@ __global__ void k_finalize(Geo g, StateTab st, const DevCtl* ctl, int use_ctl_mu
         phi[2 * P + idx] = (T)v2;
     }
     phi[idx] = p0;
+    // Az_new[0] = Az_bottom (nfgs_solver.py:6790): a buffer that held a start
+    // state with another bottom plane (the cfcf start's) is reset when reused
+    if (az_bottom != nullptr) az[idx] = az_bottom[idx];
     if (do_relax && mu < 1.0) {
         const T m1 = (T)mu, m0 = (T)(1.0 - mu);
         for (int k = 1; k < g.nz; ++k) {

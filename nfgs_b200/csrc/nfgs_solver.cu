@@ -92,9 +92,15 @@ struct Handle {
            *jz_t = nullptr, *phi_above = nullptr, *bz_above = nullptr, *d0 = nullptr, *dphi_tgt = nullptr;
     double *phi_above_hat = nullptr, *phi_below_hat = nullptr;  // modal (P)
     double *phi_bot_hat = nullptr, *der_hat = nullptr, *az_bot_hat = nullptr;
+    // bottom current of the Stable-NFPT solver behind the cfcf start: always
+    // the legacy helper-grid derivation; aliases jz_obs when that is the
+    // current in use (jz_stable_alias)
+    double* jz_stable = nullptr;
+    int jz_stable_alias = 1;
     double *bbg_d = nullptr;  // 3V FP64 background (kept for diagnostics)
     // storage-type constants
     void *bbg = nullptr, *bzobs_t = nullptr, *jzt_t = nullptr, *phiab_t = nullptr, *dphi_t = nullptr;
+    void* azb_t = nullptr;     // Az_bottom in the storage type (every candidate's A_z bottom plane)
     void *wx = nullptr, *wy = nullptr, *wz = nullptr;
     double hx = 0.0, hy = 0.0;
     int use_h = 0;
@@ -1029,8 +1035,7 @@ static int setup_boundary(Handle* h, const double* bx_h, const double* by_h, con
         h->launches += 4;
     }
     // --- bottom Jz (nfgs_solver.py:1498-1567, 4489-4546)
-    if (o->jz_mode != NFGS_JZ_PROVIDED) {
-        int legacy = o->jz_mode == NFGS_JZ_DERIVE_LEGACY_HELPER;
+    auto derive_jz = [&](int legacy, double* out) -> int {
         int hnx = nx, hny = ny, bx0 = 0, by0 = 0;
         if (legacy) {
             hnx = mudpack_axis(nx);
@@ -1065,14 +1070,20 @@ static int setup_boundary(Handle* h, const double* bx_h, const double* by_h, con
             }
         }
         dim3 gc((nx + 127) / 128, ny);
-        k_jz_finish<<<gc, 128, 0, s>>>(jzh, hnx, hny, bx0, by0, fp, fn, legacy, jzo, nx, ny);
+        k_jz_finish<<<gc, 128, 0, s>>>(jzh, hnx, hny, bx0, by0, fp, fn, legacy, out, nx, ny);
         CK(cudaGetLastError());
         h->launches += 3;
-    }
+        return NFGS_OK;
+    };
+    if (o->jz_mode != NFGS_JZ_PROVIDED) TRY(derive_jz(o->jz_mode == NFGS_JZ_DERIVE_LEGACY_HELPER, jzo));
+    // the Stable-NFPT solver of the cfcf start derives its own current on the
+    // legacy helper grid from the same maps (nfgs_solver.py:2071-2072)
+    h->jz_stable_alias = o->jz_mode == NFGS_JZ_DERIVE_LEGACY_HELPER;
+    if (!h->jz_stable_alias) TRY(derive_jz(1, h->jz_stable));
     // --- smoothing (nfgs_solver.py:2085-2090)
     if (o->smooth_passes > 0) {
-        double* arr[4] = {bzo, jzo, bxo, byo};
-        for (int a = 0; a < 4; ++a)
+        double* arr[5] = {bzo, jzo, bxo, byo, h->jz_stable};
+        for (int a = 0; a < (h->jz_stable_alias ? 4 : 5); ++a)
             for (int pass = 0; pass < o->smooth_passes; ++pass) {
                 dim3 gc((nx + 127) / 128, ny);
                 k_smooth<<<gc, 128, 0, s>>>(arr[a], w, nx, ny);
@@ -1087,6 +1098,12 @@ static int setup_boundary(Handle* h, const double* bx_h, const double* by_h, con
         TRY(reduce4(h, jzo, P, r));
         double mean = r[0] / (double)P;
         CK(launch_map(P, s, [=] __device__(long long i) { jzo[i] -= mean; }));
+        if (!h->jz_stable_alias) {
+            double* jst = h->jz_stable;
+            TRY(reduce4(h, jst, P, r));
+            const double ms = r[0] / (double)P;
+            CK(launch_map(P, s, [=] __device__(long long i) { jst[i] -= ms; }));
+        }
     }
     // --- Az_bottom: endpoint-Dirichlet 2-D Poisson of -Jz (nfgs_solver.py:1132-1144)
     const int nxi = nx - 2, nyi = ny - 2;
@@ -1519,8 +1536,7 @@ static int build_constants(Handle* h) {
         CK(cudaGetLastError());
     }
     // state buffers: zero, then the fixed bottom planes
-    void* azb_t = nullptr;
-    TRY(alloc(h, &azb_t, P * h->esz));
+    void* azb_t = h->azb_t;
     TRY(to_storage(h, h->az_bot, azb_t, P));
     for (int b = 0; b < 3; ++b) {
         CK(cudaMemsetAsync(h->st.phi[b], 0, V * h->esz, s));
@@ -1530,7 +1546,7 @@ static int build_constants(Handle* h) {
     }
     CK(cudaStreamSynchronize(s));
     for (auto it = h->owned.begin(); it != h->owned.end();) {
-        if (it->p == tmp || it->p == tmp2 || it->p == azb_t) { cudaFreeAsync(it->p, h->s); it = h->owned.erase(it); }
+        if (it->p == tmp || it->p == tmp2) { cudaFreeAsync(it->p, h->s); it = h->owned.erase(it); }
         else ++it;
     }
     return NFGS_OK;
@@ -1548,7 +1564,7 @@ static int enqueue_iteration(Handle* h) {
         const long long P = h->g.P;
         k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(
             h->g, h->st, c, 1, 1.0, &c->cand, &c->cur, (const T*)h->phiab_t, (const T*)h->dphi_t,
-            h->prm.projection_weight, 1, 1);
+            h->prm.projection_weight, 1, 1, (const T*)h->azb_t);
         CK(cudaGetLastError());
         h->launches++;
     }
@@ -1672,7 +1688,7 @@ static int iterate_begin_t(Handle* h, const NfgsStop* stop) {
         const long long P = h->g.P;
         k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(
             h->g, h->st, nullptr, 0, 1.0, &h->consts[0], &h->consts[0], (const T*)h->phiab_t, (const T*)h->dphi_t,
-            h->prm.projection_weight, 0, 1);
+            h->prm.projection_weight, 0, 1, (const T*)h->azb_t);
         CK(cudaGetLastError());
         h->launches++;
     }
@@ -1861,7 +1877,7 @@ static int soft_cfcf_start_t(Handle* h, double eps, double ridge, double* out) {
     TRY(inverse_transforms<T>(h, nullptr, &h->consts[2], 1));
     k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(g, h->st, nullptr, 0, 1.0, &h->consts[2],
                                                                 &h->consts[2], (const T*)h->phiab_t,
-                                                                (const T*)h->dphi_t, 0.0, 0, 0);
+                                                                (const T*)h->dphi_t, 0.0, 0, 0, (const T*)h->azb_t);
     CK(cudaGetLastError());
     h->launches++;
     const double fac = g.dx * g.dy * g.dz / (4.0 * (double)(g.nx - 1) * (double)(g.ny - 1));
@@ -1872,6 +1888,206 @@ static int soft_cfcf_start_t(Handle* h, double eps, double ridge, double* out) {
     TRY(adopt_buffer2<T>(h, 2, ad));
     out[3] = ad[0];
     return NFGS_OK;
+}
+
+// Zero-source modal solve along z with a Dirichlet bottom u0 and a
+// Dirichlet (zero) or mirrored-ghost Neumann top, one thread per mode, FP64
+// in the reference's operation order (_thomas_solve_batched_lowmem,
+// nfgs_solver.py:536-608).  out is [nz][M]; cs is [nz][M] scratch.
+__global__ void k_modal_harmonic(long long M, int nz, double dz, const double* __restrict__ lam,
+                                 const double* __restrict__ u0, int top_dirichlet, double* __restrict__ out,
+                                 double* __restrict__ cs) {
+    const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const double dz2 = dz * dz, a = 1.0 / dz2, c = 1.0 / dz2;
+    const double b = lam[m] - 2.0 / dz2;
+    const int n = top_dirichlet ? nz - 2 : nz - 1;
+    const double ub = u0[m];
+    out[m] = ub;
+    for (int k = 1; k < nz; ++k) out[(long long)k * M + m] = 0.0;
+    if (n <= 0) return;
+    // forward sweep: c*_i in cs, d*_i in out row i + 1
+    const double bottom_a = (n == 1 && !top_dirichlet) ? 2.0 * a : a;
+    const double d0 = 0.0 - bottom_a * ub;
+    double cp, dp;
+    if (n == 1) {
+        cp = 0.0;
+        dp = d0 / b;
+    } else {
+        cp = c / b;
+        dp = d0 / b;
+    }
+    cs[m] = cp;
+    out[M + m] = dp;
+    for (int i = 1; i < n; ++i) {
+        double ae = a, ce = c;
+        if (i == n - 1) {
+            ce = 0.0;
+            if (!top_dirichlet) ae = 2.0 * a;
+        }
+        const double den = b - ae * cp;
+        cp = ce / den;
+        dp = (0.0 - ae * dp) / den;
+        cs[(long long)i * M + m] = cp;
+        out[(long long)(i + 1) * M + m] = dp;
+    }
+    // back substitution: u_{i} = d*_i - c*_i u_{i+1}
+    double up = dp;
+    for (int i = n - 2; i >= 0; --i) {
+        const long long q = (long long)(i + 1) * M + m;
+        up = out[q] - cs[(long long)i * M + m] * up;
+        out[q] = up;
+    }
+}
+
+// cfcf start (nfgs_solver.py:6080-6147): the Stable-NFPT curl-free-current
+// state projected into the NFGS scalars, after iterate_begin.
+//  * A_z: the zero-source Dirichlet extension of the stable solver's
+//    T = Poisson2D(-Jz) (nfgs_solver.py:2331-2351, 1305-1333, 3394-3398): the
+//    gs_cfcf start's A_z when the stable current is the one in use, else
+//    built from the legacy helper-grid current;
+//  * B_z of the stable state: the potential field's, the harmonic extension
+//    of Bz_obs with a Neumann top (nfgs_solver.py:1611-1627), with the BC1
+//    wall and top copies when lateral_bc1 (nfgs_solver.py:2138-2164) and
+//    Bz_obs on the bottom plane (nfgs_solver.py:2180);
+//  * Phi_c: lap_xy Phi_c = B_z - B_background,z on planes 1..nz-1 (mean
+//    mode dropped, nfgs_solver.py:1120-1130, 1146-1181), Phi_c(0) = Phi^>.
+// The state replaces the gs_cfcf start (buffer 2 -> 0).  mean_out (nz
+// doubles, optional): the mean B_c,z per height the reference reports;
+// out[0]: sigma_J of the start, out[1]: 1 when A_z differs from gs_cfcf's.
+template <typename T>
+static int cfcf_start_t(Handle* h, int lateral_bc1, double* mean_out, double* out) {
+    if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
+    if (h->advanced) return fail(NFGS_ESTATE, "the iteration has already advanced");
+    const Geo& g = h->g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz, nxi = nx - 2, nyi = ny - 2;
+    const long long P = g.P, V = g.V, PI = h->PI;
+    cudaStream_t s = h->s;
+    double *vol = nullptr, *cs = nullptr, *tmp = nullptr, *pl = nullptr;
+    auto cleanup = [&]() {
+        if (vol) release(h, vol);
+        if (cs) release(h, cs);
+        if (tmp) release(h, tmp);
+        if (pl) release(h, pl);
+    };
+    int rc = NFGS_OK;
+    do {
+        if ((rc = alloc(h, &vol, (size_t)V * 8)) != NFGS_OK) break;
+        if ((rc = alloc(h, &cs, (size_t)V * 8)) != NFGS_OK) break;
+        if ((rc = alloc(h, &tmp, (size_t)V * 8)) != NFGS_OK) break;
+        if ((rc = alloc(h, &pl, (size_t)4 * P * 8)) != NFGS_OK) break;
+    } while (0);
+    if (rc != NFGS_OK) { cleanup(); return rc; }
+    rc = [&]() -> int {
+        // B_z of the potential field: modal harmonic extension of Bz_obs
+        double* bzh = pl;
+        TRY(dct2_d(h, h->bz_obs, bzh, pl + P));
+        k_modal_harmonic<<<(unsigned)((P + 127) / 128), 128, 0, s>>>(P, nz, g.dz, h->lamN, bzh, 0, tmp, cs);
+        CK(cudaGetLastError());
+        h->launches++;
+        TRY(idct2_d(h, tmp, vol, cs, nz));
+        // BC1: x walls on rows 1..ny-2, then y walls, then the top plane
+        if (lateral_bc1) {
+            if (nx > 1)
+                CK(launch_map((long long)nz * ny, s, [=] __device__(long long q) {
+                    const long long k = q / ny, j = q % ny;
+                    if (j < 1 || j > ny - 2) return;
+                    double* r = vol + k * P + j * nx;
+                    r[0] = r[1];
+                    r[nx - 1] = r[nx - 2];
+                }));
+            if (ny > 1)
+                CK(launch_map((long long)nz * nx, s, [=] __device__(long long q) {
+                    const long long k = q / nx, i = q % nx;
+                    double* c0 = vol + k * P + i;
+                    c0[0] = c0[nx];
+                    c0[(long long)(ny - 1) * nx] = c0[(long long)(ny - 2) * nx];
+                }));
+            if (nz > 1)
+                CK(launch_map(P, s, [=] __device__(long long q) {
+                    vol[(long long)(nz - 1) * P + q] = vol[(long long)(nz - 2) * P + q];
+                }));
+        }
+        // B_c,z = B_z - B_background,z (bottom plane: Bz_obs - B_background,z)
+        {
+            const double* bzo = h->bz_obs;
+            const double* bgz = h->bbg_d + 2 * V;
+            CK(launch_map(V, s, [=] __device__(long long q) {
+                const double bz = q < P ? bzo[q] : vol[q];
+                vol[q] = bz - bgz[q];
+            }));
+        }
+        TRY(dct2_d(h, vol, tmp, cs, nz));
+        if (mean_out) {
+            const double norm = 4.0 * (double)std::max(nx - 1, 1) * (double)std::max(ny - 1, 1);
+            std::vector<double> mh(nz);
+            CK(cudaMemcpy2DAsync(mh.data(), 8, tmp, (size_t)P * 8, 8, nz, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            for (int k = 0; k < nz; ++k) mean_out[k] = mh[k] / norm;
+        }
+        // Phi_c modes of planes 1..nz-1 into the Robin chain's modal buffer
+        {
+            T* hat = (T*)h->sb;
+            const double* lam = h->lamN;
+            CK(launch_map(V - P, s, [=] __device__(long long q) {
+                const long long m = q % P;
+                const double v = m == 0 ? 0.0 : tmp[P + q] / lam[m];
+                hat[P + q] = (T)v;
+            }));
+        }
+        // A_z modes of the stable solver's current (planes 1..nz-2) when it
+        // differs from the one in use
+        const bool own_az = !h->jz_stable_alias && nx >= 3 && ny >= 3;
+        double* tst = pl + P;  // T of the stable solver, calculation grid
+        if (own_az) {
+            double *t1 = pl + 2 * P, *t2 = pl + 3 * P;
+            const double* jst = h->jz_stable;
+            const double* lamD = h->lamD;
+            CK(launch_map(PI, s, [=] __device__(long long q) {
+                const long long j = q / nxi, i = q % nxi;
+                t1[q] = -jst[(j + 1) * nx + (i + 1)];
+            }));
+            TRY(apply_x<double>(h, h->dstx, t1, nxi, PI, t2, nxi, PI, nyi, nxi, nxi, 1));
+            TRY(apply_y<double>(h, h->dsty, t2, nxi, PI, t1, nxi, PI, nyi, nyi, nxi, 1));
+            CK(launch_map(PI, s, [=] __device__(long long q) { t1[q] /= lamD[q]; }));  // modes of T
+            TRY(apply_y<double>(h, h->idsty, t1, nxi, PI, t2, nxi, PI, nyi, nyi, nxi, 1));
+            TRY(apply_x<double>(h, h->idstx, t2, nxi, PI, cs, nxi, PI, nyi, nxi, nxi, 1));
+            CK(launch_map(P, s, [=] __device__(long long q) {
+                const long long j = q / nx, i = q % nx;
+                tst[q] = (j >= 1 && j <= ny - 2 && i >= 1 && i <= nx - 2) ? cs[(j - 1) * nxi + (i - 1)] : 0.0;
+            }));
+            k_modal_harmonic<<<(unsigned)((PI + 127) / 128), 128, 0, s>>>(PI, nz, g.dz, lamD, t1, 1, tmp, cs);
+            CK(cudaGetLastError());
+            h->launches++;
+            T* hat = (T*)h->sj;
+            CK(launch_map((long long)(nz - 2) * PI, s, [=] __device__(long long q) { hat[PI + q] = (T)tmp[PI + q]; }));
+        }
+        // inverse transforms into buffer 2; Phi_c bottom plane Phi^>
+        TRY(inverse_transforms<T>(h, nullptr, &h->consts[2], 0));
+        k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, s>>>(g, h->st, nullptr, 0, 1.0, &h->consts[2],
+                                                                   &h->consts[2], (const T*)h->phiab_t,
+                                                                   (const T*)h->dphi_t, 0.0, 0, 0, (const T*)h->azb_t);
+        CK(cudaGetLastError());
+        h->launches++;
+        if (own_az) {
+            T* az2 = (T*)h->st.az[2];
+            CK(launch_map(V, s, [=] __device__(long long q) {
+                const long long k = q / P, r = q % P, j = r / nx, i = r % nx;
+                if (k == 0) az2[q] = (T)tst[r];
+                else if (k == nz - 1 || i == 0 || i == nx - 1 || j == 0 || j == ny - 1) az2[q] = T(0);
+            }));
+        } else {
+            CK(cudaMemcpyAsync(h->st.az[2], h->st.az[0], (size_t)V * h->esz, cudaMemcpyDeviceToDevice, s));
+        }
+        double ad[3];
+        TRY(adopt_buffer2<T>(h, 2, ad));
+        out[0] = ad[0];
+        out[1] = own_az ? 1.0 : 0.0;
+        return NFGS_OK;
+    }();
+    CK(cudaStreamSynchronize(s));
+    cleanup();
+    return rc;
 }
 
 // Capture the per-iteration launch sequence of a handle into its CUDA graph
@@ -2268,7 +2484,7 @@ static int step_t(Handle* h, double mu, int polarity) {
     const long long P = h->g.P;
     k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(h->g, h->st, nullptr, 0, mu, &h->consts[cand],
                                                                 &h->consts[cur], (const T*)h->phiab_t,
-                                                                (const T*)h->dphi_t, h->prm.projection_weight, 1, 1);
+                                                                (const T*)h->dphi_t, h->prm.projection_weight, 1, 1, (const T*)h->azb_t);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->s));
     h->cur_host = cand;
@@ -2440,7 +2656,7 @@ static int time_phases_t(Handle* h, int n_iters, double* ms_out) {
         CK(cudaEventRecord(ev[4], h->s));
         k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(h->g, h->st, nullptr, 0, 1.0, &h->consts[cand],
                                                                     &h->consts[cur], (const T*)h->phiab_t,
-                                                                    (const T*)h->dphi_t, h->prm.projection_weight, 1, 1);
+                                                                    (const T*)h->dphi_t, h->prm.projection_weight, 1, 1, (const T*)h->azb_t);
         CK(cudaGetLastError());
         CK(cudaEventRecord(ev[5], h->s));
         CK(cudaEventSynchronize(ev[5]));
@@ -2591,13 +2807,14 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
     // boundary planes
     double** planes[] = {&h->bz_obs, &h->bx_obs, &h->by_obs, &h->jz_obs, &h->az_bot, &h->jz_t,
                          &h->phi_above, &h->bz_above, &h->d0, &h->dphi_tgt, &h->phi_above_hat,
-                         &h->phi_below_hat, &h->phi_bot_hat, &h->der_hat};
+                         &h->phi_below_hat, &h->phi_bot_hat, &h->der_hat, &h->jz_stable};
     for (auto pp : planes) { TRYC(alloc(h, pp, P * 8)); CKC(cudaMemset(*pp, 0, P * 8)); }
     TRYC(alloc(h, &h->az_bot_hat, PI * 8));
     TRYC(alloc(h, &h->bbg_d, 3 * V * 8));
     TRYC(alloc(h, &h->bbg, 3 * V * h->esz));
     TRYC(alloc(h, &h->bzobs_t, P * h->esz)); TRYC(alloc(h, &h->jzt_t, P * h->esz));
     TRYC(alloc(h, &h->phiab_t, P * h->esz)); TRYC(alloc(h, &h->dphi_t, P * h->esz));
+    TRYC(alloc(h, &h->azb_t, P * h->esz));
     // buffer window (nfgs_solver.py:1569-1591)
     if (prm->buffer_thickness > 0) {
         const int t = prm->buffer_thickness;
@@ -2969,6 +3186,15 @@ int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int
     if (!h || !out3 || (mode != 4 && (!phi || !az))) return fail(NFGS_EINVAL, "null argument");
     if (mode < 0 || mode > 4) return fail(NFGS_EINVAL, "mode must be 0 to 4");
     return h->f32 ? restart_from_t<float>(h, phi, az, mode, out3) : restart_from_t<double>(h, phi, az, mode, out3);
+}
+
+int nfgs_iterate_cfcf_start(void* handle, int32_t lateral_bc1, double* mean_bcz_out, double* out2) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h || !out2) return fail(NFGS_EINVAL, "null argument");
+    if (cudaSetDevice(h->geom.device) != cudaSuccess) return fail(NFGS_ECUDA, "cudaSetDevice failed");
+    return h->f32 ? cfcf_start_t<float>(h, lateral_bc1, mean_bcz_out, out2)
+                  : cfcf_start_t<double>(h, lateral_bc1, mean_bcz_out, out2);
 }
 
 int nfgs_iterate_soft_cfcf_start(void* handle, double epsilon, double normal_ridge, double* out4) {

@@ -3,15 +3,14 @@
 Mirrors the public API of the reference ``nfgs_solver.NFGSSolverGPU``
 (nfgs_solver.py:3905-7196 in spaceprod/NFGS): the constructor with its
 policy keywords, ``set_bottom_vector_boundary`` / ``set_bottom_boundary``,
-``iterate`` (gs_cfcf or soft_cfcf start, sigma_best stop, optional adaptive mu) and
+``iterate`` (gs_cfcf, cfcf or soft_cfcf start, sigma_best stop, optional adaptive mu) and
 ``fields_to_numpy``.  All numerical work runs in libnfgs_b200.so on the
 GPU; this module only validates options, sizes the grid, places the
 observed maps and assembles the ``history`` dictionary.
 
 Options that select the reference's ablation branches (coupled k=0 modes,
-the cfcf start, two-stage poloidal update, collocated current,
-fixed-point stop mode with per-iteration diagnostics) raise
-``NotImplementedError``.
+two-stage poloidal update, collocated current, fixed-point stop mode with
+per-iteration diagnostics) raise ``NotImplementedError``.
 """
 
 from __future__ import annotations
@@ -241,6 +240,10 @@ class NFGSSolverGPU:
                                 "potentialpin", "pin", "legacy"}:
             raise ValueError("lateral_wall must be one of: 'potential_pin', 'legacy_potential_pin', 'BC1', "
                              f"'paper_bc1', 'paper'; got {lateral_wall!r}")
+        # wall condition of the Stable-NFPT field behind the cfcf start
+        self._lateral_bc1 = lateral_wall in {"bc1", "paper_bc1", "paper"}
+        self.handoff_projection_policy = handoff
+        self.handoff_projection_tolerance = handoff_tol
         if rhs_lap not in ("fd", "spectral"):
             raise ValueError("rhs_lap_xy must be 'fd' or 'spectral'")
         if rhs_ext not in ("neumann", "dirichlet"):
@@ -544,7 +547,7 @@ class NFGSSolverGPU:
     # ------------------------------------------------------------------
     def compute_initial_conditions(self, *, init_mode="gs_cfcf", **_unused):
         """The start state of `init_mode` (gs_cfcf, nfgs_solver.py:6613-6645;
-        soft_cfcf, 6427-6484) as host arrays (B, J, Phi_c, A_z, B_c) on the
+        cfcf, 6080-6147; soft_cfcf, 6427-6484) as host arrays (B, J, Phi_c, A_z, B_c) on the
         calculation grid, B_c = B - B_background.  It is built on the device
         as iterate() builds it; until the next iterate(), fields_to_numpy()
         returns this state."""
@@ -608,8 +611,13 @@ class NFGSSolverGPU:
             raise ValueError("fixed-point tolerances must be positive")
         if int(fixed_point_patience) < 1:
             raise ValueError("fixed_point_patience must be >= 1")
-        if mode not in ("gs_cfcf", "soft_cfcf", "learned"):
-            raise NotImplementedError(f"init_mode={init_mode!r}: the gs_cfcf and soft_cfcf starts are built for B200")
+        if mode == "curl_free_current":
+            mode = "cfcf"
+        if mode == "cfcf" and self.handoff_projection_policy == "error":
+            raise NotImplementedError(
+                "handoff_projection_policy='error' needs the Stable-NFPT field's projection errors "
+                "(its Fortran-compatible bjt00 reconstruction), which this build does not form; "
+                "the cfcf start runs with handoff_projection_policy='project'")
         if mode == "soft_cfcf" and self.Nz < 5:
             raise ValueError("soft_cfcf requires Nz >= 5")
         if mode == "soft_cfcf" and (self.Nx < 3 or self.Ny < 3):
@@ -637,6 +645,8 @@ class NFGSSolverGPU:
                                   "coupled_k0": self._k0_diagnostics}
         if mode == "soft_cfcf":
             self._init_diagnostics = self._soft_cfcf_start()
+        if mode == "cfcf":
+            self._init_diagnostics = self._cfcf_start()
         self.learned_start_info = None
         if mode == "learned":
             from . import learned as _learned
@@ -653,6 +663,24 @@ class NFGSSolverGPU:
                     check_every=check_every, max_iter=max_iter, stop_mode=stop_mode, update_tol=update_tol,
                     observable_tol=observable_tol, fixed_point_pde_tol=fixed_point_pde_tol,
                     fixed_point_patience=fixed_point_patience, eps=eps, use_imp=use_imp)
+
+    def _cfcf_start(self):
+        """cfcf start on the device (nfgs_solver.py:6080-6147), after
+        nfgs_iterate_begin: the Stable-NFPT curl-free-current state projected
+        into the NFGS scalars replaces the gs_cfcf start.  The projection's
+        field and current RMS differences (diagnostics of the stable solver's
+        own Fortran-compatible field) are not formed: those keys are None."""
+        mean = np.zeros(self.Nz)
+        out = np.zeros(2)
+        L.check(self._lib.nfgs_iterate_cfcf_start(self._h, int(self._lateral_bc1), L.dptr(mean), L.dptr(out)))
+        return {"init_mode": "cfcf", "mfr_count": 0, "stable_cfcf_handoff": True,
+                "stable_cfcf_handoff_projected": True,
+                "stable_cfcf_field_rms_difference": None, "stable_cfcf_current_rms_difference": None,
+                "stable_cfcf_field_relative_difference": None, "stable_cfcf_current_relative_difference": None,
+                "stable_cfcf_mean_bcz_by_height": [float(v) for v in mean],
+                "stable_cfcf_own_az": bool(out[1]),
+                "gaussian_separation": self.gaussian_separation_diagnostics,
+                "coupled_k0": self._k0_diagnostics}
 
     def _soft_cfcf_start(self):
         """soft_cfcf start on the device (nfgs_solver.py:6427-6484), after

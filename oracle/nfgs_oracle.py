@@ -330,8 +330,12 @@ class OracleNFGS:
                  weak_field_floor_b2=1e-20, gaussian_horizontal_operator="spectral",
                  bottom_parallel_current_mode="observed_full",
                  user_supplied_open_bz=None, user_supplied_horizontal_field=None,
-                 external_potential_field=None, soft_cfcf_epsilon=None, soft_cfcf_normal_ridge=0.0):
+                 external_potential_field=None, soft_cfcf_epsilon=None, soft_cfcf_normal_ridge=0.0,
+                 lateral_wall="paper_bc1"):
         ix, iy, iz = int(Nx), int(Ny), int(Nz)
+        # the wall condition of the Stable-NFPT field behind the cfcf start
+        # (nfgs_solver.py:845-853, 2161-2170)
+        self.lateral_bc1 = str(lateral_wall).lower().replace("-", "_") in ("bc1", "paper_bc1", "paper")
         mode = str(calculation_domain_mode).lower().replace("-", "_")
         # nfgs_solver.py:771-819
         if pad_calculation_domain:
@@ -586,13 +590,21 @@ class OracleNFGS:
                 jz = derive_bottom_jz_calc(bx, by, self.dx, self.dy, ijzbcor)
         else:
             self.bottom_current_grid_mode = "provided"
+        # the Stable-NFPT solver behind the cfcf start derives its own bottom
+        # current, always on the legacy helper grid (nfgs_solver.py:2071-2072,
+        # 1498-1567), from the same maps
+        jz_st = jz if self.bottom_current_grid_mode == "legacy_helper" else \
+            derive_bottom_jz_legacy(bx, by, self.Nz, self.dx, self.dy, ijzbcor)
         if int(smooth_passes) > 0:
             bz = _smooth_bottom_2d(bz, smooth_passes)
             jz = _smooth_bottom_2d(jz, smooth_passes)
+            jz_st = _smooth_bottom_2d(jz_st, smooth_passes)
             bx = _smooth_bottom_2d(bx, smooth_passes)
             by = _smooth_bottom_2d(by, smooth_passes)
         if zero_net_current:
             jz = jz - jz.mean()
+            jz_st = jz_st - jz_st.mean()
+        self.Jz_stable = jz_st.copy()
         self.Bz_obs, self.Jz_obs, self.Bx_obs, self.By_obs = bz.copy(), jz.copy(), bx.copy(), by.copy()
         # nfgs_solver.py:2105 and 3039-3057
         self.Az_bottom = self.poisson2d_dirichlet(-self.Jz_obs)
@@ -1056,14 +1068,104 @@ class OracleNFGS:
         mode = str(init_mode).lower().replace("-", "_")
         if mode in ("soft_cfcf", "yi_soft"):
             return self.soft_cfcf_initial_state()
+        if mode in ("cfcf", "curl_free_current"):
+            return self.cfcf_initial_state(lateral_bc1=getattr(self, "lateral_bc1", True))
         if mode != "gs_cfcf":
-            raise NotImplementedError("the oracle restates the gs_cfcf and soft_cfcf starts")
+            raise NotImplementedError("the oracle restates the gs_cfcf, cfcf and soft_cfcf starts")
         zeros = np.zeros((self.Nz, self.Ny, self.Nx))
         phi = self.solve_phi_c(zeros, self.Phi_above_bottom)
         phi = self.apply_projection(phi)
         bcz = lap_xy(phi, self.dx, self.dy)
         az = self.solve_az(zeros)
         B, J, Bc = self.reconstruct(phi, az, bcz)
+        return B, J, phi, az, Bc
+
+    def harmonic_modal(self, u0_hat, lam, top_dirichlet):
+        """Zero-source modal Thomas solve along z with Dirichlet bottom u0_hat
+        and a Dirichlet (zero) or mirrored-ghost Neumann top
+        (_thomas_solve_batched_lowmem, nfgs_solver.py:536-608)."""
+        nz = self.Nz
+        dz2 = self.dz * self.dz
+        a = c = 1.0 / dz2
+        b = lam - 2.0 / dz2
+        n = nz - 2 if top_dirichlet else nz - 1
+        u = np.zeros((nz,) + lam.shape)
+        u[0] = u0_hat
+        if n <= 0:
+            return u
+        cs = np.empty((n,) + lam.shape)
+        ds = np.empty_like(cs)
+        bottom_a = 2.0 * a if (n == 1 and not top_dirichlet) else a
+        d0 = 0.0 - bottom_a * u0_hat
+        if n == 1:
+            cs[0] = 0.0
+            ds[0] = d0 / b
+        else:
+            cs[0] = c / b
+            ds[0] = d0 / b
+            for i in range(1, n):
+                ae, ce = a, c
+                if i == n - 1:
+                    ce = 0.0
+                    if not top_dirichlet:
+                        ae = 2.0 * a
+                den = b - ae * cs[i - 1]
+                cs[i] = ce / den
+                ds[i] = (0.0 - ae * ds[i - 1]) / den
+        for i in range(n - 2, -1, -1):
+            ds[i] = ds[i] - cs[i] * ds[i + 1]
+        u[1:1 + n] = ds
+        return u
+
+    def cfcf_initial_state(self, lateral_bc1=True):
+        """cfcf start (nfgs_solver.py:6080-6147): the Stable-NFPT
+        curl-free-current state (nfgs_solver.py:2331-2376, 3343-3405) projected
+        into the NFGS scalars.  Its A_z is the zero-source Dirichlet extension
+        of the stable solver's T = Poisson2D(-Jz) (nfgs_solver.py:2331-2351,
+        1305-1333, 3394-3398); its B_z is the potential field's, the harmonic extension of
+        Bz_obs with a Neumann top (nfgs_solver.py:1611-1627), with the BC1
+        wall and top copies (nfgs_solver.py:2138-2156) and Bz_obs on the bottom
+        plane.  Phi_c solves lap_xy Phi_c = B_z - B_background,z plane by plane
+        above the bottom (mean mode dropped, nfgs_solver.py:1120-1130,
+        1146-1181), Phi_c(0) = Phi^>.  Returns (B, J, Phi_c, A_z, B_c) and sets
+        cfcf_diagnostics (the mean B_c,z per height)."""
+        nz, ny, nx = self.Nz, self.Ny, self.Nx
+        lamN = self.lam_neumann()
+        bz_hat = dct2(self.Bz_obs)
+        bzp = idct2(self.harmonic_modal(bz_hat, lamN, top_dirichlet=False))
+        if lateral_bc1:
+            if nx > 1:
+                bzp[:, 1:-1, 0] = bzp[:, 1:-1, 1]
+                bzp[:, 1:-1, -1] = bzp[:, 1:-1, -2]
+            if ny > 1:
+                bzp[:, 0, :] = bzp[:, 1, :]
+                bzp[:, -1, :] = bzp[:, -2, :]
+            if nz > 1:
+                bzp[-1] = bzp[-2]
+        bzp[0] = self.Bz_obs
+        bcz = bzp - self.B_background[2]
+        hat = dct2(bcz)
+        norm = 4.0 * max(nx - 1, 1) * max(ny - 1, 1)
+        mean_by_height = hat[:, 0, 0] / norm
+        lam = lamN.copy()
+        lam[0, 0] = 1.0
+        ph = hat / lam[None]
+        ph[:, 0, 0] = 0.0
+        phi = idct2(ph)
+        phi[0] = self.Phi_above_bottom
+        if self.bottom_current_grid_mode == "legacy_helper":
+            t_st = self.Az_bottom
+        else:
+            t_st = self.poisson2d_dirichlet(-self.Jz_stable)
+        az = np.zeros((nz, ny, nx))
+        if nx >= 3 and ny >= 3:
+            lamD = self.lam_dirichlet()
+            az[:, 1:-1, 1:-1] = idst2(self.harmonic_modal(dst2(t_st[1:-1, 1:-1]), lamD, top_dirichlet=True))
+        az[0] = t_st
+        az[-1] = 0.0
+        self._az_walls_zero(az)
+        self.cfcf_diagnostics = {"stable_cfcf_mean_bcz_by_height": [float(v) for v in mean_by_height]}
+        B, J, Bc = self.reconstruct(phi, az, lap_xy(phi, self.dx, self.dy))
         return B, J, phi, az, Bc
 
     def soft_cfcf_initial_state(self):
@@ -1144,7 +1246,7 @@ class OracleNFGS:
                 mu_min=0.02, mu_max=1.0, mu_backoff=0.5, mu_growth=1.1, growth_streak=5,
                 divergence_factor=2.0, max_rollbacks=12, stop_mode="sigma_best", **_ignored):
         """Stable driver (nfgs_solver.py:3522-3850) with the NFGS wrapper (6937-7009)."""
-        if str(init_mode).lower().replace("-", "_") not in ("gs_cfcf", "soft_cfcf", "yi_soft"):
+        if str(init_mode).lower().replace("-", "_") not in ("gs_cfcf", "soft_cfcf", "yi_soft", "cfcf", "curl_free_current"):
             raise NotImplementedError("the oracle restates the gs_cfcf and soft_cfcf starts")
         if stop_mode != "sigma_best":
             raise ValueError("stop_mode='fixed_point' requires record_iteration_diagnostics=True")
