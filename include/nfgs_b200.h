@@ -62,6 +62,7 @@ extern "C" {
 #define NFGS_STOP_SIGMA_STALL 4
 #define NFGS_STOP_MAX_ROLLBACKS 5
 #define NFGS_STOP_POLICY_ERROR 6
+#define NFGS_STOP_FIXED_POINT 7
 
 /* Calculation grid and observed field of view (host-computed sizing,
  * nfgs_solver.py:771-819). */
@@ -355,6 +356,24 @@ int nfgs_iterate_soft_cfcf_start(void* handle, double epsilon, double normal_rid
  * mean B_c,z per height (stable_cfcf_mean_bcz_by_height).  out2 = {sigma_J
  * of the start, 1 if A_z differs from the gs_cfcf start's}. */
 int nfgs_iterate_cfcf_start(void* handle, int32_t lateral_bc1, double* mean_bcz_out, double* out2);
+
+/* Per-step diagnostics of record_iteration_diagnostics=True
+ * (nfgs_solver.py:6660-6681, 6806-6933) for the candidate of the last step,
+ * after nfgs_iterate_advance(handle, 1, ...): out15 = {phi_update,
+ * az_update, phi_map_residual, az_map_residual, h_k0_update,
+ * h_k0_map_residual, bcz_pde_residual, jz_pde_residual,
+ * poloidal_pde_residual, toroidal_pde_residual, mixed_row_residual,
+ * bottom_field_imprint, bottom_jz_imprint (all relative),
+ * alpha_clip_fraction, weak_field_floor_fraction}.  NFGS_ESTATE unless the
+ * last advance ran exactly one step. */
+#define NFGS_NSTEPDIAG 15
+int nfgs_step_diagnostics(void* handle, double* out15);
+
+/* stop_mode="fixed_point" (nfgs_solver.py:3707-3776, 3815-3818): the
+ * solution becomes the final accepted iterate rather than the best-sigma
+ * state; stop_now != 0 also ends the iteration with NFGS_STOP_FIXED_POINT
+ * (the host decides the fixed point from the step diagnostics). */
+int nfgs_iterate_fixed_point(void* handle, int32_t stop_now);
 
 /* ------------------------------------------------------------------------
  * Evaluation metrics of a solution on a region of interest, in one FP64-

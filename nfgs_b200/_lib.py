@@ -26,6 +26,7 @@ NFGS_F32, NFGS_F64 = 0, 1
 NFGS_NDIAG = 40
 NFGS_NSRCDIAG = 12
 NFGS_HIST_COLS = 8
+NFGS_NSTEPDIAG = 15
 NFGS_MET_COUNT = 13
 
 STOP_REASONS = {
@@ -36,6 +37,7 @@ STOP_REASONS = {
     4: "sigma_stall",
     5: "max_rollbacks",
     6: "source_zero_mode_error",
+    7: "fixed_point",
 }
 
 
@@ -120,6 +122,8 @@ SIGNATURES = {
     "nfgs_iterate_restart_from": (C.c_int, [_P, _P, _P, C.c_int32, _DP]),
     "nfgs_iterate_soft_cfcf_start": (C.c_int, [_P, C.c_double, C.c_double, _DP]),
     "nfgs_iterate_cfcf_start": (C.c_int, [_P, C.c_int32, _DP, _DP]),
+    "nfgs_step_diagnostics": (C.c_int, [_P, _DP]),
+    "nfgs_iterate_fixed_point": (C.c_int, [_P, C.c_int32]),
     "nfgs_trace_field_lines": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int64, _DP,
                                          C.c_double, C.c_int32, _P, _P, _P, _P, _P, _P]),
     "nfgs_qmap_plane": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P, _P]),

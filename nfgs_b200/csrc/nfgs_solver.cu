@@ -11,6 +11,7 @@
 #include "nfgs_tc.cuh"
 #include "nfgs_stencil.cuh"
 #include "nfgs_stencil2.cuh"
+#include "nfgs_diag.cuh"
 #include "nfgs_metrics.cuh"
 #include "nfgs_soft.cuh"
 #include "nfgs_trace.cuh"
@@ -97,6 +98,11 @@ struct Handle {
     // current in use (jz_stable_alias)
     double* jz_stable = nullptr;
     int jz_stable_alias = 1;
+    // the last single step's state indices and relaxation factor, for the
+    // per-step diagnostics (record_iteration_diagnostics)
+    int diag_prev = 0, diag_cand = 1, diag_valid = 0;
+    int select_final = 0;      // stop_mode="fixed_point": the solution is the final state
+    double diag_mu = 1.0;
     double *bbg_d = nullptr;  // 3V FP64 background (kept for diagnostics)
     // storage-type constants
     void *bbg = nullptr, *bzobs_t = nullptr, *jzt_t = nullptr, *phiab_t = nullptr, *dphi_t = nullptr;
@@ -1700,6 +1706,8 @@ static int iterate_begin_t(Handle* h, const NfgsStop* stop) {
     h->launches += 2;
     h->init_zr = 0.0;
     h->iter_active = 1;
+    h->select_final = 0;
+    h->diag_valid = 0;
     h->advanced = 0;
     h->solution = -1;
     h->total_ms = 0.0f;
@@ -2090,6 +2098,155 @@ static int cfcf_start_t(Handle* h, int lateral_bc1, double* mean_out, double* ou
     return rc;
 }
 
+// Per-step diagnostics of record_iteration_diagnostics (nfgs_solver.py:
+// 6660-6681, 6806-6933) for the candidate of the last single step: built from
+// the state it came from (diag_prev) and the candidate (diag_cand), both
+// still in their buffers right after the step.  out[15] in the order of the
+// reference's dictionary: phi_update, az_update, phi_map_residual,
+// az_map_residual, h_k0_update, h_k0_map_residual, bcz_pde_residual,
+// jz_pde_residual, poloidal_pde_residual, toroidal_pde_residual,
+// mixed_row_residual, bottom_field_imprint, bottom_jz_imprint (relative),
+// alpha_clip_fraction, weak_field_floor_fraction.  Uses the export buffers
+// (B, J_z, face current) and FP64 scratch; the iteration state and the
+// sources awaiting the next step are untouched.
+template <typename T>
+static int step_diagnostics_t(Handle* h, double* out) {
+    if (!h->iter_active || !h->advanced || !h->diag_valid)
+        return fail(NFGS_ESTATE, "no single iteration step to diagnose (advance one step at a time)");
+    const Geo& g = h->g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz, nxi = nx - 2, nyi = ny - 2;
+    const long long P = g.P, V = g.V, PI = h->PI;
+    cudaStream_t s = h->s;
+    const int prev = h->diag_prev, cand = h->diag_cand;
+    const double mu = h->diag_mu;
+    const long long nbf = h->nb_face;
+    std::vector<double*> sc;
+    auto cleanup = [&]() { for (double* p : sc) release(h, p); };
+    auto get = [&](double** p, size_t n) -> int {
+        int r = alloc(h, p, n * 8);
+        if (r == NFGS_OK) sc.push_back(*p);
+        return r;
+    };
+    double *phs, *azs, *bcz, *jzs, *sb, *sj, *sphi, *saz, *t1, *t2, *pf, *pc, *pd;
+    int rc = NFGS_OK;
+    do {
+        if ((rc = get(&phs, V)) || (rc = get(&azs, V)) || (rc = get(&bcz, V)) || (rc = get(&jzs, V))) break;
+        if ((rc = get(&sb, V)) || (rc = get(&sj, V)) || (rc = get(&sphi, V)) || (rc = get(&saz, V))) break;
+        if ((rc = get(&t1, V)) || (rc = get(&t2, V))) break;
+        if ((rc = get(&pf, 5 * nbf)) || (rc = get(&pc, 2 * nbf)) || (rc = get(&pd, diag::NS * nbf))) break;
+    } while (0);
+    if (rc != NFGS_OK) { cleanup(); return rc; }
+    rc = [&]() -> int {
+        const unsigned nb = (unsigned)((V + 255) / 256);
+        // unrelaxed candidate and its Laplacians
+        diag::k_unrelaxed<T><<<nb, 256, 0, s>>>(g, (const T*)h->st.phi[cand], (const T*)h->st.phi[prev],
+                                                (const T*)h->st.az[cand], (const T*)h->st.az[prev], mu, phs, azs);
+        diag::k_laps<<<nb, 256, 0, s>>>(g, phs, azs, bcz, jzs);
+        CK(cudaGetLastError());
+        // sources and face fractions of the state the candidate came from
+        const double am = h->prm.alpha_max;
+        const double amax = (am > 0 && std::isfinite(am)) ? am : -1.0;
+        k_recon<T><<<h->sgrid, h->sblock, 0, s>>>(g, h->st, &h->consts[prev], nullptr, (const T*)h->bbg,
+                                                  (const T*)h->bzobs_t, (const T*)h->jzt_t, (T)h->hx, (T)h->hy,
+                                                  h->use_h, (T*)h->B, (T*)h->jz);
+        k_face<T><<<h->sgrid, h->sblock, 0, s>>>(g, nullptr, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz,
+                                                 h->box, (T)amax, (T)h->prm.weak_field_floor_b2, (T*)h->jpf,
+                                                 (T*)h->jb, pf, 0);
+        diag::k_face_counts<T><<<h->sgrid, h->sblock, 0, s>>>(g, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz,
+                                                              amax, h->prm.weak_field_floor_b2, pc);
+        SrcOpts o{h->stop.polarity_mask, h->prm.face_parallel_exact_jz, h->wx != nullptr};
+        diag::k_src_full<T><<<h->sgrid, h->sblock, 0, s>>>(g, (const T*)h->jpf, (const T*)h->jb, (const T*)h->jzt_t,
+                                                           (const T*)h->bzobs_t, o, (const T*)h->wx,
+                                                           (const T*)h->wy, (const T*)h->wz, sb, sj);
+        CK(cudaGetLastError());
+        // source_phi = idct2(dct2(S_B) / lambda), mean mode zero
+        TRY(dct2_d(h, sb, t1, t2, nz));
+        {
+            const double* lam = h->lamN;
+            CK(launch_map(V, s, [=] __device__(long long q) {
+                const long long m = q % P;
+                t1[q] = m == 0 ? 0.0 : t1[q] / lam[m];
+            }));
+        }
+        TRY(idct2_d(h, t1, sphi, t2, nz));
+        // source_az_rhs = -idst2(dst2(S_J interior) / lambda_D) on the interior
+        CK(cudaMemsetAsync(saz, 0, (size_t)V * 8, s));
+        if (nx >= 3 && ny >= 3) {
+            CK(launch_map((long long)nz * PI, s, [=] __device__(long long q) {
+                const long long k = q / PI, r = q % PI, j = r / nxi, i = r % nxi;
+                t1[q] = sj[k * P + (j + 1) * nx + (i + 1)];
+            }));
+            TRY(apply_x<double>(h, h->dstx, t1, nxi, PI, t2, nxi, PI, nyi, nxi, nxi, nz));
+            TRY(apply_y<double>(h, h->dsty, t2, nxi, PI, t1, nxi, PI, nyi, nyi, nxi, nz));
+            const double* lamD = h->lamD;
+            CK(launch_map((long long)nz * PI, s, [=] __device__(long long q) { t1[q] = -t1[q] / lamD[q % PI]; }));
+            TRY(apply_x<double>(h, h->idstx, t1, nxi, PI, t2, nxi, PI, nyi, nxi, nxi, nz));
+            TRY(apply_y<double>(h, h->idsty, t2, nxi, PI, t1, nxi, PI, nyi, nyi, nxi, nz));
+            CK(launch_map((long long)nz * PI, s, [=] __device__(long long q) {
+                const long long k = q / PI, r = q % PI, j = r / nxi, i = r % nxi;
+                saz[k * P + (j + 1) * nx + (i + 1)] = t1[q];
+            }));
+        }
+        // the candidate's field for the bottom imprints
+        k_recon<T><<<h->sgrid, h->sblock, 0, s>>>(g, h->st, &h->consts[cand], nullptr, (const T*)h->bbg,
+                                                  (const T*)h->bzobs_t, (const T*)h->jzt_t, (T)h->hx, (T)h->hy,
+                                                  h->use_h, (T*)h->B, (T*)h->jz);
+        diag::k_diag_sums<T><<<h->sgrid, h->sblock, 0, s>>>(
+            g, (const T*)h->st.phi[prev], (const T*)h->st.az[prev], (const T*)h->st.phi[cand],
+            (const T*)h->st.az[cand], phs, azs, bcz, jzs, sb, sj, sphi, saz,
+            h->prm.robin_weight > 0.0 ? h->dphi_tgt : nullptr, h->prm.robin_weight, (const T*)h->B,
+            (const T*)h->bbg, (const T*)h->jz, h->bx_obs, h->by_obs, h->bz_obs, h->jz_t, pd);
+        CK(cudaGetLastError());
+        h->launches += 9;
+        std::vector<double> hd((size_t)diag::NS * nbf), hc((size_t)2 * nbf);
+        CK(cudaMemcpyAsync(hd.data(), pd, hd.size() * 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(hc.data(), pc, hc.size() * 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        double S[diag::NS], C[2] = {0.0, 0.0};
+        for (int q = 0; q < diag::NS; ++q) {
+            double a = 0.0;
+            for (long long b = 0; b < nbf; ++b) a += hd[(size_t)q * nbf + b];
+            S[q] = a;
+        }
+        for (int q = 0; q < 2; ++q)
+            for (long long b = 0; b < nbf; ++b) C[q] += hc[(size_t)q * nbf + b];
+        // counts of each slice (rms = sqrt(sum / count), clamped at 1e-30)
+        const double nV = (double)V;
+        const double nbi = (double)((nz > 4) ? std::max(0, nz - 3) : std::max(0, nz - 2)) * (double)P;
+        const double njz = (double)std::max(0, nz - 2) * (double)P;
+        const double ntor = (double)std::max(0, nz - 2) * (double)std::max(0, nxi) * (double)std::max(0, nyi);
+        const double nmix = (double)P, nbot = 3.0 * (double)P, njb = (double)P;
+        auto rms = [](double sum, double n) { return n > 0 ? std::sqrt(sum / n) : 0.0; };
+        auto rel = [&](double num, double den, double n) { return rms(num, n) / std::max(rms(den, n), 1e-30); };
+        auto relop = [&](double num, std::initializer_list<double> terms, double n) {
+            double m = 0.0;
+            for (double t : terms) m = std::max(m, rms(t, n));
+            return rms(num, n) / std::max(m, 1e-30);
+        };
+        using namespace diag;
+        out[0] = rel(S[S_DPHI_U], S[S_PHI], nV);
+        out[1] = rel(S[S_DAZ_U], S[S_AZ], nV);
+        out[2] = rel(S[S_DPHI_M], S[S_PHI], nV);
+        out[3] = rel(S[S_DAZ_M], S[S_AZ], nV);
+        out[4] = 0.0;
+        out[5] = 0.0;
+        out[6] = rel(S[S_BCZ_R], S[S_SB_BI], nbi);
+        out[7] = rel(S[S_JZ_R], S[S_SJ_I], njz);
+        out[8] = relop(S[S_POL_R], {S[S_POL_D2], S[S_POL_LX], S[S_POL_SRC]}, nbi);
+        out[9] = relop(S[S_TOR_R], {S[S_TOR_D2], S[S_TOR_LX], S[S_TOR_SRC]}, ntor);
+        out[10] = relop(S[S_MIX_R], {S[S_MIX_PDE], S[S_MIX_DER], S[S_MIX_SRC]}, nmix);
+        out[11] = rel(S[S_BOT_E], S[S_BOT_O], nbot);
+        out[12] = rel(S[S_JZB_E], S[S_JZB_O], njb);
+        const double nfaces = (double)std::max(0, nz - 1) * (double)P;
+        out[13] = (am > 0 && std::isfinite(am) && nfaces > 0) ? C[1] / nfaces : 0.0;
+        out[14] = nfaces > 0 ? C[0] / nfaces : 0.0;
+        return NFGS_OK;
+    }();
+    cudaStreamSynchronize(s);
+    cleanup();
+    return rc;
+}
+
 // Capture the per-iteration launch sequence of a handle into its CUDA graph
 // (once per iterate call; the graph holds device-side indices only).
 template <typename T>
@@ -2129,6 +2286,10 @@ static int iterate_advance_t(Handle* h, int max_steps, int32_t* stop_reason, int
     int done = 0;
     while (!h->ctl_h->stopped && done < max_steps) {
         int k = std::min(h->stop.check_every, max_steps - done);
+        h->diag_prev = h->ctl_h->cur;
+        h->diag_cand = h->ctl_h->cand;
+        h->diag_mu = h->ctl_h->mu_cur;
+        h->diag_valid = (k == 1);
         if (h->stop.use_graph) {
             TRY(ensure_graph_t<T>(h));
             for (int q = 0; q < k; ++q) CK(cudaGraphLaunch(h->gexec, h->s));
@@ -2258,7 +2419,8 @@ static int iterate_end_t(Handle* h, NfgsIterResult* res, double* hist, int hist_
         if (n > 0) CK(cudaMemcpy(hist, h->hist, (size_t)n * NFGS_HCOLS * 8, cudaMemcpyDeviceToHost));
     }
     h->iter_active = 0;
-    h->solution = c.best;
+    h->solution = h->select_final ? c.cur : c.best;
+    h->select_final = 0;
     h->cur_host = c.cur;
     // final-vs-best relative B difference (nfgs_solver.py:3820-3824)
     if (c.cur != c.best) {
@@ -3186,6 +3348,36 @@ int nfgs_iterate_restart_from(void* handle, const void* phi, const void* az, int
     if (!h || !out3 || (mode != 4 && (!phi || !az))) return fail(NFGS_EINVAL, "null argument");
     if (mode < 0 || mode > 4) return fail(NFGS_EINVAL, "mode must be 0 to 4");
     return h->f32 ? restart_from_t<float>(h, phi, az, mode, out3) : restart_from_t<double>(h, phi, az, mode, out3);
+}
+
+__global__ void k_ctl_force_stop(DevCtl* c, int reason) {
+    if (!c->stopped) {
+        c->stopped = 1;
+        c->stop_reason = reason;
+    }
+}
+
+int nfgs_iterate_fixed_point(void* handle, int32_t stop_now) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h) return fail(NFGS_EINVAL, "null argument");
+    if (cudaSetDevice(h->geom.device) != cudaSuccess) return fail(NFGS_ECUDA, "cudaSetDevice failed");
+    if (!h->iter_active) return fail(NFGS_ESTATE, "iterate_begin() has not been called");
+    h->select_final = 1;
+    if (stop_now) {
+        k_ctl_force_stop<<<1, 1, 0, h->s>>>(h->ctl, NFGS_STOP_FIXED_POINT);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(h->s));
+    }
+    return NFGS_OK;
+}
+
+int nfgs_step_diagnostics(void* handle, double* out15) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h || !out15) return fail(NFGS_EINVAL, "null argument");
+    if (cudaSetDevice(h->geom.device) != cudaSuccess) return fail(NFGS_ECUDA, "cudaSetDevice failed");
+    return h->f32 ? step_diagnostics_t<float>(h, out15) : step_diagnostics_t<double>(h, out15);
 }
 
 int nfgs_iterate_cfcf_start(void* handle, int32_t lateral_bc1, double* mean_bcz_out, double* out2) {

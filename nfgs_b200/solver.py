@@ -208,8 +208,6 @@ class NFGSSolverGPU:
             unsupported.append("poloidal_update_mode='two_stage'")
         if vco != "staggered_face":
             unsupported.append("vertical_current_operator='collocated_centered'")
-        if record:
-            unsupported.append("record_iteration_diagnostics=True")
         # --- Stable-NFPT / base keywords (nfgs_solver.py:2910-2965, 736-937)
         alpha_limit_factor = kw.pop("alpha_limit_factor", 1.0)
         bottom_jperp_zero = bool(kw.pop("bottom_jperp_zero", True))
@@ -629,17 +627,24 @@ class NFGSSolverGPU:
         max_iter = int(max_iter)
         use_imp = sigma_improvement_tol is not None and float(sigma_improvement_tol) > 0.0
         eps = float(sigma_improvement_tol) if use_imp else 0.0
-        step_by_step = per_step_callback is not None or verbose
+        record = bool(self.record_iteration_diagnostics)
+        fixed = stop_mode == "fixed_point"
+        step_by_step = per_step_callback is not None or verbose or record
+        # the fixed-point mode replaces the sigma_best stop rules (nfgs_solver.py:3777-3812):
+        # on the device only max_iter and the rollback limit remain
         stop = L.NfgsStop(
-            max_iter=max_iter, patience=int(patience), tol=float(tol), mu=float(mu),
-            sigma_improvement_tol=eps if use_imp else -1.0, polarity_mask=_POLARITY[polarity_mask],
+            max_iter=max_iter, patience=0 if fixed else int(patience), tol=-1.0 if fixed else float(tol),
+            mu=float(mu),
+            sigma_improvement_tol=eps if (use_imp and not fixed) else -1.0, polarity_mask=_POLARITY[polarity_mask],
             adaptive_mu=int(bool(adaptive_mu)), mu_min=float(mu_min), mu_max=float(mu_max),
             mu_backoff=float(mu_backoff), mu_growth=float(mu_growth), growth_streak=int(growth_streak),
             max_rollbacks=int(max_rollbacks), divergence_factor=float(divergence_factor),
-            check_every=1 if per_step_callback is not None else max(1, int(check_every)),
+            check_every=1 if (per_step_callback is not None or record) else max(1, int(check_every)),
             use_graph=int(bool(use_graph)))
         lib = self._lib
         L.check(lib.nfgs_iterate_begin(self._h, L.C.byref(stop)))
+        if fixed:
+            L.check(lib.nfgs_iterate_fixed_point(self._h, 0))
         self._init_diagnostics = {"init_mode": "gs_cfcf", "mfr_count": 0,
                                   "gaussian_separation": self.gaussian_separation_diagnostics,
                                   "coupled_k0": self._k0_diagnostics}
@@ -660,6 +665,7 @@ class NFGSSolverGPU:
             print(f"Initial  sigma={sc[0]:.4e}  divB={sc[1]:.4e}  E={sc[2]:.4e} "
                   f"(mu0={mu}, adaptive={adaptive_mu}, alpha_max={am_text}, toroidal_bc=True)")
         return dict(lib=lib, mode=mode, verbose=verbose, per_step_callback=per_step_callback, step_by_step=step_by_step,
+                    record=record, diag_rows=[], fp_met=[], fp_streak=0, fp_converged=False,
                     check_every=check_every, max_iter=max_iter, stop_mode=stop_mode, update_tol=update_tol,
                     observable_tol=observable_tol, fixed_point_pde_tol=fixed_point_pde_tol,
                     fixed_point_patience=fixed_point_patience, eps=eps, use_imp=use_imp)
@@ -703,9 +709,16 @@ class NFGSSolverGPU:
         rows_seen = 0
         reason = L.C.c_int32(0)
         ndone = L.C.c_int32(0)
+        record = ctx.get("record", False)
         while True:
-            steps = 1 if per_step_callback is not None else max(1, int(check_every))
+            steps = 1 if (per_step_callback is not None or record) else max(1, int(check_every))
             L.check(lib.nfgs_iterate_advance(self._h, steps, L.C.byref(reason), L.C.byref(ndone)))
+            if record:
+                tot = L.C.c_int32(0)
+                L.check(lib.nfgs_get_history(self._h, 0, 0, None, L.C.byref(tot)))
+                if tot.value > len(ctx["diag_rows"]):
+                    if self._record_step(ctx, tot.value):
+                        break
             if step_by_step:
                 tot = L.C.c_int32(0)
                 L.check(lib.nfgs_get_history(self._h, 0, 0, None, L.C.byref(tot)))
@@ -726,6 +739,43 @@ class NFGSSolverGPU:
                             print(f"Iter {n:4d} | sigma={r[0]:.4e} DIVERGED -> rollback, mu={r[3]:.3f}")
             if reason.value != 0:
                 break
+
+    _DIAG_KEYS = ("phi_update_relative", "az_update_relative", "phi_map_residual_relative",
+                  "az_map_residual_relative", "h_k0_update_relative", "h_k0_map_residual_relative",
+                  "bcz_pde_residual_relative", "jz_pde_residual_relative", "poloidal_pde_residual_relative",
+                  "toroidal_pde_residual_relative", "mixed_row_residual_relative", "bottom_field_imprint_relative",
+                  "bottom_jz_imprint_relative", "alpha_clip_fraction", "weak_field_floor_fraction")
+
+    def _record_step(self, ctx, rows):
+        """One step of record_iteration_diagnostics: the device diagnostics of
+        the attempted candidate (nfgs_solver.py:6806-6933) and the fixed-point
+        criteria of an accepted step (nfgs_solver.py:3707-3735, 3764-3776).
+        Returns True when the fixed-point stop is reached."""
+        out = np.zeros(L.NFGS_NSTEPDIAG)
+        L.check(self._lib.nfgs_step_diagnostics(self._h, L.dptr(out)))
+        d = {k: float(v) for k, v in zip(self._DIAG_KEYS, out)}
+        ctx["diag_rows"].append(d)
+        row = np.zeros((1, L.NFGS_HIST_COLS))
+        tot = L.C.c_int32(0)
+        L.check(self._lib.nfgs_get_history(self._h, rows - 1, 1, L.dptr(row), L.C.byref(tot)))
+        src, erc, rollback = float(row[0, 5]), float(row[0, 6]), int(row[0, 4])
+        if rollback:
+            ctx["fp_met"].append(0)
+            ctx["fp_streak"] = 0
+            return False
+        map_res = max(d["phi_map_residual_relative"], d["az_map_residual_relative"], d["h_k0_map_residual_relative"])
+        pde_res = max(d["poloidal_pde_residual_relative"], d["toroidal_pde_residual_relative"],
+                      d["mixed_row_residual_relative"])
+        met = (ctx["stop_mode"] == "fixed_point" and math.isfinite(map_res) and math.isfinite(pde_res)
+               and map_res <= ctx["update_tol"] and pde_res <= float(ctx["fixed_point_pde_tol"])
+               and src <= ctx["observable_tol"] and erc <= ctx["observable_tol"])
+        ctx["fp_met"].append(int(met))
+        ctx["fp_streak"] = ctx["fp_streak"] + 1 if met else 0
+        if ctx["stop_mode"] == "fixed_point" and ctx["fp_streak"] >= int(ctx["fixed_point_patience"]):
+            ctx["fp_converged"] = True
+            L.check(self._lib.nfgs_iterate_fixed_point(self._h, 1))
+            return True
+        return False
 
     def _iterate_finish(self, ctx):
         lib, verbose, max_iter, stop_mode = ctx["lib"], ctx["verbose"], ctx["max_iter"], ctx["stop_mode"]
@@ -769,18 +819,19 @@ class NFGSSolverGPU:
             "rollback": [int(v) for v in hist[:, 4]],
             "sigma_relative_change": [float(v) for v in hist[:, 5]],
             "energy_relative_change": [float(v) for v in hist[:, 6]],
-            "fixed_point_criteria_met": [0] * n,
+            "fixed_point_criteria_met": (list(ctx["fp_met"][:n]) + [0] * max(0, n - len(ctx["fp_met"]))
+                                         if ctx.get("record") else [0] * n),
             "best_sigma": float(res.best_sigma),
             "best_iter": int(res.best_iter),
             "rollbacks": int(res.rollbacks),
             "stop_reason": stop_reason,
             "stop_mode": stop_mode,
-            "selected_state": "best_sigma",
+            "selected_state": "final_accepted_iterate" if stop_mode == "fixed_point" else "best_sigma",
             "final_iter": int(res.final_iter),
             "final_sigma": float(res.final_sigma),
             "final_vs_best_B_relative": float(res.final_vs_best_B_relative),
-            "fixed_point_converged": False,
-            "fixed_point_streak": 0,
+            "fixed_point_converged": bool(ctx.get("fp_converged", False)),
+            "fixed_point_streak": int(ctx.get("fp_streak", 0)),
             "fixed_point_tolerances": {"update": update_tol, "pde": float(fixed_point_pde_tol),
                                        "observable": observable_tol, "patience": int(fixed_point_patience)},
             "sigma_improvement_tol": eps if use_imp else None,
@@ -798,6 +849,19 @@ class NFGSSolverGPU:
             "device_ms": float(res.device_ms), "kernel_launches": int(res.kernel_launches),
             "learned_start": self.learned_start_info,
         }
+        if ctx.get("record"):
+            rows = ctx["diag_rows"][:n]
+            for key in (sorted(rows[0]) if rows else []):
+                history[key] = [float(r[key]) for r in rows]
+            history["iteration_diagnostics_definition"] = {
+                "state": "the candidate each step proposed (before acceptance); history.rollback marks rejected ones",
+                "map_residual": "RMS of the unrelaxed map T(x_n) - x_n over the RMS of x_n",
+                "pde_scope": "interior rows of the scalar poloidal / toroidal equations; the mixed first interior "
+                             "row on its own",
+                "relative_norm": "RMS residual over the largest RMS of the operator and source terms",
+                "weak_field_floor_B2": self.weak_field_floor_b2,
+                "alpha_clip_scale": self.alpha_clip_scale,
+            }
         history["source_diagnostics"] = self.compute_source_diagnostics()
         return history
 

@@ -331,11 +331,13 @@ class OracleNFGS:
                  bottom_parallel_current_mode="observed_full",
                  user_supplied_open_bz=None, user_supplied_horizontal_field=None,
                  external_potential_field=None, soft_cfcf_epsilon=None, soft_cfcf_normal_ridge=0.0,
-                 lateral_wall="paper_bc1"):
+                 lateral_wall="paper_bc1", record_iteration_diagnostics=False):
         ix, iy, iz = int(Nx), int(Ny), int(Nz)
         # the wall condition of the Stable-NFPT field behind the cfcf start
         # (nfgs_solver.py:845-853, 2161-2170)
         self.lateral_bc1 = str(lateral_wall).lower().replace("-", "_") in ("bc1", "paper_bc1", "paper")
+        self.record_iteration_diagnostics = bool(record_iteration_diagnostics)
+        self.last_iteration_diagnostics = {}
         mode = str(calculation_domain_mode).lower().replace("-", "_")
         # nfgs_solver.py:771-819
         if pad_calculation_domain:
@@ -1201,8 +1203,92 @@ class OracleNFGS:
         B, J, Bc = self.reconstruct(phi, az, bcz)
         return B, J, phi, az, Bc
 
+    def face_fractions(self, B, J):
+        """Weak-field and alpha-clip fractions of the face state
+        (nfgs_solver.py:6660-6681): means over every vertical face."""
+        Bf, Jf = self.face_state(B, J[2])
+        b2 = (Bf * Bf).sum(0)
+        weak = float(np.mean(b2 <= self.weak_floor))
+        alpha = (Jf * Bf).sum(0) / np.maximum(b2, self.weak_floor)
+        am = self.alpha_max()
+        clip = float(np.mean(np.abs(alpha) > am)) if am is not None else 0.0
+        return clip, weak
+
+    @staticmethod
+    def _rms(v):
+        return float(np.sqrt(np.mean(np.asarray(v, dtype=np.float64) ** 2)))
+
+    def d2dz2(self, f):
+        """nfgs_solver.py:1717-1727."""
+        dz2 = self.dz ** 2
+        d2 = np.zeros_like(f)
+        if f.shape[0] >= 3:
+            d2[1:-1] = (f[2:] - 2 * f[1:-1] + f[:-2]) / dz2
+        if f.shape[0] >= 2:
+            if f.shape[0] >= 4:
+                d2[0] = (2.0 * f[0] - 5.0 * f[1] + 4.0 * f[2] - f[3]) / dz2
+            else:
+                d2[0] = (f[1] - f[0]) / dz2
+            d2[-1] = (-2.0 * f[-1] + 2.0 * f[-2]) / dz2
+        return d2
+
+    def step_diagnostics(self, phi, az, phi_s, az_s, s_b, s_j, phi_n, az_n, Bn, Jn, clip, weak):
+        """The per-step diagnostics of record_iteration_diagnostics
+        (nfgs_solver.py:6806-6929) for one attempted candidate."""
+        rms = self._rms
+
+        def rel(delta, scale):
+            return rms(delta) / max(rms(scale), 1e-30)
+
+        def rel_op(residual, *terms):
+            return rms(residual) / max(max(rms(t) for t in terms), 1e-30)
+
+        nz = self.Nz
+        lx = lambda f: lap_xy(f, self.dx, self.dy)  # noqa: E731
+        bcz_s = lx(phi_s)
+        bcz_res = self.d2dz2(bcz_s) + lx(bcz_s) - s_b
+        jz_s = -lx(az_s)
+        jz_res = self.d2dz2(jz_s) + lx(jz_s) - s_j
+        bi = slice(2, -1) if nz > 4 else slice(1, -1)
+        lam = self.lam_neumann().copy()
+        lam[0, 0] = 1.0
+        sp_hat = dct2(s_b) / lam[None]
+        sp_hat[:, 0, 0] = 0.0
+        source_phi = idct2(sp_hat)
+        d2p, lxp = self.d2dz2(phi_s), lx(phi_s)
+        phi_res = d2p + lxp - source_phi
+        source_az = np.zeros_like(az_s)
+        source_az[:, 1:-1, 1:-1] = idst2(-dst2(s_j[:, 1:-1, 1:-1]) / self.lam_dirichlet()[None])
+        d2a, lxa = self.d2dz2(az_s), lx(az_s)
+        az_res = d2a + lxa - source_az
+        dphi_bottom = (-3.0 * phi_s[0] + 4.0 * phi_s[1] - phi_s[2]) / (2.0 * self.dz)
+        target = self.bottom_dphi_c_target if self.bottom_dphi_c_target is not None else np.zeros_like(dphi_bottom)
+        mixed_pde = (1.0 - self.rho) * phi_res[1]
+        mixed_der = -self.rho * (dphi_bottom - target) / self.dz
+        obs = np.stack([self.Bx_obs, self.By_obs, self.Bz_obs])
+        ii = (slice(1, -1), slice(1, -1), slice(1, -1))
+        return {
+            "phi_update_relative": rel(phi_n - phi, phi),
+            "az_update_relative": rel(az_n - az, az),
+            "phi_map_residual_relative": rel(phi_s - phi, phi),
+            "az_map_residual_relative": rel(az_s - az, az),
+            "h_k0_update_relative": 0.0,
+            "h_k0_map_residual_relative": 0.0,
+            "bcz_pde_residual_relative": rel(bcz_res[bi], s_b[bi]),
+            "jz_pde_residual_relative": rel(jz_res[1:-1], s_j[1:-1]),
+            "poloidal_pde_residual_relative": rel_op(phi_res[bi], d2p[bi], lxp[bi], source_phi[bi]),
+            "toroidal_pde_residual_relative": rel_op(az_res[ii], d2a[ii], lxa[ii], source_az[ii]),
+            "mixed_row_residual_relative": rel_op(mixed_pde + mixed_der, mixed_pde, mixed_der, source_phi[1]),
+            "bottom_field_imprint_relative": rel(Bn[:, 0] - obs, obs),
+            "bottom_jz_imprint_relative": rel(Jn[2, 0] - self.Jz_T, self.Jz_T),
+            "alpha_clip_fraction": clip,
+            "weak_field_floor_fraction": weak,
+        }
+
     def iteration_step(self, B, J, phi, az, Bc, mu=1.0, polarity_mask="both"):
         """NFGS NFPT update (nfgs_solver.py:6647-6935, production branch)."""
+        if self.record_iteration_diagnostics:
+            clip, weak = self.face_fractions(B, J)
         jp = self.parallel_current(J, B)
         if polarity_mask == "positive":
             jp[:, 0] = J[:, 0] * (self.Bz_obs > 0)
@@ -1238,18 +1324,35 @@ class OracleNFGS:
         az_n[-1] = 0.0
         self._az_walls_zero(az_n)
         Bn, Jn, Bcn = self.reconstruct(phi_n, az_n, bcz)
+        if self.record_iteration_diagnostics:
+            self.last_iteration_diagnostics = self.step_diagnostics(
+                phi, az, phi_s, az_s, s_b, s_j, phi_n, az_n, Bn, Jn, clip, weak)
         return Bn, Jn, phi_n, az_n, Bcn
 
     def iterate(self, max_iter=200, tol=1e-5, mu=1.0, patience=1, verbose=False,
                 polarity_mask="both", init_mode="gs_cfcf", sigma_improvement_tol=1e-5,
                 per_step_callback: Optional[Callable] = None, *, adaptive_mu=False,
                 mu_min=0.02, mu_max=1.0, mu_backoff=0.5, mu_growth=1.1, growth_streak=5,
-                divergence_factor=2.0, max_rollbacks=12, stop_mode="sigma_best", **_ignored):
-        """Stable driver (nfgs_solver.py:3522-3850) with the NFGS wrapper (6937-7009)."""
+                divergence_factor=2.0, max_rollbacks=12, stop_mode="sigma_best",
+                fixed_point_update_tol=None, fixed_point_pde_tol=1.0e-8, fixed_point_observable_tol=None,
+                fixed_point_patience=10, **_ignored):
+        """Stable driver (nfgs_solver.py:3522-3850) with the NFGS wrapper (6937-7009),
+        including the fixed-point stop (nfgs_solver.py:3572-3584, 3707-3776) and the
+        per-step diagnostics history (nfgs_solver.py:6962-6990)."""
         if str(init_mode).lower().replace("-", "_") not in ("gs_cfcf", "soft_cfcf", "yi_soft", "cfcf", "curl_free_current"):
             raise NotImplementedError("the oracle restates the gs_cfcf and soft_cfcf starts")
-        if stop_mode != "sigma_best":
+        stop_mode = str(stop_mode).lower().replace("-", "_")
+        if stop_mode not in ("sigma_best", "fixed_point"):
+            raise ValueError("stop_mode must be 'sigma_best' or 'fixed_point'")
+        if stop_mode == "fixed_point" and not self.record_iteration_diagnostics:
             raise ValueError("stop_mode='fixed_point' requires record_iteration_diagnostics=True")
+        update_tol = float(tol if fixed_point_update_tol is None else fixed_point_update_tol)
+        pde_tol = float(fixed_point_pde_tol)
+        observable_tol = float(tol if fixed_point_observable_tol is None else fixed_point_observable_tol)
+        fixed_required = int(fixed_point_patience)
+        fp_streak = 0
+        fp_converged = False
+        diag_rows = []
         B, J, phi, az, Bc = self.compute_initial_conditions(init_mode)
         sigma0, divb0, e0 = self.compute_sigma(B, J), self.compute_divB(B), self.compute_energy(B)
         hist = {k: [] for k in ("sigma", "divB", "energy", "mu", "rollback", "sigma_relative_change",
@@ -1267,6 +1370,8 @@ class OracleNFGS:
         final_iter = 0
         for n in range(1, max_iter + 1):
             Bn, Jn, phin, azn, Bcn = self.iteration_step(B, J, phi, az, Bc, mu=mu_cur, polarity_mask=polarity_mask)
+            if self.record_iteration_diagnostics:
+                diag_rows.append(dict(self.last_iteration_diagnostics))
             sigma = self.compute_sigma(Bn, Jn)
             diverged = (not math.isfinite(sigma)) or sigma > divergence_factor * max(best_sigma, 1e-30)
             if adaptive_mu and diverged:
@@ -1282,6 +1387,7 @@ class OracleNFGS:
                 hist["sigma_relative_change"].append(float("nan"))
                 hist["energy_relative_change"].append(float("nan"))
                 hist["fixed_point_criteria_met"].append(0)
+                fp_streak = 0
                 if rollbacks >= max_rollbacks:
                     stop = "max_rollbacks"
                     break
@@ -1298,7 +1404,16 @@ class OracleNFGS:
             hist["rollback"].append(0)
             hist["sigma_relative_change"].append(src)
             hist["energy_relative_change"].append(erc)
-            hist["fixed_point_criteria_met"].append(0)
+            d = self.last_iteration_diagnostics if self.record_iteration_diagnostics else {}
+            map_res = max(d.get("phi_map_residual_relative", math.inf), d.get("az_map_residual_relative", math.inf),
+                          d.get("h_k0_map_residual_relative", 0.0))
+            pde_res = max(d.get("poloidal_pde_residual_relative", math.inf),
+                          d.get("toroidal_pde_residual_relative", math.inf), d.get("mixed_row_residual_relative", 0.0))
+            met = (stop_mode == "fixed_point" and math.isfinite(map_res) and math.isfinite(pde_res)
+                   and map_res <= update_tol and pde_res <= pde_tol and src <= observable_tol
+                   and erc <= observable_tol)
+            hist["fixed_point_criteria_met"].append(int(met))
+            fp_streak = fp_streak + 1 if met else 0
             final_iter = n
             if per_step_callback is not None:
                 per_step_callback(n, sigma, B, J)
@@ -1317,23 +1432,30 @@ class OracleNFGS:
             else:
                 stall += 1
                 streak = 0
-            if sigma < tol:
+            if stop_mode == "fixed_point" and fp_streak >= fixed_required:
+                stop = "fixed_point"
+                fp_converged = True
+                break
+            if stop_mode == "sigma_best" and sigma < tol:
                 stop = "tol"
                 break
-            if use_imp and flat >= flat_req:
+            if stop_mode == "sigma_best" and use_imp and flat >= flat_req:
                 stop = "sigma_improvement_tol"
                 break
-            if patience > 0 and stall >= patience:
+            if stop_mode == "sigma_best" and patience > 0 and stall >= patience:
                 stop = "sigma_stall"
                 break
         final = (B, J, phi, az, Bc)
-        self._B, self._J, self._Phi_c, self._Az = best[0], best[1], best[2], best[3]
+        sel = final if stop_mode == "fixed_point" else best
+        self._B, self._J, self._Phi_c, self._Az = sel[0], sel[1], sel[2], sel[3]
         fvb = math.sqrt(np.mean((final[0] - best[0]) ** 2)) / max(math.sqrt(np.mean(best[0] ** 2)), 1e-30)
         hist.update({
             "best_sigma": best_sigma, "best_iter": best_iter, "rollbacks": rollbacks,
-            "stop_reason": stop, "stop_mode": stop_mode, "selected_state": "best_sigma",
+            "stop_reason": stop, "stop_mode": stop_mode,
+            "selected_state": "final_accepted_iterate" if stop_mode == "fixed_point" else "best_sigma",
             "final_iter": final_iter, "final_sigma": self.compute_sigma(final[0], final[1]),
-            "final_vs_best_B_relative": fvb, "fixed_point_converged": False,
+            "final_vs_best_B_relative": fvb, "fixed_point_converged": fp_converged,
+            "fixed_point_streak": fp_streak,
             "sigma_improvement_tol": eps if use_imp else None,
             "auto_rbsl_improvement_grace": 0, "last_sigma_improvement": last_imp,
             "source_partition_mode": "gaussian_separated",
@@ -1342,6 +1464,10 @@ class OracleNFGS:
             "sigma_placement": "vertical_faces",
             "initial_sigma": sigma0, "initial_divB": divb0, "initial_energy": e0,
         })
+        if self.record_iteration_diagnostics:
+            rows = diag_rows[:len(hist["sigma"])]
+            for key in (sorted(rows[0]) if rows else []):
+                hist[key] = [float(r[key]) for r in rows]
         hist["source_diagnostics"] = self.compute_source_diagnostics()
         return hist
 
