@@ -38,6 +38,8 @@ extern "C" {
 /* enumerations of reference string options */
 #define NFGS_HZM_OMIT 0                    /* horizontal_zero_mode_policy="omit" */
 #define NFGS_HZM_FROZEN_LINEAR_HARMONIC 1  /* "frozen_linear_harmonic" (default) */
+#define NFGS_HZM_COUPLED_K0 2              /* "coupled_k0" (nfgs_solver.py:5058-5431) */
+#define NFGS_HZM_CONSTRAINED_SPLINE 3      /* "constrained_spline_harmonic" (nfgs_solver.py:5099-5260) */
 #define NFGS_MEANBZ_UNIFORM_OPEN 0
 #define NFGS_MEANBZ_REQUIRE_BALANCED 1
 #define NFGS_MEANBZ_USER_SUPPLIED 2
@@ -93,6 +95,13 @@ typedef struct NfgsParams {
     int32_t face_parallel_exact_jz;/* bottom_parallel_current_mode */
     int32_t buffer_thickness;      /* 0: no window */
     int32_t buffer_xy_only;
+    /* k_h=0 closures (NFGS_HZM_COUPLED_K0, NFGS_HZM_CONSTRAINED_SPLINE) */
+    double k0_smoothness;          /* k0_ode_smoothness (>= 0) */
+    double k0_update_mu;           /* k0_update_mu in (0, 1]; <= 0: the step's scalar mu */
+    int32_t k0_spline_basis;       /* k0_spline_basis_size (4 <= n <= nz) */
+    int32_t k0_legacy;             /* coupled_k0_discretization="legacy_plane_centred" */
+    int32_t k0_face_target;        /* k0_current_target_placement="face" */
+    int32_t k0_reserved;
 } NfgsParams;
 
 /* set_bottom_vector_boundary keywords (nfgs_solver.py:4661, 2000-2113). */
@@ -374,6 +383,31 @@ int nfgs_step_diagnostics(void* handle, double* out15);
  * state; stop_now != 0 also ends the iteration with NFGS_STOP_FIXED_POINT
  * (the host decides the fixed point from the step diagnostics). */
 int nfgs_iterate_fixed_point(void* handle, int32_t stop_now);
+
+/* State of the k_h=0 closure (coupled_k0, constrained_spline_harmonic):
+ * the horizontally uniform field H(z) = (H_x, H_y) by plane that the next
+ * start state carries (the selected state's after iterate, the target
+ * constant after set_boundary; nfgs_solver.py:5058-5097, 6991-7004), and
+ * the last update's fit (nfgs_solver.py:5952-6067).  Layout, nz planes:
+ *   out[0 .. 2nz)    H of the selected state (x then y)
+ *   out[2nz .. 4nz)  last fitted profile H* (before the k0_update_mu blend)
+ *   out[4nz .. 6nz)  last target mean current (mean J_x, mean J_y) by plane
+ *   out[6nz]         running maximum of the relative fit residual
+ *   out[6nz + 1]     2-norm condition number of the spline KKT matrix (NaN
+ *                    for coupled_k0)
+ *   out[6nz + 2]     number of updates since iterate_begin
+ * n >= 6nz + 3.  NFGS_EUNSUPPORTED for the other horizontal policies. */
+#define NFGS_K0_EXTRA 3
+int nfgs_k0_state(void* handle, double* out, int32_t n);
+
+/* The k_h=0 closure's fit as a linear map, host only (no device needed):
+ * profile = G q + m h0 for a target mean current q by plane and bottom
+ * value h0, G row-major nz x nz, m of length nz.  spline != 0 selects
+ * constrained_spline_harmonic (basis n_basis), else coupled_k0 (legacy != 0:
+ * "legacy_plane_centred").  cond_out: the spline KKT matrix's 2-norm
+ * condition number, NaN for coupled_k0 (nfgs_solver.py:5149-5404). */
+int nfgs_k0_operator(int32_t nz, double dz, int32_t spline, int32_t legacy, int32_t n_basis, double smoothness,
+                     double* G, double* m, double* cond_out);
 
 /* ------------------------------------------------------------------------
  * Evaluation metrics of a solution on a region of interest, in one FP64-

@@ -56,7 +56,10 @@ class NfgsParams(C.Structure):
                 ("horizontal_zero_mode", C.c_int32), ("mean_bz_policy", C.c_int32),
                 ("d0_policy", C.c_int32), ("source_policy", C.c_int32), ("harmonic_policy", C.c_int32),
                 ("gaussian_spectral", C.c_int32), ("face_parallel_exact_jz", C.c_int32),
-                ("buffer_thickness", C.c_int32), ("buffer_xy_only", C.c_int32)]
+                ("buffer_thickness", C.c_int32), ("buffer_xy_only", C.c_int32),
+                ("k0_smoothness", C.c_double), ("k0_update_mu", C.c_double),
+                ("k0_spline_basis", C.c_int32), ("k0_legacy", C.c_int32),
+                ("k0_face_target", C.c_int32), ("k0_reserved", C.c_int32)]
 
 
 class NfgsBoundaryOpts(C.Structure):
@@ -124,6 +127,9 @@ SIGNATURES = {
     "nfgs_iterate_cfcf_start": (C.c_int, [_P, C.c_int32, _DP, _DP]),
     "nfgs_step_diagnostics": (C.c_int, [_P, _DP]),
     "nfgs_iterate_fixed_point": (C.c_int, [_P, C.c_int32]),
+    "nfgs_k0_state": (C.c_int, [_P, _DP, C.c_int32]),
+    "nfgs_k0_operator": (C.c_int, [C.c_int32, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_double, _DP, _DP,
+                                   _DP]),
     "nfgs_trace_field_lines": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int64, _DP,
                                          C.c_double, C.c_int32, _P, _P, _P, _P, _P, _P]),
     "nfgs_qmap_plane": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P, _P]),

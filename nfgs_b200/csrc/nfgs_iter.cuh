@@ -44,12 +44,20 @@ __device__ __forceinline__ T lap1(F f, int i, int n) {
 // J_z = -lap_xy A_z with zero walls/top and J_z(0) = Jz_T.  The carrier is
 // formed directly: the reference forms it as (B_bg + B_c + H) - B_bg
 // (nfgs_solver.py:5759), which in FP32 cancels where B_c << B_bg.
+//
+// With a k_h=0 closure (hk3 != null) H is the selected buffer's profile by
+// plane, which block (0, 0, k) also copies to hsel for the kernels that
+// follow; with the constrained spline the state J_z is the face average
+// mapped back to the planes (nfgs_solver.py:5915-5935: all three current
+// components come from the face current there).
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(128) k_recon(Geo g, StateTab st, const int* sel, const int* skip,
                                                const T* __restrict__ bbg, const T* __restrict__ bzobs,
                                                const T* __restrict__ jzt, T hx, T hy, int use_h,
-                                               T* __restrict__ Bout, T* __restrict__ jzout) {
+                                               T* __restrict__ Bout, T* __restrict__ jzout,
+                                               const double* __restrict__ hk3 = nullptr,
+                                               double* __restrict__ hsel = nullptr, int spline = 0) {
     if (skip != nullptr && *skip) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -77,16 +85,36 @@ __global__ void __launch_bounds__(128) k_recon(Geo g, StateTab st, const int* se
     T bcz = lap1<T>([&](int q) { return PH(k, j, q); }, i, nx) * idx2 +
             lap1<T>([&](int q) { return PH(k, q, i); }, j, ny) * idy2;
     T cx = bcx, cy = bcy, cz = bcz;
-    if (use_h) { cx = cx + hx; cy = cy + hy; }
+    if (hk3 != nullptr) {
+        const double* hp = hk3 + (long long)(*sel) * 2 * nz;
+        cx = cx + (T)hp[k];
+        cy = cy + (T)hp[nz + k];
+        if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+            hsel[k] = hp[k];
+            hsel[nz + k] = hp[nz + k];
+        }
+    } else if (use_h) {
+        cx = cx + hx;
+        cy = cy + hy;
+    }
     if (k == 0) cz = ldg(bzobs, (long long)j * nx + i) - ldg(bbg, 2 * g.V + c);
     Bout[c] = cx;
     Bout[g.V + c] = cy;
     Bout[2 * g.V + c] = cz;
-    T jz;
-    if (k == 0) jz = ldg(jzt, (long long)j * nx + i);
-    else if (k == nz - 1 || i == 0 || i == nx - 1 || j == 0 || j == ny - 1) jz = T(0);
-    else jz = -(lap1<T>([&](int q) { return AZ(k, j, q); }, i, nx) * idx2 +
-                lap1<T>([&](int q) { return AZ(k, q, i); }, j, ny) * idy2);
+    const bool wall = i == 0 || i == nx - 1 || j == 0 || j == ny - 1;
+    // state J_z of plane kk: J_z(0) = Jz_T, zero walls and top, -lap_xy A_z
+    auto jzp = [&](int kk) -> T {
+        if (kk == 0) return ldg(jzt, (long long)j * nx + i);
+        if (kk == nz - 1 || wall) return T(0);
+        return -(lap1<T>([&](int q) { return AZ(kk, j, q); }, i, nx) * idx2 +
+                 lap1<T>([&](int q) { return AZ(kk, q, i); }, j, ny) * idy2);
+    };
+    T jz = jzp(k);
+    if (spline && k >= 1 && k <= nz - 2 && !wall) {
+        const T f0 = T(0.5) * (jz + jzp(k - 1));
+        const T f1 = T(0.5) * (jzp(k + 1) + jz);
+        jz = T(0.5) * (f0 + f1);
+    }
     jzout[c] = jz;
 }
 
@@ -100,7 +128,8 @@ template <typename T>
 __global__ void __launch_bounds__(128) k_face(Geo g, const int* skip, const T* __restrict__ B,
                                               const T* __restrict__ bbg, const T* __restrict__ jz, Box box,
                                               T alpha_max, T floor_b2, T* __restrict__ jpf,
-                                              T* __restrict__ jb, double* __restrict__ partials, int raw_j) {
+                                              T* __restrict__ jb, double* __restrict__ partials, int raw_j,
+                                              const double* __restrict__ jh_wall = nullptr) {
     __shared__ double sh[NFGS_NRED * 32];
     if (skip != nullptr && *skip) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -174,9 +203,22 @@ __global__ void __launch_bounds__(128) k_face(Geo g, const int* skip, const T* _
                 jpf[2 * FV + f] = alpha * bfz;
             }
             if (k == 0) {
+                // the state current on the bottom plane: zero walls, or the
+                // open harmonic current of the constrained spline there
+                // (nfgs_solver.py:5920-5933)
                 bool wall = (i == 0 || i == nx - 1 || j == 0 || j == ny - 1);
-                jb[(long long)j * nx + i] = wall ? T(0) : jxf;
-                jb[P + (long long)j * nx + i] = wall ? T(0) : jyf;
+                T wx = T(0), wy = T(0);
+                if (jh_wall != nullptr) {
+                    const double dz = g.dz;
+                    const int n = nz;
+                    const double* hp = jh_wall;
+                    const double dhx = (-3.0 * hp[0] + 4.0 * hp[1] - hp[2]) / (2.0 * dz);
+                    const double dhy = (-3.0 * hp[n] + 4.0 * hp[n + 1] - hp[n + 2]) / (2.0 * dz);
+                    wx = (T)(-dhy);
+                    wy = (T)dhx;
+                }
+                jb[(long long)j * nx + i] = wall ? wx : jxf;
+                jb[P + (long long)j * nx + i] = wall ? wy : jyf;
             }
         }
     }
@@ -206,7 +248,8 @@ __global__ void __launch_bounds__(128) k_src(Geo g, const int* skip, const T* __
                                              const T* __restrict__ jb, const T* __restrict__ jzt,
                                              const T* __restrict__ bzobs, SrcOpts o, const T* __restrict__ wx,
                                              const T* __restrict__ wy, const T* __restrict__ wz,
-                                             T* __restrict__ sb, T* __restrict__ sj, double* __restrict__ partials) {
+                                             T* __restrict__ sb, T* __restrict__ sj, double* __restrict__ partials,
+                                             double* __restrict__ kpart = nullptr) {
     __shared__ double sh[NFGS_NRED * 32];
     if (skip != nullptr && *skip) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -216,6 +259,7 @@ __global__ void __launch_bounds__(128) k_src(Geo g, const int* skip, const T* __
     const long long P = g.P;
     const long long FV = (long long)(nz - 1) * P;
     double red[1] = {0};
+    double kz[4] = {0, 0, 0, 0};
     if (i < nx && j < ny) {
         auto JP = [&](int comp, int kk, int jj, int ii) -> T {
             const long long q = (long long)jj * nx + ii;
@@ -246,6 +290,18 @@ __global__ void __launch_bounds__(128) k_src(Geo g, const int* skip, const T* __
         const long long c = k * P + (long long)j * nx + i;
         sb[c] = s_b;
         red[0] = (double)s_b * (double)s_b;
+        if (kpart != nullptr) {
+            // plane sums for the k_h=0 closure: the parallel current with the
+            // DCT-I zero-mode weights (nfgs_solver.py:4466-4468, 5944-5950)
+            // and the face-aligned current of face k (nfgs_solver.py:5876-5879)
+            const double w = (i == 0 || i == nx - 1 ? 1.0 : 2.0) * (j == 0 || j == ny - 1 ? 1.0 : 2.0);
+            kz[0] = w * (double)JP(0, k, j, i);
+            kz[1] = w * (double)JP(1, k, j, i);
+            if (k < nz - 1) {
+                kz[2] = (double)ldg(jpf, (long long)k * P + (long long)j * nx + i);
+                kz[3] = (double)ldg(jpf, FV + (long long)k * P + (long long)j * nx + i);
+            }
+        }
         if (k >= 1 && k <= nz - 2 && i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) {
             const T idx2 = T(1.0 / (g.dx * g.dx)), idy2 = T(1.0 / (g.dy * g.dy));
             const T i4xz = T(1.0 / (4.0 * g.dx * g.dz)), i4yz = T(1.0 / (4.0 * g.dy * g.dz));
@@ -264,6 +320,15 @@ __global__ void __launch_bounds__(128) k_src(Geo g, const int* skip, const T* __
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
         partials[b] = red[0];
+    }
+    if (kpart != nullptr) {
+        __syncthreads();
+        block_reduce<4>(kz, sh);
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            long long b = ((long long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) kpart[4 * b + q] = kz[q];
+        }
     }
 }
 

@@ -12,6 +12,7 @@
 #include "nfgs_stencil.cuh"
 #include "nfgs_stencil2.cuh"
 #include "nfgs_diag.cuh"
+#include "nfgs_k0.cuh"
 #include "nfgs_metrics.cuh"
 #include "nfgs_soft.cuh"
 #include "nfgs_trace.cuh"
@@ -110,6 +111,13 @@ struct Handle {
     void *wx = nullptr, *wy = nullptr, *wz = nullptr;
     double hx = 0.0, hy = 0.0;
     int use_h = 0;
+    // k_h=0 closure (coupled_k0 / constrained_spline_harmonic): per-buffer H(z)
+    bool k0_on = false;
+    int k0_spline = 0;
+    k0::Dev k0d{};
+    double* k0_hsel = nullptr;  // [2][nz] profile of the last reconstructed state
+    double k0_t[2] = {0.0, 0.0};  // bottom target H(0)
+    double k0_cond = 0.0;
     double open_bz = 0.0;
     int boundary_set = 0;
     int fov_y0 = 0, fov_x0 = 0, nyo = 0, nxo = 0, nzo = 0;
@@ -561,6 +569,59 @@ static int fs_setup(Handle* h) {
     return NFGS_OK;
 }
 
+// k_h=0 closure set-up (nfgs_solver.py:5058-5097, 5149-5225, 5262-5360):
+// the FP64 linear map of the fit, the window's zero mode per plane and the
+// per-buffer profile storage.
+static int k0_setup(Handle* h, const std::vector<double>& wfac) {
+    const NfgsParams& p = h->prm;
+    const int nz = h->g.nz;
+    const bool spline = p.horizontal_zero_mode == NFGS_HZM_CONSTRAINED_SPLINE;
+    if (!(p.k0_smoothness >= 0.0) || !std::isfinite(p.k0_smoothness))
+        return fail(NFGS_EINVAL, "k0_ode_smoothness must be non-negative");
+    if (p.k0_update_mu > 1.0 || !std::isfinite(p.k0_update_mu))
+        return fail(NFGS_EINVAL, "k0_update_mu must be in (0, 1]");
+    if (spline) {
+        if (p.k0_spline_basis < 4) return fail(NFGS_EINVAL, "k0_spline_basis_size must be >= 4");
+        if (p.k0_spline_basis > nz) return fail(NFGS_EINVAL, "k0_spline_basis_size must not exceed Nz");
+        if (p.k0_legacy) return fail(NFGS_EINVAL, "legacy coupled_k0 operator is not initialized");
+    }
+    std::vector<double> G, m;
+    double cond = 0.0;
+    if (!k0::build_operator(nz, h->g.dz, spline, p.k0_legacy != 0, p.k0_spline_basis, p.k0_smoothness, G, m, &cond))
+        return fail(NFGS_EINVAL, "the k_h=0 closure's normal matrix is not positive definite");
+    h->k0_on = true;
+    h->k0_spline = spline ? 1 : 0;
+    h->k0_cond = cond;
+    k0::Dev& d = h->k0d;
+    const size_t n2 = 2 * (size_t)nz;
+    TRY(alloc(h, &d.hk, 3 * n2 * 8));
+    TRY(alloc(h, &d.hlast, n2 * 8));
+    TRY(alloc(h, &d.hbefore, n2 * 8));
+    TRY(alloc(h, &d.hstar, n2 * 8));
+    TRY(alloc(h, &d.target, n2 * 8));
+    TRY(alloc(h, &d.stats, 4 * 8));
+    TRY(alloc(h, &d.ptm, n2 * 8));
+    TRY(alloc(h, &d.cell, 2 * n2 * 8));
+    TRY(alloc(h, &d.kpart, 4 * (size_t)h->nb_src * 8));
+    TRY(alloc(h, &h->k0_hsel, n2 * 8));
+    TRY(upload(h, &d.G, G));
+    TRY(upload(h, &d.m, m));
+    TRY(upload(h, &d.wfac, wfac));
+    for (double* q : {d.hk, d.hlast, d.hbefore, d.hstar, d.target, d.stats, d.ptm, d.cell, h->k0_hsel})
+        CK(cudaMemsetAsync(q, 0, (q == d.hk ? 3 * n2 : (q == d.cell ? 2 * n2 : (q == d.stats ? 4 : n2))) * 8, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    return NFGS_OK;
+}
+
+// Profile of the selected state as the closure's running H (its bottom
+// value the target, nfgs_solver.py:6999-7004).
+__global__ void k_k0_select(const double* hk, int idx, int nz, double t0, double t1, double* hlast) {
+    for (int r = threadIdx.x; r < nz; r += blockDim.x) {
+        hlast[r] = r == 0 ? t0 : hk[(long long)idx * 2 * nz + r];
+        hlast[nz + r] = r == 0 ? t1 : hk[(long long)idx * 2 * nz + nz + r];
+    }
+}
+
 static int tc_setup(Handle* h) {
     const int nx = h->g.nx, ny = h->g.ny;
     if (!h->f32 || (nx % 2) || (ny % 2)) return NFGS_OK;
@@ -775,16 +836,19 @@ static int run_fused(Handle* h, const int* sel, const int* skip, int polarity) {
 template <typename T>
 static int run_stencil(Handle* h, const int* sel, const int* skip, int with_src, int polarity, int raw_j = 0) {
     const Geo& g = h->g;
-    if (with_src && !raw_j && h->fs_on) return run_fused<T>(h, sel, skip, polarity);
+    // the k_h=0 closures need per-plane sums of the parallel current, which
+    // the three-pass kernels provide
+    if (with_src && !raw_j && h->fs_on && !h->k0_on) return run_fused<T>(h, sel, skip, polarity);
     k_recon<T><<<h->sgrid, h->sblock, 0, h->s>>>(g, h->st, sel, skip, (const T*)h->bbg, (const T*)h->bzobs_t,
                                                  (const T*)h->jzt_t, (T)h->hx, (T)h->hy, h->use_h, (T*)h->B,
-                                                 (T*)h->jz);
+                                                 (T*)h->jz, h->k0_on ? h->k0d.hk : nullptr, h->k0_hsel,
+                                                 h->k0_spline);
     CK(cudaGetLastError());
     double am = h->prm.alpha_max;
     k_face<T><<<h->sgrid, h->sblock, 0, h->s>>>(g, skip, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz, h->box,
                                                 (T)(am > 0 && std::isfinite(am) ? am : -1.0),
                                                 (T)h->prm.weak_field_floor_b2, (T*)h->jpf, (T*)h->jb, h->pface,
-                                                raw_j);
+                                                raw_j, h->k0_spline ? h->k0_hsel : nullptr);
     CK(cudaGetLastError());
     h->launches += 2;
     h->sum_pf = h->pface;
@@ -795,10 +859,41 @@ static int run_stencil(Handle* h, const int* sel, const int* skip, int with_src,
         SrcOpts o{polarity, h->prm.face_parallel_exact_jz, h->wx != nullptr};
         k_src<T><<<h->sgrid, h->sblock, 0, h->s>>>(g, skip, (const T*)h->jpf, (const T*)h->jb, (const T*)h->jzt_t,
                                                    (const T*)h->bzobs_t, o, (const T*)h->wx, (const T*)h->wy,
-                                                   (const T*)h->wz, (T*)h->sb, (T*)h->sj, h->psrc);
+                                                   (const T*)h->wz, (T*)h->sb, (T*)h->sj, h->psrc,
+                                                   h->k0_on ? h->k0d.kpart : nullptr);
         CK(cudaGetLastError());
         h->launches++;
     }
+    return NFGS_OK;
+}
+
+// Candidate finalisation.  With a k_h=0 closure the candidate's profile is
+// fitted between the bottom projection of the un-relaxed scalars and their
+// relaxation (nfgs_solver.py:6760-6799): finalise without relaxing, sum the
+// PT current of the candidate, fit and blend H, then relax the scalars.
+template <typename T>
+static int finalize_candidate(Handle* h, const DevCtl* ctl, int use_ctl_mu, double mu, const int* cand_sel,
+                              const int* cur_sel) {
+    const long long P = h->g.P;
+    const unsigned nb = (unsigned)((P + 255) / 256);
+    if (!h->k0_on) {
+        k_finalize<T><<<nb, 256, 0, h->s>>>(h->g, h->st, ctl, use_ctl_mu, mu, cand_sel, cur_sel, (const T*)h->phiab_t,
+                                            (const T*)h->dphi_t, h->prm.projection_weight, 1, 1,
+                                            (const T*)h->azb_t);
+        CK(cudaGetLastError());
+        h->launches++;
+        return NFGS_OK;
+    }
+    k_finalize<T><<<nb, 256, 0, h->s>>>(h->g, h->st, ctl, use_ctl_mu, mu, cand_sel, cur_sel, (const T*)h->phiab_t,
+                                        (const T*)h->dphi_t, h->prm.projection_weight, 0, 1, (const T*)h->azb_t);
+    k0::k_k0_pt<T><<<h->g.nz, 256, 0, h->s>>>(h->g, h->st, cand_sel, ctl ? &ctl->stopped : nullptr, h->k0d.ptm);
+    k0::k_k0_update<<<1, 256, 0, h->s>>>(h->g, h->k0d, cand_sel, cur_sel, ctl, use_ctl_mu, mu, h->prm.k0_update_mu,
+                                         h->prm.k0_face_target, (int)(h->sgrid.x * h->sgrid.y), h->k0_t[0],
+                                         h->k0_t[1]);
+    k_finalize<T><<<nb, 256, 0, h->s>>>(h->g, h->st, ctl, use_ctl_mu, mu, cand_sel, cur_sel, (const T*)h->phiab_t,
+                                        (const T*)h->dphi_t, 0.0, 1, 1, (const T*)h->azb_t);
+    CK(cudaGetLastError());
+    h->launches += 4;
     return NFGS_OK;
 }
 
@@ -1471,6 +1566,18 @@ static int setup_boundary(Handle* h, const double* bx_h, const double* by_h, con
         } else {
             h->hx = h->hy = 0.0; h->use_h = 0;
         }
+        if (h->k0_on) {
+            // H starts as the bottom target on every plane and the fit's
+            // residual history restarts (nfgs_solver.py:5058-5067, 5200-5203)
+            h->k0_t[0] = hxc;
+            h->k0_t[1] = hyc;
+            std::vector<double> hl(2 * (size_t)nz);
+            for (int k = 0; k < nz; ++k) { hl[k] = hxc; hl[nz + k] = hyc; }
+            double st[4] = {0.0, 0.0, h->k0_cond, 0.0};
+            CK(cudaMemcpyAsync(h->k0d.hlast, hl.data(), hl.size() * 8, cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(h->k0d.stats, st, sizeof st, cudaMemcpyHostToDevice, s));
+            CK(cudaStreamSynchronize(s));
+        }
     }
     dg[24] = (double)o->jz_mode;
     CK(cudaStreamSynchronize(s));
@@ -1566,14 +1673,7 @@ static int enqueue_iteration(Handle* h) {
     DevCtl* c = h->ctl;
     // solve from the sources of the current state into the candidate buffer
     TRY(run_solve<T>(h, c, &c->cand, 0));
-    {
-        const long long P = h->g.P;
-        k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(
-            h->g, h->st, c, 1, 1.0, &c->cand, &c->cur, (const T*)h->phiab_t, (const T*)h->dphi_t,
-            h->prm.projection_weight, 1, 1, (const T*)h->azb_t);
-        CK(cudaGetLastError());
-        h->launches++;
-    }
+    TRY(finalize_candidate<T>(h, c, 1, 1.0, &c->cand, &c->cur));
     TRY(run_stencil<T>(h, &c->cand, &c->stopped, 1, h->stop.polarity_mask));
     k_sum_stage1<<<dim3(NCHUNK, 6), 256, 0, h->s>>>(h->sum_pf, h->sum_nbf, h->sum_ps, h->sum_nbs, h->scal + 8);
     k_sum_stage2_ctl<<<1, 192, 0, h->s>>>(h->g, h->scal + 8, h->scal, c, h->hist);
@@ -1600,7 +1700,7 @@ static std::map<std::tuple<int, int, int, int>, int> g_tune_nseg;
 
 template <typename T>
 static int autotune_stencil(Handle* h, int polarity) {
-    if (!h->fs_on || h->fs_tuned) return NFGS_OK;
+    if (!h->fs_on || h->fs_tuned || h->k0_on) return NFGS_OK;
     h->fs_tuned = 1;
     if (getenv("NFGS_STENCIL_NSEG") != nullptr) return NFGS_OK;
     if (const char* e = getenv("NFGS_AUTOTUNE"))
@@ -1688,6 +1788,13 @@ static int iterate_begin_t(Handle* h, const NfgsStop* stop) {
     CK(cudaMemcpyAsync(h->ctl, &c, sizeof c, cudaMemcpyHostToDevice, h->s));
     h->launches = 0;
     CK(cudaEventRecord(h->ev0, h->s));
+    if (h->k0_on) {
+        // every start state carries the closure's running H
+        // (nfgs_solver.py:6613-6645 reconstructs with the current _H_k0)
+        const size_t n2 = 2 * (size_t)h->g.nz;
+        for (int b = 0; b < 3; ++b)
+            CK(cudaMemcpyAsync(h->k0d.hk + b * n2, h->k0d.hlast, n2 * 8, cudaMemcpyDeviceToDevice, h->s));
+    }
     // gs_cfcf: zero-source modal solves into state 0 (nfgs_solver.py:6630-6645)
     TRY(run_solve<T>(h, nullptr, &h->consts[0], 1));
     {
@@ -2148,10 +2255,11 @@ static int step_diagnostics_t(Handle* h, double* out) {
         const double amax = (am > 0 && std::isfinite(am)) ? am : -1.0;
         k_recon<T><<<h->sgrid, h->sblock, 0, s>>>(g, h->st, &h->consts[prev], nullptr, (const T*)h->bbg,
                                                   (const T*)h->bzobs_t, (const T*)h->jzt_t, (T)h->hx, (T)h->hy,
-                                                  h->use_h, (T*)h->B, (T*)h->jz);
+                                                  h->use_h, (T*)h->B, (T*)h->jz, h->k0_on ? h->k0d.hk : nullptr,
+                                                  h->k0_hsel, h->k0_spline);
         k_face<T><<<h->sgrid, h->sblock, 0, s>>>(g, nullptr, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz,
                                                  h->box, (T)amax, (T)h->prm.weak_field_floor_b2, (T*)h->jpf,
-                                                 (T*)h->jb, pf, 0);
+                                                 (T*)h->jb, pf, 0, h->k0_spline ? h->k0_hsel : nullptr);
         diag::k_face_counts<T><<<h->sgrid, h->sblock, 0, s>>>(g, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz,
                                                               amax, h->prm.weak_field_floor_b2, pc);
         SrcOpts o{h->stop.polarity_mask, h->prm.face_parallel_exact_jz, h->wx != nullptr};
@@ -2190,7 +2298,8 @@ static int step_diagnostics_t(Handle* h, double* out) {
         // the candidate's field for the bottom imprints
         k_recon<T><<<h->sgrid, h->sblock, 0, s>>>(g, h->st, &h->consts[cand], nullptr, (const T*)h->bbg,
                                                   (const T*)h->bzobs_t, (const T*)h->jzt_t, (T)h->hx, (T)h->hy,
-                                                  h->use_h, (T*)h->B, (T*)h->jz);
+                                                  h->use_h, (T*)h->B, (T*)h->jz, h->k0_on ? h->k0d.hk : nullptr,
+                                                  h->k0_hsel, h->k0_spline);
         diag::k_diag_sums<T><<<h->sgrid, h->sblock, 0, s>>>(
             g, (const T*)h->st.phi[prev], (const T*)h->st.az[prev], (const T*)h->st.phi[cand],
             (const T*)h->st.az[cand], phs, azs, bcz, jzs, sb, sj, sphi, saz,
@@ -2230,6 +2339,22 @@ static int step_diagnostics_t(Handle* h, double* out) {
         out[3] = rel(S[S_DAZ_M], S[S_AZ], nV);
         out[4] = 0.0;
         out[5] = 0.0;
+        if (h->k0_on) {
+            // h_k0_update / h_k0_map_residual (nfgs_solver.py:6884-6893)
+            std::vector<double> hb(2 * nz), hl(2 * nz), hs(2 * nz);
+            CK(cudaMemcpyAsync(hb.data(), h->k0d.hbefore, 16 * (size_t)nz, cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(hl.data(), h->k0d.hlast, 16 * (size_t)nz, cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(hs.data(), h->k0d.hstar, 16 * (size_t)nz, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            double db = 0.0, du = 0.0, dm = 0.0;
+            for (int q = 0; q < 2 * nz; ++q) {
+                db += hb[q] * hb[q];
+                du += (hl[q] - hb[q]) * (hl[q] - hb[q]);
+                dm += (hs[q] - hb[q]) * (hs[q] - hb[q]);
+            }
+            out[4] = rel(du, db, 2.0 * nz);
+            out[5] = rel(dm, db, 2.0 * nz);
+        }
         out[6] = rel(S[S_BCZ_R], S[S_SB_BI], nbi);
         out[7] = rel(S[S_JZ_R], S[S_SJ_I], njz);
         out[8] = relop(S[S_POL_R], {S[S_POL_D2], S[S_POL_LX], S[S_POL_SRC]}, nbi);
@@ -2316,7 +2441,7 @@ namespace {
 template <typename T, typename O>
 __global__ void k_gather_fields(Geo g, const T* __restrict__ B, const T* __restrict__ bbg, const T* __restrict__ jz,
                                 const T* __restrict__ jf, int nzc, int y0, int ny_c, int x0, int nx_c,
-                                O* __restrict__ out) {
+                                O* __restrict__ out, const double* __restrict__ jh_wall = nullptr) {
     long long n = (long long)nzc * ny_c * nx_c;
     long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
@@ -2332,7 +2457,20 @@ __global__ void k_gather_fields(Geo g, const T* __restrict__ B, const T* __restr
     out[2 * n + q] = (O)(bbg[2 * V + c] + B[2 * V + c]);
     bool wall = (i == 0 || i == g.nx - 1 || j == 0 || j == g.ny - 1 || k == g.nz - 1);
     double jx = 0.0, jy = 0.0;
-    if (!wall) {
+    if (wall && jh_wall != nullptr && k < g.nz - 1) {
+        // constrained spline: the open harmonic current (-dH_y/dz, dH_x/dz)
+        // on the side walls (nfgs_solver.py:5920-5933, 5406-5432)
+        const int n = g.nz;
+        const double dz = g.dz;
+        double der[2];
+        for (int c2 = 0; c2 < 2; ++c2) {
+            const double* p = jh_wall + c2 * n;
+            der[c2] = k == 0 ? (-3.0 * p[0] + 4.0 * p[1] - p[2]) / (2.0 * dz)
+                             : 0.5 * ((p[k] - p[k - 1]) / dz + (p[k + 1] - p[k]) / dz);
+        }
+        jx = -der[1];
+        jy = der[0];
+    } else if (!wall) {
         if (k == 0) {
             jx = (double)jf[pq];
             jy = (double)jf[FV + pq];
@@ -2420,6 +2558,11 @@ static int iterate_end_t(Handle* h, NfgsIterResult* res, double* hist, int hist_
     }
     h->iter_active = 0;
     h->solution = h->select_final ? c.cur : c.best;
+    if (h->k0_on) {
+        k_k0_select<<<1, 256, 0, h->s>>>(h->k0d.hk, h->solution, h->g.nz, h->k0_t[0], h->k0_t[1], h->k0d.hlast);
+        CK(cudaGetLastError());
+        h->launches++;
+    }
     h->select_final = 0;
     h->cur_host = c.cur;
     // final-vs-best relative B difference (nfgs_solver.py:3820-3824)
@@ -2643,11 +2786,7 @@ static int step_t(Handle* h, double mu, int polarity) {
     const int cand = (cur + 1) % 3 == h->solution ? (cur + 2) % 3 : (cur + 1) % 3;
     TRY(run_stencil<T>(h, &h->consts[cur], nullptr, 1, polarity));
     TRY(run_solve<T>(h, nullptr, &h->consts[cand], 0));
-    const long long P = h->g.P;
-    k_finalize<T><<<(unsigned)((P + 255) / 256), 256, 0, h->s>>>(h->g, h->st, nullptr, 0, mu, &h->consts[cand],
-                                                                &h->consts[cur], (const T*)h->phiab_t,
-                                                                (const T*)h->dphi_t, h->prm.projection_weight, 1, 1, (const T*)h->azb_t);
-    CK(cudaGetLastError());
+    TRY(finalize_candidate<T>(h, nullptr, 0, mu, &h->consts[cand], &h->consts[cur]));
     CK(cudaStreamSynchronize(h->s));
     h->cur_host = cand;
     return NFGS_OK;
@@ -2796,6 +2935,7 @@ static int source_diag_t(Handle* h, double* out) {
 template <typename T>
 static int time_phases_t(Handle* h, int n_iters, double* ms_out) {
     if (!h->boundary_set) return fail(NFGS_ESTATE, "boundary is not set");
+    if (h->k0_on) return fail(NFGS_EUNSUPPORTED, "phase timing covers the frozen and omitted k_h=0 policies only");
     cudaEvent_t ev[6];
     for (auto& e : ev) CK(cudaEventCreate(&e));
     double acc[5] = {0, 0, 0, 0, 0};
@@ -2978,6 +3118,7 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
     TRYC(alloc(h, &h->phiab_t, P * h->esz)); TRYC(alloc(h, &h->dphi_t, P * h->esz));
     TRYC(alloc(h, &h->azb_t, P * h->esz));
     // buffer window (nfgs_solver.py:1569-1591)
+    std::vector<double> k0_wfac(nz, 1.0);
     if (prm->buffer_thickness > 0) {
         const int t = prm->buffer_thickness;
         auto bell = [&](int n) {
@@ -2990,6 +3131,7 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
             return w;
         };
         std::vector<double> wz(nz, 1.0);
+        const std::vector<double> bx_w = bell(nx), by_w = bell(ny);
         if (!prm->buffer_xy_only) {
             int tz = std::min(t, std::max(1, nz - 1));
             for (int k = 0; k < nz; ++k) {
@@ -2998,9 +3140,15 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
             }
             wz[0] = 1.0;
         }
-        TRYC(upload_t(h, &h->wx, bell(nx)));
-        TRYC(upload_t(h, &h->wy, bell(ny)));
+        TRYC(upload_t(h, &h->wx, bx_w));
+        TRYC(upload_t(h, &h->wy, by_w));
         TRYC(upload_t(h, &h->wz, wz));
+        // DCT-I zero mode of the window on each plane (the face-placed k_h=0
+        // target is a uniform plane times the window, nfgs_solver.py:6718-6724)
+        double sx = 0.0, sy = 0.0;
+        for (int i = 0; i < nx; ++i) sx += (i == 0 || i == nx - 1 ? 1.0 : 2.0) * bx_w[i];
+        for (int j = 0; j < ny; ++j) sy += (j == 0 || j == ny - 1 ? 1.0 : 2.0) * by_w[j];
+        for (int k = 0; k < nz; ++k) k0_wfac[k] = wz[k] * sx * sy / (4.0 * (nx - 1) * (double)(ny - 1));
     }
     // state and work buffers
     for (int b = 0; b < 3; ++b) {
@@ -3025,6 +3173,8 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
     h->sgrid = dim3((nx + 31) / 32, (ny + 3) / 4, nz);
     h->nb_face = h->nb_src = (int)(h->sgrid.x * h->sgrid.y * h->sgrid.z);
     TRYC(fs_setup(h));
+    if (prm->horizontal_zero_mode == NFGS_HZM_COUPLED_K0 || prm->horizontal_zero_mode == NFGS_HZM_CONSTRAINED_SPLINE)
+        TRYC(k0_setup(h, k0_wfac));
     {
         // room for the tuner's largest candidate (16 z segments)
         const long long fs_max = (long long)h->fs_grid.x * h->fs_grid.y * std::max(16u, h->fs_grid.z) * NFGS_NRED;
@@ -3355,6 +3505,44 @@ __global__ void k_ctl_force_stop(DevCtl* c, int reason) {
         c->stopped = 1;
         c->stop_reason = reason;
     }
+}
+
+int nfgs_k0_state(void* handle, double* out, int32_t n) {
+    g_err.clear();
+    Handle* h = (Handle*)handle;
+    if (!h || !out) return fail(NFGS_EINVAL, "null argument");
+    if (!h->k0_on) return fail(NFGS_EUNSUPPORTED, "the horizontal zero mode has no k_h=0 closure");
+    const int nz = h->g.nz;
+    if (n < 6 * nz + NFGS_K0_EXTRA) return fail(NFGS_EINVAL, "output too small: need 6 nz + 3 doubles");
+    if (cudaSetDevice(h->geom.device) != cudaSuccess) return fail(NFGS_ECUDA, "cudaSetDevice failed");
+    const size_t n2 = 2 * (size_t)nz;
+    double st[4];
+    CK(cudaMemcpyAsync(out, h->k0d.hlast, n2 * 8, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaMemcpyAsync(out + n2, h->k0d.hstar, n2 * 8, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaMemcpyAsync(out + 2 * n2, h->k0d.target, n2 * 8, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaMemcpyAsync(st, h->k0d.stats, sizeof st, cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    out[3 * n2] = st[0];
+    out[3 * n2 + 1] = h->k0_spline ? h->k0_cond : std::nan("");
+    out[3 * n2 + 2] = st[1];
+    return NFGS_OK;
+}
+
+int nfgs_k0_operator(int32_t nz, double dz, int32_t spline, int32_t legacy, int32_t n_basis, double smoothness,
+                     double* G, double* m, double* cond_out) {
+    g_err.clear();
+    if (!G || !m || !cond_out) return fail(NFGS_EINVAL, "null argument");
+    if (nz < 3 || !(dz > 0.0)) return fail(NFGS_EINVAL, "the closure needs nz >= 3 and dz > 0");
+    if (!(smoothness >= 0.0)) return fail(NFGS_EINVAL, "k0_ode_smoothness must be non-negative");
+    if (spline && (n_basis < 4 || n_basis > nz)) return fail(NFGS_EINVAL, "k0_spline_basis_size must be in [4, Nz]");
+    std::vector<double> g, mm;
+    double cond = 0.0;
+    if (!k0::build_operator(nz, dz, spline != 0, legacy != 0, n_basis, smoothness, g, mm, &cond))
+        return fail(NFGS_EINVAL, "the k_h=0 closure's normal matrix is not positive definite");
+    std::memcpy(G, g.data(), g.size() * sizeof(double));
+    std::memcpy(m, mm.data(), mm.size() * sizeof(double));
+    *cond_out = cond;
+    return NFGS_OK;
 }
 
 int nfgs_iterate_fixed_point(void* handle, int32_t stop_now) {

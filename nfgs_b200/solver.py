@@ -170,8 +170,13 @@ class NFGSSolverGPU:
             raise ValueError("k0_update_mu must be in (0, 1]")
         if k0_basis < 4:
             raise ValueError("k0_spline_basis_size must be >= 4")
-        if k0_place is not None and str(k0_place).lower().replace("-", "_") not in {"face", "cell"}:
+        if k0_mu is None and hzm == "constrained_spline_harmonic":
+            k0_mu = 0.2  # the closure's own conservative default (nfgs_solver.py:4141-4146)
+        k0_place = "cell" if k0_place is None else str(k0_place).lower().replace("-", "_")
+        if k0_place not in {"face", "cell"}:
             raise ValueError("k0_current_target_placement must be 'face' or 'cell'")
+        if k0_place == "face" and vco != "staggered_face":
+            raise ValueError("k0_current_target_placement='face' requires vertical_current_operator='staggered_face'")
         if bpcm not in {"observed_full", "face_parallel_exact_jz"}:
             raise ValueError("bottom_parallel_current_mode must be one of ['face_parallel_exact_jz', 'observed_full']")
         if handoff_tol <= 0.0:
@@ -198,7 +203,7 @@ class NFGSSolverGPU:
         unsupported = []
         if source_partition_mode != "gaussian_separated":
             unsupported.append("source_partition_mode='legacy_single_field'")
-        if hzm not in {"omit", "frozen_linear_harmonic"}:
+        if hzm not in {"omit", "frozen_linear_harmonic", "coupled_k0", "constrained_spline_harmonic"}:
             unsupported.append(f"horizontal_zero_mode_policy={hzm!r}")
         if mean_bz_policy == "external_potential" or external is not None:
             unsupported.append("external_potential_field")
@@ -248,6 +253,11 @@ class NFGSSolverGPU:
             raise ValueError("rhs_lap_xy_spectral_ext must be 'neumann' or 'dirichlet'")
         if not 0.0 <= imprint <= 1.0:
             raise ValueError("bottom_imprint_robin_weight must be between 0 and 1")
+        # k_h=0 closure checks that follow the base initialiser (nfgs_solver.py:4252-4270)
+        if hzm in {"coupled_k0", "constrained_spline_harmonic"} and not relax_scalars:
+            raise ValueError("coupled horizontal harmonic modes require relax_scalars=True")
+        if hzm == "constrained_spline_harmonic" and vco != "staggered_face":
+            raise ValueError("constrained_spline_harmonic requires vertical_current_operator='staggered_face'")
         if fdo != 2:
             unsupported.append("finite_difference_order=4")
         if rhs_lap != "fd":
@@ -276,6 +286,18 @@ class NFGSSolverGPU:
         self.dx, self.dy, self.dz = float(dx), float(dy), float(dz)
         if self.Nz < 3:
             raise ValueError("NFGS requires Nz >= 3")
+        if hzm == "constrained_spline_harmonic" and k0_basis > self.Nz:
+            raise ValueError("k0_spline_basis_size must not exceed Nz")
+        if hzm == "constrained_spline_harmonic" and k0_disc == "legacy_plane_centred":
+            # the reference's centre derivative of this combination has no
+            # operator (nfgs_solver.py:5406-5411)
+            raise RuntimeError("legacy coupled_k0 operator is not initialized")
+        self.k0_ode_smoothness = k0_smooth
+        self.coupled_k0_discretization = ("staggered_face_D1_true_three_point_curvature"
+                                          if k0_disc == "staggered_face_d1_true_three_point_curvature" else k0_disc)
+        self.k0_update_mu = None if k0_mu is None else float(k0_mu)
+        self.k0_spline_basis_size = k0_basis
+        self.k0_current_target_placement = k0_place
         self.device = str(device)
         self._dtype_code, self._np_dtype = _dtype_code(dtype)
         self.dtype = dtype
@@ -325,12 +347,16 @@ class NFGSSolverGPU:
             weak_field_floor_b2=weak_floor, mean_mode_tolerance=mean_tol,
             source_zero_mode_tolerance=src_tol,
             user_open_bz=float(np.asarray(user_open).reshape(())) if user_open is not None else 0.0,
-            horizontal_zero_mode=1 if hzm == "frozen_linear_harmonic" else 0,
+            horizontal_zero_mode={"frozen_linear_harmonic": 1, "coupled_k0": 2,
+                                  "constrained_spline_harmonic": 3}.get(hzm, 0),
             mean_bz_policy={"uniform_open": 0, "require_balanced": 1, "user_supplied": 2}[mean_bz_policy],
             d0_policy=_VALID_PROJECTION[d0_policy], source_policy=_VALID_PROJECTION[src_policy],
             harmonic_policy=_VALID_HARMONIC[harm_policy], gaussian_spectral=1 if ghop == "spectral" else 0,
             face_parallel_exact_jz=1 if bpcm == "face_parallel_exact_jz" else 0,
-            buffer_thickness=self.buffer_thickness, buffer_xy_only=int(buffer_xy_only))
+            buffer_thickness=self.buffer_thickness, buffer_xy_only=int(buffer_xy_only),
+            k0_smoothness=k0_smooth, k0_update_mu=(-1.0 if k0_mu is None else float(k0_mu)),
+            k0_spline_basis=k0_basis, k0_legacy=int(k0_disc == "legacy_plane_centred"),
+            k0_face_target=int(k0_place == "face"))
         if mean_bz_policy == "user_supplied" and user_open is None:
             self._user_open_missing = True
         else:
@@ -462,14 +488,34 @@ class NFGSSolverGPU:
             "harmonic_residual_curl_rms": float(diag[d["harm_curl_rms"]]),
         }
         self.gaussian_separation_diagnostics = gsd
-        if self.horizontal_zero_mode_policy == "frozen_linear_harmonic":
-            target = gsd["harmonic_residual_constant"]
+        target = [float(v) for v in gsd["harmonic_residual_constant"]]
+        hzm = self.horizontal_zero_mode_policy
+        if hzm == "frozen_linear_harmonic":
             self._k0_diagnostics = {
                 "enabled": True, "closure": "frozen_linear_harmonic",
                 "representation": "analytic_Az_linear_lift", "bottom_target": list(target),
                 "current_free": True, "open_side_current": False, "top_derivative": [0.0, 0.0],
                 "profile_max_abs": float(max(abs(target[0]), abs(target[1]))),
             }
+        elif hzm == "coupled_k0":
+            # nfgs_solver.py:5296-5310, 5347-5358
+            legacy = self.coupled_k0_discretization == "legacy_plane_centred"
+            self._k0_diagnostics = {"enabled": True, "smoothness": self.k0_ode_smoothness,
+                                    "discretization": self.coupled_k0_discretization,
+                                    "bottom_target": list(target), "open_side_current": True}
+            if legacy:
+                self._k0_diagnostics["diagnosis_only"] = True
+        elif hzm == "constrained_spline_harmonic":
+            # nfgs_solver.py:5209-5225
+            st = self._k0_state()
+            self._k0_diagnostics = {
+                "enabled": True, "closure": "constrained_spline_harmonic",
+                "representation": "cubic_bspline_explicit_linear_harmonic_lift",
+                "basis_size": self.k0_spline_basis_size, "smoothness": self.k0_ode_smoothness,
+                "update_mu": self.k0_update_mu, "bottom_target": list(target), "bottom_constraint": "exact",
+                "top_constraint": "discrete_second_order_Hprime_zero",
+                "lateral_current_contract": "open_harmonic_plus_closed_PT", "open_side_current": True,
+                "top_derivative": [0.0, 0.0], "kkt_condition_number": st["kkt_condition_number"]}
         else:
             self._k0_diagnostics = {}
         self._source_zero_mode_history = []
@@ -811,6 +857,8 @@ class NFGSSolverGPU:
                       f"(best sigma={res.best_sigma:.4e} at iter {res.best_iter})")
         self._have_solution = True
         self._last_result = res
+        if self.horizontal_zero_mode_policy in ("coupled_k0", "constrained_spline_harmonic"):
+            self._k0_update_diagnostics()
         history = {
             "sigma": [float(v) for v in hist[:, 0]],
             "divB": [float(v) for v in hist[:, 1]],
@@ -959,7 +1007,57 @@ class NFGSSolverGPU:
             t = fr.get("bottom_target", [0.0, 0.0])
             fr["profile_by_height"] = [[float(t[0])] * self.Nz, [float(t[1])] * self.Nz]
             diag["frozen_linear_harmonic"] = fr
+        elif self.horizontal_zero_mode_policy in ("coupled_k0", "constrained_spline_harmonic"):
+            # nfgs_solver.py:7171-7196: the closure's block with the selected
+            # state's profile by height
+            fr = dict(self._k0_diagnostics)
+            fr["profile_by_height"] = [[float(v) for v in comp] for comp in self._k0_state()["profile"]]
+            diag[self.horizontal_zero_mode_policy] = fr
         return diag
+
+    def _k0_state(self):
+        """The device's k_h=0 closure state (nfgs_k0_state)."""
+        nz = self.Nz
+        out = np.zeros(6 * nz + 3)
+        L.check(self._lib.nfgs_k0_state(self._h, L.dptr(out), out.size))
+        return {"profile": out[:2 * nz].reshape(2, nz), "fit": out[2 * nz:4 * nz].reshape(2, nz),
+                "target": out[4 * nz:6 * nz].reshape(2, nz), "residual_relative_max": float(out[6 * nz]),
+                "kkt_condition_number": float(out[6 * nz + 1]), "updates": int(out[6 * nz + 2])}
+
+    def _k0_update_diagnostics(self):
+        """The closure's fit diagnostics of the last update
+        (nfgs_solver.py:5965-6009, 6024-6065), from the device's last fitted
+        profile H* and target mean current q: the fitted current is
+        (-dH_y/dz, dH_x/dz) at the planes, the face fit H_x' = avg q_y,
+        H_y' = -avg q_x."""
+        st = self._k0_state()
+        if st["updates"] <= 0:
+            return
+        prof, desired, dz = st["fit"], st["target"], float(self.dz)
+        face = (prof[:, 1:] - prof[:, :-1]) / dz
+        der = np.zeros_like(prof)
+        der[:, 1:-1] = 0.5 * (face[:, :-1] + face[:, 1:])
+        der[:, 0] = (-3.0 * prof[:, 0] + 4.0 * prof[:, 1] - prof[:, 2]) / (2.0 * dz)
+        der[:, -1] = (3.0 * prof[:, -1] - 4.0 * prof[:, -2] + prof[:, -3]) / (2.0 * dz)
+        rms = lambda a: float(np.sqrt(np.mean(np.square(a))))  # noqa: E731
+        res = np.stack([-der[1], der[0]]) - desired
+        des_rms = rms(desired)
+        dface = np.stack([0.5 * (desired[1, :-1] + desired[1, 1:]), -0.5 * (desired[0, :-1] + desired[0, 1:])])
+        grid = prof[:, 1:-1] - 0.25 * (prof[:, :-2] + 2.0 * prof[:, 1:-1] + prof[:, 2:])
+        prof_rms = rms(prof)
+        self._k0_diagnostics.update({
+            "ode_residual_rms": rms(res),
+            "ode_residual_relative": rms(res) / max(des_rms, 1e-30),
+            "ode_residual_relative_max": st["residual_relative_max"],
+            "face_ode_residual_rms": rms(face - dface),
+            "face_ode_residual_relative": rms(face - dface) / max(rms(dface), 1e-30),
+            "gridscale_profile_rms": rms(grid),
+            "gridscale_profile_relative": rms(grid) / max(prof_rms, 1e-30),
+            "top_derivative": [float(v) for v in der[:, -1]],
+            "profile_max_abs": float(np.abs(prof).max()),
+            "profile_top": [float(v) for v in prof[:, -1]],
+            "desired_mean_current_rms": des_rms,
+        })
 
     # ------------------------------------------------------------------
     # Step-level access (used by parity tests; not in the reference API)

@@ -29,6 +29,8 @@ from typing import Callable, Optional
 import numpy as np
 from scipy import fft as _sfft
 
+from .k0_oracle import CoupledK0, SplineK0, centre_derivative_fd2, fit_diagnostics
+
 # SciPy FFT worker threads (batch-parallel transforms give identical results)
 _WORKERS = -1
 
@@ -302,7 +304,8 @@ def derive_bottom_jz_calc(bx, by, dx, dy, ijzbcor):
 # The solver restatement
 # ---------------------------------------------------------------------------
 _PROD_POLICIES = dict(
-    horizontal_zero_mode_policy={"omit", "frozen_linear_harmonic", "external_potential", "user_supplied"},
+    horizontal_zero_mode_policy={"omit", "frozen_linear_harmonic", "external_potential", "user_supplied",
+                                 "coupled_k0", "constrained_spline_harmonic"},
     mean_bz_policy={"uniform_open", "require_balanced", "external_potential", "user_supplied"},
 )
 
@@ -331,7 +334,10 @@ class OracleNFGS:
                  bottom_parallel_current_mode="observed_full",
                  user_supplied_open_bz=None, user_supplied_horizontal_field=None,
                  external_potential_field=None, soft_cfcf_epsilon=None, soft_cfcf_normal_ridge=0.0,
-                 lateral_wall="paper_bc1", record_iteration_diagnostics=False):
+                 lateral_wall="paper_bc1", record_iteration_diagnostics=False,
+                 k0_ode_smoothness=1.0e-3,
+                 coupled_k0_discretization="staggered_face_D1_true_three_point_curvature",
+                 k0_update_mu=None, k0_spline_basis_size=8, k0_current_target_placement=None):
         ix, iy, iz = int(Nx), int(Ny), int(Nz)
         # the wall condition of the Stable-NFPT field behind the cfcf start
         # (nfgs_solver.py:845-853, 2161-2170)
@@ -375,6 +381,18 @@ class OracleNFGS:
         self.mean_bz_policy = str(mean_bz_policy).lower()
         if self.hzm not in _PROD_POLICIES["horizontal_zero_mode_policy"]:
             raise NotImplementedError(self.hzm)
+        # k_h=0 closure settings (nfgs_solver.py:3966-3976, 4120-4170, 4252-4270)
+        self.k0_smoothness = float(k0_ode_smoothness)
+        self.k0_legacy = str(coupled_k0_discretization).lower().replace("-", "_") == "legacy_plane_centred"
+        if k0_update_mu is None and self.hzm == "constrained_spline_harmonic":
+            k0_update_mu = 0.2
+        self.k0_update_mu = None if k0_update_mu is None else float(k0_update_mu)
+        self.k0_basis = int(k0_spline_basis_size)
+        place = "cell" if k0_current_target_placement is None else str(k0_current_target_placement).lower()
+        self.k0_face_target = place.replace("-", "_") == "face"
+        self.k0 = None
+        self.k0_diagnostics = {}
+        self.k0_history: list[float] = []
         if self.mean_bz_policy not in _PROD_POLICIES["mean_bz_policy"]:
             raise ValueError(self.mean_bz_policy)
         self.d0_policy = str(d0_zero_mode_policy).lower()
@@ -754,10 +772,54 @@ class OracleNFGS:
             "background_scalar_plus_explicit_rms": _rms(inv),
         }
         self.gaussian_separation_diagnostics.update(self._bottom_harmonic_diagnostics())
+        self._init_k0()
+
+    def _init_k0(self):
+        """H(z) start and closure operators (nfgs_solver.py:4911-4919,
+        5058-5097, 5149-5225, 5262-5360)."""
+        nz = self.Nz
+        tgt = [float(v) for v in self.H_bottom_target]
+        self.k0 = None
+        self.k0_history = []
         if self.hzm == "frozen_linear_harmonic":
-            self.H = self.H_bottom_target.copy()
+            self.H = np.repeat(self.H_bottom_target[:, None], nz, axis=1)
+            self.k0_diagnostics = {"enabled": True, "closure": "frozen_linear_harmonic",
+                                   "representation": "analytic_Az_linear_lift", "bottom_target": tgt,
+                                   "current_free": True, "open_side_current": False, "top_derivative": [0.0, 0.0],
+                                   "profile_max_abs": float(np.abs(self.H).max())}
+        elif self.hzm == "coupled_k0":
+            self.H = np.repeat(self.H_bottom_target[:, None], nz, axis=1)
+            self.k0 = CoupledK0(nz, self.dz, self.k0_smoothness, self.k0_legacy)
+            self.k0_diagnostics = {"enabled": True, "smoothness": self.k0_smoothness,
+                                   "discretization": ("legacy_plane_centred" if self.k0_legacy else
+                                                      "staggered_face_D1_true_three_point_curvature"),
+                                   "bottom_target": tgt, "open_side_current": True}
+            if self.k0_legacy:
+                self.k0_diagnostics["diagnosis_only"] = True
+        elif self.hzm == "constrained_spline_harmonic":
+            self.H = np.repeat(self.H_bottom_target[:, None], nz, axis=1)
+            self.k0 = SplineK0(nz, self.dz, self.k0_basis, self.k0_smoothness)
+            self.k0_diagnostics = {"enabled": True, "closure": "constrained_spline_harmonic",
+                                   "representation": "cubic_bspline_explicit_linear_harmonic_lift",
+                                   "basis_size": self.k0_basis, "smoothness": self.k0_smoothness,
+                                   "update_mu": self.k0_update_mu, "bottom_target": tgt,
+                                   "bottom_constraint": "exact",
+                                   "top_constraint": "discrete_second_order_Hprime_zero",
+                                   "lateral_current_contract": "open_harmonic_plus_closed_PT",
+                                   "open_side_current": True, "top_derivative": [0.0, 0.0],
+                                   "kkt_condition_number": float(np.linalg.cond(self.k0.kkt))}
         else:
             self.H = None
+            self.k0_diagnostics = {}
+
+    def k0_field_and_current(self, prof):
+        """Uniform field H and current (-dH_y/dz, dH_x/dz, 0) by plane
+        (nfgs_solver.py:5434-5455)."""
+        if self.k0 is not None:
+            der = self.k0.centre_derivative(prof)
+        else:
+            der = centre_derivative_fd2(prof, self.dz)
+        return prof, np.stack([-der[1], der[0]])
 
     def _bottom_harmonic_diagnostics(self):
         """nfgs_solver.py:4962-5029."""
@@ -1001,18 +1063,92 @@ class OracleNFGS:
         self._zero_j_walls(J)
         B[2, 0] = self.Bz_obs
         J[2, 0] = self.Jz_T
+        jh = None
         if self.H is not None:
-            B[0] = B[0] + self.H[0]
-            B[1] = B[1] + self.H[1]
+            hb, jh = self.k0_field_and_current(self.H)
+            B[0] = B[0] + hb[0][:, None, None]
+            B[1] = B[1] + hb[1][:, None, None]
+            J[0] = J[0] + jh[0][:, None, None]
+            J[1] = J[1] + jh[1][:, None, None]
             B[2, 0] = self.Bz_obs
             J[2, 0] = self.Jz_T
             J[:, -1] = 0.0
         _bf, jf = self.face_state(B, J[2])
         Js = self.faces_to_centres(jf)
-        J[:2] = Js[:2]
-        self._zero_j_walls(J)
+        if self.hzm == "constrained_spline_harmonic":
+            # the closed PT current gets zero walls, the explicit harmonic
+            # current stays open on them (nfgs_solver.py:5920-5933); all
+            # three components come from the face current, so J_z is the
+            # face average of J_z mapped back to the planes
+            jt = Js.copy()
+            jt[0] -= jh[0][:, None, None]
+            jt[1] -= jh[1][:, None, None]
+            self._zero_j_walls(jt)
+            jt[0] += jh[0][:, None, None]
+            jt[1] += jh[1][:, None, None]
+            J = jt
+            J[:, -1] = 0.0
+        else:
+            J[:2] = Js[:2]
+            self._zero_j_walls(J)
         J[2, 0] = self.Jz_T
         return B, J, Bc
+
+    def pt_current_xy(self, phi_c, az, bc_z):
+        """Horizontal current of the PT scalars alone (ccu_pure_current,
+        nfgs_solver.py:3311-3341 with 1760-1768), walls and top zero
+        (nfgs_solver.py:6069-6078)."""
+        dazdz = d_dz(az, self.dz)
+        lphi = bc_z + self.d2dz2(phi_c)
+        jx = d_dx(dazdz, self.dx) + d_dy(lphi, self.dy)
+        jy = d_dy(dazdz, self.dy) - d_dx(lphi, self.dx)
+        J = np.stack([jx, jy, np.zeros_like(jx)])
+        self._zero_j_walls(J)
+        return J[:2]
+
+    def plane_means(self, f):
+        """DCT-I zero mode of each plane (nfgs_solver.py:5944-5950)."""
+        return np.stack([self.const_mode(dct2(f[0])), self.const_mode(dct2(f[1]))])
+
+    def k0_target(self, jp, B, J):
+        """Target mean current of the H(z) fit (nfgs_solver.py:5859-5880,
+        6718-6724): the cell parallel current, or the face-aligned current's
+        plain plane means mapped to the planes."""
+        if not self.k0_face_target:
+            return jp
+        Bf, Jf = self.face_state(B, J[2])
+        b2 = np.maximum((Bf * Bf).sum(0), self.weak_floor)
+        alpha = (Jf * Bf).sum(0) / b2
+        am = self.alpha_max()
+        if am is not None and math.isfinite(am):
+            alpha = np.clip(alpha, -am, am)
+        mf = (alpha[None] * Bf).mean(axis=(-2, -1))
+        mc = np.empty((3, self.Nz))
+        mc[:, 0] = mf[:, 0]
+        mc[:, -1] = mf[:, -1]
+        mc[:, 1:-1] = 0.5 * (mf[:, :-1] + mf[:, 1:])
+        out = np.broadcast_to(mc[:, :, None, None], jp.shape).copy()
+        w = self.buffer_window()
+        if w is not None:
+            out = out * w
+        return out
+
+    def k0_update(self, jpk0, phi_s, az_s):
+        """H* from the mean-current fit (nfgs_solver.py:5952-6067)."""
+        jpt = self.pt_current_xy(phi_s, az_s, lap_xy(phi_s, self.dx, self.dy))
+        desired = self.plane_means(jpk0) - self.plane_means(jpt)
+        hx = self.k0.solve(desired[1], float(self.H_bottom_target[0]))
+        hy = self.k0.solve(-desired[0], float(self.H_bottom_target[1]))
+        prof = np.stack([hx, hy])
+        self.k0_diagnostics.update(fit_diagnostics(self.k0, prof, desired, self.k0_history))
+        return prof
+
+    def recover_h(self, B, Bc):
+        """H of a stored state: plane means of B - B_background - B_c with the
+        bottom target (nfgs_solver.py:6685-6693, 6991-7004)."""
+        h = (B[:2] - self.B_background[:2] - Bc[:2]).mean(axis=(-2, -1))
+        h[:, 0] = self.H_bottom_target
+        return h
 
     # -------------------------------------------------------- diagnostics
     def cwsin_slices(self, nz_faces):
@@ -1232,7 +1368,8 @@ class OracleNFGS:
             d2[-1] = (-2.0 * f[-1] + 2.0 * f[-2]) / dz2
         return d2
 
-    def step_diagnostics(self, phi, az, phi_s, az_s, s_b, s_j, phi_n, az_n, Bn, Jn, clip, weak):
+    def step_diagnostics(self, phi, az, phi_s, az_s, s_b, s_j, phi_n, az_n, Bn, Jn, clip, weak,
+                         h_before=None, h_star=None):
         """The per-step diagnostics of record_iteration_diagnostics
         (nfgs_solver.py:6806-6929) for one attempted candidate."""
         rms = self._rms
@@ -1272,8 +1409,10 @@ class OracleNFGS:
             "az_update_relative": rel(az_n - az, az),
             "phi_map_residual_relative": rel(phi_s - phi, phi),
             "az_map_residual_relative": rel(az_s - az, az),
-            "h_k0_update_relative": 0.0,
-            "h_k0_map_residual_relative": 0.0,
+            "h_k0_update_relative": (rel(self.H - h_before, h_before)
+                                     if h_before is not None and self.H is not None else 0.0),
+            "h_k0_map_residual_relative": (rel(h_star - h_before, h_before)
+                                           if h_star is not None and h_before is not None else 0.0),
             "bcz_pde_residual_relative": rel(bcz_res[bi], s_b[bi]),
             "jz_pde_residual_relative": rel(jz_res[1:-1], s_j[1:-1]),
             "poloidal_pde_residual_relative": rel_op(phi_res[bi], d2p[bi], lxp[bi], source_phi[bi]),
@@ -1287,8 +1426,11 @@ class OracleNFGS:
 
     def iteration_step(self, B, J, phi, az, Bc, mu=1.0, polarity_mask="both"):
         """NFGS NFPT update (nfgs_solver.py:6647-6935, production branch)."""
+        h_before = self.H.copy() if (self.record_iteration_diagnostics and self.H is not None) else None
         if self.record_iteration_diagnostics:
             clip, weak = self.face_fractions(B, J)
+        if self.k0 is not None:
+            self.H = self.recover_h(B, Bc)
         jp = self.parallel_current(J, B)
         if polarity_mask == "positive":
             jp[:, 0] = J[:, 0] * (self.Bz_obs > 0)
@@ -1304,6 +1446,7 @@ class OracleNFGS:
         w = self.buffer_window()
         if w is not None:
             jp = jp * w
+        jpk0 = self.k0_target(jp, B, J) if self.k0 is not None else None
         s_b = d_dy(jp[0], self.dy) - d_dx(jp[1], self.dx)
         phi_s = self.solve_phi_c(s_b, self.Phi_above_bottom)
         s_j = lap_xy(jp[2], self.dx, self.dy) - d2_dxdz(jp[0], self.dx, self.dz) - d2_dydz(jp[1], self.dy, self.dz)
@@ -1313,6 +1456,11 @@ class OracleNFGS:
         az_s[0] = self.Az_bottom
         az_s[-1] = 0.0
         self._az_walls_zero(az_s)
+        h_star = None
+        if self.k0 is not None:
+            h_star = self.k0_update(jpk0, phi_s, az_s)
+            mu_k0 = self.k0_update_mu if self.k0_update_mu is not None else float(mu)
+            self.H = mu_k0 * h_star + (1.0 - mu_k0) * self.H if mu_k0 < 1.0 else h_star
         if mu < 1.0:
             phi_n = mu * phi_s + (1.0 - mu) * phi
             az_n = mu * az_s + (1.0 - mu) * az
@@ -1326,7 +1474,7 @@ class OracleNFGS:
         Bn, Jn, Bcn = self.reconstruct(phi_n, az_n, bcz)
         if self.record_iteration_diagnostics:
             self.last_iteration_diagnostics = self.step_diagnostics(
-                phi, az, phi_s, az_s, s_b, s_j, phi_n, az_n, Bn, Jn, clip, weak)
+                phi, az, phi_s, az_s, s_b, s_j, phi_n, az_n, Bn, Jn, clip, weak, h_before, h_star)
         return Bn, Jn, phi_n, az_n, Bcn
 
     def iterate(self, max_iter=200, tol=1e-5, mu=1.0, patience=1, verbose=False,
@@ -1448,6 +1596,8 @@ class OracleNFGS:
         final = (B, J, phi, az, Bc)
         sel = final if stop_mode == "fixed_point" else best
         self._B, self._J, self._Phi_c, self._Az = sel[0], sel[1], sel[2], sel[3]
+        if self.k0 is not None:
+            self.H = self.recover_h(sel[0], sel[4])
         fvb = math.sqrt(np.mean((final[0] - best[0]) ** 2)) / max(math.sqrt(np.mean(best[0] ** 2)), 1e-30)
         hist.update({
             "best_sigma": best_sigma, "best_iter": best_iter, "rollbacks": rollbacks,
@@ -1510,7 +1660,18 @@ class OracleNFGS:
             "bottom_divergence_rms": _rms(derr),
             "bottom_divergence_relative": _rms(derr) / max(_rms(self.D0), 1e-30),
             "bottom_dphi_residual_rms": _rms(dphi_b - self.bottom_dphi_c_target),
+            **self.k0_source_diagnostics(),
         }
+
+    def k0_source_diagnostics(self):
+        """The closure's block with the selected state's H by height
+        (nfgs_solver.py:7171-7196)."""
+        if self.hzm not in ("coupled_k0", "frozen_linear_harmonic", "constrained_spline_harmonic"):
+            return {}
+        d = dict(self.k0_diagnostics)
+        if self.H is not None:
+            d["profile_by_height"] = [[float(v) for v in comp] for comp in self.H]
+        return {self.hzm: d}
 
     def fields_to_numpy(self, crop_to_observed_fov=True):
         """nfgs_solver.py:2881-2903."""

@@ -106,7 +106,26 @@ def test_option_validation_before_device():
     with pytest.raises(ValueError, match="between 0 and 1"):
         NFGSSolverGPU(16, 16, 8, 1, 1, 1, bottom_divergence_robin_weight=1.5)
     with pytest.raises(NotImplementedError):
-        NFGSSolverGPU(16, 16, 8, 1, 1, 1, horizontal_zero_mode_policy="coupled_k0")
+        NFGSSolverGPU(16, 16, 8, 1, 1, 1, horizontal_zero_mode_policy="external_potential")
+    # k_h=0 closure options (nfgs_solver.py:4120-4170, 4252-4270)
+    with pytest.raises(ValueError, match="relax_scalars=True"):
+        NFGSSolverGPU(16, 16, 8, 1, 1, 1, horizontal_zero_mode_policy="coupled_k0", relax_scalars=False)
+    with pytest.raises(ValueError, match="must not exceed Nz"):
+        NFGSSolverGPU(16, 16, 8, 1, 1, 1, horizontal_zero_mode_policy="constrained_spline_harmonic",
+                      k0_spline_basis_size=500)
+    with pytest.raises(ValueError, match=">= 4"):
+        NFGSSolverGPU(16, 16, 8, 1, 1, 1, horizontal_zero_mode_policy="constrained_spline_harmonic",
+                      k0_spline_basis_size=3)
+    with pytest.raises(RuntimeError, match="legacy coupled_k0 operator"):
+        NFGSSolverGPU(16, 16, 8, 1, 1, 1, horizontal_zero_mode_policy="constrained_spline_harmonic",
+                      coupled_k0_discretization="legacy_plane_centred")
+    with pytest.raises(ValueError, match=r"k0_update_mu must be in \(0, 1\]"):
+        NFGSSolverGPU(16, 16, 8, 1, 1, 1, horizontal_zero_mode_policy="coupled_k0", k0_update_mu=1.5)
+    with pytest.raises(ValueError, match="k0_current_target_placement"):
+        NFGSSolverGPU(16, 16, 8, 1, 1, 1, horizontal_zero_mode_policy="coupled_k0",
+                      k0_current_target_placement="middle")
+    with pytest.raises(ValueError, match="k0_ode_smoothness"):
+        NFGSSolverGPU(16, 16, 8, 1, 1, 1, horizontal_zero_mode_policy="coupled_k0", k0_ode_smoothness=-1.0)
     with pytest.raises(NotImplementedError):
         NFGSSolverGPU(16, 16, 8, 1, 1, 1, vertical_current_operator="collocated_centered")
     with pytest.raises(ValueError, match="alpha_clip_scale"):
