@@ -2661,10 +2661,12 @@ static int gather_t(Handle* h, int which, int crop, void* dst, int odtype) {
     const unsigned grid = (unsigned)((n + 255) / 256);
     if (odtype == NFGS_F32)
         k_gather_fields<T, float><<<grid, 256, 0, h->s>>>(h->g, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz,
-                                                          (const T*)h->jpf, nzc, y0, nyc, x0, nxc, (float*)dst);
+                                                          (const T*)h->jpf, nzc, y0, nyc, x0, nxc, (float*)dst,
+                                                          h->k0_spline ? h->k0_hsel : nullptr);
     else
         k_gather_fields<T, double><<<grid, 256, 0, h->s>>>(h->g, (const T*)h->B, (const T*)h->bbg, (const T*)h->jz,
-                                                           (const T*)h->jpf, nzc, y0, nyc, x0, nxc, (double*)dst);
+                                                           (const T*)h->jpf, nzc, y0, nyc, x0, nxc, (double*)dst,
+                                                          h->k0_spline ? h->k0_hsel : nullptr);
     CK(cudaGetLastError());
     return NFGS_OK;
 }

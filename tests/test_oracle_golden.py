@@ -53,7 +53,7 @@ def test_setup_products(name):
     if "B_background" in data:
         assert rel(o.B_background, data["B_background"]) < 1e-11
     if o.H is not None:
-        np.testing.assert_allclose(o.H, data["H_bottom"], rtol=1e-10, atol=1e-13)
+        np.testing.assert_allclose(o.H[:, 0], data["H_bottom"], rtol=1e-10, atol=1e-13)
     gd = meta["gaussian_separation_diagnostics"]
     for k, v in gd.items():
         ov = o.gaussian_separation_diagnostics[k]
