@@ -509,6 +509,35 @@ int nfgs_trace_qperp(const void* b, int32_t dtype, int32_t nz, int32_t ny, int32
                      double delta, double step, int32_t max_steps, void* ends, int32_t* flags, void* bn, void* length,
                      void* q, void* twist, void* stream);
 
+/* FastQSL-compatible tracing and Q: the reference's topology maps
+ * (compute_y0_qmap / compute_bottom_qmap, nfgs/_backend/util/
+ * fastqsl_plane.py:203-506) trace with the vendored FastQSL adaptive tracer
+ * (TraceAllBline, third_party/FastQSL/fastqslpy/cu/TraceBlineAdaptive.cu:
+ * 429-512) and form Q with QCalcPlane (fastqslpy/FastQSL.py:65-122).  These
+ * two entry points restate both in the reference's FP32 arithmetic.
+ *
+ * nfgs_trace_fastqsl: b (3, nz, ny, nx) FP32 device field; seeds (n, 3) xyz
+ * grid coordinates; normal3 the seed plane's unit normal; step the initial
+ * step (1/8 in the reference), tol_coef its tol (0.1).  Per seed, the line
+ * along +B gives the end and along -B the start (embedded RKF4(5) with the
+ * reference's step control, face handling and limits).  Outputs (device):
+ * ends (2, n, 3): [0] end, [1] start; flags (2, n): 1..6 the face reached
+ * (x min, x max, y min, y max, z min, z max), 0 stopped inside, 42 through an
+ * edge or corner; bsamp (3, 3, n): B (x, y, z rows) at the seed, the end and
+ * the start; bflag (n): 1 where |B.n| < |B| / 100 at the seed; length (n):
+ * both halves' path length; twist (n, with_twist != 0): both halves'
+ * integral of J.B / (4 pi |B|^2) ds with J the centred grid curl.
+ *
+ * nfgs_qcalc_plane: the seeds formed an nv x nu plane (seed u + nu v);
+ * q (nv, nu) FP32: QCalcPlane's Q from the face-projected end coordinates
+ * and the z components of B at the ends, at least 1, NaN on the border and
+ * where a neighbour's flags differ; stride the seed spacing (1). */
+int nfgs_trace_fastqsl(const float* b, int32_t nz, int32_t ny, int32_t nx, const float* seeds, int64_t n,
+                       const double* normal3, double step, double tol_coef, int32_t with_twist, float* ends,
+                       int32_t* flags, float* bsamp, int32_t* bflag, double* length, double* twist, void* stream);
+int nfgs_qcalc_plane(int32_t nu, int32_t nv, const float* ends, const int32_t* flags, const float* bsamp,
+                     const double* normal3, double stride, float* q, void* stream);
+
 /* ------------------------------------------------------------------------
  * Learned warm start: operator kernels of a 3-D neural operator on a
  * truncated cosine basis.  No reference counterpart (the reference starts

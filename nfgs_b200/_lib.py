@@ -133,6 +133,9 @@ SIGNATURES = {
     "nfgs_trace_field_lines": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int64, _DP,
                                          C.c_double, C.c_int32, _P, _P, _P, _P, _P, _P]),
     "nfgs_qmap_plane": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P, _P]),
+    "nfgs_trace_fastqsl": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int64, _DP, C.c_double, C.c_double,
+                                     C.c_int32, _P, _P, _P, _P, _P, _P, _P]),
+    "nfgs_qcalc_plane": (C.c_int, [C.c_int32, C.c_int32, _P, _P, _P, _DP, C.c_double, _P, _P]),
     "nfgs_trace_qperp": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int64, C.c_double,
                                    C.c_double, C.c_int32, _P, _P, _P, _P, _P, _P, _P]),
     # learned warm start operator kernels (device pointers)

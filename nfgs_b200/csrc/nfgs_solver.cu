@@ -16,6 +16,7 @@
 #include "nfgs_metrics.cuh"
 #include "nfgs_soft.cuh"
 #include "nfgs_trace.cuh"
+#include "nfgs_fastqsl.cuh"
 #include <cuda_fp16.h>
 
 #include <cmath>
@@ -3841,6 +3842,54 @@ int nfgs_trace_qperp(const void* b, int32_t dtype, int32_t nz, int32_t ny, int32
                                                     length, q, twist, s)
                              : trace_qperp_t<double>(b, nz, ny, nx, seeds, n, delta, step, max_steps, ends, flags,
                                                      bn, length, q, twist, s);
+}
+
+int nfgs_trace_fastqsl(const float* b, int32_t nz, int32_t ny, int32_t nx, const float* seeds, int64_t n,
+                       const double* normal3, double step, double tol_coef, int32_t with_twist, float* ends,
+                       int32_t* flags, float* bsamp, int32_t* bflag, double* length, double* twist, void* stream) {
+    g_err.clear();
+    if (!b || !normal3 || (n > 0 && (!seeds || !ends || !flags || !bsamp || !bflag || !length)))
+        return fail(NFGS_EINVAL, "null argument");
+    if (with_twist && n > 0 && !twist) return fail(NFGS_EINVAL, "null twist output");
+    if (nz < 3 || ny < 3 || nx < 3) return fail(NFGS_EINVAL, "the field needs at least 3 nodes per axis");
+    if (n < 0 || n > (int64_t)INT32_MAX * 128) return fail(NFGS_EINVAL, "bad seed count");
+    if (!(step > 0.0) || !std::isfinite(step)) return fail(NFGS_EINVAL, "step must be positive");
+    if (!(tol_coef > 0.0) || !std::isfinite(tol_coef)) return fail(NFGS_EINVAL, "tol must be positive");
+    cudaStream_t s = (cudaStream_t)stream;
+    float* pk = nullptr;
+    cudaError_t e = pack_field<float>(b, nx, ny, nz, with_twist != 0, &pk, s);
+    if (e == cudaSuccess && n > 0) {
+        const fq::Field f{pk, nx, ny, nz, with_twist ? 8 : 4};
+        const fq::F3 n0 = fq::f3((float)normal3[0], (float)normal3[1], (float)normal3[2]);
+        const unsigned grid = (unsigned)((n + 127) / 128);
+        if (with_twist)
+            fq::k_trace_fq<true><<<grid, 128, 0, s>>>(f, seeds, n, n0, (float)step, (float)tol_coef, ends, flags,
+                                                      bsamp, bflag, length, twist);
+        else
+            fq::k_trace_fq<false><<<grid, 128, 0, s>>>(f, seeds, n, n0, (float)step, (float)tol_coef, ends, flags,
+                                                       bsamp, bflag, length, nullptr);
+        e = cudaGetLastError();
+    }
+    if (pk) cudaFreeAsync(pk, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(NFGS_ECUDA, std::string("trace_fastqsl: ") + cudaGetErrorString(e));
+    return NFGS_OK;
+}
+
+int nfgs_qcalc_plane(int32_t nu, int32_t nv, const float* ends, const int32_t* flags, const float* bsamp,
+                     const double* normal3, double stride, float* q, void* stream) {
+    g_err.clear();
+    if (!ends || !flags || !bsamp || !normal3 || !q) return fail(NFGS_EINVAL, "null argument");
+    if (nu < 1 || nv < 1 || nv > 65535) return fail(NFGS_EINVAL, "bad seed plane size");
+    if (!(stride > 0.0) || !std::isfinite(stride)) return fail(NFGS_EINVAL, "stride must be positive");
+    cudaStream_t s = (cudaStream_t)stream;
+    const dim3 grid((unsigned)((nu + 127) / 128), (unsigned)nv);
+    const fq::F3 n0 = fq::f3((float)normal3[0], (float)normal3[1], (float)normal3[2]);
+    fq::k_qcalc_plane<<<grid, 128, 0, s>>>(nu, nv, ends, flags, bsamp, n0, (float)stride, q);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(NFGS_ECUDA, std::string("qcalc_plane: ") + cudaGetErrorString(e));
+    return NFGS_OK;
 }
 
 int nfgs_qmap_plane(int32_t dtype, int32_t nu, int32_t nv, const void* ends, const int32_t* flags, const void* bn,

@@ -3,30 +3,28 @@
 Drop-in for the reference's topology-map helpers
 ``compute_y0_qmap`` / ``compute_bottom_qmap``
 (nfgs/_backend/util/fastqsl_plane.py:203-506), which trace every seed of a
-plane with FastQSL through CuPy and evaluate Q with its QCalcPlane.  Here the
-library's own tracer (``nfgs_trace_field_lines``: trilinear B, fixed-step
-RK4, ends snapped onto the face the line leaves through) and Q kernel
-(``nfgs_qmap_plane``: Q = ||D||^2/|det D| of the footpoint map from central
-differences over the seed plane) run on device tensors; nothing of the field
-goes through the host when it is passed as a CUDA tensor, e.g. from
-``NFGSSolverGPU.fields_to_torch()``.
+plane with FastQSL through CuPy and evaluate Q with its QCalcPlane.  Here,
+by default (``q_method="fastqsl"``), the library restates both on device
+tensors: ``nfgs_trace_fastqsl`` traces every seed with FastQSL's adaptive
+RKF4(5) step control, face handling and limits in FP32, and
+``nfgs_qcalc_plane`` forms QCalcPlane's Q; flags are FastQSL's face codes
+(1..6 for x min, x max, y min, y max, z min, z max, 0 stopped inside, 42
+through an edge or corner).  Nothing of the field goes through the host when
+it is passed as a CUDA tensor, e.g. from ``NFGSSolverGPU.fields_to_torch()``.
+``block_x`` and ``trace_chunk_seeds`` are recorded only (every seed is
+launched at once) and ``fastqsl_root`` is ignored.  ``include_twist=True``
+integrates J.B / (4 pi |B|^2) along both halves of each line, J the centred
+grid curl (fastqsl_plane.py:287-305).
 
-Q comes by default from Titov's (2007) Q_perp: each seed gets four more
-lines offset by +-delta perpendicular to B (``nfgs_trace_qperp``), so Q is
-defined also where B lies in the seed plane (By = 0 on the y = 0 midplane of
-a symmetric rope, where the seed-grid form divides by Bn0 = 0);
-``q_method="plane"`` selects the seed-grid central differences instead.
-
-Differences from the reference helpers, by design:
-* one fixed RK4 step (``step_len``, default 1/8 cell) instead of FastQSL's
-  adaptive RKF45; ``tol``, ``block_x`` and ``trace_chunk_seeds`` are accepted
-  and recorded only (the library launches every seed at once), and
-  ``fastqsl_root`` is accepted and ignored;
-* flags are the face codes of ``nfgs_trace_field_lines`` (1..6 for
-  x=0, x=nx-1, y=0, y=ny-1, z=0, z=nz-1; 0 unfinished; -1 zero field);
-* ``include_twist=True`` integrates J.B / (4 pi |B|^2) along both halves of
-  the central line with the RK4 stages of the trace (J = curl B by
-  second-order differences in grid units, as fastqsl_plane.py:287-305).
+Two other methods use the library's fixed-step RK4 tracer
+(``nfgs_trace_field_lines``: trilinear B, ends snapped onto the face a line
+leaves through; flags 1..6 for x=0, x=nx-1, y=0, y=ny-1, z=0, z=nz-1, 0
+unfinished, -1 zero field): ``q_method="perp"``, Titov's (2007) Q_perp from
+four more lines offset by +-delta perpendicular to B (``nfgs_trace_qperp``),
+which is defined also where B lies in the seed plane (By = 0 on the y = 0
+midplane of a symmetric rope, where the seed-plane forms divide by
+Bn0 = 0), and ``q_method="plane"``, Q = ||D||^2/|det D| of the footpoint map
+from central differences over the seed grid (``nfgs_qmap_plane``).
 
     python -m nfgs_b200.qmap --n 256 --nz 128 --report qmap.json
 """
@@ -163,9 +161,61 @@ def trace_qperp(b, seeds, *, delta: float = 0.25, step_len: float = 1.0 / 8.0, m
     return out
 
 
-def _plane_q(b, seeds, nu, nv, normal, q_method, step_len, max_steps, delta, twist=False):
+def trace_fastqsl(b, seeds, *, normal=(0.0, 0.0, 1.0), step_len: float = 1.0 / 8.0, tol: float = 0.1,
+                  twist: bool = False):
+    """FastQSL's adaptive trace of every seed (``nfgs_trace_fastqsl``: the
+    reference's RKF4(5) step control, face handling and limits in FP32).
+    b (3, nz, ny, nx) CUDA tensor (cast to float32, as the reference does);
+    seeds (n, 3) xyz grid coordinates.  Returns device tensors ends (2, n, 3)
+    ([0] end along +B, [1] start along -B), flags (2, n) int32, bsamp
+    (3, 3, n) (B components at the seed, end and start), bflag (n,) int32,
+    length (n,) float64 (both halves) and with twist=True twist (n,)."""
+    torch = _torch()
+    if b.device.type != "cuda" or b.ndim != 4 or b.shape[0] != 3:
+        raise ValueError("b must be a (3, nz, ny, nx) CUDA tensor")
+    b = b.to(torch.float32).contiguous()
+    _, nz, ny, nx = (int(v) for v in b.shape)
+    seeds = seeds.to(device=b.device, dtype=torch.float32).reshape(-1, 3).contiguous()
+    n = int(seeds.shape[0])
+    dev = b.device
+    out = {"ends": torch.empty((2, n, 3), dtype=torch.float32, device=dev),
+           "flags": torch.empty((2, n), dtype=torch.int32, device=dev),
+           "bsamp": torch.empty((3, 3, n), dtype=torch.float32, device=dev),
+           "bflag": torch.empty((n,), dtype=torch.int32, device=dev),
+           "length": torch.empty((n,), dtype=torch.float64, device=dev)}
+    if twist:
+        out["twist"] = torch.empty((n,), dtype=torch.float64, device=dev)
+    nrm = np.asarray(normal, dtype=np.float64)
+    stream = torch.cuda.current_stream(dev)
+    ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    L.check(L.lib().nfgs_trace_fastqsl(
+        ptr(b), nz, ny, nx, ptr(seeds), n, L.dptr(nrm), float(step_len), float(tol), int(bool(twist)),
+        ptr(out["ends"]), ptr(out["flags"]), ptr(out["bsamp"]), ptr(out["bflag"]), ptr(out["length"]),
+        C.c_void_p(out["twist"].data_ptr() if twist else None), C.c_void_p(stream.cuda_stream)))
+    return out
+
+
+def qcalc_plane(tr, nu: int, nv: int, normal, stride: float = 1.0):
+    """QCalcPlane's Q (nv, nu) on the device from a trace_fastqsl of an
+    nv x nu seed grid (``nfgs_qcalc_plane``)."""
+    torch = _torch()
+    q = torch.empty((nv, nu), dtype=torch.float32, device=tr["ends"].device)
+    nrm = np.asarray(normal, dtype=np.float64)
+    stream = torch.cuda.current_stream(q.device)
+    L.check(L.lib().nfgs_qcalc_plane(int(nu), int(nv), C.c_void_p(tr["ends"].data_ptr()),
+                                     C.c_void_p(tr["flags"].data_ptr()), C.c_void_p(tr["bsamp"].data_ptr()),
+                                     L.dptr(nrm), float(stride), C.c_void_p(q.data_ptr()),
+                                     C.c_void_p(stream.cuda_stream)))
+    return q
+
+
+def _plane_q(b, seeds, nu, nv, normal, q_method, step_len, max_steps, delta, twist=False, tol=0.1):
     """Trace the nv x nu seed grid and evaluate Q by the chosen method; the
     plane's border is NaN either way (the reference keeps only the interior)."""
+    if q_method == "fastqsl":
+        tr = trace_fastqsl(b, seeds, normal=normal, step_len=step_len, tol=tol, twist=twist)
+        tr["max_steps"] = None
+        return tr, qcalc_plane(tr, nu, nv, normal)
     if q_method == "perp":
         tr = trace_qperp(b, seeds, delta=delta, step_len=step_len, max_steps=max_steps, twist=twist)
         q = tr["q"].reshape(nv, nu).clone()
@@ -177,7 +227,7 @@ def _plane_q(b, seeds, nu, nv, normal, q_method, step_len, max_steps, delta, twi
     if q_method == "plane":
         tr = trace_field_lines(b, seeds, normal=normal, step_len=step_len, max_steps=max_steps, twist=twist)
         return tr, q_on_plane(tr, nu, nv)
-    raise ValueError("q_method must be 'perp' or 'plane'")
+    raise ValueError("q_method must be 'fastqsl', 'perp' or 'plane'")
 
 
 def q_on_plane(tr, nu: int, nv: int):
@@ -196,10 +246,12 @@ def _bundle(tr, q, plane_shape, meta):
     nv, nu = plane_shape
     ends = tr["ends"].float().cpu().numpy()
     flags = tr["flags"].cpu().numpy()
-    length = (tr["length"][0] + tr["length"][1]).float().cpu().numpy()
+    both = tr["length"].ndim == 1  # the FastQSL trace sums the halves itself
+    length = (tr["length"] if both else tr["length"][0] + tr["length"][1]).float().cpu().numpy()
     extra = {}
     if "twist" in tr:
-        extra["twist"] = (tr["twist"][0] + tr["twist"][1]).double().cpu().numpy().reshape(nv, nu)
+        tw = tr["twist"] if both else tr["twist"][0] + tr["twist"][1]
+        extra["twist"] = tw.double().cpu().numpy().reshape(nv, nu)
     return {**extra,
         "q": q.float().cpu().numpy(),
         "flag_start": flags[1].reshape(nv, nu).astype(np.int32),
@@ -213,13 +265,15 @@ def _bundle(tr, q, plane_shape, meta):
 
 def compute_y0_qmap(bx, by, bz, *, fastqsl_root=None, y_index=None, step_len: float = 1.0 / 8.0, tol: float = 0.1,
                     block_x: int = 128, trace_chunk_seeds: int = 8192, b_smooth_sigma_cells: float = 0.0,
-                    include_twist: bool = False, dtype: str = "float32", max_steps=None, q_method: str = "perp",
-                    delta: float = 0.25):
+                    include_twist: bool = False, dtype: str = "float32", max_steps=None,
+                    q_method: str = "fastqsl", delta: float = 0.25):
     """Q on the x-z plane at y = y_index (default the physical midplane),
     shape (nz, nx), seeds at every x-z node (fastqsl_plane.py:203-383).
-    q_method "perp" (default): Q_perp from lines offset perpendicular to B by
-    +-delta, defined where B lies in the plane (By = 0 on the midplane of a
-    symmetric field); "plane": central differences over the seed grid."""
+    q_method "fastqsl" (default): the reference's FastQSL adaptive trace and
+    QCalcPlane in FP32; "perp": Q_perp from RK4 lines offset perpendicular to
+    B by +-delta, defined where B lies in the plane (By = 0 on the midplane of
+    a symmetric field); "plane": RK4 lines and central differences over the
+    seed grid."""
     torch = _torch()
     dt = torch.float64 if str(dtype) in ("float64", "torch.float64") else torch.float32
     b = spectral_gaussian_lowpass(_volume(bx, by, bz, dt), b_smooth_sigma_cells)
@@ -233,9 +287,10 @@ def compute_y0_qmap(bx, by, bz, *, fastqsl_root=None, y_index=None, step_len: fl
                           indexing="ij")
     seeds = torch.stack([x.reshape(-1), torch.full_like(x.reshape(-1), iy), z.reshape(-1)], dim=1)
     tr, q = _plane_q(b, seeds, nx, nz, (0.0, 1.0, 0.0), q_method, step_len, max_steps, delta,
-                     twist=bool(include_twist))
+                     twist=bool(include_twist), tol=tol)
     torch.cuda.synchronize()
-    meta = {"algorithm": f"B200 RK4 tracer + Q ({q_method}) on y=0", "q_method": q_method, "delta": float(delta),
+    algo = "FastQSL QCalcPlane on y=0" if q_method == "fastqsl" else f"B200 RK4 tracer + Q ({q_method}) on y=0"
+    meta = {"algorithm": algo, "q_method": q_method, "delta": float(delta),
             "shape_zyx": [nz, ny, nx],
             "plane_y_index": iy, "plane_coordinate_contract": Y0_PLANE_COORDINATE_CONTRACT,
             "plane_is_fractional": bool(not float(iy).is_integer()), "plane_shape_zx": [nz, nx],
@@ -250,9 +305,10 @@ def compute_y0_qmap(bx, by, bz, *, fastqsl_root=None, y_index=None, step_len: fl
 def compute_bottom_qmap(bx, by, bz, *, fastqsl_root=None, z_index=None, step_len: float = 1.0 / 8.0,
                         tol: float = 0.1, block_x: int = 128, trace_chunk_seeds: int = 8192,
                         b_smooth_sigma_cells: float = 0.0, dtype: str = "float32", max_steps=None,
-                        q_method: str = "perp", delta: float = 0.25):
+                        q_method: str = "fastqsl", delta: float = 0.25):
     """Q on the bottom x-y plane, shape (ny, nx); seeds half a cell above the
-    bottom face by default (z = 0.5), normal +z (fastqsl_plane.py:385-506)."""
+    bottom face by default (z = 0.5), normal +z (fastqsl_plane.py:385-506).
+    q_method as compute_y0_qmap."""
     torch = _torch()
     dt = torch.float64 if str(dtype) in ("float64", "torch.float64") else torch.float32
     b = spectral_gaussian_lowpass(_volume(bx, by, bz, dt), b_smooth_sigma_cells)
@@ -265,9 +321,11 @@ def compute_bottom_qmap(bx, by, bz, *, fastqsl_root=None, z_index=None, step_len
     y, x = torch.meshgrid(torch.arange(ny, dtype=dt, device=b.device), torch.arange(nx, dtype=dt, device=b.device),
                           indexing="ij")
     seeds = torch.stack([x.reshape(-1), y.reshape(-1), torch.full_like(x.reshape(-1), iz)], dim=1)
-    tr, q = _plane_q(b, seeds, nx, ny, (0.0, 0.0, 1.0), q_method, step_len, max_steps, delta)
+    tr, q = _plane_q(b, seeds, nx, ny, (0.0, 0.0, 1.0), q_method, step_len, max_steps, delta, tol=tol)
     torch.cuda.synchronize()
-    meta = {"algorithm": f"B200 RK4 tracer + Q ({q_method}) on the bottom plane", "q_method": q_method,
+    algo = ("FastQSL QCalcPlane on the bottom plane" if q_method == "fastqsl"
+            else f"B200 RK4 tracer + Q ({q_method}) on the bottom plane")
+    meta = {"algorithm": algo, "q_method": q_method,
             "delta": float(delta), "shape_zyx": [nz, ny, nx],
             "plane_z_index": iz, "plane_shape_yx": [ny, nx], "step_len_grid": float(step_len),
             "tolerance": float(tol), "max_steps": tr["max_steps"], "block": [int(block_x), 1, 1],

@@ -135,7 +135,8 @@ def test_reference_helpers_contract():
     assert r["q"].shape == (17, 33) and r["start_xyz"].shape == (17, 33, 3) and r["line_len"].shape == (17, 33)
     assert np.isnan(r["q"][0]).all() and np.isnan(r["q"][:, -1]).all()
     assert r["metadata"]["plane_y_index"] == 13.5 and r["metadata"]["plane_is_fractional"]
-    ok = r["flag_start"] > 0
+    assert r["metadata"]["q_method"] == "fastqsl"
+    ok = (r["flag_start"] > 0) & (r["flag_start"] <= 6)
     assert ok.sum() > 0.5 * ok.size and (r["start_xyz"][ok] >= 0.0).all()
     rb = Q.compute_bottom_qmap(b[0], b[1], b[2])
     assert rb["q"].shape == (28, 33) and np.isfinite(rb["q"]).sum() > 100
@@ -195,13 +196,13 @@ def test_qperp_fp64_matches_oracle():
     np.testing.assert_allclose(r["q"][fin], q[fin], rtol=1e-6)
 
 
-def test_y0_helper_defaults_to_qperp():
+def test_y0_helper_qperp_method():
     from nfgs_b200 import qmap as Q
     from oracle import trace_oracle as T
 
     nx, ny, nz, L = 41, 41, 21, 20.0
     b = T.hyperbolic_field(nx, ny, nz, L).astype(np.float32)
-    r = Q.compute_y0_qmap(b[0], b[1], b[2])  # y index 20: the plane containing B
+    r = Q.compute_y0_qmap(b[0], b[1], b[2], q_method="perp")  # y index 20: the plane containing B
     assert r["metadata"]["q_method"] == "perp"
     np.testing.assert_allclose(r["q"][3:18, 14:27], 2.0 * np.cosh(2.0), rtol=5e-3)
     rp = Q.compute_y0_qmap(b[0], b[1], b[2], q_method="plane")
