@@ -109,45 +109,34 @@ __device__ __forceinline__ F3 interp_dir(const Field& f, F3 p, bool norm, int of
 }
 
 // trilinear sample of one component (offset c of the packed field) inside
-// [1e-4, N - 1 - 1e-4], the weights and the sum in double (Interp3d), for
-// the field recorded at the seed and the ends; written as the reference
-// writes it so that the compiler forms the same operations
-__device__ __noinline__ float interp3d(const Field& f, int c, float inPoint_0, float inPoint_1, float inPoint_2) {
-    float rx, ry, rz;
-    float Arr000, Arr001, Arr010, Arr011, Arr100, Arr101, Arr110, Arr111;
-    float Aget;
-    int x_Idx, y_Idx, z_Idx;
-    inPoint_0 = (inPoint_0 > 0) ? inPoint_0 : 0.0001;
-    inPoint_1 = (inPoint_1 > 0) ? inPoint_1 : 0.0001;
-    inPoint_2 = (inPoint_2 > 0) ? inPoint_2 : 0.0001;
-    inPoint_0 = (inPoint_0 < f.nx - 1) ? inPoint_0 : ((float)f.nx - 1 - 0.0001);
-    inPoint_1 = (inPoint_1 < f.ny - 1) ? inPoint_1 : ((float)f.ny - 1 - 0.0001);
-    inPoint_2 = (inPoint_2 < f.nz - 1) ? inPoint_2 : ((float)f.nz - 1 - 0.0001);
-    rx = inPoint_0 - floorf(inPoint_0);
-    ry = inPoint_1 - floorf(inPoint_1);
-    rz = inPoint_2 - floorf(inPoint_2);
-    x_Idx = __float2int_rd(inPoint_0);
-    y_Idx = __float2int_rd(inPoint_1);
-    z_Idx = __float2int_rd(inPoint_2);
-    if (!(x_Idx >= 0 && x_Idx <= f.nx - 2)) x_Idx = 0;  // a non-finite position
-    if (!(y_Idx >= 0 && y_Idx <= f.ny - 2)) y_Idx = 0;
-    if (!(z_Idx >= 0 && z_Idx <= f.nz - 2)) z_Idx = 0;
-    auto at = [&](int i, int j, int k) -> float {
-        return __ldg(f.pk + ((long long)k * f.ny * f.nx + (long long)j * f.nx + i) * f.st + c);
+// [1e-4, N - 1 - 1e-4], the weights and the sum in double, for the field
+// recorded at the seed and the ends (TraceBlineAdaptive.cu:46-99).  The sum
+// keeps the reference's term order and operand types (FP32 corner value
+// times double weights, left to right), and stays a separate function as
+// there, so that its rounding is the reference's bit for bit.
+__device__ __noinline__ float interp3d(const Field& f, int c, float px, float py, float pz) {
+    px = (px > 0) ? px : 0.0001;
+    py = (py > 0) ? py : 0.0001;
+    pz = (pz > 0) ? pz : 0.0001;
+    px = (px < f.nx - 1) ? px : ((float)f.nx - 1 - 0.0001);
+    py = (py < f.ny - 1) ? py : ((float)f.ny - 1 - 0.0001);
+    pz = (pz < f.nz - 1) ? pz : ((float)f.nz - 1 - 0.0001);
+    const float tx = px - floorf(px), ty = py - floorf(py), tz = pz - floorf(pz);
+    int i = __float2int_rd(px), j = __float2int_rd(py), k = __float2int_rd(pz);
+    if (!(i >= 0 && i <= f.nx - 2)) i = 0;  // a non-finite position
+    if (!(j >= 0 && j <= f.ny - 2)) j = 0;
+    if (!(k >= 0 && k <= f.nz - 2)) k = 0;
+    auto at = [&](int ii, int jj, int kk) -> float {
+        return __ldg(f.pk + ((long long)kk * f.ny * f.nx + (long long)jj * f.nx + ii) * f.st + c);
     };
-    Arr000 = at(x_Idx, y_Idx, z_Idx);
-    Arr001 = at(x_Idx, y_Idx, z_Idx + 1);
-    Arr010 = at(x_Idx, y_Idx + 1, z_Idx);
-    Arr011 = at(x_Idx, y_Idx + 1, z_Idx + 1);
-    Arr100 = at(x_Idx + 1, y_Idx, z_Idx);
-    Arr101 = at(x_Idx + 1, y_Idx, z_Idx + 1);
-    Arr110 = at(x_Idx + 1, y_Idx + 1, z_Idx);
-    Arr111 = at(x_Idx + 1, y_Idx + 1, z_Idx + 1);
-    Aget = Arr000 * (1. - rx) * (1. - ry) * (1. - rz) + Arr001 * (1. - rx) * (1. - ry) * (rz) +
-           Arr010 * (1. - rx) * (ry) * (1. - rz) + Arr011 * (1. - rx) * (ry) * (rz) +
-           Arr100 * (rx) * (1. - ry) * (1. - rz) + Arr101 * (rx) * (1. - ry) * (rz) +
-           Arr110 * (rx) * (ry) * (1. - rz) + Arr111 * (rx) * (ry) * (rz);
-    return Aget;
+    const float c000 = at(i, j, k), c001 = at(i, j, k + 1), c010 = at(i, j + 1, k), c011 = at(i, j + 1, k + 1);
+    const float c100 = at(i + 1, j, k), c101 = at(i + 1, j, k + 1), c110 = at(i + 1, j + 1, k);
+    const float c111 = at(i + 1, j + 1, k + 1);
+    const float v = c000 * (1. - tx) * (1. - ty) * (1. - tz) + c001 * (1. - tx) * (1. - ty) * (tz) +
+                    c010 * (1. - tx) * (ty) * (1. - tz) + c011 * (1. - tx) * (ty) * (tz) +
+                    c100 * (tx) * (1. - ty) * (1. - tz) + c101 * (tx) * (1. - ty) * (tz) +
+                    c110 * (tx) * (ty) * (1. - tz) + c111 * (tx) * (ty) * (tz);
+    return v;
 }
 
 __device__ __forceinline__ F3 interp_sample(const Field& f, F3 p) {

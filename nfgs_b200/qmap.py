@@ -350,6 +350,7 @@ def main(argv=None):
     ap.add_argument("--field", choices=["solve", "td"], default="solve")
     ap.add_argument("--iters", type=int, default=400)
     ap.add_argument("--report", default=None)
+    ap.add_argument("--q-method", default="fastqsl", choices=["fastqsl", "perp", "plane"])
     args = ap.parse_args(argv)
     if args.field == "solve":
         h = 16.0 / (args.n - 1)
@@ -364,17 +365,16 @@ def main(argv=None):
                             device="cuda")
         out = {"field": "analytic TD (td_volume seed 1)", "grid_zyx": [int(v) for v in f.shape[1:]]}
     for name, fn in (("y0", compute_y0_qmap), ("bottom", compute_bottom_qmap)):
-        fn(f[0], f[1], f[2])  # warm-up
-        r = fn(f[0], f[1], f[2])
+        fn(f[0], f[1], f[2], q_method=args.q_method)  # warm-up
+        r = fn(f[0], f[1], f[2], q_method=args.q_method)
         lens = r["line_len"]
         qv = r["q"][np.isfinite(r["q"])]
         seeds = r["q"].size
-        out[name] = {"seeds": seeds, "seconds": r["metadata"]["elapsed_s"],
+        out[name] = {"seeds": seeds, "seconds": r["metadata"]["elapsed_s"], "q_method": r["metadata"]["q_method"],
                      "lines_per_s": (10 if r["metadata"]["q_method"] == "perp" else 2) * seeds
                      / r["metadata"]["elapsed_s"],
                      "mean_line_len": float(np.mean(lens)),
-                     "central_rk4_steps_per_s": float(np.sum(lens)) / r["metadata"]["step_len_grid"]
-                     / r["metadata"]["elapsed_s"],
+                     "cells_traced_per_s": float(np.sum(lens)) / r["metadata"]["elapsed_s"],
                      "q_valid": int(qv.size), "q_median": float(np.median(qv)) if qv.size else None,
                      "log10_q_p99": float(np.log10(np.percentile(qv, 99))) if qv.size else None}
     torch.cuda.synchronize()
