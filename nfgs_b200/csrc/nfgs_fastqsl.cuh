@@ -59,21 +59,26 @@ __device__ __forceinline__ float len3(F3 a) { return sqrtf(a.x * a.x + a.y * a.y
 __device__ __forceinline__ float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 __device__ __forceinline__ float comp(F3 a, int d) { return d == 0 ? a.x : (d == 1 ? a.y : a.z); }
 
+// B (and, for the twist, J) as (3, nz, ny, nx) component-major FP32 volumes:
+// three FP32 values per node, the footprint the reference reads (a 256^2 x 128
+// field, 101 MB, stays in the 126 MB L2; padded to four values it would not)
 struct Field {
-    const float* pk;  // packed (Bx, By, Bz, 0[, Jx, Jy, Jz, 0]) per node
-    int nx, ny, nz, st;
+    const float* b;  // (3, V)
+    const float* j;  // (3, V) or null
+    int nx, ny, nz;
+    long long V;
 };
 
-// node value (three components at offset off) of the packed field
-__device__ __forceinline__ F3 node(const Field& f, int i, int j, int k, int off) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(
-        f.pk + ((long long)k * f.ny * f.nx + (long long)j * f.nx + i) * f.st + off));
-    return f3(v.x, v.y, v.z);
+// node value of B (cur == false) or J (cur == true)
+__device__ __forceinline__ F3 node(const Field& f, int i, int j, int k, bool cur) {
+    const float* a = cur ? f.j : f.b;
+    const unsigned q = ((unsigned)k * (unsigned)f.ny + (unsigned)j) * (unsigned)f.nx + (unsigned)i;  // V < 2^31
+    return f3(__ldg(a + q), __ldg(a + f.V + q), __ldg(a + 2 * f.V + q));
 }
 
 // trilinear vector at p with the faces' outermost cell (TraceBlineAdaptive
 // Interp3dxyzn); unit length when norm
-__device__ __forceinline__ F3 interp_dir(const Field& f, F3 p, bool norm, int off = 0) {
+__device__ __forceinline__ F3 interp_dir(const Field& f, F3 p, bool norm, bool off = false) {
     float rx = p.x - floorf(p.x), ry = p.y - floorf(p.y), rz = p.z - floorf(p.z);
     int i = __float2int_rd(p.x), j = __float2int_rd(p.y), k = __float2int_rd(p.z);
     if (p.x <= 0.f) { rx = 0.f; i = 0; }
@@ -127,7 +132,7 @@ __device__ __noinline__ float interp3d(const Field& f, int c, float px, float py
     if (!(j >= 0 && j <= f.ny - 2)) j = 0;
     if (!(k >= 0 && k <= f.nz - 2)) k = 0;
     auto at = [&](int ii, int jj, int kk) -> float {
-        return __ldg(f.pk + ((long long)kk * f.ny * f.nx + (long long)jj * f.nx + ii) * f.st + c);
+        return __ldg(f.b + c * f.V + (((unsigned)kk * (unsigned)f.ny + (unsigned)jj) * (unsigned)f.nx + (unsigned)ii));
     };
     const float c000 = at(i, j, k), c001 = at(i, j, k + 1), c010 = at(i, j + 1, k), c011 = at(i, j + 1, k + 1);
     const float c100 = at(i + 1, j, k), c101 = at(i + 1, j, k + 1), c110 = at(i + 1, j + 1, k);
@@ -141,6 +146,22 @@ __device__ __noinline__ float interp3d(const Field& f, int c, float px, float py
 
 __device__ __forceinline__ F3 interp_sample(const Field& f, F3 p) {
     return f3(interp3d(f, 0, p.x, p.y, p.z), interp3d(f, 1, p.x, p.y, p.z), interp3d(f, 2, p.x, p.y, p.z));
+}
+
+// J = curl B in grid units, centred with second-order one-sided edges (the
+// current fastqsl_plane.py:287-305 passes to the tracer), (3, V) FP32
+__global__ void k_curl(const float* __restrict__ b, int nx, int ny, int nz, float* __restrict__ jo) {
+    const long long V = (long long)nx * ny * nz;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= V) return;
+    const int i = (int)(c % nx), j = (int)((c / nx) % ny), k = (int)(c / ((long long)nx * ny));
+    const long long P = (long long)nx * ny;
+    auto ax = [&](int comp) { return [=](int q) { return b[comp * V + c + (q - i)]; }; };
+    auto ay = [&](int comp) { return [=](int q) { return b[comp * V + c + (long long)(q - j) * nx]; }; };
+    auto az = [&](int comp) { return [=](int q) { return b[comp * V + c + (long long)(q - k) * P]; }; };
+    jo[c] = trace::grad1<float>(ay(2), j, ny) - trace::grad1<float>(az(1), k, nz);
+    jo[V + c] = trace::grad1<float>(az(0), k, nz) - trace::grad1<float>(ax(2), i, nx);
+    jo[2 * V + c] = trace::grad1<float>(ax(1), i, nx) - trace::grad1<float>(ay(0), j, ny);
 }
 
 // Fehlberg 4(5) stage coefficients (Fehlberg 1969, as single-precision
@@ -231,8 +252,8 @@ __device__ int trace_line(const Field& f, F3 p0, F3 n0, float h, float tol_coef,
         len += dl;
         double dtw = 0.0;
         if (TW) {
-            const F3 c1 = interp_dir(f, p1, false, 4);
-            const F3 b1 = interp_dir(f, p1, false, 0);
+            const F3 c1 = interp_dir(f, p1, false, true);
+            const F3 b1 = interp_dir(f, p1, false, false);
             dtw = (double)(dot3(c1, b1) / dot3(b1, b1)) / 4.0 / PI_REF * (double)dl;
             tw += dtw;
         }
@@ -270,39 +291,63 @@ __device__ int trace_line(const Field& f, F3 p0, F3 n0, float h, float tol_coef,
     return code;
 }
 
-// One thread per seed (TraceAllBline): the forward line (+B) gives the end,
-// the backward line (-B) the start.  ends (2, n, 3): [0] end, [1] start;
+// Lines are handed out dynamically: each warp takes the next 32 of the 2n
+// half-lines (t = dir * n + seed) from a global counter, so that warps that
+// drew short lines move on while others finish long ones, and the lanes of a
+// warp follow neighbouring lines.  (TraceAllBline runs both halves of a seed
+// in one thread; each half's result is the same.)  dir 0 traces along +B to
+// the end, dir 1 along -B to the start.  ends (2, n, 3): [0] end, [1] start;
 // flags (2, n); bs (3, 3, n): B at the seed, the end and the start (x, y, z
-// rows); bflag (n): 1 where |B.n| < |B| / 100 at the seed; len (n): the two
-// path lengths summed; tw (n): the twist of both halves (with TW).
+// rows); bflag (n): 1 where |B.n| < |B| / 100 at the seed; half (2, 2, n):
+// each half's path length and twist, summed by k_fq_sum; counter zeroed.
 template <bool TW>
 __global__ void __launch_bounds__(128) k_trace_fq(Field f, const float* __restrict__ seeds, long long n, F3 n0,
                                                   float h, float tol_coef, float* __restrict__ ends,
                                                   int* __restrict__ flags, float* __restrict__ bs,
-                                                  int* __restrict__ bflag, double* __restrict__ len,
-                                                  double* __restrict__ tw) {
+                                                  int* __restrict__ bflag, double* __restrict__ half,
+                                                  unsigned long long* __restrict__ counter) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long total = 2ull * (unsigned long long)n;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(counter, 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) return;
+        const unsigned long long tt = base + lane;
+        if (tt >= total) continue;
+        const long long t = (long long)tt;
+        const int dir = t >= n ? 1 : 0;
+        const long long si = t - (long long)dir * n;
+        const F3 p0 = f3(seeds[3 * si], seeds[3 * si + 1], seeds[3 * si + 2]);
+        F3 pe;
+        double le, te;
+        const int code = trace_line<TW>(f, p0, n0, h, tol_coef, dir == 0 ? 1.0f : -1.0f, pe, le, te);
+        ends[3 * t] = pe.x; ends[3 * t + 1] = pe.y; ends[3 * t + 2] = pe.z;
+        flags[t] = code;
+        const F3 be = interp_sample(f, pe);
+        bs[(0 * 3 + 1 + dir) * n + si] = be.x;
+        bs[(1 * 3 + 1 + dir) * n + si] = be.y;
+        bs[(2 * 3 + 1 + dir) * n + si] = be.z;
+        half[t] = le;
+        if (TW) half[2 * n + t] = te;
+        if (dir == 0) {
+            const F3 b0 = interp_sample(f, p0);
+            bs[0 * n + si] = b0.x;
+            bs[3 * n + si] = b0.y;
+            bs[6 * n + si] = b0.z;
+            bflag[si] = (double)fabsf(b0.x * n0.x + b0.y * n0.y + b0.z * n0.z) * 100.0 < (double)len3(b0) ? 1 : 0;
+        }
+    }
+}
+
+// length (n) = forward + backward half, twist likewise (the reference's
+// order of the two additions)
+__global__ void k_fq_sum(long long n, const double* __restrict__ half, double* __restrict__ len,
+                         double* __restrict__ tw) {
     const long long si = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (si >= n) return;
-    const F3 p0 = f3(seeds[3 * si], seeds[3 * si + 1], seeds[3 * si + 2]);
-    F3 pe, ps;
-    double le, ls, te, ts;
-    const int ce = trace_line<TW>(f, p0, n0, h, tol_coef, 1.0f, pe, le, te);
-    const int cs = trace_line<TW>(f, p0, n0, h, tol_coef, -1.0f, ps, ls, ts);
-    ends[3 * si] = pe.x; ends[3 * si + 1] = pe.y; ends[3 * si + 2] = pe.z;
-    ends[3 * (n + si)] = ps.x; ends[3 * (n + si) + 1] = ps.y; ends[3 * (n + si) + 2] = ps.z;
-    flags[si] = ce;
-    flags[n + si] = cs;
-    const F3 b0 = interp_sample(f, p0), be = interp_sample(f, pe), bst = interp_sample(f, ps);
-    const F3 b3[3] = {b0, be, bst};
-#pragma unroll
-    for (int w = 0; w < 3; ++w) {
-        bs[(0 * 3 + w) * n + si] = b3[w].x;
-        bs[(1 * 3 + w) * n + si] = b3[w].y;
-        bs[(2 * 3 + w) * n + si] = b3[w].z;
-    }
-    bflag[si] = (double)fabsf(b0.x * n0.x + b0.y * n0.y + b0.z * n0.z) * 100.0 < (double)len3(b0) ? 1 : 0;
-    len[si] = le + ls;
-    if (TW) tw[si] = te + ts;
+    len[si] = half[si] + half[n + si];
+    if (tw != nullptr) tw[si] = half[2 * n + si] + half[3 * n + si];
 }
 
 // QCalcPlane on an nv x nu seed plane (seed u + nu v), the end of each seed

@@ -3852,24 +3852,46 @@ int nfgs_trace_fastqsl(const float* b, int32_t nz, int32_t ny, int32_t nx, const
         return fail(NFGS_EINVAL, "null argument");
     if (with_twist && n > 0 && !twist) return fail(NFGS_EINVAL, "null twist output");
     if (nz < 3 || ny < 3 || nx < 3) return fail(NFGS_EINVAL, "the field needs at least 3 nodes per axis");
-    if (n < 0 || n > (int64_t)INT32_MAX * 128) return fail(NFGS_EINVAL, "bad seed count");
+    if ((long long)nx * ny * nz >= (1LL << 31)) return fail(NFGS_EINVAL, "the field needs fewer than 2^31 nodes");
+    if (n < 0 || 2 * n > (int64_t)INT32_MAX * 128) return fail(NFGS_EINVAL, "bad seed count");
     if (!(step > 0.0) || !std::isfinite(step)) return fail(NFGS_EINVAL, "step must be positive");
     if (!(tol_coef > 0.0) || !std::isfinite(tol_coef)) return fail(NFGS_EINVAL, "tol must be positive");
     cudaStream_t s = (cudaStream_t)stream;
-    float* pk = nullptr;
-    cudaError_t e = pack_field<float>(b, nx, ny, nz, with_twist != 0, &pk, s);
+    const long long V = (long long)nx * ny * nz;
+    float* pk = nullptr;   // J for the twist
+    double* half = nullptr;  // per-half path lengths and twists
+    cudaError_t e = cudaSuccess;
+    if (n > 0) e = cudaMallocAsync((void**)&half, (size_t)(4 * n + 1) * sizeof(double), s);
+    unsigned long long* counter = half ? (unsigned long long*)(half + 4 * n) : nullptr;
+    if (e == cudaSuccess && n > 0) e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess && with_twist && n > 0) {
+        e = cudaMallocAsync((void**)&pk, (size_t)3 * V * sizeof(float), s);
+        if (e == cudaSuccess) {
+            fq::k_curl<<<(unsigned)((V + 255) / 256), 256, 0, s>>>(b, nx, ny, nz, pk);
+            e = cudaGetLastError();
+        }
+    }
     if (e == cudaSuccess && n > 0) {
-        const fq::Field f{pk, nx, ny, nz, with_twist ? 8 : 4};
+        const fq::Field f{b, pk, nx, ny, nz, V};
         const fq::F3 n0 = fq::f3((float)normal3[0], (float)normal3[1], (float)normal3[2]);
-        const unsigned grid = (unsigned)((n + 127) / 128);
+        // enough resident warps to keep every SM busy; each pulls lines until none are left
+        int dev = 0, nsm = 148, per_sm = 8;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (with_twist) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fq::k_trace_fq<true>, 128, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fq::k_trace_fq<false>, 128, 0);
+        const long long need = (2 * n + 127) / 128;
+        const unsigned grid = (unsigned)std::max(1LL, std::min(need, (long long)nsm * std::max(per_sm, 1)));
         if (with_twist)
             fq::k_trace_fq<true><<<grid, 128, 0, s>>>(f, seeds, n, n0, (float)step, (float)tol_coef, ends, flags,
-                                                      bsamp, bflag, length, twist);
+                                                      bsamp, bflag, half, counter);
         else
             fq::k_trace_fq<false><<<grid, 128, 0, s>>>(f, seeds, n, n0, (float)step, (float)tol_coef, ends, flags,
-                                                       bsamp, bflag, length, nullptr);
+                                                       bsamp, bflag, half, counter);
+        fq::k_fq_sum<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, half, length, with_twist ? twist : nullptr);
         e = cudaGetLastError();
     }
+    if (half) cudaFreeAsync(half, s);
     if (pk) cudaFreeAsync(pk, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(NFGS_ECUDA, std::string("trace_fastqsl: ") + cudaGetErrorString(e));

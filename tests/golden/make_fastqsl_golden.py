@@ -165,6 +165,90 @@ def qcalc_case(name):
     print(name, "q finite", int(np.isfinite(q).sum()), "median", float(np.nanmedian(q)))
 
 
+def time_against_reference(path, reps=5):
+    """Phase ``time`` (GPU box): the reference kernel, in one launch and in
+    the 8192-seed chunks of fastqsl_plane.py:221-338, against the library's
+    nfgs_trace_fastqsl on the TD99 field at 256 x 256 x 128 (y = 0 midplane and
+    bottom seed planes), CUDA-event times and a bitwise comparison."""
+    import torch
+
+    from nfgs_b200 import qmap
+    from nfgs_b200.synthetic import td_volume
+
+    lib = ctypes.CDLL(str(ROOT / "oracle" / "_ref" / "libfastqsl_ref.so"))
+    lib.fq_ref_trace_all.restype = ctypes.c_int
+    dev = torch.device("cuda")
+    b = torch.as_tensor(td_volume(256, 256, 128, seed=1).astype(np.float32), device=dev)
+    nz, ny, nx = b.shape[1:]
+    out = {}
+
+    def ref(sx, sy, sz, normal, chunk):
+        n = sx.numel()
+        z = lambda dt: torch.zeros(n, dtype=dt, device=dev)  # noqa: E731
+        o = [z(torch.float32) for _ in range(15)]
+        oi = [z(torch.int32) for _ in range(3)]
+        ll = z(torch.float64)
+        dummy = torch.zeros((1, 1), dtype=torch.float32, device=dev)
+        consts = [torch.tensor([nx, ny, nz], dtype=torch.int32, device=dev), torch.tensor([False], device=dev),
+                  torch.tensor(normal, dtype=torch.float32, device=dev),
+                  torch.tensor([STEP], dtype=torch.float32, device=dev),
+                  torch.tensor([TOL], dtype=torch.float32, device=dev)]
+        P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+        comps = [b[c].contiguous() for c in range(3)]
+        for s0 in range(0, n, chunk):
+            s1 = min(n, s0 + chunk)
+            sl = lambda t: t[s0:s1]  # noqa: E731
+            ntr = torch.tensor([s1 - s0], dtype=torch.int64, device=dev)
+            rc = lib.fq_ref_trace_all(
+                *map(P, comps), P(consts[0]), P(dummy), P(dummy), P(dummy), P(dummy), P(consts[1]),
+                P(sl(sx)), P(sl(sy)), P(sl(sz)), P(consts[2]),
+                *(P(sl(o[k])) for k in (0, 1, 2)), P(sl(oi[0])), *(P(sl(o[k])) for k in (3, 4, 5)), P(sl(oi[1])),
+                *(P(sl(o[k])) for k in (6, 7, 8)), P(sl(oi[2])), *(P(sl(o[k])) for k in (9, 10, 11, 12, 13, 14)),
+                P(consts[3]), P(ntr), P(sl(ll)), P(consts[4]), ctypes.c_longlong(s1 - s0), ctypes.c_int(BLOCK),
+                ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+            if rc != 0:
+                raise RuntimeError(f"reference trace launch failed: {rc}")
+        return o, oi, ll
+
+    def timed(fn):
+        r = fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            r = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms)), r
+
+    for plane in ("y0", "bottom"):
+        ar = lambda n: torch.arange(n, dtype=torch.float32, device=dev)  # noqa: E731
+        if plane == "y0":
+            x, zz = torch.meshgrid(ar(nx), ar(nz), indexing="xy")
+            sx, sz = x.reshape(-1), zz.reshape(-1)
+            sy = torch.full_like(sx, 0.5 * (ny - 1))
+            normal = [0.0, 1.0, 0.0]
+        else:
+            x, y = torch.meshgrid(ar(nx), ar(ny), indexing="xy")
+            sx, sy = x.reshape(-1), y.reshape(-1)
+            sz = torch.full_like(sx, 0.5)
+            normal = [0.0, 0.0, 1.0]
+        seeds = torch.stack([sx, sy, sz], 1).contiguous()
+        t_chunk, _ = timed(lambda: ref(sx, sy, sz, normal, 8192))
+        t_one, (o, oi, ll) = timed(lambda: ref(sx, sy, sz, normal, sx.numel()))
+        t_lib, tr = timed(lambda: qmap.trace_fastqsl(b, seeds, normal=normal, step_len=STEP, tol=TOL))
+        same = (torch.equal(tr["ends"][0], torch.stack(o[3:6], 1)) and torch.equal(tr["ends"][1], torch.stack(o[0:3], 1))
+                and torch.equal(tr["flags"][0], oi[1]) and torch.equal(tr["flags"][1], oi[0])
+                and torch.equal(tr["length"], ll))
+        out[plane] = {"seeds": int(sx.numel()), "reference_chunked_8192_ms": t_chunk, "reference_one_launch_ms": t_one,
+                      "library_ms": t_lib, "bitwise_identical": bool(same),
+                      "mean_line_len_cells": float(ll.mean())}
+        print(plane, out[plane], flush=True)
+    Path(path).write_text(json.dumps(out, indent=1) + "\n")
+
+
 if __name__ == "__main__":
     phase = sys.argv[1] if len(sys.argv) > 1 else "trace"
     only = set(sys.argv[2:])
@@ -174,9 +258,11 @@ if __name__ == "__main__":
         for name, spec in CASES.items():
             if not only or name in only:
                 trace_case(name, spec, lib)
+    elif phase == "time":
+        time_against_reference(sys.argv[2] if len(sys.argv) > 2 else "fastqsl_time.json")
     elif phase == "q":
         for name in CASES:
             if not only or name in only:
                 qcalc_case(name)
     else:
-        raise SystemExit("phase must be 'trace' or 'q'")
+        raise SystemExit("phase must be 'trace', 'q' or 'time'")
