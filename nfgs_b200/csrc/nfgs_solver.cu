@@ -25,7 +25,9 @@
 #include <tuple>
 #include <cstdio>
 #include <cstring>
+#include <sys/mman.h>
 #include <string>
+#include <condition_variable>
 #include <thread>
 #include <vector>
 
@@ -158,6 +160,7 @@ struct Handle {
     int graph_kernels = 0;
     int cur_host = 0;       // current state index outside iterate
     void* bscratch = nullptr;  // 3V storage-type scratch (final-vs-best)
+    double* fvb_part = nullptr;  // block partials of the final-vs-best sums
     double* dscratch = nullptr; // V FP64 scratch for host transfers
     int nzo_crop = 0;
     // tensor-core transform plan (FP32 storage, even N with (N-2)/2 <= 128)
@@ -2573,11 +2576,20 @@ static int iterate_end_t(Handle* h, NfgsIterResult* res, double* hist, int hist_
         TRY(run_stencil<T>(h, &h->consts[c.best], nullptr, 0, 0));
         CK(cudaMemcpyAsync(h->bscratch, h->B, V3 * h->esz, cudaMemcpyDeviceToDevice, h->s));
         TRY(run_stencil<T>(h, &h->consts[c.cur], nullptr, 0, 0));
-        k_diff_sums<T><<<1, 1024, 0, h->s>>>((const T*)h->B, (const T*)h->bscratch, (const T*)h->bbg, V3, h->scal);
+        // block partials over the whole device, summed on the host in block order
+        constexpr int kFvbBlocks = 592;
+        if (!h->fvb_part) TRY(alloc(h, &h->fvb_part, 2 * kFvbBlocks * sizeof(double)));
+        k_diff_sums<T><<<kFvbBlocks, 256, 0, h->s>>>((const T*)h->B, (const T*)h->bscratch, (const T*)h->bbg, V3,
+                                                     h->fvb_part);
         CK(cudaGetLastError());
-        double sums[2];
-        CK(cudaMemcpyAsync(sums, h->scal, 16, cudaMemcpyDeviceToHost, h->s));
+        std::vector<double> part(2 * kFvbBlocks);
+        CK(cudaMemcpyAsync(part.data(), h->fvb_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->s));
         CK(cudaStreamSynchronize(h->s));
+        double sums[2] = {0.0, 0.0};
+        for (int b = 0; b < kFvbBlocks; ++b) {
+            sums[0] += part[2 * b];
+            sums[1] += part[2 * b + 1];
+        }
         r.final_vs_best_B_relative = std::sqrt(sums[0] / V3) / std::max(std::sqrt(sums[1] / V3), 1e-30);
         h->launches += 5;
     } else {
@@ -2598,24 +2610,87 @@ static int iterate_end_t(Handle* h, NfgsIterResult* res, double* hist, int hist_
 
 // Host copy of one chunk on up to 8 threads (a fresh pageable destination
 // costs a page fault per page; the threads take those in parallel).
-static void host_copy(char* dst, const char* src, size_t len) {
-    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-    const size_t per = ((len + hw - 1) / hw + 4095) & ~(size_t)4095;
-    if (hw == 1 || len <= per) {
-        std::memcpy(dst, src, len);
-        return;
+// A persistent pool of host-copy workers (up to 16, one per hardware thread),
+// created on first use: the copies of a chunk into a fresh destination take
+// its page faults in parallel, and no thread is created per chunk.
+class CopyPool {
+public:
+    // never destroyed: the workers wait on its condition variable until the
+    // process ends
+    static CopyPool& get() {
+        static CopyPool* pool = new CopyPool();
+        return *pool;
     }
-    std::vector<std::thread> th;
-    for (size_t off = per; off < len; off += per)
-        th.emplace_back([=] { std::memcpy(dst + off, src + off, std::min(per, len - off)); });
-    std::memcpy(dst, src, std::min(per, len));
-    for (auto& t : th) t.join();
-}
+    // copy len bytes in page-aligned slices, one per worker plus the caller
+    void copy(char* dst, const char* src, size_t len) {
+        const size_t parts = workers_.size() + 1;
+        const size_t per = ((len + parts - 1) / parts + 4095) & ~(size_t)4095;
+        if (workers_.empty() || len <= per) {
+            std::memcpy(dst, src, len);
+            return;
+        }
+        std::unique_lock<std::mutex> call(call_mu_);  // one copy at a time through the pool
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            dst_ = dst; src_ = src; len_ = len; per_ = per;
+            pending_ = (int)workers_.size();
+            ++gen_;
+        }
+        cv_.notify_all();
+        std::memcpy(dst, src, std::min(per, len));
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [&] { return pending_ == 0; });
+    }
+
+private:
+    CopyPool() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const unsigned n = std::min(16u, hw > 1 ? hw : 1u) - 1;
+        for (unsigned w = 0; w < n; ++w) workers_.emplace_back([this, w] { run(w + 1); });
+        for (auto& t : workers_) t.detach();
+    }
+    void run(unsigned slot) {
+        unsigned long long seen = 0;
+        for (;;) {
+            char* dst;
+            const char* src;
+            size_t len, per;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return gen_ != seen; });
+                seen = gen_;
+                dst = dst_; src = src_; len = len_; per = per_;
+            }
+            const size_t off = (size_t)slot * per;
+            if (off < len) std::memcpy(dst + off, src + off, std::min(per, len - off));
+            std::lock_guard<std::mutex> lk(mu_);
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex mu_, call_mu_;
+    std::condition_variable cv_, done_;
+    char* dst_ = nullptr;
+    const char* src_ = nullptr;
+    size_t len_ = 0, per_ = 0;
+    int pending_ = 0;
+    unsigned long long gen_ = 0;
+};
+
+static void host_copy(char* dst, const char* src, size_t len) { CopyPool::get().copy(dst, src, len); }
 
 // Copy n bytes from device memory to pageable host memory through two pinned
 // chunks: the DMA of chunk k overlaps the host copy of chunk k-1.
 static int d2h_chunked(Handle* h, void* host, const void* dev, size_t n) {
     const size_t CH = PIN_CHUNK;
+    // a fresh destination faults its pages in during the copy: ask for 2 MB
+    // pages on the 2 MB-aligned part of it (advice only; ignored where the
+    // memory is not anonymous or the kernel declines)
+    {
+        const uintptr_t lo = ((uintptr_t)host + (2u << 20) - 1) & ~(uintptr_t)((2u << 20) - 1);
+        const uintptr_t hi = ((uintptr_t)host + n) & ~(uintptr_t)((2u << 20) - 1);
+        if (hi > lo) (void)madvise((void*)lo, hi - lo, MADV_HUGEPAGE);
+    }
     struct Pins {
         void* p[2] = {nullptr, nullptr};
         ~Pins() { pin_release(p[0]); pin_release(p[1]); }
