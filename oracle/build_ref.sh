@@ -15,5 +15,5 @@ if [ ! -f "$SRC/TraceBlineAdaptive.cu" ]; then
 fi
 mkdir -p "$HERE/_ref"
 "$NVCC" -O3 -std=c++17 -gencode arch=compute_100a,code=sm_100a -Xcompiler -fPIC -shared \
-    -diag-suppress 177,550,1444,2464 -I "$SRC" "$HERE/fastqsl_ref_launch.cu" -o "$HERE/_ref/libfastqsl_ref.so"
+    -diag-suppress 177,550,1444,2464 -Xcompiler -w -I "$SRC" "$HERE/fastqsl_ref_launch.cu" -o "$HERE/_ref/libfastqsl_ref.so"
 echo "built $HERE/_ref/libfastqsl_ref.so"
