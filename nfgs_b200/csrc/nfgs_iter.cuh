@@ -339,8 +339,17 @@ __global__ void __launch_bounds__(128) k_src(Geo g, const int* skip, const T* __
 // both values equal their converged limits (checked bitwise when the
 // tables are built), which are kept in registers instead of being re-read.
 // ---------------------------------------------------------------------------
-// rows per batch of independent loads in the z-solves
-#define ZB 16
+// Rows per batch of independent loads in the z-solves: rows whose factors
+// still come from the tables load them with the values (ZB rows); rows past
+// the warp's largest rconv use the converged factors held in registers and
+// load only the values (ZBV rows: 32 in FP32, 16 in FP64), so a thread needs
+// few round trips to memory with 64 registers, and both chains of the
+// benchmark grid fit on the GPU in one wave.
+#define ZB 8
+template <typename T>
+struct ZRows {
+    static constexpr int V = 64 / (int)sizeof(T);
+};
 
 struct ZTab {
     const double* c;      // [rows][modes]
@@ -351,26 +360,128 @@ struct ZTab {
     const int* rconv;
 };
 
+// Forward elimination over rows r_lo..r_hi (row r at plane r + 1):
+// d = (hat * sc - low * d) * inv_r, inv_r from the table below row rc and
+// iinf from it on; s_last is the scaled source of the last row.  Addresses
+// advance by the plane stride, so a batch holds only its values.
+template <typename T, int B, bool TAB>
+__device__ __forceinline__ void zs_forward(T* __restrict__ hat, long long stride, long long m, int r_lo, int r_hi,
+                                           double sc, double low, double& d, double& s_last,
+                                           const double* __restrict__ inv, int rc, double iinf) {
+    for (int r0 = r_lo; r0 <= r_hi; r0 += B) {
+        T sv[B];
+        double ivb[TAB ? B : 1];
+        T* const row0 = hat + (long long)(r0 + 1) * stride + m;
+        {
+            const T* q = row0;
+            const double* ti = inv + (long long)r0 * stride + m;
+#pragma unroll
+            for (int u = 0; u < B; ++u, q += stride, ti += stride) {
+                const int r = r0 + u;
+                sv[u] = (r <= r_hi) ? *q : T(0);
+                if constexpr (TAB) ivb[u] = (r <= r_hi && r < rc) ? *ti : iinf;
+            }
+        }
+        T* q = row0;
+#pragma unroll
+        for (int u = 0; u < B; ++u, q += stride) {
+            const int r = r0 + u;
+            if (r <= r_hi) {
+                const double s = (double)sv[u] * sc;
+                s_last = s;
+                if constexpr (TAB) d = (s - low * d) * ivb[u];
+                else d = (s - low * d) * iinf;
+                *q = (T)d;
+            }
+        }
+    }
+}
+
+// Back substitution over rows r_hi down to r_lo: u = hat - c_r u.
+template <typename T, int B, bool TAB>
+__device__ __forceinline__ void zs_back(T* __restrict__ hat, long long stride, long long m, int r_hi, int r_lo,
+                                        double& u, const double* __restrict__ c, int rc, double cinf) {
+    for (int r0 = r_hi; r0 >= r_lo; r0 -= B) {
+        T dv[B];
+        double crb[TAB ? B : 1];
+        T* const row0 = hat + (long long)(r0 + 1) * stride + m;
+        {
+            const T* q = row0;
+            const double* tc = c + (long long)r0 * stride + m;
+#pragma unroll
+            for (int k = 0; k < B; ++k, q -= stride, tc -= stride) {
+                const int r = r0 - k;
+                dv[k] = (r >= r_lo) ? *q : T(0);
+                if constexpr (TAB) crb[k] = (r >= r_lo && r < rc) ? *tc : cinf;
+            }
+        }
+        T* q = row0;
+#pragma unroll
+        for (int k = 0; k < B; ++k, q -= stride) {
+            const int r = r0 - k;
+            if (r >= r_lo) {
+                if constexpr (TAB) u = (double)dv[k] - crb[k] * u;
+                else u = (double)dv[k] - cinf * u;
+                *q = (T)u;
+            }
+        }
+    }
+}
+
+// Both sweeps of rows 0..last (hat rows at planes 1..last+1); row 0's
+// forward value d0 and the row after last (the closing row, solved by the
+// caller between the sweeps) are handled outside.  rcw >= rc: the warp's
+// split between table rows and converged rows.
+template <typename T>
+struct ZSweep {
+    T* hat;
+    long long stride, m;
+    int rc, rcw;
+    const double* inv;
+    const double* c;
+    double iinf, cinf;
+    __device__ __forceinline__ void forward(int last, double sc, double low, double& d, double& s_last) const {
+        const int a_hi = min(rcw - 1, last);
+        if (a_hi >= 1) zs_forward<T, ZB, true>(hat, stride, m, 1, a_hi, sc, low, d, s_last, inv, rc, iinf);
+        zs_forward<T, ZRows<T>::V, false>(hat, stride, m, max(1, rcw), last, sc, low, d, s_last, inv, rc, iinf);
+    }
+    __device__ __forceinline__ void back(int last, double& u) const {
+        zs_back<T, ZRows<T>::V, false>(hat, stride, m, last, max(0, rcw), u, c, rc, cinf);
+        const int a_hi = min(rcw - 1, last);
+        if (a_hi >= 0) zs_back<T, ZB, true>(hat, stride, m, a_hi, 0, u, c, rc, cinf);
+    }
+};
+
 // Robin chain (nfgs_solver.py:5512-5625 with 5627-5672): unknown planes
 // 1..nz-1, rhs_r = S_hat(plane r+1) / lambda (FP64), mode (0,0) forced 0.
 template <typename T>
 __device__ void zsolve_robin_mode(Geo g, long long m, T* __restrict__ hat, ZTab t, const double* __restrict__ lam,
                                   const double* __restrict__ bot_hat, const double* __restrict__ der_hat,
-                                  double rho, double* __restrict__ s00) {
+                                  double rho, double* __restrict__ s00, int rcw) {
     const long long P = g.P;
     const int nz = g.nz;
     const int n = nz - 1;
     if (m == 0) {
-        if (s00 != nullptr)
-            for (int p = 0; p < nz; ++p) s00[p] = (double)hat[(long long)p * P];
-        for (int p = 1; p < nz; ++p) hat[(long long)p * P] = T(0);
+        // the (0,0) profile for the zero-mode diagnostic, loaded in batches
+        for (int p0 = 0; p0 < nz; p0 += ZRows<T>::V) {
+            T v[ZRows<T>::V];
+#pragma unroll
+            for (int q = 0; q < ZRows<T>::V; ++q) v[q] = (p0 + q < nz) ? hat[(long long)(p0 + q) * P] : T(0);
+#pragma unroll
+            for (int q = 0; q < ZRows<T>::V; ++q) {
+                const int p = p0 + q;
+                if (p < nz) {
+                    if (s00 != nullptr) s00[p] = (double)v[q];
+                    if (p >= 1) hat[(long long)p * P] = T(0);
+                }
+            }
+        }
         return;
     }
     const double dz = g.dz, dz2 = dz * dz, low = 1.0 / dz2;
     const double ls = lam[m];
     const double ils = 1.0 / ls;
     const int rc = t.rconv[m];
-    const double cinf = t.c_inf[m], iinf = t.i_inf[m];
     double rhs0;
     double s1 = (double)hat[P + m] * ils;
     if (rho > 0.0) {
@@ -381,50 +492,14 @@ __device__ void zsolve_robin_mode(Geo g, long long m, T* __restrict__ hat, ZTab 
     double d = rhs0 * t.inv[m];
     hat[P + m] = (T)d;
     double s_last = s1;  // source of plane nz-2 (used again by the Robin row)
-    // interior rows in batches: the loads of a batch are issued together
-    for (int r0 = 1; r0 <= n - 2; r0 += ZB) {
-        T sv[ZB];
-        double ivb[ZB];
-#pragma unroll
-        for (int u = 0; u < ZB; ++u) {
-            const int r = r0 + u;
-            sv[u] = (r <= n - 2) ? hat[(long long)(r + 1) * P + m] : T(0);
-            ivb[u] = (r <= n - 2 && r < rc) ? t.inv[(long long)r * P + m] : iinf;
-        }
-#pragma unroll
-        for (int u = 0; u < ZB; ++u) {
-            const int r = r0 + u;
-            if (r <= n - 2) {
-                double s = (double)sv[u] * ils;
-                s_last = s;
-                d = (s - low * d) * ivb[u];
-                hat[(long long)(r + 1) * P + m] = (T)d;
-            }
-        }
-    }
+    const ZSweep<T> sw{hat, P, m, rc, rcw, t.inv, t.c, t.i_inf[m], t.c_inf[m]};
+    sw.forward(n - 2, ils, low, d, s_last);
     // Robin row after eliminating u_{N-2} (top_robin_hat = 0)
     const double rl = -ls * dz2 - 2.0;
     const double rr = -s_last * dz2;
     double u = (rr - rl * d) * t.inv_last[m];
     hat[(long long)nz * P - P + m] = (T)u;
-    for (int r0 = n - 2; r0 >= 0; r0 -= ZB) {
-        T dv[ZB];
-        double crb[ZB];
-#pragma unroll
-        for (int q = 0; q < ZB; ++q) {
-            const int r = r0 - q;
-            dv[q] = (r >= 0) ? hat[(long long)(r + 1) * P + m] : T(0);
-            crb[q] = (r >= 0 && r < rc) ? t.c[(long long)r * P + m] : cinf;
-        }
-#pragma unroll
-        for (int q = 0; q < ZB; ++q) {
-            const int r = r0 - q;
-            if (r >= 0) {
-                u = (double)dv[q] - crb[q] * u;
-                hat[(long long)(r + 1) * P + m] = (T)u;
-            }
-        }
-    }
+    sw.back(n - 2, u);
 }
 
 // Dirichlet chain (nfgs_solver.py:3263-3306 with the Thomas solve at
@@ -432,13 +507,12 @@ __device__ void zsolve_robin_mode(Geo g, long long m, T* __restrict__ hat, ZTab 
 // modes, rhs = -S_hat / lambda_D, bottom T_hat, top 0.
 template <typename T>
 __device__ void zsolve_dir_mode(Geo g, long long m, long long PI, T* __restrict__ hat, ZTab t,
-                                const double* __restrict__ lam, const double* __restrict__ bot_hat) {
+                                const double* __restrict__ lam, const double* __restrict__ bot_hat, int rcw) {
     const int nz = g.nz;
     const int n = nz - 2;
     const double dz2 = g.dz * g.dz, a = 1.0 / dz2;
     const double ilam = -1.0 / lam[m];
     const int rc = t.rconv[m];
-    const double cinf = t.c_inf[m], iinf = t.i_inf[m];
     double r1 = (double)hat[PI + m] * ilam;
     double d;
     if (n == 1) {
@@ -448,25 +522,9 @@ __device__ void zsolve_dir_mode(Geo g, long long m, long long PI, T* __restrict_
     }
     d = (r1 - a * bot_hat[m]) * t.inv[m];
     hat[PI + m] = (T)d;
-    for (int r0 = 1; r0 <= n - 2; r0 += ZB) {
-        T sv[ZB];
-        double ivb[ZB];
-#pragma unroll
-        for (int u = 0; u < ZB; ++u) {
-            const int r = r0 + u;
-            sv[u] = (r <= n - 2) ? hat[(long long)(r + 1) * PI + m] : T(0);
-            ivb[u] = (r <= n - 2 && r < rc) ? t.inv[(long long)r * PI + m] : iinf;
-        }
-#pragma unroll
-        for (int u = 0; u < ZB; ++u) {
-            const int r = r0 + u;
-            if (r <= n - 2) {
-                double s = (double)sv[u] * ilam;
-                d = (s - a * d) * ivb[u];
-                hat[(long long)(r + 1) * PI + m] = (T)d;
-            }
-        }
-    }
+    double s_unused = 0.0;
+    const ZSweep<T> sw{hat, PI, m, rc, rcw, t.inv, t.c, t.i_inf[m], t.c_inf[m]};
+    sw.forward(n - 2, ilam, a, d, s_unused);
     {
         const long long q = (long long)n * PI + m;
         double s = (double)hat[q] * ilam;
@@ -474,40 +532,34 @@ __device__ void zsolve_dir_mode(Geo g, long long m, long long PI, T* __restrict_
         hat[q] = (T)d;
     }
     double u = d;
-    for (int r0 = n - 2; r0 >= 0; r0 -= ZB) {
-        T dv[ZB];
-        double crb[ZB];
-#pragma unroll
-        for (int q = 0; q < ZB; ++q) {
-            const int r = r0 - q;
-            dv[q] = (r >= 0) ? hat[(long long)(r + 1) * PI + m] : T(0);
-            crb[q] = (r >= 0 && r < rc) ? t.c[(long long)r * PI + m] : cinf;
-        }
-#pragma unroll
-        for (int q = 0; q < ZB; ++q) {
-            const int r = r0 - q;
-            if (r >= 0) {
-                u = (double)dv[q] - crb[q] * u;
-                hat[(long long)(r + 1) * PI + m] = (T)u;
-            }
-        }
-    }
+    sw.back(n - 2, u);
 }
 
+// threads per z-solve block (one mode each); FP32 storage keeps 7 blocks
+// (28 warps) resident per SM, so the 132k modes of the benchmark grid run in
+// one wave
+constexpr int ZS_THREADS = 128;
 template <typename T>
-__global__ void __launch_bounds__(256) k_zsolve(Geo g, const int* skip, T* __restrict__ shat, ZTab tr,
-                                                const double* __restrict__ lamN, const double* __restrict__ phi_bot_hat,
-                                                const double* __restrict__ der_hat, double rho, double* s00,
-                                                T* __restrict__ jhat, ZTab td, const double* __restrict__ lamD,
-                                                const double* __restrict__ az_bot_hat, int nb_robin) {
+__global__ void __launch_bounds__(ZS_THREADS, sizeof(T) == 4 ? 7 : 4) k_zsolve(Geo g, const int* skip, T* __restrict__ shat, ZTab tr,
+                                                   const double* __restrict__ lamN,
+                                                   const double* __restrict__ phi_bot_hat,
+                                                   const double* __restrict__ der_hat, double rho, double* s00,
+                                                   T* __restrict__ jhat, ZTab td, const double* __restrict__ lamD,
+                                                   const double* __restrict__ az_bot_hat, int nb_robin) {
     if (skip != nullptr && *skip) return;
+    // blocks are either all Robin or all Dirichlet modes, so every lane of a
+    // warp takes part in the rconv maximum
     if ((int)blockIdx.x < nb_robin) {
-        long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        if (m < g.P) zsolve_robin_mode<T>(g, m, shat, tr, lamN, phi_bot_hat, der_hat, rho, s00);
+        const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        const bool ok = m < g.P;
+        const int rcw = __reduce_max_sync(0xffffffffu, ok ? tr.rconv[m] : 0);
+        if (ok) zsolve_robin_mode<T>(g, m, shat, tr, lamN, phi_bot_hat, der_hat, rho, s00, rcw);
     } else if (jhat != nullptr) {
-        long long PI = (long long)(g.nx - 2) * (g.ny - 2);
-        long long m = (long long)(blockIdx.x - nb_robin) * blockDim.x + threadIdx.x;
-        if (m < PI) zsolve_dir_mode<T>(g, m, PI, jhat, td, lamD, az_bot_hat);
+        const long long PI = (long long)(g.nx - 2) * (g.ny - 2);
+        const long long m = (long long)(blockIdx.x - nb_robin) * blockDim.x + threadIdx.x;
+        const bool ok = m < PI;
+        const int rcw = __reduce_max_sync(0xffffffffu, ok ? td.rconv[m] : 0);
+        if (ok) zsolve_dir_mode<T>(g, m, PI, jhat, td, lamD, az_bot_hat, rcw);
     }
 }
 

@@ -928,9 +928,9 @@ static int zsolve_launch(Handle* h, const int* skip) {
     const int nz = g.nz;
     ZTab tr{h->zr_c, h->zr_i, h->zr_il, h->zr_ci, h->zr_ii, h->zr_rc};
     ZTab td{h->zd_c, h->zd_i, h->zd_il, h->zd_ci, h->zd_ii, h->zd_rc};
-    int nbr = (int)((P + 255) / 256);
-    int nbd = nz > 2 ? (int)((PI + 255) / 256) : 0;
-    k_zsolve<T><<<nbr + nbd, 256, 0, h->s>>>(g, skip, (T*)h->sb, tr, h->lamNs, h->phi_bot_hat, h->der_hat,
+    int nbr = (int)((P + ZS_THREADS - 1) / ZS_THREADS);
+    int nbd = nz > 2 ? (int)((PI + ZS_THREADS - 1) / ZS_THREADS) : 0;
+    k_zsolve<T><<<nbr + nbd, ZS_THREADS, 0, h->s>>>(g, skip, (T*)h->sb, tr, h->lamNs, h->phi_bot_hat, h->der_hat,
                                              h->prm.robin_weight, h->s00, nz > 2 ? (T*)h->sj : nullptr, td, h->lamD,
                                              h->az_bot_hat, nbr);
     CK(cudaGetLastError());
