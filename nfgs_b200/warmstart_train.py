@@ -213,6 +213,69 @@ def evaluate(model, seeds, n: int = 256, nz: int = 128, eps=(1e-4, 1e-3), max_it
     return rows
 
 
+def headroom(model, seeds, n: int = 256, nz: int = 128, eps: float = 1e-3,
+             bands=(None, (32, 32, 32), (24, 24, 24), (12, 12, 12)), lams=(0.6,), noise=(1e-3, 1e-2, 1e-1),
+             max_iter: int = 3000, log=print):
+    """How much any predicted start can gain on these seeds: each seed is
+    solved plainly, and then restarted from ideal starts built out of that
+    solve's own best state -- the exact best state, its correction over the
+    gs_cfcf start band-limited to a few cosine bands (the network's output
+    lives in 24^3 modes), the correction scaled down by lams, and the exact
+    correction plus white noise of relative rms `noise` (seeded) -- next to
+    the network's start.  Every start goes through the same hand-off as the
+    network's (accepted only when its sigma_J beats the gs_cfcf start's) and
+    runs with tol = sigma* (1 + eps) under the plain stop rule."""
+    torch = _torch()
+    solver = NFGSSolverGPU(n, n, nz, 1.0, 1.0, 1.0, **SOLVER_KW)
+    mask = None
+    rows = []
+    for sd in seeds:
+        phi, az, (pb, ab), h0 = solve_sample(solver, sd, n, max_iter)
+        if mask is None:
+            mask = LN.masks(solver.Nz, solver.Ny, solver.Nx, phi.device)
+        sstar = float(h0["best_sigma"])
+        kw = dict(STOP, tol=sstar * (1 + eps))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hp = solver.iterate(max_iter=max_iter, verbose=False, **kw)
+        torch.cuda.synchronize()
+        tp = time.perf_counter() - t0
+        row = dict(seed=sd, sigma_star=sstar, plain_iterations=len(hp["sigma"]), plain_s=tp,
+                   plain_reached=hp["stop_reason"] == "tol")
+        corr = torch.stack([(pb.double() - phi.double()), (ab.double() - az.double())])
+        cases = [("best_state" if b is None else "band_%d" % b[0], b, 1.0) for b in bands]
+        cases += [("scaled_%g" % lam, None, lam) for lam in lams]
+        cases += [("noise_%g" % e, ("noise", e), 1.0) for e in noise]
+        cases += [("network", "network", None)]
+        for name, band, lam in cases:
+            if band == "network":
+                start = model
+            else:
+                if isinstance(band, tuple) and band[0] == "noise":
+                    gen = torch.Generator(device=corr.device).manual_seed(int(sd))
+                    w = torch.randn(corr.shape, generator=gen, device=corr.device, dtype=torch.float64) * mask
+                    rms = corr.pow(2).mean(dim=(1, 2, 3), keepdim=True).sqrt()
+                    d = corr + band[1] * rms * w
+                else:
+                    d = corr if band is None else (LN.band_limit(model, corr, band) * mask).double()
+
+                def start(s, p0, a0, d=d, lam=lam):
+                    return p0.double() + lam * d[0], a0.double() + lam * d[1]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            hl = solver.iterate(max_iter=max_iter, verbose=False, init_mode="learned", warm_start=start, **kw)
+            torch.cuda.synchronize()
+            tl = time.perf_counter() - t0
+            info = hl["learned_start"]
+            row[name] = dict(iterations=len(hl["sigma"]), s=tl, reached=hl["stop_reason"] == "tol",
+                             accepted=bool(info["accepted"]), sigma_start=float(info["sigma_learned"]),
+                             sigma_gs_start=float(info["sigma_gs_cfcf"]), speedup=tp / tl if tl > 0 else None,
+                             iteration_ratio=len(hp["sigma"]) / max(1, len(hl["sigma"])))
+        rows.append(row)
+        log("  " + json.dumps(row))
+    return rows
+
+
 def parse_filters(text: str) -> tuple:
     """'none;10,10,10' -> (None, (10, 10, 10))."""
     out = []
@@ -240,8 +303,21 @@ def main(argv=None):
     ap.add_argument("--skip-train-size", action="store_true", help="evaluate at --eval-n/--eval-nz only")
     ap.add_argument("--start-filters", default="none",
                     help="band limits the learned start tries, e.g. 'none;10,10,10' (none = unfiltered)")
+    ap.add_argument("--headroom", action="store_true",
+                    help="with --load: restart each held-out seed from ideal starts built from its own solve")
     args = ap.parse_args(argv)
     report = {}
+    if args.headroom:
+        if not args.load:
+            ap.error("--headroom needs --load")
+        model = LN.NeuralOperator.load(args.load)
+        seeds = [1_000_000 + i for i in range(args.eval_seeds)]
+        print(f"headroom at {args.eval_n}x{args.eval_n}x{args.eval_nz}", flush=True)
+        report["headroom"] = headroom(model, seeds, args.eval_n, args.eval_nz, log=lambda m: print(m, flush=True))
+        if args.report:
+            with open(args.report, "w") as f:
+                json.dump(report, f, indent=1)
+        return 0
     if args.load:
         model = LN.NeuralOperator.load(args.load)
     else:
