@@ -6,9 +6,10 @@ observed box), fields compared on the device.
 
     python -m nfgs_b200.large_solve --fp64 --report large.json
 
-The transforms (256 pairs per axis) run on the four-role tensor-core
-kernel; NFGS_DISABLE_TC=1 in the environment runs them on the SIMT
-contractions instead.  --soft also solves from the soft_cfcf start and
+The transforms (256 pairs per axis) run on the SIMT contractions by
+default; NFGS_TC_WIDE=1 in the environment runs them on the four-role
+tensor-core kernel (3x faster, but FP32 solves through it end twice as far
+from the FP64 solve).  --soft also solves from the soft_cfcf start and
 times both starts (iterate_begin with the start's evaluation, CUDA-synchronised
 wall time, best of three).
 """
@@ -78,9 +79,12 @@ def main(argv=None):
     args = ap.parse_args(argv)
 
     out = {"grid": [args.n, args.n, args.nz], "seed": args.seed,
-           "transforms": "simt" if os.environ.get("NFGS_DISABLE_TC") else "tcgen05"}
+           "transforms": None}
     s = _solver(args.n, args.nz, args.seed, "float32")
     out["calc_grid"] = [s.Nx, s.Ny, s.Nz]
+    wide = max(s.Nx, s.Ny) - 2 > 2 * 128
+    tc = not os.environ.get("NFGS_DISABLE_TC") and (not wide or bool(os.environ.get("NFGS_TC_WIDE")))
+    out["transforms"] = ("tcgen05 four-role" if wide else "tcgen05") if tc else "simt"
     cells = s.Nx * s.Ny * s.Nz
     s.iterate(max_iter=0, verbose=False)
     s._time_phases(2)

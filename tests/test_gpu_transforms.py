@@ -1,8 +1,9 @@
 """DCT-I / DST-I transforms of the CUDA path against SciPy (FP64).
 
 FP32 storage on grids with even N and (N-2)/2 <= 256 runs the tcgen05
-tensor-core contractions (above 128 pairs the four-role kernel; FP16 hi/lo
-split operands, FP32 accumulation in 32-pair chunks);
+tensor-core contractions (above 128 pairs the four-role kernel, which solves
+use only on request -- NFGS_TC_WIDE=1 -- and which these tests switch on;
+FP16 hi/lo split operands, FP32 accumulation in 32-pair chunks);
 their error against the FP64 transform must stay at FP32 level: relative
 L2 error <= 2e-6 (forward) and <= 2e-6 (inverse) per volume (measured
 1.5e-7 to 6e-7).  FP64 storage
@@ -19,9 +20,20 @@ pytestmark = pytest.mark.gpu
 
 
 def _solver(nx, ny, nz, dtype):
+    import os
+
     from nfgs_b200 import NFGSSolverGPU
 
-    return NFGSSolverGPU(nx, ny, nz, 1.0, 1.0, 1.0, device="cuda:0", dtype=dtype, pad_calculation_domain=False)
+    # the wide tensor-core kernel is read from the environment when the handle is made
+    old = os.environ.get("NFGS_TC_WIDE")
+    os.environ["NFGS_TC_WIDE"] = "1"
+    try:
+        return NFGSSolverGPU(nx, ny, nz, 1.0, 1.0, 1.0, device="cuda:0", dtype=dtype, pad_calculation_domain=False)
+    finally:
+        if old is None:
+            os.environ.pop("NFGS_TC_WIDE")
+        else:
+            os.environ["NFGS_TC_WIDE"] = old
 
 
 def _apply(s, chain, inverse, x):
