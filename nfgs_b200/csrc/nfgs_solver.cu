@@ -2688,6 +2688,16 @@ static void host_copy(char* dst, const char* src, size_t len) { CopyPool::get().
 // chunks: the DMA of chunk k overlaps the host copy of chunk k-1.
 static int d2h_chunked(Handle* h, void* host, const void* dev, size_t n) {
     const size_t CH = PIN_CHUNK;
+    // a page-locked destination takes the copy directly
+    {
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, host) == cudaSuccess && pa.type == cudaMemoryTypeHost) {
+            CK(cudaMemcpyAsync(host, dev, n, cudaMemcpyDeviceToHost, h->s));
+            CK(cudaStreamSynchronize(h->s));
+            return NFGS_OK;
+        }
+        (void)cudaGetLastError();
+    }
     // a fresh destination faults its pages in during the copy: ask for 2 MB
     // pages on the 2 MB-aligned part of it (advice only; ignored where the
     // memory is not anonymous or the kernel declines)

@@ -932,7 +932,14 @@ class NFGSSolverGPU:
             shape = (nzo, sy.stop - sy.start, sx.stop - sx.start)
         else:
             shape = (self.Nz, self.Ny, self.Nx)
-        out = np.empty(6 * int(np.prod(shape)), dtype=self._np_dtype)
+        # a reused page-locked block when one is free (the device copy lands
+        # in it directly), else pageable memory
+        from .hostmem import POOL
+
+        n = 6 * int(np.prod(shape))
+        out = POOL.empty(n, self._np_dtype)
+        if out is None:
+            out = np.empty(n, dtype=self._np_dtype)
         dims = (L.C.c_int32 * 3)()
         code = L.NFGS_F32 if out.dtype == np.float32 else L.NFGS_F64
         L.check(self._lib.nfgs_fields_into(self._h, 0, int(bool(crop_to_observed_fov)),
