@@ -249,13 +249,30 @@ static void pin_release(void* p) {
     g_pin_free.push_back(p);
 }
 
+// Page-locked host mirrors of the control block, kept for the next solver
+// (pinning and unpinning cost far more than the block's copy).
+static std::mutex g_ctl_mu;
+static std::vector<DevCtl*> g_ctl_free;
+static int ctl_mirror_acquire(DevCtl** p) {
+    {
+        std::lock_guard<std::mutex> lk(g_ctl_mu);
+        if (!g_ctl_free.empty()) { *p = g_ctl_free.back(); g_ctl_free.pop_back(); return NFGS_OK; }
+    }
+    CK(cudaMallocHost(p, sizeof(DevCtl)));
+    return NFGS_OK;
+}
+static void ctl_mirror_release(DevCtl* p) {
+    std::lock_guard<std::mutex> lk(g_ctl_mu);
+    g_ctl_free.push_back(p);
+}
+
 static void free_all(Handle* h) {
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->graph) cudaGraphDestroy(h->graph);
     for (auto& b : h->owned) cudaFreeAsync(b.p, h->s);
     h->owned.clear();
     if (h->s) cudaStreamSynchronize(h->s);
-    if (h->ctl_h) cudaFreeHost(h->ctl_h);
+    if (h->ctl_h) ctl_mirror_release(h->ctl_h);
     for (int q = 0; q < 2; ++q)
         if (h->pin_ev[q]) cudaEventDestroy(h->pin_ev[q]);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -507,6 +524,32 @@ static std::vector<double> dst_matrix(int n, bool inverse) {
     if (v.empty()) v = dst_matrix_build(n, inverse);
     return v;
 }
+// Device copies of the transform matrices, shared by every solver of the
+// same size on a device (they are constant): keyed by (device, DCT/DST,
+// length, inverse, element size).  They live until the process ends (a few
+// MB per grid size), so creating a solver uploads nothing for a size seen
+// before.
+static std::mutex g_dmat_mu;
+static std::map<std::tuple<int, int, int, int, int>, void*> g_dmat_cache;
+static int shared_matrix(int device, int kind, int n, bool inverse, size_t esz, void** out) {
+    std::lock_guard<std::mutex> lk(g_dmat_mu);
+    void*& d = g_dmat_cache[std::make_tuple(device, kind, n, (int)inverse, (int)esz)];
+    if (d == nullptr) {
+        const std::vector<double> v = kind == 0 ? dct_matrix(n, inverse) : dst_matrix(n, inverse);
+        void* q = nullptr;
+        CK(cudaMalloc(&q, v.size() * esz));
+        if (esz == 4) {
+            std::vector<float> f(v.begin(), v.end());
+            CK(cudaMemcpy(q, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+        } else {
+            CK(cudaMemcpy(q, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+        }
+        d = q;
+    }
+    *out = d;
+    return NFGS_OK;
+}
+
 static std::vector<uint16_t> tc_image(int kind, int n, int P) {
     std::lock_guard<std::mutex> lk(g_mat_mu);
     auto& v = g_img_cache[std::make_tuple(0, kind, n, P)];
@@ -3150,18 +3193,18 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
     const long long P = g.P, V = g.V, PI = h->PI;
     // transforms
     {
-        auto cx = dct_matrix(nx, false), icx = dct_matrix(nx, true);
-        auto cy = dct_matrix(ny, false), icy = dct_matrix(ny, true);
-        auto sx = dst_matrix(nx - 2, false), isx = dst_matrix(nx - 2, true);
-        auto sy = dst_matrix(ny - 2, false), isy = dst_matrix(ny - 2, true);
-        TRYC(upload(h, &h->dctx, cx)); TRYC(upload(h, &h->idctx, icx));
-        TRYC(upload(h, &h->dcty, cy)); TRYC(upload(h, &h->idcty, icy));
-        TRYC(upload(h, &h->dstx, sx)); TRYC(upload(h, &h->idstx, isx));
-        TRYC(upload(h, &h->dsty, sy)); TRYC(upload(h, &h->idsty, isy));
-        TRYC(upload_t(h, &h->dctx_t, cx)); TRYC(upload_t(h, &h->idctx_t, icx));
-        TRYC(upload_t(h, &h->dcty_t, cy)); TRYC(upload_t(h, &h->idcty_t, icy));
-        TRYC(upload_t(h, &h->dstx_t, sx)); TRYC(upload_t(h, &h->idstx_t, isx));
-        TRYC(upload_t(h, &h->dsty_t, sy)); TRYC(upload_t(h, &h->idsty_t, isy));
+        const int dv = h->geom.device;
+        struct M { double** d64; void** dt; int kind, n; bool inv; };
+        const M ms[8] = {{&h->dctx, &h->dctx_t, 0, nx, false}, {&h->idctx, &h->idctx_t, 0, nx, true},
+                         {&h->dcty, &h->dcty_t, 0, ny, false}, {&h->idcty, &h->idcty_t, 0, ny, true},
+                         {&h->dstx, &h->dstx_t, 1, nx - 2, false}, {&h->idstx, &h->idstx_t, 1, nx - 2, true},
+                         {&h->dsty, &h->dsty_t, 1, ny - 2, false}, {&h->idsty, &h->idsty_t, 1, ny - 2, true}};
+        for (const M& m : ms) {
+            void* q = nullptr;
+            TRYC(shared_matrix(dv, m.kind, m.n, m.inv, 8, &q));
+            *m.d64 = (double*)q;
+            TRYC(shared_matrix(dv, m.kind, m.n, m.inv, h->esz, m.dt));
+        }
     }
     // eigenvalues (nfgs_solver.py:1083-1118, 4357-4383, 4811)
     {
@@ -3278,7 +3321,7 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
     TRYC(alloc(h, &h->s00, (size_t)nz * 8));
     TRYC(alloc(h, &h->scal, (8 + 6 * NCHUNK) * 8));
     TRYC(alloc(h, &h->ctl, sizeof(DevCtl)));
-    CKC(cudaMallocHost(&h->ctl_h, sizeof(DevCtl)));
+    TRYC(ctl_mirror_acquire(&h->ctl_h));
     std::memset(h->ctl_h, 0, sizeof(DevCtl));
     TRYC(alloc(h, &h->consts, 4 * sizeof(int)));
     {
