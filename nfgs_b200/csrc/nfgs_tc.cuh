@@ -264,9 +264,15 @@ __device__ __forceinline__ bool role_any(bool x) {
     return r != 0;
 }
 
-__device__ __forceinline__ void split_h(float x, __half& hi, __half& lo) {
-    hi = __float2half_rn(x);
-    lo = __float2half_rn(x - __half2float(hi));
+// FP16 hi / lo split of two values at once: hi = rn(x), lo = rn(x - hi), by
+// packed conversions (round to nearest even, element by element); hi in `h`,
+// lo in `l`, the first value in the low 16 bits of each
+__device__ __forceinline__ void split_h2(float x0, float x1, uint32_t& h, uint32_t& l) {
+    const __half2 hh = __floats2half2_rn(x0, x1);
+    const float2 hf = __half22float2(hh);
+    const __half2 ll = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+    h = *reinterpret_cast<const uint32_t*>(&hh);
+    l = *reinterpret_cast<const uint32_t*>(&ll);
 }
 
 template <bool WIDE>
@@ -518,15 +524,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                 uint32_t hs[4], ls[4], hd[4], ld[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    __half a0, a1, b0, b1;
-                    split_h(sv[2 * q] * up, a0, b0);
-                    split_h(sv[2 * q + 1] * up, a1, b1);
-                    hs[q] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
-                    ls[q] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
-                    split_h(dv[2 * q] * up, a0, b0);
-                    split_h(dv[2 * q + 1] * up, a1, b1);
-                    hd[q] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
-                    ld[q] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
+                    split_h2(sv[2 * q] * up, sv[2 * q + 1] * up, hs[q], ls[q]);
+                    split_h2(dv[2 * q] * up, dv[2 * q + 1] * up, hd[q], ld[q]);
                 }
                 const uint32_t o = dat_off(0, vl, 8 * kq);
                 *(uint4*)(db + 0 * DAT_BYTES + o) = make_uint4(hs[0], hs[1], hs[2], hs[3]);
@@ -538,15 +537,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                 uint32_t h0[4], l0[4], h1[4], l1[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    __half a0, a1, b0, b1;
-                    split_h(sv[2 * q] * up, a0, b0);
-                    split_h(sv[2 * q + 1] * up, a1, b1);
-                    h0[q] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
-                    l0[q] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
-                    split_h(dv[2 * q] * up, a0, b0);
-                    split_h(dv[2 * q + 1] * up, a1, b1);
-                    h1[q] = (uint32_t)__half_as_ushort(a0) | ((uint32_t)__half_as_ushort(a1) << 16);
-                    l1[q] = (uint32_t)__half_as_ushort(b0) | ((uint32_t)__half_as_ushort(b1) << 16);
+                    split_h2(sv[2 * q] * up, sv[2 * q + 1] * up, h0[q], l0[q]);
+                    split_h2(dv[2 * q] * up, dv[2 * q + 1] * up, h1[q], l1[q]);
                 }
                 const uint32_t o0 = dat_off_w(vl, 16 * kq), o1 = dat_off_w(vl, 16 * kq + 8);
                 *(uint4*)(db + o0) = make_uint4(h0[0], h0[1], h0[2], h0[3]);
