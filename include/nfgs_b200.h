@@ -291,9 +291,12 @@ const char* nfgs_version(void);
  * comes from one stream-ordered memory pool per device that keeps freed
  * memory reserved, so creating and destroying solvers does not pay
  * cudaMalloc / cudaFree after the first one; device-to-host staging uses
- * pinned chunks shared by the process.  This call hands the reserved device
- * memory of `device` and the idle pinned chunks back (after a device
- * synchronisation).  No reference counterpart: the reference's PyTorch
+ * pinned chunks shared by the process, the transform matrices are one
+ * device copy per grid size shared by the solvers of a device, and the
+ * page-locked control mirrors are reused.  This call hands the reserved
+ * device memory of `device`, the idle pinned chunks and mirrors, and (when no
+ * solver of `device` is alive) its shared matrices back, after a device
+ * synchronisation.  No reference counterpart: the reference's PyTorch
  * tensors come from torch's caching allocator, whose equivalent is
  * torch.cuda.empty_cache(). */
 int nfgs_release_cached_memory(int32_t device);

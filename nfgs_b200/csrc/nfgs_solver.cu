@@ -526,11 +526,12 @@ static std::vector<double> dst_matrix(int n, bool inverse) {
 }
 // Device copies of the transform matrices, shared by every solver of the
 // same size on a device (they are constant): keyed by (device, DCT/DST,
-// length, inverse, element size).  They live until the process ends (a few
-// MB per grid size), so creating a solver uploads nothing for a size seen
-// before.
+// length, inverse, element size).  They stay (a few MB per grid size), so
+// creating a solver uploads nothing for a size seen before, until
+// nfgs_release_cached_memory is called with no solver alive on the device.
 static std::mutex g_dmat_mu;
 static std::map<std::tuple<int, int, int, int, int>, void*> g_dmat_cache;
+static std::map<int, int> g_live_handles;  // per device
 static int shared_matrix(int device, int kind, int n, bool inverse, size_t esz, void** out) {
     std::lock_guard<std::mutex> lk(g_dmat_mu);
     void*& d = g_dmat_cache[std::make_tuple(device, kind, n, (int)inverse, (int)esz)];
@@ -3181,7 +3182,21 @@ static int create_impl(const NfgsGeom* geom, const NfgsParams* prm, void** out) 
     g.V = g.P * g.nz;
     g.dx = geom->dx; g.dy = geom->dy; g.dz = geom->dz;
     h->PI = (long long)(g.nx - 2) * (g.ny - 2);
-    auto bail = [&](int r) { free_all(h); delete h; return r; };
+    // counted alive from here, so that a concurrent nfgs_release_cached_memory
+    // keeps the shared matrices this solver is about to take
+    {
+        std::lock_guard<std::mutex> lk(g_dmat_mu);
+        ++g_live_handles[geom->device];
+    }
+    auto bail = [&](int r) {
+        free_all(h);
+        {
+            std::lock_guard<std::mutex> lk(g_dmat_mu);
+            --g_live_handles[geom->device];
+        }
+        delete h;
+        return r;
+    };
 #define TRYC(call) do { int r_ = (call); if (r_ != NFGS_OK) return bail(r_); } while (0)
 #define CKC(call) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) { fail(NFGS_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); return bail(NFGS_ECUDA); } } while (0)
     CKC(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
@@ -3545,6 +3560,25 @@ int nfgs_release_cached_memory(int32_t device) {
             CK(cudaMemPoolTrimTo(it->second, 0));
         }
     }
+    {
+        // shared transform matrices of a device no solver uses any more
+        std::lock_guard<std::mutex> lk(g_dmat_mu);
+        if (g_live_handles[device] == 0) {
+            for (auto it = g_dmat_cache.begin(); it != g_dmat_cache.end();) {
+                if (std::get<0>(it->first) == device) {
+                    if (it->second) cudaFree(it->second);
+                    it = g_dmat_cache.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_ctl_mu);
+        for (DevCtl* p : g_ctl_free) cudaFreeHost(p);
+        g_ctl_free.clear();
+    }
     std::lock_guard<std::mutex> lk(g_pin_mu);
     for (void* p : g_pin_free) cudaFreeHost(p);
     g_pin_free.clear();
@@ -3565,6 +3599,10 @@ int nfgs_destroy(void* handle) {
     if (h->s && h->ev_na_out) cudaStreamWaitEvent(h->s, h->ev_na_out, 0);
     if (h->s) cudaStreamSynchronize(h->s);
     free_all(h);
+    {
+        std::lock_guard<std::mutex> lk(g_dmat_mu);
+        --g_live_handles[h->geom.device];
+    }
     delete h;
     return NFGS_OK;
 }

@@ -45,3 +45,9 @@ def test_reused_memory_gives_identical_solves_and_release_returns_it():
     # what the library reserved is back (allow for the CUDA context's own growth)
     assert free1 >= free0 - (64 << 20)
     release_cached_memory(0)  # idempotent
+    # a solver made after the release (its matrices uploaded again) repeats the first result
+    s, h3, f3 = _solve()
+    assert h1["sigma"] == h3["sigma"]
+    for k in f1:
+        np.testing.assert_array_equal(f1[k], f3[k])
+    del s
