@@ -564,7 +564,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (lane == 0) {
                 if constexpr (!WIDE) {
-#pragma unroll 1
+                    // descriptors of K-step ks are those of step 0 plus 256 ks bytes in the
+                    // address field (address >> 4: + 16 ks; shared memory stays below 256 KB,
+                    // so the 14-bit field never carries), so the issuing thread only adds
+#pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         // hi x hi in chunks of KC_STEPS K-steps (columns (h (NCH_N + 1) + chunk) TV),
                         // the correction products after them
@@ -572,16 +575,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                         const uint32_t acc2 = accb + NCH_N * TV;
                         const uint32_t mh = mat0 + (uint32_t)(2 * h) * MAT_BYTES, ml = mh + MAT_BYTES;
                         const uint32_t dh = dat0 + (uint32_t)(b * 4 + 2 * h) * DAT_BYTES, dl = dh + DAT_BYTES;
-#pragma unroll 1
+                        const uint64_t a_hi0 = sdesc(mh, 128u, 2048u), a_lo0 = sdesc(ml, 128u, 2048u);
+                        const uint64_t b_hi0 = sdesc(dh, 128u, 2048u), b_lo0 = sdesc(dl, 128u, 2048u);
+#pragma unroll
                         for (int ks = 0; ks < PP / 16; ++ks) {
-                            const uint64_t a_hi = sdesc(mh + 256u * ks, 128u, 2048u);
-                            const uint64_t a_lo = sdesc(ml + 256u * ks, 128u, 2048u);
-                            const uint64_t b_hi = sdesc(dh + 256u * ks, 128u, 2048u);
-                            const uint64_t b_lo = sdesc(dl + 256u * ks, 128u, 2048u);
-                            mma_f16(accb + (uint32_t)((ks / KC_STEPS) * TV), a_hi, b_hi, idesc,
+                            const uint64_t o = (uint64_t)(16 * ks);
+                            mma_f16(accb + (uint32_t)((ks / KC_STEPS) * TV), a_hi0 + o, b_hi0 + o, idesc,
                                     (ks % KC_STEPS) > 0 ? 1u : 0u);
-                            mma_f16(acc2, a_hi, b_lo, idesc, ks > 0 ? 1u : 0u);
-                            mma_f16(acc2, a_lo, b_hi, idesc, 1u);
+                            mma_f16(acc2, a_hi0 + o, b_lo0 + o, idesc, ks > 0 ? 1u : 0u);
+                            mma_f16(acc2, a_lo0 + o, b_hi0 + o, idesc, 1u);
                         }
                     }
                 } else {
@@ -590,16 +592,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                     const uint32_t accb = tbase + (uint32_t)(b * ACC_COLS), acc2 = accb + NCH_W * TV;
                     const uint32_t mh = mat0, ml = mat0 + 2 * MAT_BYTES;
                     const uint32_t dh = dat0 + (uint32_t)(b * 4) * DAT_BYTES, dl = dh + 2 * DAT_BYTES;
-#pragma unroll 1
+                    const uint64_t a_hi0 = sdesc(mh, 128u, 4096u), a_lo0 = sdesc(ml, 128u, 4096u);
+                    const uint64_t b_hi0 = sdesc(dh, 128u, 4096u), b_lo0 = sdesc(dl, 128u, 4096u);
+#pragma unroll
                     for (int ks = 0; ks < PW_K / 16; ++ks) {
-                        const uint64_t a_hi = sdesc(mh + 256u * ks, 128u, 4096u);
-                        const uint64_t a_lo = sdesc(ml + 256u * ks, 128u, 4096u);
-                        const uint64_t b_hi = sdesc(dh + 256u * ks, 128u, 4096u);
-                        const uint64_t b_lo = sdesc(dl + 256u * ks, 128u, 4096u);
-                        mma_f16(accb + (uint32_t)((ks / KC_STEPS) * TV), a_hi, b_hi, idesc,
+                        const uint64_t o = (uint64_t)(16 * ks);
+                        mma_f16(accb + (uint32_t)((ks / KC_STEPS) * TV), a_hi0 + o, b_hi0 + o, idesc,
                                 (ks % KC_STEPS) > 0 ? 1u : 0u);
-                        mma_f16(acc2, a_hi, b_lo, idesc, ks > 0 ? 1u : 0u);
-                        mma_f16(acc2, a_lo, b_hi, idesc, 1u);
+                        mma_f16(acc2, a_hi0 + o, b_lo0 + o, idesc, ks > 0 ? 1u : 0u);
+                        mma_f16(acc2, a_lo0 + o, b_hi0 + o, idesc, 1u);
                     }
                 }
                 mma_commit(mmad0 + 8 * b);
