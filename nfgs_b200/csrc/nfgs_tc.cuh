@@ -480,13 +480,20 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                 e0[b * TV + vl] = (WIDE && hh == 1) ? x0 - xn : x0 + xn;
                 e1[b * TV + vl] = x0 - xn;
             }
-            if (t < TV) {
-                const long long v = v0 + t;
-                obase[b * TV + t] = v < g.nvec ? vaddr(g.oa, v) : -1;
+            // warp 0: lanes 0..TV-1 the input bases of the tile prefetched next,
+            // lanes TV..2TV-1 the output bases of this tile, one address each
+            if (t < 2 * TV) {
+                const bool in = t < TV;
+                const int c = t & (TV - 1);
+                const int inext = i + (WIDE ? 1 : 2);
+                const Addr& ad = in ? g.ia : g.oa;
+                const long long v = in ? (long long)(grp + (long long)inext * ngrp) * TV + c : v0 + c;
+                const bool valid = v < g.nvec && (!in || inext < nlocal);
+                const long long base = valid ? vaddr(ad, v) : -1;
+                if (in) ibase[(inext & 1) * TV + c] = base;
+                else obase[b * TV + c] = base;
             }
-            bases(i + (WIDE ? 1 : 2));
             producer_sync();     // raw buffer consumed, partials and bases of the next prefetch ready
-            prefetch(i + (WIDE ? 1 : 2));
             // every thread forms the scale of its own vector from the 8 warp
             // partials (threads 0..TV-1 also publish it for the epilogue)
             int ex = 0;
@@ -548,6 +555,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_arrive(full0 + 8 * b);
+            // the next raw tile into the buffer this one left (off the path to
+            // the MMA: it lands two tiles ahead of its use)
+            prefetch(i + (WIDE ? 1 : 2));
         }
         cp_wait0();
     } else if (warp == NPW + NEW) {
