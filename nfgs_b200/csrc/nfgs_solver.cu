@@ -670,6 +670,17 @@ __global__ void k_k0_select(const double* hk, int idx, int nz, double t0, double
     }
 }
 
+// The transform kernel instantiated for (wide, axis, kind).
+using TcKernel = void (*)(tc::Args);
+static TcKernel tc_kernel(bool wide, int axis, int kind) {
+    static const TcKernel k[2][2][2] = {
+        {{tc::k_tc_transform<false, 0, 0>, tc::k_tc_transform<false, 0, 1>},
+         {tc::k_tc_transform<false, 1, 0>, tc::k_tc_transform<false, 1, 1>}},
+        {{tc::k_tc_transform<true, 0, 0>, tc::k_tc_transform<true, 0, 1>},
+         {tc::k_tc_transform<true, 1, 0>, tc::k_tc_transform<true, 1, 1>}}};
+    return k[wide ? 1 : 0][axis ? 1 : 0][kind ? 1 : 0];
+}
+
 static int tc_setup(Handle* h) {
     const int nx = h->g.nx, ny = h->g.ny;
     if (!h->f32 || (nx % 2) || (ny % 2)) return NFGS_OK;
@@ -684,8 +695,11 @@ static int tc_setup(Handle* h) {
     int dev = 0, nsm = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    CK(cudaFuncSetAttribute(tc::k_tc_transform<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_TOTAL));
-    CK(cudaFuncSetAttribute(tc::k_tc_transform<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_TOTAL));
+    for (int w = 0; w < 2; ++w)
+        for (int ax = 0; ax < 2; ++ax)
+            for (int kd = 0; kd < 2; ++kd)
+                CK(cudaFuncSetAttribute(tc_kernel(w != 0, ax, kd), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        tc::SMEM_TOTAL));
     if (nsm < 4) return NFGS_OK;
     const int kinds[4] = {0, 0, 1, 1};
     const int lens[4] = {nx, ny, nx - 2, ny - 2};
@@ -742,10 +756,10 @@ static int tc_launch(Handle* h, int which, int inverse, const float* in, tc::Add
     if (h->tc_wide[which]) {
         // four roles per tile group: one CTA per SM in groups of four
         cfg.gridDim = dim3((unsigned)(4 * std::min(ntiles, h->tc_nsm / 4)));
-        CK(cudaLaunchKernelEx(&cfg, tc::k_tc_transform<true>, a));
+        CK(cudaLaunchKernelEx(&cfg, tc_kernel(true, a.axis, a.kind), a));
     } else {
         cfg.gridDim = dim3((unsigned)std::min(ntiles, h->tc_nsm));
-        CK(cudaLaunchKernelEx(&cfg, tc::k_tc_transform<false>, a));
+        CK(cudaLaunchKernelEx(&cfg, tc_kernel(false, a.axis, a.kind), a));
     }
     CK(cudaGetLastError());
     h->launches++;

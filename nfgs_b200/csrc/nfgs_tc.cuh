@@ -275,7 +275,10 @@ __device__ __forceinline__ void split_h2(float x0, float x1, uint32_t& h, uint32
     l = *reinterpret_cast<const uint32_t*>(&ll);
 }
 
-template <bool WIDE>
+// AX: the axis (0 rows, 1 columns), KIND: 0 DCT-I, 1 DST-I -- compile-time, so
+// the per-element index and layout choices are not branches (g.axis and
+// g.kind must agree)
+template <bool WIDE, int AX, int KIND>
 __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* smat = smem;
@@ -324,7 +327,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tbase = *tslot;
     const int P = g.P, N = g.N;
-    const bool dct = g.kind == 0;
+    constexpr bool dct = KIND == 0;
     bool failed = false;
 
     // The matrix operands (128 KB, constant) are copied in by the MMA and
@@ -369,7 +372,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             }
         };
         // 8-byte copies when every axis-0 row starts on an 8-byte boundary
-        const bool pairs8 = g.axis == 0 && g.ia.estride == 1 && ((uintptr_t)g.in & 7) == 0 &&
+        const bool pairs8 = AX == 0 && g.ia.estride == 1 && ((uintptr_t)g.in & 7) == 0 &&
                             (g.ia.off & 1) == 0 && (g.ia.bstride & 1) == 0 && (g.ia.vstride & 1) == 0;
         constexpr int SP = WIDE ? STG_PITCH_W : STG_PITCH;   // axis-0 staging pitch
         auto stg_buf = [&](int i) { return WIDE ? 0 : (i & 1); };
@@ -377,7 +380,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             if (i < nlocal) {
                 const uint32_t dst = stg0 + (uint32_t)(stg_buf(i) * STG_FLOATS * 4);
                 const long long* ib = ibase + (i & 1) * TV;
-                if (g.axis == 0) {
+                if constexpr (AX == 0) {
                     // warp w: rows (TV/NPW) w ..., lanes along the row
 #pragma unroll
                     for (int rr = 0; rr < TV / NPW; ++rr) {
@@ -426,7 +429,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
             const float* raw = stg + stg_buf(i) * STG_FLOATS;
             const bool okv = v0 + vl < g.nvec;
             auto X = [&](int m) -> float {
-                return g.axis == 0 ? raw[vl * SP + m] : raw[m * TV + vl];
+                if constexpr (AX == 0) return raw[vl * SP + m];
+                else return raw[m * TV + vl];
             };
             // normal: pair sums sv / differences dv of vector vl, pairs 8 kq .. 8 kq + 7;
             // wide: the values of half hh (sums or differences), pairs 16 kq .. 16 kq + 15
@@ -653,7 +657,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                         const float down = vdown[b * TV + c];
                         float av = va[cc] * down, bv = vb[cc] * down;
                         if (dct) { av += e0[b * TV + c]; bv += e1[b * TV + c]; }
-                        if (g.axis == 0) {
+                        if constexpr (AX == 0) {
                             S[c * (2 * PP) + ia] = av;
                             S[c * (2 * PP) + ib] = bv;
                         } else {
@@ -663,7 +667,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                     }
                 }
                 epilogue_sync();
-                if (g.axis == 0) {
+                if constexpr (AX == 0) {
                     for (int c = e; c < TV; c += NEW) {
                         const long long ob = obase[b * TV + c];
                         if (ob < 0) continue;
@@ -701,11 +705,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_tc_transform(Args g) {
                     const int c = 8 * ch + cc;
                     float av = va[cc] * vdown[b * TV + c];
                     if (dct) av += e0[b * TV + c];
-                    if (g.axis == 0) S[c * 128 + j] = av;
+                    if constexpr (AX == 0) S[c * 128 + j] = av;
                     else S[j * TV + (c ^ ((j >> 1) & 15))] = av;
                 }
                 epilogue_sync();
-                if (g.axis == 0) {
+                if constexpr (AX == 0) {
                     for (int c = e; c < TV; c += NEW) {
                         const long long ob = obase[b * TV + c];
                         if (ob < 0) continue;
