@@ -311,6 +311,10 @@ int nfgs_release_cached_memory(int32_t device);
  * handle with nfgs_iterate_end.  All handles must be on one device. */
 int nfgs_scan_create(void* const* handles, int32_t n, int32_t iters, void** scan_out);
 int nfgs_scan_launch(void* scan, int32_t* n_active_out);
+/* Add solves begun since (nfgs_iterate_begin with use_graph) to a scan
+ * between launches: the scan's graph is rebuilt with them, so a caller can
+ * start launching while the rest of its solves are still being set up. */
+int nfgs_scan_add(void* scan, void* const* handles, int32_t n);
 int nfgs_scan_destroy(void* scan);
 
 /* Learned warm start (no reference counterpart; the reference always starts

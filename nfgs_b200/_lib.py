@@ -120,6 +120,7 @@ SIGNATURES = {
     "nfgs_release_cached_memory": (C.c_int, [C.c_int32]),
     "nfgs_scan_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
     "nfgs_scan_launch": (C.c_int, [_P, _IP]),
+    "nfgs_scan_add": (C.c_int, [_P, C.POINTER(C.c_void_p), C.c_int32]),
     "nfgs_scan_destroy": (C.c_int, [_P]),
     "nfgs_iterate_start_state": (C.c_int, [_P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "nfgs_iterate_restart_from": (C.c_int, [_P, _P, _P, C.c_int32, _DP]),

@@ -3844,6 +3844,30 @@ int nfgs_scan_create(void* const* handles, int32_t n, int32_t iters, void** scan
     return NFGS_OK;
 }
 
+int nfgs_scan_add(void* scan, void* const* handles, int32_t n) {
+    g_err.clear();
+    auto* sc = (NfgsScanObj*)scan;
+    if (!sc || !handles || n <= 0) return fail(NFGS_EINVAL, "scan: bad arguments");
+    cudaSetDevice(sc->device);
+    for (int i = 0; i < n; ++i) {
+        Handle* h = (Handle*)handles[i];
+        if (!h || h->geom.device != sc->device) return fail(NFGS_EINVAL, "scan: handles must share a device");
+        if (!h->iter_active) return fail(NFGS_ESTATE, "scan: every handle needs nfgs_iterate_begin");
+        if (!h->stop.use_graph) return fail(NFGS_EINVAL, "scan: handles must iterate with use_graph");
+        for (Handle* q : sc->hs)
+            if (q == h) return fail(NFGS_EINVAL, "scan: handle already in the scan");
+    }
+    for (int i = 0; i < n; ++i) {
+        Handle* h = (Handle*)handles[i];
+        TRY(h->f32 ? ensure_graph_t<float>(h) : ensure_graph_t<double>(h));
+        CK(cudaStreamSynchronize(h->s));
+        h->advanced = 1;
+        sc->hs.push_back(h);
+    }
+    // the running graph finished with the last launch (nfgs_scan_launch waits for it)
+    return scan_build(sc);
+}
+
 int nfgs_scan_launch(void* scan, int32_t* n_active_out) {
     g_err.clear();
     auto* sc = (NfgsScanObj*)scan;
