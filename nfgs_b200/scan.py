@@ -9,9 +9,11 @@ until every solve has met its stop rule.  Solves that stopped skip their work
 on the device, and the graph is rebuilt from the running solves whenever
 half have stopped; the results are those of the same solves run one by one.
 The solvers are set up by a thread pool (the first of each grid shape alone,
-so that the fused stencil's per-shape z-segment tuning runs on a quiet GPU).
+so that the fused stencil's per-shape z-segment tuning runs on a quiet GPU);
+run_scan_overlapped starts launching with those first solves and joins the
+others to the running scan between launches as the threads finish them.
 
-    python -m nfgs_b200.scan --boundaries 33 --report scan.json
+    python -m nfgs_b200.scan --boundaries 33 --overlap --serial --report scan.json
 
 Under torchrun (one process per GPU) the solves are dealt round-robin to the
 ranks, each rank runs its share as one batched scan, and rank 0 reports the
